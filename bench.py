@@ -1,0 +1,326 @@
+"""Benchmark: Msamples/s of the B200 wavefront integrator on the mesh + glossy workload.
+
+One step = one full frame of the workload (1920x1080, 64 spp, max depth 12 on a
+1,310,720-triangle displaced icosphere + ground quad, rough dielectric and GGX
+metal, 1024x512 environment with a sun lobe, f/2.8 thin lens). Synthetic,
+seeded scene data (no assets). `value` is device-timed with the scene resident
+on the GPU; `e2e` is the same metric through the C ABI call a host makes
+(luz_gpu_render with a host film, device->host copy included).
+
+Multi-GPU (torchrun, one process per GPU): every rank renders the full frame
+with its own sample range (sample_offset = rank * spp), and the films are
+summed with one NCCL all-reduce per step: weak scaling over samples.
+
+--impl reference times the Luz reference renderer (built from its own sources
+into oracle/_ref/libluzref_fast.so) on the host cores on a bounded sample of
+the same workload (the 1080p frame at 1 spp per step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Msamples/s"
+UNIT = "Msamples/s"
+REFERENCE_DIR = os.path.join(ROOT, "oracle")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mesh_glossy")
+    ap.add_argument("--spp", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name, spp=None):
+    from luz_b200 import scenes
+    w = scenes.WORKLOADS[name]()
+    if spp:
+        w.spp = spp
+    return w
+
+
+def config_of(w, n_gpus):
+    return {"workload": f"{w.name} {w.width}x{w.height} {w.spp}spp depth{w.max_bounces}",
+            "width": w.width, "height": w.height, "spp": w.spp, "max_bounces": w.max_bounces,
+            "triangles": int(sum(m["positions"].shape[0] for m in w.scene.meshes)),
+            "shards": f"sample ranges x{n_gpus}", "l2": "path state and scene > 126 MB L2; L2 flushed between steps",
+            "seed": w.seed}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per k_extend launch from the committed ncu summary (profiles/), if any."""
+    p = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(w, threads):
+    """The reference renderer (oracle/_ref/libluzref_fast.so) on a bounded sample: the frame at 1 spp."""
+    sys.path.insert(0, REFERENCE_DIR)
+    from luz_b200 import native
+    import oracle as O
+    if not O.reference_available(fast=True):
+        return None, "reference library oracle/_ref/libluzref_fast.so not built"
+    ro = O.RefOracle(fast=True)
+    rs = ro.scene(w.scene.build())
+    p = native.params(w.width, w.height, 1, w.max_bounces, w.seed)
+    _, ms, ns = rs.render(p, threads)
+    spp = 1
+    if ms < 8000.0:   # grow to about 10 s of CPU work
+        spp = max(1, min(w.spp, int(10000.0 / max(ms, 1.0))))
+        if spp > 1:
+            p = native.params(w.width, w.height, spp, w.max_bounces, w.seed)
+            _, ms, ns = rs.render(p, threads)
+    rs.close()
+    return {"value": ns / ms / 1e3, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{w.width}x{w.height} at {spp} spp ({int(ns)} samples), render_ms {ms:.0f}"}, None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(args.workload, args.spp)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, REFERENCE_DIR)
+    import oracle as O
+    from luz_b200 import native
+    if not O.reference_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libluzref_fast.so not built"}))
+        return
+    ro = O.RefOracle(fast=True)
+    rs = ro.scene(w.scene.build())
+    p = native.params(w.width, w.height, 1, w.max_bounces, w.seed)
+    for _ in range(args.warmup):
+        rs.render(p, threads)
+    times, samples = [], 0.0
+    for _ in range(args.steps):
+        _, ms, ns = rs.render(p, threads)
+        times.append(ms)
+        samples = ns
+    ms = float(np.mean(times))
+    value = samples / ms / 1e3
+    cfg = config_of(w, 1)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)", "config": cfg,
+           "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                            "sample": f"{w.width}x{w.height} at 1 spp per step ({int(samples)} samples)"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    from luz_b200 import native
+    from luz_b200.desc import RENDER_COUNT, RENDER_PROFILE
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = workload(args.workload, args.spp)
+    built = w.scene.build()
+    g = native.GpuScene(built, device=local)
+    npix = w.width * w.height
+    film = torch.zeros(npix * 3, dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed, 0, rank * w.spp)
+
+    def step():
+        st = g.render_device(p, film.data_ptr(), stream.cuda_stream)
+        if dist is not None:
+            dist.all_reduce(film)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    times, launches = [], 0
+    clocks.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches += st.kernel_launches
+        times.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    ms = float(np.mean(times))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    samples_all = float(npix) * w.spp * world
+    value = samples_all / ms / 1e3
+
+    # end to end through the C ABI with a host film (device -> host copy in the timed region)
+    e2e_ms = []
+    host = None
+    for i in range(max(1, min(args.steps, 3))):
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        host, _ = g.render(p)
+        if dist is not None:
+            ht = torch.from_numpy(host).cuda()
+            dist.all_reduce(ht)
+            host = ht.cpu().numpy()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2 = float(np.mean(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([e2], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2 = float(t.item())
+
+    # roofline of the dominant kernel (closest-hit traversal), from an instrumented extra frame
+    pp = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed, 0, rank * w.spp)
+    pp.flags = RENDER_PROFILE | RENDER_COUNT
+    prof = g.render_device(pp, film.data_ptr(), stream.cuda_stream)
+    pt = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed, 0, rank * w.spp)
+    pt.flags = RENDER_PROFILE
+    timed = g.render_device(pt, film.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ext_rays = prof.extension_rays
+    alg_bytes = 64.0 * prof.ext_nodes + 48.0 * prof.ext_tris + 32.0 * prof.ext_top + 64.0 * ext_rays
+    launch_ms = timed.extend_ms / max(1, timed.extend_launches)
+    bytes_per_launch = alg_bytes / max(1, prof.extend_launches)
+    achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9 if launch_ms > 0 else None
+    peak, peak_kind = measured_peak()
+    tr = profile_traffic()
+    traffic = None
+    if tr:
+        traffic = tr.get("bytes_per_launch")
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+               "config": config_of(w, world),
+               "e2e": {"value": samples_all / e2 / 1e3, "unit": UNIT, "h2d_bytes_per_step": 32,
+                       "d2h_bytes_per_step": npix * 3 * 4},
+               "gpu_launches": int(launches),
+               "clocks": clk,
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                            "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                            "algorithmic_bytes_per_ray": alg_bytes / max(1.0, ext_rays),
+                            "rays_per_launch": ext_rays / max(1, prof.extend_launches),
+                            "launch_ms": launch_ms},
+               "stages_ms": {"extend": timed.extend_ms, "shade": timed.shade_ms, "shadow": timed.shadow_ms,
+                             "total": timed.render_ms},
+               "mrays_per_s": (timed.extension_rays + timed.shadow_rays) / timed.render_ms / 1e3 * world}
+        if world == 1 and not args.no_cpu_baseline:
+            cb, why = cpu_baseline(w, os.cpu_count() or 1)
+            out["cpu_baseline"] = cb if cb else {"value": None, "unavailable": why}
+        print(json.dumps(out), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

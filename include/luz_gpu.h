@@ -1,0 +1,279 @@
+/*
+ * luz_gpu.h — C ABI of the B200 Monte Carlo integrator for Luz.
+ *
+ * The integrator replaces the per-pixel sample loop of the Luz CPU renderer:
+ *   Renderer::internal::_manageThreads   (src/renderer/Threads.cpp:375)
+ *   Renderer::internal::_threadRender    (src/renderer/Threads.cpp:551)
+ *   calculateLightRaysColor              (src/renderer/ColorHelper.cpp:1136-1326)
+ *   Renderer::internal::_checkHits       (src/renderer/HitHelper.cpp:5-32)
+ *   isShadowOccluded                     (src/renderer/ColorHelper.cpp:801-829)
+ * The C++20 host keeps the .luz loader, CLI, NFOR denoiser, post-processing
+ * and image writers; it flattens its Scene into a LuzSceneDesc, calls
+ * luz_gpu_render and copies the returned FP32 film into its Image.
+ *
+ * Conventions (mirroring the reference's error behaviour):
+ *   - every entry point returns int status: 0 = ok, < 0 = error;
+ *   - the last error message of the calling thread is available through
+ *     luz_gpu_last_error (the host turns it into std::runtime_error, as
+ *     src/cli/main.cpp:209-213 expects of the CPU renderer);
+ *   - invalid scene parameters are rejected with LUZ_E_INVALID and the same
+ *     wording as the reference's std::invalid_argument messages;
+ *   - the caller owns every array it passes; the library copies what it keeps.
+ *   - one host thread per scene handle; handles are independent.
+ */
+#ifndef LUZ_GPU_H
+#define LUZ_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUZ_GPU_ABI_VERSION 1
+
+/* status codes */
+#define LUZ_OK            0
+#define LUZ_E_INVALID    -1   /* bad argument / scene description            */
+#define LUZ_E_CUDA       -2   /* CUDA runtime error (no device, OOM, launch)  */
+#define LUZ_E_UNSUPPORTED -3  /* feature of the reference not on this path   */
+#define LUZ_E_LIMIT      -4   /* BVH deeper than the traversal stack, etc.   */
+#define LUZ_E_DEVICE     -5   /* a kernel reported a device-side error flag  */
+
+/* Material types: values equal enum MaterialType (include/luz/Materials/MaterialTypes.hpp:3-15). */
+#define LUZ_MAT_LAMBERTIAN         1
+#define LUZ_MAT_METAL              2
+#define LUZ_MAT_DIELECTRIC         3
+#define LUZ_MAT_EMISSIVE           4
+#define LUZ_MAT_ISOTROPIC          5
+#define LUZ_MAT_HENYEY_GREENSTEIN  6
+#define LUZ_MAT_PRINCIPLED         7
+
+/* Sky types: values equal enum SkyTypes (include/luz/SkyTypes.hpp). */
+#define LUZ_SKY_NONE         0
+#define LUZ_SKY_ENVIRONMENT  3
+
+/* Scene object kinds (one per reference Hittable class on the path). */
+#define LUZ_OBJ_RECTANGLE          1   /* src/core/Hittables/Rectangle.cpp        */
+#define LUZ_OBJ_SPHERE             2   /* src/core/Hittables/Sphere.cpp           */
+#define LUZ_OBJ_CUBE               3   /* src/core/Hittables/Cube.cpp             */
+#define LUZ_OBJ_PLANE              4   /* src/core/Hittables/Plane.cpp            */
+#define LUZ_OBJ_MESH               5   /* src/core/Hittables/Mesh.cpp             */
+#define LUZ_OBJ_MESH_INSTANCE      6   /* src/core/Hittables/MeshInstance.cpp     */
+#define LUZ_OBJ_VOLUME             7   /* src/core/Hittables/ConstantVolume.cpp   */
+#define LUZ_OBJ_DIRECTIONAL_LIGHT  8   /* src/core/Hittables/DirectionalLight.cpp */
+
+/* Material parameters; which fields are read depends on type, exactly as the
+ * reference constructors/setters (Lambertian.cpp, Metal.cpp, Dielectric.cpp,
+ * Emissive.cpp, Isotropic.cpp, HenyeyGreenstein.cpp, Principled.cpp). */
+typedef struct LuzMaterialDesc {
+    int32_t type;                 /* LUZ_MAT_*                                     */
+    int32_t texture;              /* -1 or index into LuzSceneDesc.textures         */
+    double  color[3];             /* albedo / base colour / emitted radiance       */
+    double  roughness;            /* Metal fuzz, Dielectric/Principled roughness   */
+    double  ior;                  /* Dielectric / Principled refractive index      */
+    double  anisotropy;           /* Henyey-Greenstein g                            */
+    int32_t conductor;            /* Metal: 1 = conductor Fresnel (eta, k)          */
+    int32_t subsurface_method;    /* Principled: 0 = Burley, 1 = thin               */
+    double  eta[3];               /* Metal conductor eta                            */
+    double  k[3];                 /* Metal conductor extinction                     */
+    double  absorption[3];        /* Dielectric/Principled absorption (1/m)         */
+    double  metallic, transmission, clearcoat, clearcoat_roughness, sheen, subsurface;
+    double  subsurface_radius[3];
+    double  subsurface_scale;
+    double  subsurface_color[3];
+} LuzMaterialDesc;
+
+/* Bilinear albedo texture (src/core/Texture.cpp:142-172): width*height RGB, row 0 = top. */
+typedef struct LuzTextureDesc {
+    int32_t width, height;
+    const double* rgb;
+} LuzTextureDesc;
+
+/* Triangle soup of one Mesh (Mesh(position, material, std::vector<Triangle>),
+ * src/core/Hittables/Mesh.cpp:343-350). Degenerate triangles are dropped as the
+ * reference does (Mesh.cpp:353-365); primitive ids count surviving triangles. */
+typedef struct LuzMeshDesc {
+    int64_t triangle_count;
+    const double* positions;      /* triangle_count * 9                             */
+    const double* normals;        /* NULL or triangle_count * 9 (vertex normals)    */
+    const double* uvs;            /* NULL or triangle_count * 6                     */
+    int32_t material;             /* material of the triangles and of the mesh      */
+    int32_t _pad;
+} LuzMeshDesc;
+
+typedef struct LuzObjectDesc {
+    int32_t kind;                 /* LUZ_OBJ_*                                      */
+    int32_t material;             /* VOLUME: phase-function material                */
+    int32_t mesh;                 /* MESH / MESH_INSTANCE: index into meshes        */
+    int32_t boundary_kind;        /* VOLUME: LUZ_OBJ_CUBE or LUZ_OBJ_SPHERE         */
+    double  position[3];          /* centre / translation; PLANE: y = position[1]   */
+    double  orientation[3];       /* rect normal, plane normal, light direction     */
+    double  size[3];              /* rect (w,h,-), cube (w,h,d), sphere (r,-,-)     */
+    double  width_axis[3];        /* rect: optional explicit axes                   */
+    double  height_axis[3];
+    int32_t has_axes;
+    int32_t visible;              /* sphere: 0 = invisible (Sphere.cpp:229-232)     */
+    double  rotation_degrees[3];  /* MESH_INSTANCE Euler X->Y->Z                    */
+    double  scale[3];             /* MESH_INSTANCE                                  */
+    double  density;              /* VOLUME                                         */
+    int32_t has_uvs;              /* rect: optional uv0..uv3                        */
+    int32_t _pad;
+    double  uv[12];
+} LuzObjectDesc;
+
+/* Camera (src/core/Camera.cpp); thin lens unless pinhole != 0. */
+typedef struct LuzCameraDesc {
+    double  position[3], direction[3], up[3];
+    double  focal_length_m, sensor_width_m, sensor_height_m, f_number, focus_distance_m;
+    int32_t pinhole;
+    int32_t _pad;
+} LuzCameraDesc;
+
+/* Equirect environment (EnvironmentMap(width,height,pixels), src/core/EnvironmentMap.cpp:296). */
+typedef struct LuzEnvironmentDesc {
+    int32_t width, height;        /* 0 = no environment map                         */
+    const double* rgb;            /* width*height*3                                 */
+    double  strength;
+    double  rotation_degrees;
+    int32_t lighting;             /* Scene::setEnvironmentLighting                  */
+    int32_t _pad;
+} LuzEnvironmentDesc;
+
+typedef struct LuzSceneDesc {
+    int32_t abi_version;          /* LUZ_GPU_ABI_VERSION                            */
+    int32_t material_count;
+    const LuzMaterialDesc* materials;
+    int32_t texture_count;
+    int32_t mesh_count;
+    const LuzTextureDesc* textures;
+    const LuzMeshDesc* meshes;
+    int32_t object_count;         /* objects in Scene::addHittable order            */
+    int32_t sky;                  /* LUZ_SKY_NONE or LUZ_SKY_ENVIRONMENT            */
+    const LuzObjectDesc* objects;
+    LuzCameraDesc camera;
+    LuzEnvironmentDesc environment;
+    double  background[3];
+    double  meters_per_unit;
+} LuzSceneDesc;
+
+/* Render settings: the parts of Scene that Renderer::render reads for the
+ * sample loop. Adaptive sampling and NFOR buffers are not on this path;
+ * stream selects the Sampler stream (0 = no denoise, Threads.cpp:565).
+ * sample_offset shifts the sample indices (resume). flags may hold
+ * LUZ_RENDER_PROFILE (per-stage device times) and LUZ_RENDER_COUNT (BVH node /
+ * triangle visit counts); neither changes the image. */
+#define LUZ_RENDER_PROFILE 0x100
+#define LUZ_RENDER_COUNT   0x200
+typedef struct LuzRenderParams {
+    int32_t  width, height;
+    int32_t  spp;
+    int32_t  max_bounces;         /* Scene::getMaxLightBounces                      */
+    uint32_t seed;                /* Sampler::setRenderSeed                         */
+    uint32_t stream;
+    int32_t  sample_offset;
+    int32_t  flags;
+} LuzRenderParams;
+
+typedef struct LuzRenderStats {
+    double   render_ms;           /* device time of the sample loop (CUDA events)   */
+    double   samples;             /* rendered samples (width*height*spp)            */
+    double   extension_rays;      /* closest-hit rays traced                        */
+    double   shadow_rays;         /* any-hit rays traced                            */
+    int64_t  kernel_launches;     /* kernels launched by this call                  */
+    int64_t  waves;
+    double   extend_ms, shade_ms, shadow_ms;   /* LUZ_RENDER_PROFILE: summed stage times */
+    int64_t  extend_launches, shadow_launches;
+    double   ext_nodes, ext_tris, ext_top;     /* LUZ_RENDER_COUNT: mesh nodes, triangles,  */
+    double   sh_nodes, sh_tris, sh_top;        /* top-level records read (ext / shadow)     */
+} LuzRenderStats;
+
+/* One closest-hit / any-hit result (luz_gpu_trace_rays). */
+typedef struct LuzHit {
+    float    t;                   /* world distance; +inf on miss                   */
+    int32_t  object;              /* index into LuzSceneDesc.objects, -1 = miss     */
+    int32_t  primitive;           /* triangle id (mesh/instance), cube face, else 0 */
+    float    u, v;                /* barycentrics for triangles                     */
+} LuzHit;
+
+typedef struct LuzSceneInfo {
+    int64_t  top_nodes;           /* BVHNode count (src/core/Hittables/BVHNode.cpp)  */
+    int64_t  top_leaf_objects;
+    int64_t  mesh_nodes;          /* packed mesh BVH nodes over all meshes          */
+    int64_t  mesh_triangles;
+    int64_t  device_bytes;        /* scene arena size on the device                 */
+    int32_t  max_mesh_depth;
+    int32_t  light_count;
+} LuzSceneInfo;
+
+/* Packed mesh BVH node as the reference builds it (Mesh::PackedBVHNode,
+ * include/luz/Hittables/Mesh.hpp:37-45), in double, for layout parity. */
+typedef struct LuzMeshNode64 {
+    double   bmin[3], bmax[3];
+    int64_t  left, right, start, count;
+    int32_t  is_leaf;
+    int32_t  _pad;
+} LuzMeshNode64;
+
+typedef struct luz_gpu_scene luz_gpu_scene;      /* device scene arena + queues */
+typedef struct luz_scene_pack luz_scene_pack;    /* host-side packed scene      */
+
+/* ---- errors / device ------------------------------------------------------ */
+int luz_gpu_last_error(char* buffer, size_t length);
+int luz_gpu_device_count(int32_t* count);
+
+/* ---- host packing (no GPU needed) ----------------------------------------- */
+/* Flattens the description: lights (Scene::updateLights, Scene.cpp:615-638),
+ * top-level BVHNode (Scene::updateAccelerationStructure, Scene.cpp:655-688;
+ * BVHNode.cpp:142-185), packed binned-SAH mesh BVHs (Mesh::_buildPackedBVH,
+ * Mesh.cpp:383-521), environment CDF (EnvironmentMap::buildDistribution,
+ * EnvironmentMap.cpp:627-671). */
+int luz_pack_create(const LuzSceneDesc* desc, luz_scene_pack** out);
+int luz_pack_destroy(luz_scene_pack* pack);
+int luz_pack_info(const luz_scene_pack* pack, LuzSceneInfo* info);
+/* Copies mesh `mesh`'s node array (node_capacity entries at most) and triangle
+ * order (_triangleIndices) for comparison with the reference's own arrays. */
+int luz_pack_mesh_bvh(const luz_scene_pack* pack, int32_t mesh,
+                      LuzMeshNode64* nodes, int64_t node_capacity, int64_t* node_count,
+                      int64_t* triangle_order, int64_t order_capacity);
+/* Raw packed arrays (FP32 device layout) for a CPU traversal check.
+ * name: "top_nodes", "top_children", "objects", "mesh_nodes", "mesh_tris",
+ * "meshes", "rects". Returns pointer and byte size; valid until destroy. */
+int luz_pack_array(const luz_scene_pack* pack, const char* name, const void** data, int64_t* bytes);
+
+/* ---- device scene --------------------------------------------------------- */
+int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene** out);
+int luz_gpu_scene_destroy(luz_gpu_scene* scene);
+int luz_gpu_scene_info(const luz_gpu_scene* scene, LuzSceneInfo* info);
+
+/* ---- hot path ------------------------------------------------------------- */
+/* Full render: W*H*spp paths through the wavefront integrator; rgb_out is the
+ * host film (W*H*3, row-major, y = 0 first) holding per-pixel means, exactly
+ * what _threadRender stores with Image::setPixelUnchecked (Threads.cpp:581). */
+int luz_gpu_render(luz_gpu_scene* scene, const LuzRenderParams* params,
+                   float* rgb_out, LuzRenderStats* stats);
+/* Same, device pointer film and caller stream (cudaStream_t as void*). */
+int luz_gpu_render_device(luz_gpu_scene* scene, const LuzRenderParams* params,
+                          float* d_rgb_out, void* stream, LuzRenderStats* stats);
+
+/* Per-path radiance for explicit (x, y, sample) triples: the colour
+ * calculateLightRaysColor returns for Sampler::beginPixelSample(x, y, s, stream)
+ * (ColorHelper.cpp:1110-1115), before cleanColor. Host buffers. */
+int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
+                        const int32_t* x, const int32_t* y, const int32_t* sample,
+                        int64_t count, float* rgb_out);
+
+/* Ray batch traversal (test hook and building block): rays are
+ * (ox, oy, oz, tmin, dx, dy, dz, tmax) * count, host buffers. any_hit != 0
+ * runs the shadow traversal and reports object = 0 (occluded) / -1. The
+ * stochastic volume sample uses (seed, pixel 0, sample 0, bounce 0) unless
+ * the caller passes volume_key (x, y, sample, bounce) per ray (may be NULL). */
+int luz_gpu_trace_rays(luz_gpu_scene* scene, const float* rays, int64_t count,
+                       int32_t any_hit, uint32_t seed, const int32_t* volume_key,
+                       LuzHit* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUZ_GPU_H */

@@ -1,0 +1,205 @@
+// layout.h — device-resident scene arena layout, shared by the host packer
+// (pack.cpp) and the CUDA kernels. Everything is plain data in FP32 except the
+// sampling CDFs, which stay FP64 so that discrete selections (light, triangle,
+// environment texel) pick the same index as the reference's std::upper_bound /
+// std::lower_bound over its double prefix sums.
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define LUZ_HD __host__ __device__
+#else
+#define LUZ_HD
+#endif
+
+namespace luz {
+
+// T_MIN of include/luz/Defaults.hpp:18 as the nearest float.
+constexpr float kTMin = 0.001f;
+constexpr int kMeshStack = 128;        // MESH_BVH_STACK_SIZE, src/core/Hittables/Mesh.cpp:17
+constexpr int kTopStack = 96;
+constexpr uint32_t kLeafBit = 0x80000000u;
+
+// Object kinds inside the top-level BVH / unaccelerated list.
+enum ObjKind : int32_t {
+    OK_RECT = 1, OK_SPHERE = 2, OK_CUBE = 3, OK_PLANE = 4, OK_MESH = 5, OK_INSTANCE = 6, OK_VOLUME = 7,
+    OK_DIRECTIONAL = 8
+};
+
+// 64 B. Rectangle with its basis precomputed in double (Rectangle::_buildBasis,
+// src/core/Hittables/Rectangle.cpp:127-152) and rounded to float.
+struct alignas(16) GRect {
+    float p[3];     // centre
+    float hw;       // width / 2
+    float n[3];     // normal
+    float hh;       // height / 2
+    float wa[3];    // width axis
+    float w;        // width
+    float ha[3];    // height axis
+    float h;        // height
+};
+
+// 64 B top-level object record.
+struct alignas(16) GObject {
+    int32_t kind;
+    int32_t material;
+    int32_t aux;      // rect index (RECT/CUBE first face), mesh index (MESH/INSTANCE), boundary kind (VOLUME)
+    int32_t id;       // index in LuzSceneDesc.objects
+    // SPHERE: c[3], r, visible
+    // PLANE: y, n[3]
+    // INSTANCE: pos[3], scale[3], cx, sx, cy, sy, cz, sz
+    // VOLUME: cube bmin[3], bmax[3] | sphere c[3], r ; f[6] = negative inverse density
+    // DIRECTIONAL: dir[3] (normalised light direction)
+    float f[12];
+};
+
+// Top-level BVHNode (src/core/Hittables/BVHNode.cpp). 32 B each.
+struct alignas(16) GTopNode {
+    float bmin[3];
+    int32_t child_start;
+    float bmax[3];
+    int32_t child_count;
+};
+struct alignas(16) GTopChild {
+    float bmin[3];
+    int32_t ref;       // top node index or object index
+    float bmax[3];
+    int32_t is_node;
+};
+
+// Mesh BVH interior node with both child boxes (64 B, one 128-B line holds 2).
+// ref: interior child = node index; leaf child = kLeafBit | first << 3 | (count - 1).
+struct alignas(16) GNode {
+    float lmin[3];
+    float lmax[3];
+    float rmin[3];
+    float rmax[3];
+    uint32_t lref;
+    uint32_t rref;
+    uint32_t pad0, pad1;
+};
+
+// Triangle in leaf order: v0, e1 = v1 - v0, e2 = v2 - v0 (edges formed in double
+// as Triangle::_updateCache does, src/core/Hittables/Triangle.cpp:94-126).
+struct alignas(16) GTri {
+    float v0[3];
+    uint32_t orig;     // index into the mesh's surviving-triangle list (primitive id)
+    float e1[3];
+    float area;
+    float e2[3];
+    uint32_t pad;
+};
+
+// Per-triangle shading data (leaf order).
+struct alignas(16) GTriShade {
+    float fn[3];       // face normal (normalised in double)
+    float pad;
+};
+
+struct alignas(16) GMesh {
+    float bmin[3];
+    int32_t node_offset;      // first GNode of this mesh; -1 when the root is a leaf
+    float bmax[3];
+    int32_t tri_offset;       // first GTri
+    int32_t tri_count;
+    int32_t root_ref;         // root reference (node index or leaf ref)
+    int32_t normal_offset;    // -1 or first entry (3 float3 per tri) in vertex-normal pool
+    int32_t uv_offset;        // -1 or first entry (3 float2 per tri) in uv pool
+    int32_t cdf_offset;       // area prefix sums (double) in the CDF pool, original order
+    int32_t slot_offset;      // original index -> leaf slot map
+    int32_t material;
+    int32_t depth;
+    double total_area;
+};
+
+// Materials (src/core/Materials/*). 144 B.
+enum MatType : int32_t {
+    MT_LAMBERTIAN = 1, MT_METAL = 2, MT_DIELECTRIC = 3, MT_EMISSIVE = 4, MT_ISOTROPIC = 5, MT_HG = 6,
+    MT_PRINCIPLED = 7
+};
+enum MatFlags : int32_t {
+    MF_CONDUCTOR = 1, MF_THIN = 2, MF_SMOOTH_FULL_TRANSMISSION = 4, MF_CAN_TRANSMIT = 8, MF_ABSORPTION = 16
+};
+struct alignas(16) GMaterial {
+    int32_t type;
+    int32_t texture;
+    int32_t flags;
+    int32_t pad;
+    float color[3];
+    float roughness;
+    float alpha;              // BSDF::roughnessToAlpha(roughness)
+    float clearcoat_alpha;
+    float ior;
+    float anisotropy;
+    float metallic, transmission, clearcoat, clearcoat_roughness;
+    float sheen, subsurface, f0_diel, pad2;
+    float eta[3], pad3;
+    float k[3], pad4;
+    float absorption[3], pad5;
+    float ss_radius_m[3], pad6;  // subsurface radius * scale (metres)
+    float ss_color[3], pad7;     // clampColor01(subsurface colour)
+};
+
+struct GTexture {
+    int32_t width, height;
+    int32_t offset;     // first texel (float4) in the texel pool
+    int32_t pad;
+};
+
+// Lights (Scene::updateLights, src/scene/Scene.cpp:615-638).
+enum LightKind : int32_t { LK_NONE = 0, LK_RECT = 1, LK_SPHERE = 2, LK_MESH = 3, LK_INSTANCE = 4, LK_DIRECTIONAL = 5 };
+struct alignas(16) GLight {
+    int32_t kind;
+    int32_t object;          // GObject index (top-level object id)
+    int32_t material;
+    int32_t cdf_offset;      // INSTANCE with non-uniform scale: transformed-area prefix sums
+    float emitted[3];
+    int32_t cdf_count;
+    double area;             // surface area used by pdfValue / sampleLight
+    int32_t uniform;         // INSTANCE: uniform area scale
+    int32_t mesh;
+};
+
+// Camera prepared in double (Renderer::internal::_prepareRenderCamera,
+// src/renderer/RayHelper.cpp:50-83); kept in double for ray generation.
+struct GCamera {
+    double position[3];
+    double u[3], v[3];
+    double horizontal[3], vertical[3], lower_left[3];
+    double lens_radius;
+    double inv_w1, inv_h1;
+};
+
+struct GEnv {
+    int32_t width, height;
+    int32_t present;          // hasVisibleEnvironment
+    int32_t lighting;         // hasEnvironmentLight
+    float strength;
+    float pad;
+    double rotation;
+    double total_weight;
+    int64_t texel_offset;     // float4 texels
+    int64_t cdf_offset;       // double CDF (W*H)
+    int64_t pdf_offset;       // double (weight/total)/solidAngle per texel
+};
+
+struct GSceneConst {
+    int32_t accel_kind;       // 0 none, 1 top BVH (root node 0), 2 single object
+    int32_t accel_object;
+    int32_t unaccel_count;
+    int32_t unaccel_offset;   // into the object-index pool
+    int32_t light_count;
+    int32_t sky;              // 0 none, 3 environment
+    int32_t has_constant_background_light;
+    int32_t sampled_infinite_light;
+    float background[3];
+    float background_luminance;
+    double light_total_weight;
+    int32_t light_cdf_offset; // double cumulative weights; -1 = uniform selection
+    int32_t any_can_transmit;
+    double meters_per_unit;
+    GCamera camera;
+    GEnv env;
+};
+
+}  // namespace luz

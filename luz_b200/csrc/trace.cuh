@@ -1,0 +1,688 @@
+// trace.cuh — closest-hit and any-hit traversal of the two-level scene.
+//
+// Semantics follow the reference exactly (tie order included):
+//   Renderer::internal::_checkHits          src/renderer/HitHelper.cpp:5-32
+//   isShadowOccluded                        src/renderer/ColorHelper.cpp:801-829
+//   BVHNode::hit / hitAny                   src/core/Hittables/BVHNode.cpp:221-380
+//     1 or 3 children: index order, each child does its own test;
+//     2 children: near-first, swap only on strict <, second needs near < closest;
+//     >= 4 children: stable insertion sort by near, skip near >= closest.
+//   Mesh::hit / hitAny                      src/core/Hittables/Mesh.cpp:578-735
+//     explicit stack, prune near >= closest, ties push the right child last
+//     (visited first); leaf triangles in order, later equal-t triangle wins.
+//   Triangle::hit (Moller-Trumbore)         src/core/Hittables/Triangle.cpp:196-305
+//   MeshInstance::hit / hitAny              src/core/Hittables/MeshInstance.cpp:251-327
+//   Rectangle / Sphere / Cube / Plane / ConstantVolume intersectors.
+// Arithmetic is FP32 with the reference's operation order (-fmad=false), so
+// oracle/restate.c reproduces every hit bit for bit on the same packed arrays.
+#pragma once
+#include "dmath.cuh"
+
+namespace luz {
+
+struct DScene {
+    const GRect* rects;
+    const GObject* objects;
+    const GTopNode* top_nodes;
+    const GTopChild* top_children;
+    const GNode* nodes;
+    const GTri* tris;
+    const GTriShade* tri_shade;
+    const float* vnormals;
+    const float* vuvs;
+    const GMesh* meshes;
+    const GMaterial* materials;
+    const GTexture* textures;
+    const float4* texels;
+    const GLight* lights;
+    const double* cdf;
+    const int32_t* index_pool;
+    const float4* env_texels;
+    uint32_t* error;          // device error word (bit flags)
+    unsigned long long* counters;   // LUZ_RENDER_COUNT: ext nodes/tris/top, shadow nodes/tris/top
+    GSceneConst k;
+};
+
+enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u };
+
+// xobj / xprim name the primitive a secondary ray leaves from. A ray that
+// starts on a planar primitive cannot meet it again at t > 0 in exact
+// arithmetic (the reference's FP64 hits never do, they fall below T_MIN), so
+// the FP32 traversal skips that primitive instead of re-hitting it through
+// rounding error at grazing angles; for the source sphere an outgoing ray
+// skips it and an entering ray keeps only the far root.
+struct TRay {
+    F3 o, d, inv;
+    bool zero;
+    int32_t xobj, xprim;
+};
+
+__device__ __forceinline__ float inv_component(float c)
+{
+    if (c == 0.0f || !isfinite(c)) return 0.0f;
+    const float i = 1.0f / c;
+    return isfinite(i) ? i : 0.0f;
+}
+__device__ __forceinline__ TRay make_ray(F3 o, F3 d)
+{
+    TRay r;
+    r.o = o;
+    r.d = d;
+    r.inv = F3{inv_component(d.x), inv_component(d.y), inv_component(d.z)};
+    r.zero = (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f);
+    r.xobj = -1;
+    r.xprim = -1;
+    return r;
+}
+__device__ __forceinline__ TRay make_ray_x(F3 o, F3 d, int32_t xobj, int32_t xprim)
+{
+    TRay r = make_ray(o, d);
+    r.xobj = xobj;
+    r.xprim = xprim;
+    return r;
+}
+
+struct THit {
+    float t;
+    int32_t obj;     // GObject index, -1 = miss
+    int32_t prim;    // mesh: leaf slot of the triangle; cube: face; else 0
+    float u, v;
+};
+
+// Per-ray traversal context: the volume distance sample (evaluated once, on
+// first use) and counts of the records read (mesh nodes, triangles, top-level
+// nodes/children/objects), used for the algorithmic-bytes roofline.
+struct VolSample {
+    const Key* key;
+    double u;
+    bool have;
+    uint32_t nodes = 0, tris = 0, top = 0;
+    __device__ __forceinline__ double get()
+    {
+        if (!have) {
+            u = sample1d(*key, DIM_VOLUME_DISTANCE);
+            have = true;
+        }
+        return u;
+    }
+};
+
+// boxHitDistance / AABB::hit (Mesh.cpp:99-139, BVHNode.cpp:20-60, AABB.cpp:37-71)
+__device__ __forceinline__ bool box_hit(const float* mn, const float* mx, const TRay& r, float tmax, float& tnear)
+{
+    if (r.zero) return false;
+    float tmin = kTMin;
+    const float o[3] = {r.o.x, r.o.y, r.o.z};
+    const float iv[3] = {r.inv.x, r.inv.y, r.inv.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float inv = iv[a];
+        if (inv == 0.0f) {
+            if (o[a] < mn[a] || o[a] > mx[a]) return false;
+            continue;
+        }
+        float t0 = (mn[a] - o[a]) * inv;
+        float t1 = (mx[a] - o[a]) * inv;
+        if (inv < 0.0f) {
+            const float s = t0;
+            t0 = t1;
+            t1 = s;
+        }
+        tmin = t0 > tmin ? t0 : tmin;
+        tmax = t1 < tmax ? t1 : tmax;
+        if (tmax <= tmin) return false;
+    }
+    tnear = tmin;
+    return true;
+}
+
+__device__ __forceinline__ bool tri_test(const GTri& T, const TRay& r, float tmin, float tmax, float& t, float& u, float& v)
+{
+    const F3 e1 = f3(T.e1), e2 = f3(T.e2), v0 = f3(T.v0);
+    const F3 p = cross(r.d, e2);
+    const float det = dot(e1, p);
+    if (fabsf(det) < 1e-12f) return false;
+    const float inv_det = 1.0f / det;
+    const F3 tv = r.o - v0;
+    u = dot(tv, p) * inv_det;
+    if (u < 0.0f || u > 1.0f) return false;
+    const F3 q = cross(tv, e1);
+    v = dot(r.d, q) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot(e2, q) * inv_det;
+    return !(t > tmax || t < tmin);
+}
+
+__device__ __forceinline__ GTri load_tri(const GTri* tris, uint32_t i)
+{
+    const float4* p = reinterpret_cast<const float4*>(tris + i);
+    const float4 a = ld4(p), b = ld4(p + 1), c = ld4(p + 2);
+    GTri t;
+    t.v0[0] = a.x; t.v0[1] = a.y; t.v0[2] = a.z; t.orig = __float_as_uint(a.w);
+    t.e1[0] = b.x; t.e1[1] = b.y; t.e1[2] = b.z; t.area = b.w;
+    t.e2[0] = c.x; t.e2[1] = c.y; t.e2[2] = c.z; t.pad = 0;
+    return t;
+}
+__device__ __forceinline__ GNode load_node(const GNode* nodes, uint32_t i)
+{
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    const float4 a = ld4(p), b = ld4(p + 1), c = ld4(p + 2), d = ld4(p + 3);
+    GNode n;
+    n.lmin[0] = a.x; n.lmin[1] = a.y; n.lmin[2] = a.z; n.lmax[0] = a.w;
+    n.lmax[1] = b.x; n.lmax[2] = b.y; n.rmin[0] = b.z; n.rmin[1] = b.w;
+    n.rmin[2] = c.x; n.rmax[0] = c.y; n.rmax[1] = c.z; n.rmax[2] = c.w;
+    n.lref = __float_as_uint(d.x); n.rref = __float_as_uint(d.y);
+    return n;
+}
+
+// Mesh::hit — closest triangle; closest is updated in place.
+__device__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
+                             int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs)
+{
+    float root_near;
+    if (!box_hit(M.bmin, M.bmax, r, closest, root_near)) return false;
+    uint32_t sref[kMeshStack];
+    float snear[kMeshStack];
+    int sp = 0;
+    sref[sp] = (uint32_t)M.root_ref;
+    snear[sp] = root_near;
+    sp++;
+    bool hit = false;
+    while (sp > 0) {
+        sp--;
+        const uint32_t ref = sref[sp];
+        if (snear[sp] >= closest) continue;
+        if (ref & kLeafBit) {
+            const uint32_t first = (ref & 0x7fffffffu) >> 3;
+            const uint32_t cnt = (ref & 7u) + 1u;
+            for (uint32_t i = first; i < first + cnt; i++) {
+                if ((int32_t)i == skip) continue;
+                const GTri T = load_tri(S.tris, i);
+                vs.tris++;
+                float t, u, v;
+                if (tri_test(T, r, tmin, closest, t, u, v)) {
+                    closest = t;
+                    slot = (int32_t)i;
+                    bu = u;
+                    bv = v;
+                    hit = true;
+                }
+            }
+            continue;
+        }
+        const GNode n = load_node(S.nodes, ref);
+        vs.nodes++;
+        float ln = 0.f, rn = 0.f;
+        const bool hl = box_hit(n.lmin, n.lmax, r, closest, ln);
+        const bool hr = box_hit(n.rmin, n.rmax, r, closest, rn);
+        if (sp + 2 > kMeshStack) {
+            atomicOr(S.error, ERR_MESH_STACK);
+            return hit;
+        }
+        if (hl && hr) {
+            if (ln < rn) {
+                sref[sp] = n.rref; snear[sp] = rn; sp++;
+                sref[sp] = n.lref; snear[sp] = ln; sp++;
+            } else {
+                sref[sp] = n.lref; snear[sp] = ln; sp++;
+                sref[sp] = n.rref; snear[sp] = rn; sp++;
+            }
+        } else if (hl) {
+            sref[sp] = n.lref; snear[sp] = ln; sp++;
+        } else if (hr) {
+            sref[sp] = n.rref; snear[sp] = rn; sp++;
+        }
+    }
+    return hit;
+}
+
+// Mesh::hitAny
+__device__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax, int32_t skip,
+                         VolSample& vs)
+{
+    float root_near;
+    if (!box_hit(M.bmin, M.bmax, r, tmax, root_near)) return false;
+    uint32_t sref[kMeshStack];
+    int sp = 0;
+    sref[sp++] = (uint32_t)M.root_ref;
+    while (sp > 0) {
+        const uint32_t ref = sref[--sp];
+        if (ref & kLeafBit) {
+            const uint32_t first = (ref & 0x7fffffffu) >> 3;
+            const uint32_t cnt = (ref & 7u) + 1u;
+            for (uint32_t i = first; i < first + cnt; i++) {
+                if ((int32_t)i == skip) continue;
+                const GTri T = load_tri(S.tris, i);
+                vs.tris++;
+                float t, u, v;
+                if (tri_test(T, r, tmin, tmax, t, u, v)) return true;
+            }
+            continue;
+        }
+        const GNode n = load_node(S.nodes, ref);
+        vs.nodes++;
+        float ln = 0.f, rn = 0.f;
+        const bool hl = box_hit(n.lmin, n.lmax, r, tmax, ln);
+        const bool hr = box_hit(n.rmin, n.rmax, r, tmax, rn);
+        if (sp + 2 > kMeshStack) {
+            atomicOr(S.error, ERR_MESH_STACK);
+            return false;
+        }
+        if (hl && hr) {
+            if (ln < rn) {
+                sref[sp++] = n.rref;
+                sref[sp++] = n.lref;
+            } else {
+                sref[sp++] = n.lref;
+                sref[sp++] = n.rref;
+            }
+        } else if (hl) {
+            sref[sp++] = n.lref;
+        } else if (hr) {
+            sref[sp++] = n.rref;
+        }
+    }
+    return false;
+}
+
+// Rectangle::hit geometric test (Rectangle.cpp:212-249); returns t.
+__device__ __forceinline__ bool rect_test(const GRect& R, const TRay& r, float tmin, float tmax, float& t)
+{
+    if (R.w <= 0.0f || R.h <= 0.0f) return false;
+    const F3 p = f3(R.p), n = f3(R.n);
+    const float a = dot(r.o - p, n);
+    const float b = dot(r.d, n);
+    if (b == 0.0f || (a < 0.0f && b < 0.0f) || (a > 0.0f && b > 0.0f)) return false;
+    t = -a / b;
+    if (t > tmax || t < tmin) return false;
+    const F3 d = (r.o + (t * r.d)) - p;
+    const float wd = dot(d, f3(R.wa));
+    const float hd = dot(d, f3(R.ha));
+    return !(fabsf(wd) > R.hw || fabsf(hd) > R.hh);
+}
+
+// Sphere::hit / hitAny root selection (Sphere.cpp:227-302).
+__device__ __forceinline__ bool sphere_test(const GObject& O, const TRay& r, float tmin, float tmax, float& t,
+                                            bool source = false)
+{
+    if (O.f[4] == 0.0f || r.zero) return false;
+    const F3 c = f3(O.f);
+    const float rad = O.f[3];
+    const F3 oc = r.o - c;
+    const float b = dot(oc, r.d);
+    if (source && b >= 0.0f) return false;   // leaving the source sphere
+    // b^2 - (|oc|^2 - r^2) as r^2 - |oc - b d|^2: equal for a unit direction, free of cancellation.
+    const F3 f = oc - b * r.d;
+    const float disc = (rad * rad) - len2(f);
+    if (disc < 0.0f) return false;
+    const float sq = sqrtf(disc);
+    float root = -b - sq;
+    if (source || root < tmin || root > tmax) {
+        root = -b + sq;
+        if (root < tmin || root > tmax) return false;
+    }
+    t = root;
+    return true;
+}
+
+__device__ __forceinline__ bool plane_test(const GObject& O, const TRay& r, float tmin, float tmax, float& t)
+{
+    const F3 n = f3(O.f + 1);
+    const F3 pos = F3{0.0f, O.f[0], 0.0f};
+    const float d = dot(r.d, n);
+    if (d == 0.0f) return false;
+    t = dot(pos - r.o, n) / d;
+    return !(t > tmax || t < tmin);
+}
+
+// MeshInstance::_localRay (MeshInstance.cpp:245-265) with InstanceTransform inverses.
+__device__ __forceinline__ F3 inv_rotate(const GObject& O, F3 v)
+{
+    const float cx = O.f[6], sx = O.f[7], cy = O.f[8], sy = O.f[9], cz = O.f[10], sz = O.f[11];
+    float x = v.x, y = v.y, z = v.z;
+    float nx = (x * cz) + (y * sz);
+    float ny = (-x * sz) + (y * cz);
+    x = nx;
+    y = ny;
+    nx = (x * cy) - (z * sy);
+    float nz = (x * sy) + (z * cy);
+    x = nx;
+    z = nz;
+    ny = (y * cx) + (z * sx);
+    nz = (-y * sx) + (z * cx);
+    return F3{x, ny, nz};
+}
+__device__ __forceinline__ F3 fwd_rotate(const GObject& O, F3 v)
+{
+    const float cx = O.f[6], sx = O.f[7], cy = O.f[8], sy = O.f[9], cz = O.f[10], sz = O.f[11];
+    float x = v.x, y = v.y, z = v.z;
+    float ny = (y * cx) - (z * sx);
+    float nz = (y * sx) + (z * cx);
+    y = ny;
+    z = nz;
+    float nx = (x * cy) + (z * sy);
+    nz = (-x * sy) + (z * cy);
+    x = nx;
+    z = nz;
+    nx = (x * cz) - (y * sz);
+    ny = (x * sz) + (y * cz);
+    return F3{nx, ny, z};
+}
+__device__ __forceinline__ bool instance_invertible(const GObject& O)
+{
+    return fabsf(O.f[3]) > 1e-12f && fabsf(O.f[4]) > 1e-12f && fabsf(O.f[5]) > 1e-12f;
+}
+__device__ __forceinline__ bool local_ray(const GObject& O, const TRay& r, TRay& lr, float& scale)
+{
+    if (!instance_invertible(O)) return false;
+    const F3 s = f3(O.f + 3);
+    const F3 ur = inv_rotate(O, r.d);
+    const F3 ld = F3{ur.x / s.x, ur.y / s.y, ur.z / s.z};
+    scale = sqrtf(len2(ld));
+    if (!isfinite(scale) || scale <= 0.0f) return false;
+    const F3 uo = inv_rotate(O, r.o - f3(O.f));
+    const F3 lo = F3{uo.x / s.x, uo.y / s.y, uo.z / s.z};
+    if (!isfinite(lo.x) || !isfinite(lo.y) || !isfinite(lo.z)) return false;
+    lr = make_ray_x(lo, vdiv(ld, scale), r.xobj, r.xprim);
+    return true;
+}
+
+// ConstantVolume::sampleScatteringDistance (ConstantVolume.cpp:62-121) with the
+// boundary's hitInterval(-T_MAX, T_MAX) (Cube.cpp:134-175, Sphere.cpp:304-343).
+__device__ bool volume_distance(const GObject& O, const TRay& r, float tmin, float tmax, VolSample& vs, float& t)
+{
+    float entry, exit;
+    if (O.aux == 3 /* LUZ_OBJ_CUBE */) {
+        float imin = -kInf, imax = kInf;
+        const float o[3] = {r.o.x, r.o.y, r.o.z};
+        const float d[3] = {r.d.x, r.d.y, r.d.z};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (d[a] == 0.0f) {
+                if (o[a] < O.f[a] || o[a] > O.f[3 + a]) return false;
+                continue;
+            }
+            const float inv = 1.0f / d[a];
+            float t0 = (O.f[a] - o[a]) * inv;
+            float t1 = (O.f[3 + a] - o[a]) * inv;
+            if (t0 > t1) {
+                const float s = t0;
+                t0 = t1;
+                t1 = s;
+            }
+            imin = fmaxf(imin, t0);
+            imax = fminf(imax, t1);
+            if (imin >= imax) return false;
+        }
+        entry = imin;
+        exit = imax;
+    } else {
+        if (r.zero) return false;
+        const F3 oc = r.o - f3(O.f);
+        const float b = dot(oc, r.d);
+        const F3 f = oc - b * r.d;
+        const float disc = (O.f[3] * O.f[3]) - len2(f);
+        if (disc < 0.0f) return false;
+        const float sq = sqrtf(disc);
+        float r0 = -b - sq, r1 = -b + sq;
+        if (r0 > r1) {
+            const float s = r0;
+            r0 = r1;
+            r1 = s;
+        }
+        if (r0 >= r1) return false;
+        entry = r0;
+        exit = r1;
+    }
+    if (entry < tmin) entry = tmin;
+    if (exit > tmax) exit = tmax;
+    if (entry >= exit) return false;
+    if (entry < 0.0f) entry = 0.0f;
+    const float len = sqrtf(len2(r.d));
+    if (len <= 0.0f || !isfinite(len)) return false;
+    const float inside = (exit - entry) * len;
+    const float hd = (float)((double)O.f[6] * log(fmax(vs.get(), 1e-12)));
+    if (hd > inside) return false;
+    t = entry + hd / len;
+    return true;
+}
+
+// One object's closest hit; updates closest/hit when it wins.
+__device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, const TRay& r, float tmin, float& closest,
+                                               THit& h, VolSample& vs)
+{
+    const GObject O = S.objects[oi];
+    vs.top++;
+    const bool src = oi == r.xobj;
+    float t;
+    switch (O.kind) {
+    case OK_RECT:
+        if (!src && rect_test(S.rects[O.aux], r, tmin, closest, t)) {
+            closest = t;
+            h = THit{t, oi, 0, 0.f, 0.f};
+        }
+        break;
+    case OK_CUBE:
+        for (int f = 0; f < 6; f++)
+            if (!(src && f == r.xprim) && rect_test(S.rects[O.aux + f], r, tmin, closest, t)) {
+                closest = t;
+                h = THit{t, oi, f, 0.f, 0.f};
+            }
+        break;
+    case OK_SPHERE:
+        if (sphere_test(O, r, tmin, closest, t, src)) {
+            closest = t;
+            h = THit{t, oi, 0, 0.f, 0.f};
+        }
+        break;
+    case OK_PLANE:
+        if (!src && plane_test(O, r, tmin, closest, t)) {
+            closest = t;
+            h = THit{t, oi, 0, 0.f, 0.f};
+        }
+        break;
+    case OK_MESH: {
+        int32_t slot;
+        float u, v;
+        if (mesh_closest(S, S.meshes[O.aux], r, tmin, closest, slot, u, v, src ? r.xprim : -1, vs))
+            h = THit{closest, oi, slot, u, v};
+        break;
+    }
+    case OK_INSTANCE: {
+        TRay lr;
+        float s;
+        if (!local_ray(O, r, lr, s)) break;
+        float lc = closest * s;
+        int32_t slot;
+        float u, v;
+        if (!mesh_closest(S, S.meshes[O.aux], lr, tmin * s, lc, slot, u, v, src ? r.xprim : -1, vs)) break;
+        const float wt = lc / s;
+        if (!isfinite(wt) || wt < tmin || wt > closest) break;
+        closest = wt;
+        h = THit{wt, oi, slot, u, v};
+        break;
+    }
+    case OK_VOLUME:
+        if (volume_distance(O, r, tmin, closest, vs, t)) {
+            closest = t;
+            h = THit{t, oi, 0, 0.f, 0.f};
+        }
+        break;
+    default:
+        break;
+    }
+}
+
+__device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TRay& r, float tmin, float tmax, VolSample& vs)
+{
+    const GObject O = S.objects[oi];
+    vs.top++;
+    const bool src = oi == r.xobj;
+    float t;
+    switch (O.kind) {
+    case OK_RECT:
+        return !src && rect_test(S.rects[O.aux], r, tmin, tmax, t);
+    case OK_CUBE:
+        for (int f = 0; f < 6; f++)
+            if (!(src && f == r.xprim) && rect_test(S.rects[O.aux + f], r, tmin, tmax, t)) return true;
+        return false;
+    case OK_SPHERE:
+        return sphere_test(O, r, tmin, tmax, t, src);
+    case OK_PLANE:
+        return !src && plane_test(O, r, tmin, tmax, t);
+    case OK_MESH:
+        return mesh_any(S, S.meshes[O.aux], r, tmin, tmax, src ? r.xprim : -1, vs);
+    case OK_INSTANCE: {
+        TRay lr;
+        float s;
+        if (!local_ray(O, r, lr, s)) return false;
+        return mesh_any(S, S.meshes[O.aux], lr, tmin * s, tmax * s, src ? r.xprim : -1, vs);
+    }
+    case OK_VOLUME:
+        return volume_distance(O, r, tmin, tmax, vs, t);
+    default:
+        return false;
+    }
+}
+
+// Top-level stack entries: ref | kind << 30; kind 0 = node (near check),
+// 1 = node (own box test), 2 = object (near check), 3 = object (no check).
+#define TOP_PUSH(ref_, kind_, near_)                       \
+    do {                                                   \
+        if (sp >= kTopStack) {                             \
+            atomicOr(S.error, ERR_TOP_STACK);              \
+            sp = 0;                                        \
+            break;                                         \
+        }                                                  \
+        sref[sp] = (uint32_t)(ref_) | ((uint32_t)(kind_) << 30); \
+        snear[sp] = (near_);                               \
+        sp++;                                              \
+    } while (0)
+
+// Renderer::internal::_checkHits with explicit [tmin, tmax].
+__device__ THit closest_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs)
+{
+    THit h{kInf, -1, 0, 0.f, 0.f};
+    float closest = tmax;
+    if (S.k.accel_kind == 2) {
+        object_closest(S, S.k.accel_object, r, tmin, closest, h, vs);
+    } else if (S.k.accel_kind == 1) {
+        uint32_t sref[kTopStack];
+        float snear[kTopStack];
+        int sp = 0;
+        TOP_PUSH(0, 1, -kInf);
+        while (sp > 0) {
+            sp--;
+            const uint32_t e = sref[sp];
+            const float near = snear[sp];
+            const uint32_t kind = e >> 30;
+            const int32_t idx = (int32_t)(e & 0x3fffffffu);
+            if (kind >= 2) {
+                if (kind == 2 && near >= closest) continue;
+                object_closest(S, idx, r, tmin, closest, h, vs);
+                continue;
+            }
+            const GTopNode N = S.top_nodes[idx];
+            vs.top += 1 + (uint32_t)N.child_count;
+            float dummy;
+            if (kind == 1) {
+                if (!box_hit(N.bmin, N.bmax, r, closest, dummy)) continue;
+            } else if (near >= closest) {
+                continue;
+            }
+            const int n = N.child_count;
+            const GTopChild* C = S.top_children + N.child_start;
+            if (n != 2 && n <= 3) {
+                for (int i = n - 1; i >= 0; i--) {
+                    if (C[i].is_node) TOP_PUSH(C[i].ref, 1, -kInf);
+                    else TOP_PUSH(C[i].ref, 3, -kInf);
+                }
+            } else if (n == 2) {
+                float na = 0.f, nb = 0.f;
+                const bool ha = box_hit(C[0].bmin, C[0].bmax, r, closest, na);
+                const bool hb = box_hit(C[1].bmin, C[1].bmax, r, closest, nb);
+                int first = 0, second = 1;
+                bool hf = ha, hs = hb;
+                float nf = na, ns = nb;
+                if (ha && hb && nb < na) {
+                    first = 1;
+                    second = 0;
+                    hf = hb;
+                    hs = ha;
+                    nf = nb;
+                    ns = na;
+                }
+                if (hs) TOP_PUSH(C[second].ref, C[second].is_node ? 0 : 2, ns);
+                if (hf) TOP_PUSH(C[first].ref, C[first].is_node ? 0 : 2, nf);
+            } else {
+                int ord[16];
+                float on[16];
+                int cnt = 0;
+                for (int i = 0; i < n && i < 16; i++) {
+                    float cn;
+                    if (!box_hit(C[i].bmin, C[i].bmax, r, closest, cn)) continue;
+                    int j = cnt;
+                    while (j > 0 && on[j - 1] > cn) {
+                        on[j] = on[j - 1];
+                        ord[j] = ord[j - 1];
+                        j--;
+                    }
+                    on[j] = cn;
+                    ord[j] = i;
+                    cnt++;
+                }
+                for (int j = cnt - 1; j >= 0; j--) {
+                    const GTopChild& c = C[ord[j]];
+                    TOP_PUSH(c.ref, c.is_node ? 0 : 2, on[j]);
+                }
+            }
+        }
+    }
+    for (int i = 0; i < S.k.unaccel_count; i++) object_closest(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, closest, h, vs);
+    return h;
+}
+
+// isShadowOccluded body with explicit [tmin, tmax] (tmax <= T_MIN -> not occluded).
+__device__ bool any_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs)
+{
+    if (tmax <= kTMin) return false;
+    if (S.k.accel_kind == 2) {
+        if (object_any(S, S.k.accel_object, r, tmin, tmax, vs)) return true;
+    } else if (S.k.accel_kind == 1) {
+        uint32_t sref[kTopStack];
+        float snear[kTopStack];
+        int sp = 0;
+        TOP_PUSH(0, 1, 0.f);
+        while (sp > 0) {
+            sp--;
+            const uint32_t e = sref[sp];
+            const uint32_t kind = e >> 30;
+            const int32_t idx = (int32_t)(e & 0x3fffffffu);
+            if (kind >= 2) {
+                if (object_any(S, idx, r, tmin, tmax, vs)) return true;
+                continue;
+            }
+            const GTopNode N = S.top_nodes[idx];
+            vs.top += 1 + (uint32_t)N.child_count;
+            float dummy;
+            if (kind == 1 && !box_hit(N.bmin, N.bmax, r, tmax, dummy)) continue;
+            const int n = N.child_count;
+            const GTopChild* C = S.top_children + N.child_start;
+            const bool test_kids = !(n != 2 && n <= 3);
+            for (int i = n - 1; i >= 0; i--) {
+                if (test_kids) {
+                    float cn;
+                    if (!box_hit(C[i].bmin, C[i].bmax, r, tmax, cn)) continue;
+                    TOP_PUSH(C[i].ref, C[i].is_node ? 1 : 3, 0.f);
+                } else {
+                    TOP_PUSH(C[i].ref, C[i].is_node ? 1 : 3, 0.f);
+                }
+            }
+        }
+    }
+    for (int i = 0; i < S.k.unaccel_count; i++)
+        if (object_any(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, tmax, vs)) return true;
+    return false;
+}
+
+}  // namespace luz

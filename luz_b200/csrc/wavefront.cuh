@@ -1,0 +1,385 @@
+// wavefront.cuh — per-path device logic of the wavefront integrator (state
+// layout, camera rays, the shade step); kernels live in integrator.cu.
+#pragma once
+#include "shade.cuh"
+
+namespace luz {
+
+constexpr int kMaxBounceSlots = 256;
+constexpr int kBlock = 128;
+
+struct Ctrl {
+    uint32_t count[kMaxBounceSlots + 2];    // extension queue size entering bounce b
+    uint32_t shadow[kMaxBounceSlots + 2];   // shadow rays emitted at bounce b
+    uint32_t fetch_ext[kMaxBounceSlots + 2];
+    uint32_t fetch_sh[kMaxBounceSlots + 2];
+};
+
+struct PathBuf {
+    float4* ray_o;
+    float4* ray_d;
+    float4* thr;       // xyz throughput, w previous scatter pdf
+    float4* rad;       // xyz radiance, w flags
+    float4* prev_o;
+    float4* pend0;     // pending light-NEE contribution
+    float4* pend1;     // pending environment-NEE contribution
+    uint32_t* pixel;
+    uint32_t* sample;
+    float4* hit;       // t, u, v, object (bits)
+    int32_t* hit_prim;
+    uint32_t* queue0;
+    uint32_t* queue1;
+    float4* sh_o;      // xyz origin, w tmax
+    float4* sh_d;      // xyz direction, w path | slot << 31 (bits)
+    int2* sh_x;        // source primitive excluded from the shadow ray
+    float4* color;     // per-path final colour
+};
+
+struct WaveArgs {
+    int32_t width, height;
+    uint32_t seed, stream;
+    int32_t pix_begin, pix_count;
+    int32_t s_begin, s_count;
+    int32_t sample_offset;
+    int32_t max_bounces;
+    int64_t n;                    // paths in this wave
+    const int32_t* list_x;        // list mode (trace_paths): explicit (x, y, s)
+    const int32_t* list_y;
+    const int32_t* list_s;
+    int32_t list_mode;
+    GCamera cam;
+};
+
+enum PathFlags : uint32_t { PF_PREV_SPECULAR = 1u, PF_PREV_SVIL = 2u };
+
+__device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint32_t& x, uint32_t& y, uint32_t& s)
+{
+    if (w.list_mode) {
+        x = (uint32_t)w.list_x[p];
+        y = (uint32_t)w.list_y[p];
+        s = (uint32_t)w.list_s[p];
+        return;
+    }
+    const uint32_t pix = (uint32_t)w.pix_begin + p / (uint32_t)w.s_count;
+    s = (uint32_t)(w.s_begin + w.sample_offset) + p % (uint32_t)w.s_count;
+    x = pix % (uint32_t)w.width;
+    y = pix / (uint32_t)w.width;
+}
+
+__device__ __forceinline__ Key path_key(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, uint32_t bounce)
+{
+    return Key{base_key(w.seed, x, y, w.stream), s, bounce};
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated queue append: one atomicAdd per warp (ballot + popc).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return 0;
+    const uint32_t lane = lane_id();
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+// _generateRay (src/renderer/RayHelper.cpp:85-106) in FP64, rounded to FP32.
+__device__ void camera_ray(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, double* o, double* d)
+{
+    const Key k = path_key(w, x, y, s, 0);
+    const GCamera& c = w.cam;
+    const S2 cs = sample2d(k, DIM_CAMERA);
+    const double xu = ((double)x + (double)cs.x) * c.inv_w1;
+    const double yv = ((double)y + (double)cs.y) * c.inv_h1;
+    double off[3] = {0.0, 0.0, 0.0};
+    if (c.lens_radius > 0.0) {
+        float dx, dy;
+        unit_disk(k, DIM_LENS, dx, dy);
+        const double rx = (double)dx * c.lens_radius, ry = (double)dy * c.lens_radius;
+        for (int a = 0; a < 3; a++) off[a] = c.u[a] * rx + c.v[a] * ry;
+    }
+    for (int a = 0; a < 3; a++) {
+        o[a] = c.position[a] + off[a];
+        d[a] = (((c.lower_left[a] - (c.horizontal[a] * xu)) - (c.vertical[a] * yv)) - c.position[a]) - off[a];
+    }
+    const double len = sqrt((d[0] * d[0]) + (d[1] * d[1]) + (d[2] * d[2]));
+    if (!isfinite(len) || len <= 0.0) {
+        d[0] = d[1] = d[2] = 0.0;
+    } else {
+        const double il = 1.0 / len;
+        for (int a = 0; a < 3; a++) d[a] = il * d[a];
+    }
+}
+
+// ---------------------------------------------------------------------------- shade
+
+__device__ __forceinline__ F3 clamp_ray_color(F3 c)   // clampRayColor (ColorHelper.cpp:259-274)
+{
+    const float l = luminance(c);
+    if (!isfinite(l)) return F3{0.f, 0.f, 0.f};
+    if (l > 1.0e12f) c = c * (1.0e12f / l);
+    return c;
+}
+__device__ __forceinline__ F3 clamp_color_lum(F3 c, float maxl)
+{
+    const float l = luminance(c);
+    if (!isfinite(l)) return F3{0.f, 0.f, 0.f};
+    if (maxl > 0.0f && l > maxl) c = c * (maxl / l);
+    return c;
+}
+__device__ __forceinline__ F3 clamp_bg_miss(const DScene& S, F3 c)   // clampConstantBackgroundMiss
+{
+    const float bl = S.k.background_luminance;
+    if (!isfinite(bl) || bl <= 0.0f) return c;
+    return clamp_color_lum(c, bl * 4.0f);
+}
+__device__ __forceinline__ float power_heuristic(float a, float b)
+{
+    const float f = a * a, s = b * b, sum = f + s;
+    if (sum <= 0.0f || !isfinite(sum)) return 0.0f;
+    return f / sum;
+}
+__device__ __forceinline__ bool terminated(F3 t)
+{
+    const float m = maxc(t);
+    return !isfinite(m) || m <= 1e-6f;
+}
+__device__ __forceinline__ bool russian_roulette(F3& thr, int bounce, const Key& k)
+{
+    if (bounce < 3) return true;
+    float surv = maxc(thr);
+    surv = fmaxf(0.05f, fminf(0.95f, surv));
+    if (sample1d(k, DIM_RUSSIAN_ROULETTE) > (double)surv) return false;
+    thr = cdiv(thr, surv);
+    return true;
+}
+__device__ __forceinline__ bool leaves_opaque(const GMaterial& m, const Hit& h, F3 dir)
+{
+    if (m.flags & MF_CAN_TRANSMIT) return true;
+    F3 g = h.gn;
+    if (len2(g) <= 1e-12f) g = h.n;
+    if (len2(g) <= 1e-12f) return true;
+    return dot(g, dir) > 1e-7f;
+}
+__device__ __forceinline__ float direct_prob(int bounce) { return bounce < 2 ? 1.0f : 0.5f; }
+
+// relocateSubsurfaceExit (ColorHelper.cpp:428-504)
+__device__ void relocate_subsurface(const DScene& S, const GMaterial& m, Hit& h, Scatter& sr, F3 ray_d, const Key& k)
+{
+    if (!sr.subsurface || sr.thin) return;
+    const float dl = maxc(sr.ss_radius_m);
+    if (!isfinite(dl) || dl <= 0.0f) return;
+    const double comp = sample1d(k, DIM_SUBSURFACE_PROFILE_COMPONENT);
+    const S2 rs = sample2d(k, DIM_SUBSURFACE_SPATIAL);
+    const float u = fmaxf(1e-12f, fminf(1.0f - 1e-12f, rs.y));
+    const float scale = comp < 0.25 ? dl : 3.0f * dl;
+    const float radius_m = -scale * logf(1.0f - u);
+    const float mpu = (float)S.k.meters_per_unit;
+    if (radius_m <= 0.0f || !isfinite(radius_m) || mpu <= 0.0f) return;
+    const float radius = radius_m / mpu;
+    if (radius <= kTMin) return;
+    F3 n = h.n;
+    if (len2(n) <= 1e-12f) n = h.gn;
+    if (len2(n) <= 1e-12f) return;
+    n = normalize(n);
+    const Onb b = make_onb(n);
+    const float ang = 2.0f * kPiF * rs.x;
+    const F3 off = onb_local(b, cosf(ang) * radius, sinf(ang) * radius, 0.0f);
+    const F3 cand = h.p + off;
+    const float probe = fmaxf(radius + (4.0f * dl / mpu), 16.0f * kTMin);
+    const TRay pr = make_ray(cand + n * probe, ray_dir_normalized(n * -1.0f));
+    VolSample vs{&k, 0.0, false};
+    const THit th = closest_hit(S, pr, kTMin, kInf, vs);
+    if (th.obj < 0) return;
+    const Hit eh = make_hit(S, pr, th);
+    if (eh.material != h.material || eh.t <= kTMin || eh.t > (2.0f * probe + kTMin)) return;
+    // refreshSubsurfaceScatterAtExit (ColorHelper.cpp:395-426)
+    const F3 dir = onb_local(make_onb(eh.n), cosine_hemisphere(k, DIM_BSDF_DIRECTION));
+    const float pdf = bsdf_pdf(S, m, eh, ray_d, dir);
+    const F3 bc = bsdf_eval(S, m, eh, ray_d, dir);
+    if (pdf <= 0.0f || !isfinite(pdf) || maxc(bc) <= 0.0f) return;
+    h = eh;
+    sr.dir = dir;
+    sr.spdf = pdf;
+    sr.att = cdiv(bc, pdf);
+}
+
+struct ShadeOut {
+    int32_t xobj, xprim;   // source primitive of the next ray and the shadow rays
+    bool cont;
+    F3 next_o, next_d;
+    bool sh[2];
+    F3 sh_o[2], sh_d[2];
+    float sh_t[2];
+};
+
+__device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
+{
+    out.cont = false;
+    out.sh[0] = out.sh[1] = false;
+    out.xobj = -1;
+    out.xprim = -1;
+    const float4 t4 = P.thr[p], r4 = P.rad[p], po4 = P.prev_o[p];
+    F3 thr{t4.x, t4.y, t4.z};
+    F3 rad{r4.x, r4.y, r4.z};
+    uint32_t flags = __float_as_uint(r4.w);
+    const float prev_pdf = t4.w;
+    const F3 prev_o{po4.x, po4.y, po4.z};
+    {
+        const float4 a = P.pend0[p], b = P.pend1[p];
+        rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
+    }
+    F3 pend0{0.f, 0.f, 0.f}, pend1{0.f, 0.f, 0.f};
+    const float4 ro = P.ray_o[p], rd = P.ray_d[p];
+    const TRay ray = make_ray_x(F3{ro.x, ro.y, ro.z}, F3{rd.x, rd.y, rd.z}, __float_as_int(ro.w), __float_as_int(rd.w));
+    const float4 h4 = P.hit[p];
+    const int32_t obj = __float_as_int(h4.w);
+    const uint32_t pix = P.pixel[p];
+    const Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+    const bool prev_spec = (flags & PF_PREV_SPECULAR) != 0;
+
+    if (obj < 0) {   // miss (ColorHelper.cpp:1169-1210)
+        float env_mis = 1.0f;
+        if (bounce > 0 && !prev_spec && (flags & PF_PREV_SVIL)) {
+            float ipdf = 0.0f;
+            if (S.k.env.lighting) ipdf = env_pdf(S, ray.d);
+            else if (S.k.has_constant_background_light) ipdf = 1.0f / (4.0f * kPiF);
+            env_mis = power_heuristic(prev_pdf, ipdf);
+        }
+        F3 sky;
+        if (S.k.sky == 3 && S.k.env.present) sky = (env_radiance(S, ray.d) * S.k.env.strength) * env_mis;
+        else sky = f3(S.k.background) * env_mis;
+        F3 contrib = thr * sky;
+        if (bounce > 0 && S.k.has_constant_background_light) contrib = clamp_bg_miss(S, contrib);
+        rad = rad + clamp_ray_color(contrib);
+        goto done;
+    }
+    {
+        THit th{h4.x, obj, P.hit_prim[p], h4.y, h4.z};
+        Hit h = make_hit(S, ray, th);
+        const GMaterial m = S.materials[h.material];
+        const F3 emitted = m.type == MT_EMISSIVE ? f3(m.color) : F3{0.f, 0.f, 0.f};
+        Scatter sr;
+        if (!scatter(S, m, h, ray.d, k, sr)) {
+            const float plp = (!prev_spec && S.k.light_count > 0) ? lights_pdf(S, prev_o, ray.d) : 0.0f;
+            const float wgt = prev_spec ? 1.0f : power_heuristic(prev_pdf, plp);
+            rad = rad + clamp_ray_color((thr * emitted) * wgt);
+            goto done;
+        }
+        relocate_subsurface(S, m, h, sr, ray.d, k);
+        if (!h.volume) {
+            out.xobj = h.obj;
+            out.xprim = h.prim;
+        }
+        F3 att = sr.att;
+        if (!h.front && sr.absorb) {   // effectiveScatterAttenuation + mediumTransmittance
+            const float dm = h.t * (float)S.k.meters_per_unit;
+            if (isfinite(dm) && dm > 0.0f)
+                att = att * F3{expf(-sr.absorption.x * dm), expf(-sr.absorption.y * dm), expf(-sr.absorption.z * dm)};
+        }
+        if (sr.specular) {
+            if (!leaves_opaque(m, h, sr.dir)) goto done;
+            thr = clamp_ray_color(thr * att);
+            if (terminated(thr) || !russian_roulette(thr, bounce, k)) goto done;
+            out.cont = true;
+            out.next_o = h.p;
+            out.next_d = sr.dir;
+            flags = PF_PREV_SPECULAR;
+            P.thr[p] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+            goto done;
+        }
+        rad = rad + thr * emitted;
+        if (terminated(thr * att)) goto done;
+        if (S.k.light_count > 0) {   // estimateDirectLighting (ColorHelper.cpp:973-1033)
+            const float prob = direct_prob(bounce);
+            bool go = true;
+            if (prob < 1.0f && sample1d(k, DIM_LIGHT_STRATEGY) >= (double)prob) go = false;
+            LightSample ls;
+            if (go && sample_light(S, h.p, k, ls) && leaves_opaque(m, h, ls.dir)) {
+                const float sp = scatter_pdf(S, sr, m, h, ray.d, ls.dir);
+                const F3 bc = scatter_bsdfcos(S, sr, m, h, ray.d, ls.dir);
+                if (!(sp <= 0.0f || !isfinite(sp) || maxc(bc) <= 0.0f)) {
+                    const float mis = power_heuristic(ls.pdf, sp);
+                    const F3 c = (bc * ls.emitted) * (mis / (ls.pdf * prob));
+                    pend0 = clamp_ray_color(thr * c);
+                    out.sh[0] = true;
+                    out.sh_o[0] = h.p;
+                    out.sh_d[0] = ls.dir;
+                    out.sh_t[0] = ls.tmax - kTMin;
+                }
+            }
+        }
+        if (S.k.sampled_infinite_light) {   // estimateEnvironmentLighting (ColorHelper.cpp:1035-1098)
+            const bool cbg = S.k.has_constant_background_light != 0;
+            bool go = !(cbg && sr.pdf == PDF_BSDF);
+            const float prob = direct_prob(bounce);
+            if (go && prob < 1.0f && sample1d(k, DIM_ENVIRONMENT_STRATEGY) >= (double)prob) go = false;
+            LightSample ls;
+            ls.valid = false;
+            if (go) {
+                if (S.k.env.lighting) {
+                    F3 rdn;
+                    float pdf;
+                    if (env_sample(S, k, ls.dir, rdn, pdf)) {
+                        ls.emitted = rdn * S.k.env.strength;
+                        ls.pdf = pdf;
+                        ls.valid = maxc(ls.emitted) > 0.0f;
+                    }
+                } else if (cbg) {
+                    ls.dir = sphere_direction(k, DIM_ENVIRONMENT_POINT);
+                    ls.emitted = f3(S.k.background);
+                    ls.pdf = 1.0f / (4.0f * kPiF);
+                    ls.valid = maxc(ls.emitted) > 0.0f;
+                }
+            }
+            if (ls.valid && leaves_opaque(m, h, ls.dir)) {
+                const float sp = scatter_pdf(S, sr, m, h, ray.d, ls.dir);
+                const F3 bc = scatter_bsdfcos(S, sr, m, h, ray.d, ls.dir);
+                if (!(sp <= 0.0f || !isfinite(sp) || maxc(bc) <= 0.0f)) {
+                    const float mis = power_heuristic(ls.pdf, sp);
+                    F3 c = (bc * ls.emitted) * (mis / (ls.pdf * prob));
+                    if (cbg) c = clamp_bg_miss(S, c);
+                    pend1 = clamp_ray_color(thr * c);
+                    out.sh[1] = true;
+                    out.sh_o[1] = h.p;
+                    out.sh_d[1] = ls.dir;
+                    out.sh_t[1] = kInf;
+                }
+            }
+        }
+        const F3 dir = scatter_generate(sr, k);
+        if (!leaves_opaque(m, h, dir)) goto done;
+        const float pdf = scatter_pdf(S, sr, m, h, ray.d, dir);
+        if (pdf <= 0.0f || !isfinite(pdf)) goto done;
+        thr = clamp_ray_color(thr * att);
+        if (terminated(thr) || !russian_roulette(thr, bounce, k)) goto done;
+        out.cont = true;
+        out.next_o = h.p;
+        out.next_d = dir;
+        const bool svil = ((S.k.sky == 3) && S.k.env.lighting) || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
+        flags = svil ? PF_PREV_SVIL : 0u;
+        P.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
+        P.prev_o[p] = make_float4(h.p.x, h.p.y, h.p.z, 0.f);
+    }
+done:
+    if (bounce >= w.max_bounces) out.cont = false;
+    P.rad[p] = make_float4(rad.x, rad.y, rad.z, __uint_as_float(flags));
+    P.pend0[p] = make_float4(pend0.x, pend0.y, pend0.z, 0.f);
+    P.pend1[p] = make_float4(pend1.x, pend1.y, pend1.z, 0.f);
+    if (out.cont) {
+        P.ray_o[p] = make_float4(out.next_o.x, out.next_o.y, out.next_o.z, __int_as_float(out.xobj));
+        P.ray_d[p] = make_float4(out.next_d.x, out.next_d.y, out.next_d.z, __int_as_float(out.xprim));
+    }
+}
+
+// ---------------------------------------------------------------------------- film
+
+__device__ __forceinline__ F3 clean(F3 c)   // cleanColor (Threads.cpp:122-137)
+{
+    return F3{isfinite(c.x) ? c.x : 0.f, isfinite(c.y) ? c.y : 0.f, isfinite(c.z) ? c.z : 0.f};
+}
+
+}  // namespace luz

@@ -1,0 +1,342 @@
+"""ctypes mirror of include/luz_gpu.h and a builder for LuzSceneDesc.
+
+The builder plays the role of the C++ host-side packer a Luz maintainer adds to
+Renderer::render: it turns a scene made of the reference's
+object kinds (Rectangle, Sphere, Cube, Plane, Mesh, MeshInstance,
+ConstantVolume, DirectionalLight; src/core/Hittables/*) and materials
+(src/core/Materials/*) into the flat description both the GPU library and the
+reference oracle consume. Defaults follow the reference constructors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+ABI_VERSION = 1
+
+MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE = 1, 2, 3, 4
+MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
+
+OBJ_RECTANGLE, OBJ_SPHERE, OBJ_CUBE, OBJ_PLANE = 1, 2, 3, 4
+OBJ_MESH, OBJ_MESH_INSTANCE, OBJ_VOLUME, OBJ_DIRECTIONAL_LIGHT = 5, 6, 7, 8
+
+SKY_NONE, SKY_ENVIRONMENT = 0, 3
+
+D3 = C.c_double * 3
+D12 = C.c_double * 12
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("texture", C.c_int32),
+        ("color", D3), ("roughness", C.c_double), ("ior", C.c_double), ("anisotropy", C.c_double),
+        ("conductor", C.c_int32), ("subsurface_method", C.c_int32),
+        ("eta", D3), ("k", D3), ("absorption", D3),
+        ("metallic", C.c_double), ("transmission", C.c_double), ("clearcoat", C.c_double),
+        ("clearcoat_roughness", C.c_double), ("sheen", C.c_double), ("subsurface", C.c_double),
+        ("subsurface_radius", D3), ("subsurface_scale", C.c_double), ("subsurface_color", D3),
+    ]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("rgb", C.POINTER(C.c_double))]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("triangle_count", C.c_int64), ("positions", C.POINTER(C.c_double)),
+        ("normals", C.POINTER(C.c_double)), ("uvs", C.POINTER(C.c_double)),
+        ("material", C.c_int32), ("_pad", C.c_int32),
+    ]
+
+
+class ObjectDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("material", C.c_int32), ("mesh", C.c_int32), ("boundary_kind", C.c_int32),
+        ("position", D3), ("orientation", D3), ("size", D3), ("width_axis", D3), ("height_axis", D3),
+        ("has_axes", C.c_int32), ("visible", C.c_int32),
+        ("rotation_degrees", D3), ("scale", D3), ("density", C.c_double),
+        ("has_uvs", C.c_int32), ("_pad", C.c_int32), ("uv", D12),
+    ]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [
+        ("position", D3), ("direction", D3), ("up", D3),
+        ("focal_length_m", C.c_double), ("sensor_width_m", C.c_double), ("sensor_height_m", C.c_double),
+        ("f_number", C.c_double), ("focus_distance_m", C.c_double),
+        ("pinhole", C.c_int32), ("_pad", C.c_int32),
+    ]
+
+
+class EnvironmentDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("rgb", C.POINTER(C.c_double)),
+        ("strength", C.c_double), ("rotation_degrees", C.c_double),
+        ("lighting", C.c_int32), ("_pad", C.c_int32),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("material_count", C.c_int32), ("materials", C.POINTER(MaterialDesc)),
+        ("texture_count", C.c_int32), ("mesh_count", C.c_int32),
+        ("textures", C.POINTER(TextureDesc)), ("meshes", C.POINTER(MeshDesc)),
+        ("object_count", C.c_int32), ("sky", C.c_int32), ("objects", C.POINTER(ObjectDesc)),
+        ("camera", CameraDesc), ("environment", EnvironmentDesc),
+        ("background", D3), ("meters_per_unit", C.c_double),
+    ]
+
+
+RENDER_PROFILE = 0x100
+RENDER_COUNT = 0x200
+
+
+class RenderParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_bounces", C.c_int32),
+        ("seed", C.c_uint32), ("stream", C.c_uint32), ("sample_offset", C.c_int32), ("flags", C.c_int32),
+    ]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [
+        ("render_ms", C.c_double), ("samples", C.c_double), ("extension_rays", C.c_double),
+        ("shadow_rays", C.c_double), ("kernel_launches", C.c_int64), ("waves", C.c_int64),
+        ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double),
+        ("extend_launches", C.c_int64), ("shadow_launches", C.c_int64),
+        ("ext_nodes", C.c_double), ("ext_tris", C.c_double), ("ext_top", C.c_double),
+        ("sh_nodes", C.c_double), ("sh_tris", C.c_double), ("sh_top", C.c_double),
+    ]
+
+
+class Hit(C.Structure):
+    _fields_ = [("t", C.c_float), ("object", C.c_int32), ("primitive", C.c_int32), ("u", C.c_float), ("v", C.c_float)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [
+        ("top_nodes", C.c_int64), ("top_leaf_objects", C.c_int64), ("mesh_nodes", C.c_int64),
+        ("mesh_triangles", C.c_int64), ("device_bytes", C.c_int64),
+        ("max_mesh_depth", C.c_int32), ("light_count", C.c_int32),
+    ]
+
+
+class MeshNode64(C.Structure):
+    _fields_ = [
+        ("bmin", D3), ("bmax", D3), ("left", C.c_int64), ("right", C.c_int64),
+        ("start", C.c_int64), ("count", C.c_int64), ("is_leaf", C.c_int32), ("_pad", C.c_int32),
+    ]
+
+
+HIT_DTYPE = np.dtype([("t", "<f4"), ("object", "<i4"), ("primitive", "<i4"), ("u", "<f4"), ("v", "<f4")])
+NODE64_DTYPE = np.dtype([("bmin", "<f8", 3), ("bmax", "<f8", 3), ("left", "<i8"), ("right", "<i8"),
+                         ("start", "<i8"), ("count", "<i8"), ("is_leaf", "<i4"), ("_pad", "<i4")])
+
+
+def _d3(v):
+    return D3(*[float(x) for x in v])
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class Camera:
+    """Camera (src/core/Camera.cpp). Defaults: 50 mm lens, 36 x 20.25 mm sensor, f/8, 10 m focus."""
+    position: tuple = (0.0, 0.0, 15.0)
+    direction: tuple = (0.0, 0.0, -1.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    focal_length_m: float = 0.050
+    sensor_width_m: float = 0.036
+    sensor_height_m: float = 0.02025
+    f_number: float = 8.0
+    focus_distance_m: float = 10.0
+    pinhole: bool = False
+
+
+@dataclass
+class Scene:
+    """Flat scene: materials, textures, meshes and objects in Scene::addHittable order."""
+    materials: List[dict] = field(default_factory=list)
+    textures: List[np.ndarray] = field(default_factory=list)
+    meshes: List[dict] = field(default_factory=list)
+    objects: List[dict] = field(default_factory=list)
+    camera: Camera = field(default_factory=Camera)
+    background: tuple = (0.0, 0.0, 0.0)
+    sky: int = SKY_NONE
+    environment: Optional[np.ndarray] = None      # (H, W, 3) float64
+    environment_strength: float = 1.0
+    environment_rotation: float = 0.0
+    environment_lighting: bool = True
+    meters_per_unit: float = 1.0
+
+    # -- materials (defaults = reference constructors) --------------------------
+    def _mat(self, **kw) -> int:
+        m = dict(type=MAT_LAMBERTIAN, texture=-1, color=(0.6, 0.6, 0.6), roughness=0.0, ior=1.52,
+                 anisotropy=0.0, conductor=0, subsurface_method=0, eta=(1.0, 1.0, 1.0), k=(0.0, 0.0, 0.0),
+                 absorption=(0.0, 0.0, 0.0), metallic=0.0, transmission=0.0, clearcoat=0.0,
+                 clearcoat_roughness=0.03, sheen=0.0, subsurface=0.0, subsurface_radius=(1.0, 1.0, 1.0),
+                 subsurface_scale=0.001, subsurface_color=(1.0, 1.0, 1.0))
+        m.update(kw)
+        self.materials.append(m)
+        return len(self.materials) - 1
+
+    def lambertian(self, color, texture=-1):
+        return self._mat(type=MAT_LAMBERTIAN, color=color, texture=texture)
+
+    def metal(self, color=(0.6, 0.6, 0.6), roughness=0.0, eta=None, k=None):
+        if eta is not None:
+            return self._mat(type=MAT_METAL, color=(1.0, 1.0, 1.0), roughness=roughness, conductor=1, eta=eta, k=k)
+        return self._mat(type=MAT_METAL, color=color, roughness=roughness)
+
+    def dielectric(self, color=(1.0, 1.0, 1.0), ior=1.52, roughness=0.0, absorption=(0.0, 0.0, 0.0)):
+        return self._mat(type=MAT_DIELECTRIC, color=color, ior=ior, roughness=roughness, absorption=absorption)
+
+    def emissive(self, radiance):
+        return self._mat(type=MAT_EMISSIVE, color=radiance)
+
+    def isotropic(self, color):
+        return self._mat(type=MAT_ISOTROPIC, color=color)
+
+    def henyey_greenstein(self, color, g):
+        return self._mat(type=MAT_HENYEY_GREENSTEIN, color=color, anisotropy=g)
+
+    def principled(self, color, metallic=0.0, roughness=0.5, transmission=0.0, ior=1.52, clearcoat=0.0,
+                   clearcoat_roughness=0.03, sheen=0.0, **kw):
+        return self._mat(type=MAT_PRINCIPLED, color=color, metallic=metallic, roughness=roughness,
+                         transmission=transmission, ior=ior, clearcoat=clearcoat,
+                         clearcoat_roughness=clearcoat_roughness, sheen=sheen, **kw)
+
+    def texture(self, rgb: np.ndarray) -> int:
+        self.textures.append(np.ascontiguousarray(rgb, dtype=np.float64))
+        return len(self.textures) - 1
+
+    # -- geometry ----------------------------------------------------------------
+    def _obj(self, **kw) -> int:
+        o = dict(kind=0, material=-1, mesh=-1, boundary_kind=0, position=(0, 0, 0), orientation=(0, 0, 1),
+                 size=(1, 1, 1), width_axis=(1, 0, 0), height_axis=(0, 1, 0), has_axes=0, visible=1,
+                 rotation_degrees=(0, 0, 0), scale=(1, 1, 1), density=1.42, has_uvs=0, uv=(0,) * 12)
+        o.update(kw)
+        self.objects.append(o)
+        return len(self.objects) - 1
+
+    def rectangle(self, position, normal, width, height, material, width_axis=None, height_axis=None):
+        kw = {}
+        if width_axis is not None:
+            kw = dict(has_axes=1, width_axis=width_axis, height_axis=height_axis)
+        return self._obj(kind=OBJ_RECTANGLE, position=position, orientation=normal, size=(width, height, 0),
+                         material=material, **kw)
+
+    def sphere(self, center, radius, material, visible=True):
+        return self._obj(kind=OBJ_SPHERE, position=center, size=(radius, 0, 0), material=material,
+                         visible=1 if visible else 0)
+
+    def cube(self, center, w, h, d, material):
+        return self._obj(kind=OBJ_CUBE, position=center, size=(w, h, d), material=material)
+
+    def plane(self, y, normal, material):
+        return self._obj(kind=OBJ_PLANE, position=(0, y, 0), orientation=normal, material=material)
+
+    def mesh(self, positions: np.ndarray, material: int, normals=None, uvs=None, add_object=True):
+        """Adds a triangle soup (N, 3, 3); returns (mesh index, object index or -1)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 9)
+        m = dict(positions=pos, material=material,
+                 normals=None if normals is None else np.ascontiguousarray(normals, dtype=np.float64).reshape(-1, 9),
+                 uvs=None if uvs is None else np.ascontiguousarray(uvs, dtype=np.float64).reshape(-1, 6))
+        self.meshes.append(m)
+        mi = len(self.meshes) - 1
+        oi = self._obj(kind=OBJ_MESH, mesh=mi, material=material) if add_object else -1
+        return mi, oi
+
+    def mesh_instance(self, mesh: int, position, rotation_degrees, scale, material):
+        return self._obj(kind=OBJ_MESH_INSTANCE, mesh=mesh, position=position, rotation_degrees=rotation_degrees,
+                         scale=scale, material=material)
+
+    def volume_cube(self, center, w, h, d, phase_material, density):
+        return self._obj(kind=OBJ_VOLUME, boundary_kind=OBJ_CUBE, position=center, size=(w, h, d),
+                         material=phase_material, density=density)
+
+    def volume_sphere(self, center, radius, phase_material, density):
+        return self._obj(kind=OBJ_VOLUME, boundary_kind=OBJ_SPHERE, position=center, size=(radius, 0, 0),
+                         material=phase_material, density=density)
+
+    def directional_light(self, direction, material):
+        return self._obj(kind=OBJ_DIRECTIONAL_LIGHT, orientation=direction, material=material)
+
+    def set_environment(self, rgb: np.ndarray, strength=1.0, rotation=0.0, lighting=True):
+        self.environment = np.ascontiguousarray(rgb, dtype=np.float64)
+        self.environment_strength = strength
+        self.environment_rotation = rotation
+        self.environment_lighting = lighting
+        self.sky = SKY_ENVIRONMENT
+
+    # -- C description -------------------------------------------------------
+    def build(self) -> "BuiltDesc":
+        return BuiltDesc(self)
+
+
+class BuiltDesc:
+    """Owns the ctypes arrays behind one LuzSceneDesc (keep it alive while in use)."""
+
+    def __init__(self, s: Scene):
+        self._keep = []
+        mats = (MaterialDesc * max(1, len(s.materials)))()
+        for i, m in enumerate(s.materials):
+            md = mats[i]
+            for k, v in m.items():
+                setattr(md, k, _d3(v) if isinstance(v, (tuple, list)) else v)
+        texs = (TextureDesc * max(1, len(s.textures)))()
+        for i, t in enumerate(s.textures):
+            t = np.ascontiguousarray(t, dtype=np.float64)
+            self._keep.append(t)
+            texs[i].height, texs[i].width = t.shape[0], t.shape[1]
+            texs[i].rgb = _dptr(t)
+        meshes = (MeshDesc * max(1, len(s.meshes)))()
+        for i, m in enumerate(s.meshes):
+            meshes[i].triangle_count = m["positions"].shape[0]
+            meshes[i].positions = _dptr(m["positions"])
+            self._keep.append(m["positions"])
+            if m["normals"] is not None:
+                meshes[i].normals = _dptr(m["normals"])
+                self._keep.append(m["normals"])
+            if m["uvs"] is not None:
+                meshes[i].uvs = _dptr(m["uvs"])
+                self._keep.append(m["uvs"])
+            meshes[i].material = m["material"]
+        objs = (ObjectDesc * max(1, len(s.objects)))()
+        for i, o in enumerate(s.objects):
+            od = objs[i]
+            for k, v in o.items():
+                if k == "uv":
+                    od.uv = D12(*[float(x) for x in v])
+                else:
+                    setattr(od, k, _d3(v) if isinstance(v, (tuple, list, np.ndarray)) else v)
+        d = SceneDesc()
+        d.abi_version = ABI_VERSION
+        d.material_count, d.materials = len(s.materials), mats
+        d.texture_count, d.textures = len(s.textures), texs
+        d.mesh_count, d.meshes = len(s.meshes), meshes
+        d.object_count, d.objects = len(s.objects), objs
+        cam = s.camera
+        d.camera = CameraDesc(_d3(cam.position), _d3(cam.direction), _d3(cam.up), cam.focal_length_m,
+                              cam.sensor_width_m, cam.sensor_height_m, cam.f_number, cam.focus_distance_m,
+                              1 if cam.pinhole else 0, 0)
+        if s.environment is not None:
+            env = np.ascontiguousarray(s.environment, dtype=np.float64)
+            self._keep.append(env)
+            d.environment = EnvironmentDesc(env.shape[1], env.shape[0], _dptr(env), s.environment_strength,
+                                            s.environment_rotation, 1 if s.environment_lighting else 0, 0)
+        d.background = _d3(s.background)
+        d.sky = s.sky
+        d.meters_per_unit = s.meters_per_unit
+        self._keep += [mats, texs, meshes, objs]
+        self.desc = d
+        self.scene = s
+
+    def ptr(self):
+        return C.byref(self.desc)

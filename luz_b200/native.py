@@ -1,0 +1,190 @@
+"""ctypes binding of luz_b200/libluz_b200.so (include/luz_gpu.h).
+
+The shared library is the product: the CUDA integrator and its host packer.
+There is no fallback path: if the library is missing or the GPU call fails the
+call raises, exactly as the reference's renderer throws std::runtime_error
+(src/cli/main.cpp:209-213).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import desc as D
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libluz_b200.so")
+
+EXPORTED = [
+    "luz_gpu_last_error", "luz_gpu_device_count", "luz_pack_create", "luz_pack_destroy", "luz_pack_info",
+    "luz_pack_mesh_bvh", "luz_pack_array", "luz_gpu_scene_create", "luz_gpu_scene_destroy", "luz_gpu_scene_info",
+    "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
+]
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
+          -5: "device error"}
+
+
+class LuzError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{message} [{STATUS.get(code, code)}]")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"luz_b200 native library not built: {LIB_PATH} (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    L.luz_gpu_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.luz_gpu_device_count.argtypes = [C.POINTER(i32)]
+    L.luz_pack_create.argtypes = [vp, C.POINTER(vp)]
+    L.luz_pack_destroy.argtypes = [vp]
+    L.luz_pack_info.argtypes = [vp, C.POINTER(D.SceneInfo)]
+    L.luz_pack_mesh_bvh.argtypes = [vp, i32, vp, i64, C.POINTER(i64), vp, i64]
+    L.luz_pack_array.argtypes = [vp, C.c_char_p, C.POINTER(vp), C.POINTER(i64)]
+    L.luz_gpu_scene_create.argtypes = [vp, i32, C.POINTER(vp)]
+    L.luz_gpu_scene_destroy.argtypes = [vp]
+    L.luz_gpu_scene_info.argtypes = [vp, C.POINTER(D.SceneInfo)]
+    L.luz_gpu_render.argtypes = [vp, C.POINTER(D.RenderParams), vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_render_device.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_trace_paths.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, vp, i64, vp]
+    L.luz_gpu_trace_rays.argtypes = [vp, vp, i64, i32, C.c_uint32, vp, vp]
+    for name in EXPORTED:
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        buf = C.create_string_buffer(1024)
+        lib().luz_gpu_last_error(buf, 1024)
+        raise LuzError(rc, buf.value.decode(errors="replace"))
+
+
+def device_count() -> int:
+    n = C.c_int32(0)
+    _check(lib().luz_gpu_device_count(C.byref(n)))
+    return n.value
+
+
+def params(width, height, spp, max_bounces, seed, stream=0, sample_offset=0) -> D.RenderParams:
+    return D.RenderParams(int(width), int(height), int(spp), int(max_bounces), int(seed) & 0xFFFFFFFF,
+                          int(stream), int(sample_offset), 0)
+
+
+class Pack:
+    """Host-side packed scene (no GPU): BVH layouts and device arrays."""
+
+    def __init__(self, built: D.BuiltDesc):
+        self.built = built
+        self.h = C.c_void_p()
+        _check(lib().luz_pack_create(C.cast(built.ptr(), C.c_void_p), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().luz_pack_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> D.SceneInfo:
+        i = D.SceneInfo()
+        _check(lib().luz_pack_info(self.h, C.byref(i)))
+        return i
+
+    def mesh_bvh(self, mesh: int):
+        cnt = C.c_int64()
+        _check(lib().luz_pack_mesh_bvh(self.h, mesh, None, 0, C.byref(cnt), None, 0))
+        nodes = np.zeros(max(1, cnt.value), D.NODE64_DTYPE)
+        ntri = self.built.scene.meshes[mesh]["positions"].shape[0]
+        order = np.zeros(max(1, ntri), np.int64)
+        _check(lib().luz_pack_mesh_bvh(self.h, mesh, nodes.ctypes.data, nodes.shape[0], C.byref(cnt),
+                                       order.ctypes.data, order.shape[0]))
+        return nodes[:cnt.value], order
+
+    def array(self, name: str) -> np.ndarray:
+        p = C.c_void_p()
+        n = C.c_int64()
+        _check(lib().luz_pack_array(self.h, name.encode(), C.byref(p), C.byref(n)))
+        if n.value == 0:
+            return np.zeros(0, np.uint8)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(n.value,)).copy()
+
+
+class GpuScene:
+    """Device scene arena (luz_gpu_scene). One host thread per handle."""
+
+    def __init__(self, built: D.BuiltDesc, device: int = 0):
+        self.built = built
+        self.h = C.c_void_p()
+        _check(lib().luz_gpu_scene_create(C.cast(built.ptr(), C.c_void_p), device, C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().luz_gpu_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> D.SceneInfo:
+        i = D.SceneInfo()
+        _check(lib().luz_gpu_scene_info(self.h, C.byref(i)))
+        return i
+
+    def render(self, p: D.RenderParams) -> Tuple[np.ndarray, D.RenderStats]:
+        out = np.zeros((p.height, p.width, 3), np.float32)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_render(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
+        return out, st
+
+    def render_device(self, p: D.RenderParams, out_ptr: int, stream: int = 0) -> D.RenderStats:
+        st = D.RenderStats()
+        _check(lib().luz_gpu_render_device(self.h, C.byref(p), C.c_void_p(out_ptr), C.c_void_p(stream), C.byref(st)))
+        return st
+
+    def trace_paths(self, p: D.RenderParams, x, y, s) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.int32)
+        y = np.ascontiguousarray(y, np.int32)
+        s = np.ascontiguousarray(s, np.int32)
+        out = np.zeros((x.shape[0], 3), np.float32)
+        _check(lib().luz_gpu_trace_paths(self.h, C.byref(p), x.ctypes.data, y.ctypes.data, s.ctypes.data,
+                                         x.shape[0], out.ctypes.data))
+        return out
+
+    def trace_rays(self, rays: np.ndarray, any_hit=False, seed=0, volume_key: Optional[np.ndarray] = None):
+        rays = np.ascontiguousarray(rays, np.float32)
+        out = np.zeros(rays.shape[0], D.HIT_DTYPE)
+        vk = None if volume_key is None else np.ascontiguousarray(volume_key, np.int32)
+        _check(lib().luz_gpu_trace_rays(self.h, rays.ctypes.data, rays.shape[0], 1 if any_hit else 0, seed,
+                                        None if vk is None else vk.ctypes.data, out.ctypes.data))
+        return out
+
+
+def render(scene: D.Scene, width: int, height: int, spp: int, max_bounces: int, seed: int, device: int = 0,
+           stream: int = 0):
+    """Renderer::render (src/renderer/Renderer.cpp:10) for the sample loop: returns the
+    W x H x 3 film of per-pixel means and the render stats."""
+    g = GpuScene(scene.build(), device)
+    try:
+        return g.render(params(width, height, spp, max_bounces, seed, stream))
+    finally:
+        g.close()

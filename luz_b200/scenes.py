@@ -1,0 +1,278 @@
+"""Seeded synthetic scenes with the shapes of the five benchmark configurations.
+
+No dataset or asset is read: every scene is generated from a seed, with the
+sizes and value distributions of the workload it stands for. The same
+description feeds the GPU integrator and the reference oracle.
+
+  cornell()              300x300, 50 spp, depth 8: five 555 walls, 130x105 light,
+                         two rotated boxes as instanced 12-triangle meshes.
+  mesh_glossy()          1920x1080, 64 spp, depth 12: level-8 icosphere (1,310,720
+                         triangles) displaced by 4-octave value noise (amplitude
+                         0.1) over a ground quad; rough dielectric + GGX metal;
+                         1024x512 equirect sky with a 0.5 degree sun lobe; f/2.8.
+  instancing_volumes()   1280x720, 32 spp, depth 16: 1e5 instances of a 200-triangle
+                         mesh, uniform random rotations, log-normal scales (sigma
+                         0.3) in a 100^3 box filled with an HG medium (g 0.6,
+                         sigma_t 0.05, albedo 0.8), two sphere lights and a
+                         directional light.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .desc import Camera, Scene
+
+
+@dataclass
+class Workload:
+    name: str
+    scene: Scene
+    width: int
+    height: int
+    spp: int
+    max_bounces: int
+    seed: int = 424242424
+
+
+# ----------------------------------------------------------------------------- meshes
+
+def box_mesh() -> np.ndarray:
+    """Unit cube [0,1]^3 as 12 outward-wound triangles, shape (12, 3, 3)."""
+    c = np.array([[x, y, z] for z in (0, 1) for y in (0, 1) for x in (0, 1)], np.float64)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    tris = []
+    for a, b, cc, d in quads:
+        tris.append([c[a], c[b], c[cc]])
+        tris.append([c[a], c[cc], c[d]])
+    return np.array(tris, np.float64)
+
+
+def icosphere(level: int):
+    """Subdivided icosahedron on the unit sphere: (vertices (V,3), faces (F,3))."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        uniq, inv = np.unique(e, axis=0, return_inverse=True)
+        mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = v.shape[0]
+        v = np.concatenate([v, mid])
+        nf = f.shape[0]
+        m01, m12, m20 = (inv[:nf] + base, inv[nf:2 * nf] + base, inv[2 * nf:] + base)
+        f = np.concatenate([np.stack([f[:, 0], m01, m20], 1), np.stack([f[:, 1], m12, m01], 1),
+                            np.stack([f[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    return v, f
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 4) -> np.ndarray:
+    """Seeded 3-D value noise (smoothstep-trilinear over a hashed lattice), in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-1.0, 1.0, 4096)
+    perm = rng.permutation(4096)
+
+    def lattice(ix, iy, iz):
+        h = perm[(ix * 73856093 ^ iy * 19349663 ^ iz * 83492791) & 4095]
+        return table[h]
+
+    out = np.zeros(p.shape[0])
+    amp, freq, norm = 1.0, 2.0, 0.0
+    for _ in range(octaves):
+        q = p * freq
+        i = np.floor(q).astype(np.int64)
+        fr = q - i
+        w = fr * fr * (3.0 - 2.0 * fr)
+        acc = 0.0
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    wx = w[:, 0] if dx else 1 - w[:, 0]
+                    wy = w[:, 1] if dy else 1 - w[:, 1]
+                    wz = w[:, 2] if dz else 1 - w[:, 2]
+                    acc = acc + wx * wy * wz * lattice(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)
+        out += amp * acc
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return out / norm
+
+
+def torus_mesh(segments: int = 10, rings: int = 10, major: float = 1.0, minor: float = 0.35) -> np.ndarray:
+    """segments*rings*2 triangles (200 at the defaults)."""
+    u = np.linspace(0, 2 * np.pi, segments, endpoint=False)
+    w = np.linspace(0, 2 * np.pi, rings, endpoint=False)
+    U, W = np.meshgrid(u, w, indexing="ij")
+    P = np.stack([(major + minor * np.cos(W)) * np.cos(U), minor * np.sin(W), (major + minor * np.cos(W)) * np.sin(U)], -1)
+    tris = []
+    for a in range(segments):
+        for b in range(rings):
+            a1, b1 = (a + 1) % segments, (b + 1) % rings
+            tris.append([P[a, b], P[a1, b], P[a1, b1]])
+            tris.append([P[a, b], P[a1, b1], P[a, b1]])
+    return np.array(tris, np.float64)
+
+
+# ----------------------------------------------------------------------------- scenes
+
+def _pinhole(position, look_at, vfov_deg, aspect):
+    d = np.asarray(look_at, float) - np.asarray(position, float)
+    f = 0.050
+    sh = 2.0 * math.tan(math.radians(vfov_deg) / 2.0) * f
+    return Camera(position=tuple(position), direction=tuple(d), up=(0.0, 1.0, 0.0), focal_length_m=f,
+                  sensor_width_m=sh * aspect, sensor_height_m=sh, f_number=8.0, focus_distance_m=10.0, pinhole=True)
+
+
+def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int = 8) -> Workload:
+    s = Scene()
+    white = s.lambertian((0.73, 0.73, 0.73))
+    red = s.lambertian((0.65, 0.05, 0.05))
+    green = s.lambertian((0.12, 0.45, 0.15))
+    light = s.emissive((15.0, 15.0, 15.0))
+    s.rectangle((555.0, 277.5, 277.5), (1, 0, 0), 555.0, 555.0, red)       # image left
+    s.rectangle((0.0, 277.5, 277.5), (-1, 0, 0), 555.0, 555.0, green)      # image right
+    s.rectangle((277.5, 0.0, 277.5), (0, 1, 0), 555.0, 555.0, white)       # floor
+    s.rectangle((277.5, 555.0, 277.5), (0, -1, 0), 555.0, 555.0, white)    # ceiling
+    s.rectangle((277.5, 277.5, 555.0), (0, 0, -1), 555.0, 555.0, white)    # back
+    s.rectangle((278.0, 554.0, 279.5), (0, -1, 0), 130.0, 105.0, light)
+    cube, _ = s.mesh(box_mesh(), white, add_object=False)
+    s.mesh_instance(cube, (265.0, 0.0, 295.0), (0.0, 15.0, 0.0), (165.0, 330.0, 165.0), white)
+    s.mesh_instance(cube, (130.0, 0.0, 65.0), (0.0, -18.0, 0.0), (165.0, 165.0, 165.0), white)
+    s.camera = _pinhole((278.0, 278.0, -800.0), (278.0, 278.0, 0.0), 40.0, width / height)
+    s.background = (0.0, 0.0, 0.0)
+    return Workload("cornell", s, width, height, spp, max_bounces)
+
+
+def sky_environment(width: int = 1024, height: int = 512, seed: int = 7, sun_peak: float = 5.0e4,
+                    sun_diameter_deg: float = 0.5):
+    """Equirect RGB sky: zenith-to-horizon gradient, dark ground, seeded sun lobe.
+
+    Texel (x, y) maps to direction through EnvironmentMap::uvToDirection
+    (src/core/EnvironmentMap.cpp:616-623): u = (x+0.5)/W, v = 1-(y+0.5)/H.
+    """
+    rng = np.random.default_rng(seed)
+    u = (np.arange(width) + 0.5) / width
+    v = 1.0 - (np.arange(height) + 0.5) / height
+    phi = (u - 0.5) * 2.0 * np.pi
+    yy = np.sin((v - 0.5) * np.pi)
+    r = np.sqrt(np.maximum(0.0, 1.0 - yy * yy))
+    D = np.stack([np.outer(r, np.cos(phi)), np.repeat(yy[:, None], width, 1), np.outer(r, np.sin(phi))], -1)
+    up = np.clip(D[..., 1], 0.0, 1.0)[..., None]
+    zenith = np.array([0.25, 0.45, 0.95])
+    horizon = np.array([0.95, 0.95, 1.0])
+    ground = np.array([0.18, 0.16, 0.14])
+    sky = horizon * (1 - up) + zenith * up
+    img = np.where(D[..., 1:2] >= 0.0, sky, ground)
+    elev = math.radians(rng.uniform(20.0, 50.0))
+    azim = rng.uniform(0.0, 2.0 * math.pi)
+    sun = np.array([math.cos(elev) * math.cos(azim), math.sin(elev), math.cos(elev) * math.sin(azim)])
+    ang = np.degrees(np.arccos(np.clip(D @ sun, -1.0, 1.0)))
+    lobe = np.exp(-0.5 * (ang / (sun_diameter_deg / 2.0)) ** 2)
+    img = img + sun_peak * lobe[..., None] * np.array([1.0, 0.95, 0.85])
+    return np.ascontiguousarray(img), sun
+
+
+def mesh_glossy(width: int = 1920, height: int = 1080, spp: int = 64, max_bounces: int = 12,
+                level: int = 8, seed: int = 11) -> Workload:
+    s = Scene()
+    glass = s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.1)
+    metal = s.metal((0.85, 0.8, 0.75), roughness=0.3)
+    v, f = icosphere(level)
+    disp = 1.0 + 0.1 * value_noise(v, seed)
+    v = v * disp[:, None]
+    s.mesh(v[f], glass)
+    g = 12.0
+    y = -1.15
+    quad = np.array([[[-g, y, -g], [g, y, g], [g, y, -g]], [[-g, y, -g], [-g, y, g], [g, y, g]]], np.float64)
+    s.mesh(quad, metal)
+    env, _ = sky_environment(seed=seed + 1)
+    s.set_environment(env, strength=1.0)
+    s.camera = Camera(position=(0.0, 0.35, 4.2), direction=(0.0, -0.35 * 0.25, -4.2), up=(0.0, 1.0, 0.0),
+                      focal_length_m=0.050, sensor_width_m=0.036, sensor_height_m=0.02025, f_number=2.8,
+                      focus_distance_m=4.2)
+    return Workload("mesh_glossy", s, width, height, spp, max_bounces)
+
+
+def random_rotation_euler_xyz(rng, n):
+    """Uniform random rotations (Shoemake quaternions) as Euler angles in degrees for
+    MeshInstance's rotate(): R = Rz(z) Ry(y) Rx(x) (src/core/Hittables/MeshInstance.cpp:74-94)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], 1)
+    x, y, z, w = q.T
+    r20 = 2 * (x * z - w * y)
+    r21 = 2 * (y * z + w * x)
+    r22 = 1 - 2 * (x * x + y * y)
+    r10 = 2 * (x * y + w * z)
+    r00 = 1 - 2 * (y * y + z * z)
+    ay = np.arcsin(np.clip(-r20, -1, 1))
+    ax = np.arctan2(r21, r22)
+    az = np.arctan2(r10, r00)
+    return np.degrees(np.stack([ax, ay, az], 1))
+
+
+def instancing_volumes(width: int = 1280, height: int = 720, spp: int = 32, max_bounces: int = 16,
+                       count: int = 100_000, seed: int = 23) -> Workload:
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    palette = [s.lambertian(tuple(rng.uniform(0.2, 0.85, 3))) for _ in range(6)]
+    palette.append(s.metal((0.9, 0.85, 0.7), roughness=0.3))
+    palette.append(s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.1))
+    tor, _ = s.mesh(torus_mesh(), palette[0], add_object=False)
+    pos = rng.uniform(-48.0, 48.0, (count, 3))
+    rot = random_rotation_euler_xyz(rng, count)
+    sc = np.exp(rng.normal(0.0, 0.3, count)) * 0.8
+    mat = rng.integers(0, len(palette), count)
+    for i in range(count):
+        sv = float(sc[i])
+        s.mesh_instance(tor, tuple(pos[i]), tuple(rot[i]), (sv, sv, sv), palette[int(mat[i])])
+    hg = s.henyey_greenstein((0.8, 0.8, 0.8), 0.6)
+    s.volume_cube((0.0, 0.0, 0.0), 100.0, 100.0, 100.0, hg, 0.05)
+    s.sphere((-20.0, 30.0, -10.0), 3.0, s.emissive((40.0, 36.0, 30.0)))
+    s.sphere((25.0, -10.0, 15.0), 2.0, s.emissive((20.0, 30.0, 45.0)))
+    s.directional_light((-0.3, -1.0, -0.2), s.emissive((2.0, 2.0, 2.0)))
+    s.camera = Camera(position=(0.0, 5.0, 49.0), direction=(0.0, -0.1, -1.0), up=(0.0, 1.0, 0.0),
+                      focal_length_m=0.035, sensor_width_m=0.036, sensor_height_m=0.02025, f_number=8.0,
+                      focus_distance_m=30.0, pinhole=True)
+    return Workload("instancing_volumes", s, width, height, spp, max_bounces)
+
+
+def tiny_mixed(width: int = 24, height: int = 18, spp: int = 4, max_bounces: int = 6) -> Workload:
+    """Small scene touching every object kind and material on the path (parity tests)."""
+    rng = np.random.default_rng(5)
+    s = Scene()
+    white = s.lambertian((0.73, 0.73, 0.73))
+    red = s.lambertian((0.65, 0.05, 0.05))
+    s.rectangle((0.0, -1.0, 0.0), (0, 1, 0), 8.0, 8.0, white)
+    s.rectangle((0.0, 1.0, -3.0), (0, 0, 1), 8.0, 4.0, red)
+    s.sphere((-1.2, -0.4, 0.0), 0.6, s.metal((0.9, 0.8, 0.6), roughness=0.25))
+    s.sphere((0.2, -0.5, 0.6), 0.5, s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.0))
+    s.sphere((1.4, -0.5, -0.4), 0.5, s.principled((0.3, 0.6, 0.8), metallic=0.2, roughness=0.35, clearcoat=0.5,
+                                                   sheen=0.3))
+    s.cube((-0.2, -0.6, -1.4), 0.7, 0.8, 0.7, s.dielectric((0.9, 1.0, 0.9), ior=1.45, roughness=0.2))
+    s.sphere((0.0, 2.2, 0.5), 0.35, s.emissive((12.0, 11.0, 9.0)))
+    s.rectangle((1.5, 1.8, 1.0), (0, -1, 0), 0.8, 0.5, s.emissive((6.0, 6.0, 8.0)))
+    tri = box_mesh() - 0.5
+    m, _ = s.mesh(tri * 0.4 + np.array([1.0, 0.2, 1.2]), s.metal((0.8, 0.8, 0.8), roughness=0.0))
+    s.mesh_instance(m, (-1.5, 0.2, 1.0), tuple(rng.uniform(-40, 40, 3)), (0.7, 1.2, 0.9), white)
+    s.volume_sphere((1.0, -0.3, 1.4), 0.45, s.henyey_greenstein((0.8, 0.8, 0.8), 0.5), 1.5)
+    s.directional_light((0.3, -1.0, -0.4), s.emissive((1.5, 1.4, 1.2)))
+    s.camera = _pinhole((0.0, 0.5, 5.0), (0.0, -0.2, 0.0), 50.0, width / height)
+    s.background = (0.05, 0.06, 0.08)
+    return Workload("tiny_mixed", s, width, height, spp, max_bounces)
+
+
+WORKLOADS = {
+    "cornell": cornell,
+    "mesh_glossy": mesh_glossy,
+    "instancing_volumes": instancing_volumes,
+    "tiny_mixed": tiny_mixed,
+}

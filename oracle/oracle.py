@@ -1,0 +1,161 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes access to the oracle libraries.
+
+  oracle/_ref/libluzref.so       the Luz reference itself (built by oracle/Makefile
+                                 from the reference sources, -O2, no fast-math)
+  oracle/_ref/libluzref_fast.so  same sources with release flags (timed CPU baseline)
+  oracle/_ref/librestate.so      oracle/restate.c, the FP32 C restatement of the
+                                 sampler and the BVH traversal
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
+module, as the checker. The product (luz_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def _path(name: str) -> str:
+    return os.path.join(REF_DIR, name)
+
+
+def reference_available(fast: bool = False) -> bool:
+    return os.path.exists(_path("libluzref_fast.so" if fast else "libluzref.so"))
+
+
+def restate_available() -> bool:
+    return os.path.exists(_path("librestate.so"))
+
+
+class RefOracle:
+    """The reference renderer behind the harness in oracle/ref_harness.cpp."""
+
+    def __init__(self, fast: bool = False):
+        self.lib = C.CDLL(_path("libluzref_fast.so" if fast else "libluzref.so"))
+        L = self.lib
+        vp = C.c_void_p
+        L.luzref_scene_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+        L.luzref_scene_destroy.argtypes = [vp]
+        L.luzref_trace_rays.argtypes = [vp, vp, C.c_int64, C.c_int32, C.c_uint32, vp, vp, vp, vp]
+        L.luzref_trace_paths.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp]
+        L.luzref_render.argtypes = [vp, vp, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.luzref_mesh_bvh.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int64), vp, C.c_int64]
+        L.luzref_mesh_triangle_count.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64)]
+        L.luzref_sampler.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, C.c_int32, vp]
+        L.luzref_last_error.argtypes = [C.c_char_p, C.c_size_t]
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.lib.luzref_last_error(buf, 512)
+            raise RuntimeError("reference oracle: " + buf.value.decode())
+
+    def scene(self, built, tag: bool = False) -> "RefScene":
+        h = C.c_void_p()
+        self._check(self.lib.luzref_scene_create(C.cast(built.ptr(), C.c_void_p), 1 if tag else 0, C.byref(h)))
+        return RefScene(self, h, built)
+
+    def sampler(self, seed, x, y, s, stream, bounce, dim, which=1):
+        out = np.zeros(2, np.float64)
+        self.lib.luzref_sampler(seed, x, y, s, stream, bounce, dim, which, out.ctypes.data)
+        return out[0] if which == 1 else (out[0], out[1])
+
+
+class RefScene:
+    def __init__(self, oracle: RefOracle, handle, built):
+        self.o, self.h, self.built = oracle, handle, built
+
+    def close(self):
+        if self.h:
+            self.o.lib.luzref_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace_rays(self, rays: np.ndarray, any_hit=False, seed=0, volume_key: Optional[np.ndarray] = None):
+        rays = np.ascontiguousarray(rays, dtype=np.float64)
+        n = rays.shape[0]
+        t = np.zeros(n, np.float64)
+        obj = np.zeros(n, np.int32)
+        prim = np.zeros(n, np.int32)
+        vk = None if volume_key is None else np.ascontiguousarray(volume_key, dtype=np.int32)
+        self.o._check(self.o.lib.luzref_trace_rays(self.h, rays.ctypes.data, n, 1 if any_hit else 0, seed,
+                                                   None if vk is None else vk.ctypes.data,
+                                                   t.ctypes.data, obj.ctypes.data, prim.ctypes.data))
+        return t, obj, prim
+
+    def trace_paths(self, params, x, y, s) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.int32)
+        y = np.ascontiguousarray(y, dtype=np.int32)
+        s = np.ascontiguousarray(s, dtype=np.int32)
+        out = np.zeros((x.shape[0], 3), np.float64)
+        self.o._check(self.o.lib.luzref_trace_paths(self.h, C.addressof(params), x.ctypes.data, y.ctypes.data,
+                                                    s.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def render(self, params, threads: int):
+        out = np.zeros((params.height, params.width, 3), np.float64)
+        ms = C.c_double()
+        ns = C.c_double()
+        self.o._check(self.o.lib.luzref_render(self.h, C.addressof(params), threads, out.ctypes.data,
+                                               C.byref(ms), C.byref(ns)))
+        return out, ms.value, ns.value
+
+    def mesh_bvh(self, mesh: int):
+        from luz_b200.desc import NODE64_DTYPE
+        nt = C.c_int64()
+        self.o._check(self.o.lib.luzref_mesh_triangle_count(self.h, mesh, C.byref(nt)))
+        cap = max(1, 2 * nt.value)
+        nodes = np.zeros(cap, NODE64_DTYPE)
+        order = np.zeros(max(1, nt.value), np.int64)
+        cnt = C.c_int64()
+        self.o._check(self.o.lib.luzref_mesh_bvh(self.h, mesh, nodes.ctypes.data, cap, C.byref(cnt),
+                                                 order.ctypes.data, order.shape[0]))
+        return nodes[:cnt.value], order[:nt.value]
+
+
+class Restate:
+    """oracle/restate.cpp: FP32 restatement of the sampler and the traversal."""
+
+    def __init__(self):
+        self.lib = C.CDLL(_path("librestate.so"))
+        vp = C.c_void_p
+        self.lib.restate_sample1d.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32,
+                                              C.c_uint32, vp]
+        self.lib.restate_sample2d.argtypes = self.lib.restate_sample1d.argtypes
+        self.lib.restate_trace.argtypes = [vp] * 9 + [vp, C.c_int64, C.c_int32, C.c_uint32, vp, vp]
+
+    def sample1d(self, seed, x, y, s, stream, bounce, dim):
+        out = np.zeros(1, np.float64)
+        self.lib.restate_sample1d(seed, x, y, s, stream, bounce, dim, out.ctypes.data)
+        return out[0]
+
+    def sample2d(self, seed, x, y, s, stream, bounce, dim):
+        out = np.zeros(2, np.float32)
+        self.lib.restate_sample2d(seed, x, y, s, stream, bounce, dim, out.ctypes.data)
+        return out
+
+    def trace(self, pack, rays: np.ndarray, any_hit=False, seed=0, volume_key=None):
+        """Traverses the packed arrays of a luz_b200.native.Pack on the CPU."""
+        from luz_b200.desc import HIT_DTYPE
+        names = ["top_nodes", "top_children", "objects", "mesh_nodes", "mesh_tris", "meshes", "rects", "index_pool",
+                 "consts"]
+        arrs = [np.ascontiguousarray(pack.array(n)) for n in names]
+        ptrs = [a.ctypes.data if a.size else None for a in arrs]
+        rays = np.ascontiguousarray(rays, np.float32)
+        out = np.zeros(rays.shape[0], HIT_DTYPE)
+        vk = None if volume_key is None else np.ascontiguousarray(volume_key, np.int32)
+        self.lib.restate_trace(*ptrs, rays.ctypes.data, rays.shape[0], 1 if any_hit else 0, seed,
+                               None if vk is None else vk.ctypes.data, out.ctypes.data)
+        return out

@@ -1,0 +1,524 @@
+/*
+ * ref_harness.cpp — TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * A C entry layer over the UNMODIFIED Luz reference renderer, compiled from its
+ * own sources by oracle/Makefile into oracle/_ref/libluzref*.so. Nothing in the
+ * product links or calls this file; tests, the golden-fixture script and the
+ * CPU-baseline leg of bench.py load it through ctypes as the checker.
+ *
+ * It builds a reference Scene from the same LuzSceneDesc the GPU library
+ * consumes (include/luz_gpu.h) using only the reference's public classes, then
+ * calls the reference's own code:
+ *   - closest / any hit:   the body of Renderer::internal::_checkHits
+ *                          (src/renderer/HitHelper.cpp:5-32) and isShadowOccluded
+ *                          (src/renderer/ColorHelper.cpp:801-829) with explicit
+ *                          t ranges, calling Hittable::hit / hitAny;
+ *   - per-path radiance:   Sampler::beginPixelSample + _calculatePixelColor
+ *                          (src/renderer/ColorHelper.cpp:1110-1115), the exact
+ *                          sequence of _threadRender (src/renderer/Threads.cpp:563-566);
+ *   - full render:         Renderer::render (src/renderer/Renderer.cpp:10) with
+ *                          denoise/adaptive off and the Raw view transform;
+ *   - mesh BVH layout:     Mesh::_packedBVHNodes / _triangleIndices, read with
+ *                          private access in this translation unit only.
+ * Hit identification: in "tag" mode every object (and every mesh triangle) gets
+ * its own Lambertian-derived material so the HitRecord's material pointer names
+ * the object and primitive; traversal does not depend on material values.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "Color.hpp"
+#include "Camera.hpp"
+#include "EnvironmentMap.hpp"
+#include "Texture.hpp"
+#include "Sampler.hpp"
+#include "Random.hpp"
+#include "Defaults.hpp"
+#include "Transform.hpp"
+#include "Materials/Lambertian.hpp"
+#include "Materials/Metal.hpp"
+#include "Materials/Dielectric.hpp"
+#include "Materials/Emissive.hpp"
+#include "Materials/Isotropic.hpp"
+#include "Materials/HenyeyGreenstein.hpp"
+#include "Materials/Principled.hpp"
+#include "Hittables/Rectangle.hpp"
+#include "Hittables/Sphere.hpp"
+#include "Hittables/Cube.hpp"
+#include "Hittables/Plane.hpp"
+#include "Hittables/ConstantVolume.hpp"
+#include "Hittables/DirectionalLight.hpp"
+#include "Hittables/Triangle.hpp"
+#define private public
+#include "Hittables/Mesh.hpp"
+#include "Hittables/MeshInstance.hpp"
+#undef private
+#include "Scene/Scene.hpp"
+#include "Renderer/Renderer.hpp"
+#include "RendererInternal.hpp"
+
+#include "luz_gpu.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+struct TagMaterial : public Lambertian {
+    int32_t object;
+    int32_t primitive;
+    TagMaterial(int32_t o, int32_t p) : Lambertian(Color(0.5, 0.5, 0.5)), object(o), primitive(p) {}
+};
+struct TagHG : public HenyeyGreenstein {
+    int32_t object;
+    TagHG(int32_t o, double g) : HenyeyGreenstein(Color(0.5, 0.5, 0.5), g), object(o) {}
+};
+
+struct RefScene {
+    Scene scene;
+    bool tagged = false;
+    std::vector<std::shared_ptr<Mesh>> meshes;
+    std::vector<std::shared_ptr<Hittable>> objects;           // by desc object index (nullptr if skipped)
+    std::vector<int32_t> mesh_object;                         // mesh index -> first MESH object
+    std::unordered_map<const Material*, std::pair<int32_t, int32_t>> tags;
+    std::vector<std::shared_ptr<Material>> keep;
+};
+
+Color col(const double* c) { return Color(c[0], c[1], c[2]); }
+Vector3 vec(const double* c) { return Vector3(c[0], c[1], c[2]); }
+
+std::shared_ptr<Material> make_material(const LuzMaterialDesc& m, const std::vector<std::shared_ptr<Texture>>& textures)
+{
+    std::shared_ptr<Material> out;
+    switch (m.type) {
+    case LUZ_MAT_LAMBERTIAN: out = std::make_shared<Lambertian>(col(m.color)); break;
+    case LUZ_MAT_METAL:
+        if (m.conductor) {
+            auto metal = std::make_shared<Metal>(col(m.eta), col(m.k), m.roughness);
+            out = metal;
+        } else {
+            out = std::make_shared<Metal>(col(m.color), m.roughness);
+        }
+        break;
+    case LUZ_MAT_DIELECTRIC: {
+        auto d = std::make_shared<Dielectric>(col(m.color), m.ior, m.roughness);
+        d->setAbsorptionCoefficient(col(m.absorption));
+        out = d;
+        break;
+    }
+    case LUZ_MAT_EMISSIVE: out = std::make_shared<Emissive>(col(m.color)); break;
+    case LUZ_MAT_ISOTROPIC: out = std::make_shared<Isotropic>(col(m.color)); break;
+    case LUZ_MAT_HENYEY_GREENSTEIN: out = std::make_shared<HenyeyGreenstein>(col(m.color), m.anisotropy); break;
+    case LUZ_MAT_PRINCIPLED: {
+        auto p = std::make_shared<Principled>(col(m.color), m.metallic, m.roughness, m.transmission, m.ior,
+                                              m.clearcoat, m.clearcoat_roughness, m.sheen);
+        p->setSubsurface(m.subsurface);
+        p->setSubsurfaceRadius(col(m.subsurface_radius));
+        p->setSubsurfaceScale(m.subsurface_scale);
+        p->setSubsurfaceColor(col(m.subsurface_color));
+        p->setSubsurfaceMethod(m.subsurface_method ? SUBSURFACE_THIN : SUBSURFACE_BURLEY);
+        p->setAbsorptionCoefficient(col(m.absorption));
+        out = p;
+        break;
+    }
+    default: throw std::invalid_argument("unknown material type");
+    }
+    if (m.texture >= 0) {
+        if (m.texture >= (int32_t)textures.size()) throw std::invalid_argument("texture index out of range");
+        out->setTexture(textures[m.texture]);
+    }
+    return out;
+}
+
+void configure(Scene& scene, const LuzSceneDesc& d, int32_t width, int32_t height)
+{
+    scene.getImage()->setWidth((std::size_t)width);
+    scene.getImage()->setHeight((std::size_t)height);
+    scene.getImage()->initialize();
+    scene.setViewTransform(ViewTransform::Raw);
+    scene.setExposure(0.0);
+    scene.setBloom(false);
+    scene.setDenoise(false);
+    scene.setAdaptiveSampling(false);
+    scene.setBenchmarkMode(true);
+    (void)d;
+}
+
+RefScene* build(const LuzSceneDesc* d, int tag)
+{
+    auto rs = std::make_unique<RefScene>();
+    rs->tagged = tag != 0;
+    Scene& scene = rs->scene;
+
+    std::vector<std::shared_ptr<Texture>> textures;
+    for (int i = 0; i < d->texture_count; i++) {
+        const LuzTextureDesc& t = d->textures[i];
+        std::vector<Color> px((std::size_t)t.width * t.height);
+        for (std::size_t k = 0; k < px.size(); k++) px[k] = Color(t.rgb[3 * k], t.rgb[3 * k + 1], t.rgb[3 * k + 2]);
+        textures.push_back(std::make_shared<Texture>((std::size_t)t.width, (std::size_t)t.height, std::move(px)));
+    }
+    std::vector<std::shared_ptr<Material>> mats;
+    for (int i = 0; i < d->material_count; i++) mats.push_back(make_material(d->materials[i], textures));
+
+    rs->mesh_object.assign(d->mesh_count, -1);
+    for (int i = 0; i < d->object_count; i++)
+        if (d->objects[i].kind == LUZ_OBJ_MESH && d->objects[i].mesh >= 0 && d->objects[i].mesh < d->mesh_count
+            && rs->mesh_object[d->objects[i].mesh] < 0)
+            rs->mesh_object[d->objects[i].mesh] = i;
+
+    for (int mi = 0; mi < d->mesh_count; mi++) {
+        const LuzMeshDesc& m = d->meshes[mi];
+        std::shared_ptr<Material> mm = mats.at(m.material);
+        std::vector<Triangle> tris;
+        tris.reserve((std::size_t)m.triangle_count);
+        for (int64_t t = 0; t < m.triangle_count; t++) {
+            const double* p = m.positions + 9 * t;
+            std::shared_ptr<Material> tm = mm;
+            if (m.normals) {
+                const double* n = m.normals + 9 * t;
+                tris.emplace_back(vec(p), vec(p + 3), vec(p + 6), vec(n), vec(n + 3), vec(n + 6), tm);
+            } else {
+                tris.emplace_back(vec(p), vec(p + 3), vec(p + 6), tm);
+            }
+            if (m.uvs) {
+                const double* uv = m.uvs + 6 * t;
+                tris.back().setTextureCoordinates(Vector3(uv[0], uv[1], 0), Vector3(uv[2], uv[3], 0), Vector3(uv[4], uv[5], 0));
+            }
+        }
+        auto mesh = std::make_shared<Mesh>(Vector3(), mm, std::move(tris));
+        if (tag) {
+            for (std::size_t t = 0; t < mesh->_triangles.size(); t++) {
+                auto tm = std::make_shared<TagMaterial>(rs->mesh_object[mi], (int32_t)t);
+                rs->tags[tm.get()] = {rs->mesh_object[mi], (int32_t)t};
+                mesh->_triangles[t].setMaterial(tm);
+                rs->keep.push_back(tm);
+            }
+        }
+        rs->meshes.push_back(mesh);
+    }
+
+    for (int i = 0; i < d->object_count; i++) {
+        const LuzObjectDesc& o = d->objects[i];
+        std::shared_ptr<Material> mat;
+        if (o.kind != LUZ_OBJ_MESH) {
+            if (tag && o.kind != LUZ_OBJ_VOLUME && o.kind != LUZ_OBJ_DIRECTIONAL_LIGHT) {
+                auto tm = std::make_shared<TagMaterial>(i, 0);
+                rs->tags[tm.get()] = {i, 0};
+                rs->keep.push_back(tm);
+                mat = tm;
+            } else if (tag && o.kind == LUZ_OBJ_VOLUME) {
+                auto tm = std::make_shared<TagHG>(i, mats.at(o.material)->getType() == HENYEY_GREENSTEIN
+                                                  ? std::static_pointer_cast<HenyeyGreenstein>(mats.at(o.material))->getAnisotropy()
+                                                  : 0.0);
+                rs->tags[tm.get()] = {i, 0};
+                rs->keep.push_back(tm);
+                mat = tm;
+            } else {
+                mat = mats.at(o.material);
+            }
+        }
+        std::shared_ptr<Hittable> h;
+        switch (o.kind) {
+        case LUZ_OBJ_RECTANGLE: {
+            auto r = std::make_shared<Rectangle>(Transform(vec(o.position), vec(o.orientation), Vector3(1, 1, 1)),
+                                                 o.size[0], o.size[1], mat);
+            if (o.has_axes) r->setAxes(vec(o.width_axis), vec(o.height_axis));
+            if (o.has_uvs) r->setTextureCoordinates(vec(o.uv), vec(o.uv + 3), vec(o.uv + 6), vec(o.uv + 9));
+            h = r;
+            break;
+        }
+        case LUZ_OBJ_SPHERE:
+            h = std::make_shared<Sphere>(vec(o.position), o.size[0], mat, o.visible != 0, SphereUVProjection::LatLong);
+            break;
+        case LUZ_OBJ_CUBE:
+            h = std::make_shared<Cube>(Transform(vec(o.position), Vector3(0, 0, 1), Vector3(1, 1, 1)),
+                                       o.size[0], o.size[1], o.size[2], mat);
+            break;
+        case LUZ_OBJ_PLANE:
+            h = std::make_shared<Plane>(o.position[1], vec(o.orientation), mat);
+            break;
+        case LUZ_OBJ_MESH:
+            h = rs->meshes.at(o.mesh);
+            break;
+        case LUZ_OBJ_MESH_INSTANCE:
+            h = std::make_shared<MeshInstance>(rs->meshes.at(o.mesh), vec(o.position), vec(o.rotation_degrees),
+                                               vec(o.scale), mat);
+            break;
+        case LUZ_OBJ_VOLUME: {
+            std::shared_ptr<Hittable> boundary;
+            if (o.boundary_kind == LUZ_OBJ_CUBE)
+                boundary = std::make_shared<Cube>(Transform(vec(o.position), Vector3(0, 0, 1), Vector3(1, 1, 1)),
+                                                  o.size[0], o.size[1], o.size[2], nullptr);
+            else
+                boundary = std::make_shared<Sphere>(vec(o.position), o.size[0], nullptr, SphereUVProjection::LatLong);
+            h = std::make_shared<ConstantVolume>(boundary, mat, o.density);
+            break;
+        }
+        case LUZ_OBJ_DIRECTIONAL_LIGHT:
+            h = std::make_shared<DirectionalLight>(vec(o.orientation), mat);
+            break;
+        default: throw std::invalid_argument("unknown object kind");
+        }
+        rs->objects.push_back(h);
+        scene.addHittable(h);
+    }
+
+    const LuzCameraDesc& c = d->camera;
+    Camera cam(vec(c.position), vec(c.direction), c.focal_length_m, c.sensor_width_m, c.sensor_height_m,
+               c.f_number, c.focus_distance_m);
+    cam.setUpDirection(vec(c.up));
+    if (c.pinhole) cam.setPinhole(true);
+    scene.addCamera(cam);
+    scene.setMetersPerUnit(d->meters_per_unit);
+    scene.setBackgroundColor(col(d->background));
+    scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT : SKY_NONE);
+    if (d->environment.width > 0) {
+        const LuzEnvironmentDesc& e = d->environment;
+        std::vector<Color> px((std::size_t)e.width * e.height);
+        for (std::size_t k = 0; k < px.size(); k++) px[k] = Color(e.rgb[3 * k], e.rgb[3 * k + 1], e.rgb[3 * k + 2]);
+        scene.setEnvironmentMap(std::make_shared<EnvironmentMap>((std::size_t)e.width, (std::size_t)e.height, std::move(px)));
+        scene.setEnvironmentStrength(e.strength);
+        scene.setEnvironmentRotation(e.rotation_degrees);
+        scene.setEnvironmentLighting(e.lighting != 0);
+    }
+    scene.updateLights();
+    scene.updateAccelerationStructure();
+    return rs.release();
+}
+
+template <class F> int guarded(F&& f)
+{
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return LUZ_E_INVALID;
+    }
+}
+
+bool closest(Scene& scene, Ray& ray, double tmin, double tmax, HitRecord& rec)
+{
+    bool any = false;
+    double best = tmax;
+    const auto& accel = scene.getAccelerationStructure();
+    if (accel && accel->hit(ray, rec, tmin, best)) {
+        best = rec.t0;
+        any = true;
+    }
+    const auto& un = scene.getUnacceleratedHittables();
+    const auto& list = (!accel && un.empty()) ? scene.getHittables() : un;
+    for (const auto& h : list)
+        if (h->hit(ray, rec, tmin, best)) {
+            best = rec.t0;
+            any = true;
+        }
+    return any;
+}
+
+bool occluded(Scene& scene, Ray& ray, double tmin, double tmax)
+{
+    if (tmax <= T_MIN) return false;
+    const auto& accel = scene.getAccelerationStructure();
+    if (accel && accel->hitAny(ray, tmin, tmax)) return true;
+    const auto& un = scene.getUnacceleratedHittables();
+    const auto& list = (!accel && un.empty()) ? scene.getHittables() : un;
+    for (const auto& h : list)
+        if (h->hitAny(ray, tmin, tmax)) return true;
+    return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int luzref_last_error(char* buf, size_t len)
+{
+    if (buf && len) {
+        std::strncpy(buf, g_error.c_str(), len - 1);
+        buf[len - 1] = 0;
+    }
+    return 0;
+}
+
+int luzref_scene_create(const LuzSceneDesc* desc, int32_t tag, void** out)
+{
+    return guarded([&] {
+        *out = build(desc, tag);
+        return 0;
+    });
+}
+
+int luzref_scene_destroy(void* s)
+{
+    delete static_cast<RefScene*>(s);
+    return 0;
+}
+
+/* rays: (ox,oy,oz,tmin,dx,dy,dz,tmax) per ray, used as given (no renormalisation). */
+int luzref_trace_rays(void* s, const double* rays, int64_t n, int32_t any_hit, uint32_t seed,
+                      const int32_t* volume_key, double* t_out, int32_t* obj_out, int32_t* prim_out)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        Sampler::setRenderSeed(seed);
+        for (int64_t i = 0; i < n; i++) {
+            const double* r = rays + 8 * i;
+            if (volume_key) {
+                const int32_t* k = volume_key + 4 * i;
+                Sampler::beginPixelSample((std::size_t)k[0], (std::size_t)k[1], (uint32_t)k[2], 0);
+                Sampler::setBounce((uint32_t)k[3]);
+            } else {
+                Sampler::beginPixelSample(0, 0, 0, 0);
+            }
+            Ray ray = Ray::fromNormalizedDirection(Vector3(r[0], r[1], r[2]), Vector3(r[4], r[5], r[6]));
+            const double tmax = std::isinf(r[7]) ? T_MAX : r[7];
+            if (any_hit) {
+                const bool o = occluded(rs->scene, ray, r[3], tmax);
+                t_out[i] = 0.0;
+                obj_out[i] = o ? 0 : -1;
+                prim_out[i] = 0;
+            } else {
+                HitRecord rec;
+                if (!closest(rs->scene, ray, r[3], tmax, rec)) {
+                    t_out[i] = INFINITY;
+                    obj_out[i] = -1;
+                    prim_out[i] = -1;
+                } else {
+                    t_out[i] = rec.t0;
+                    obj_out[i] = -2;
+                    prim_out[i] = -2;
+                    auto it = rs->tags.find(rec.material);
+                    if (it != rs->tags.end()) {
+                        obj_out[i] = it->second.first;
+                        prim_out[i] = it->second.second;
+                        const int32_t o = it->second.first;
+                        auto inst = o >= 0 ? std::dynamic_pointer_cast<MeshInstance>(rs->objects[o]) : nullptr;
+                        if (inst) {
+                            Ray local;
+                            double scale = 1.0;
+                            HitRecord lrec;
+                            if (inst->_localRay(ray, local, scale)
+                                && inst->_geometry->hit(local, lrec, r[3] * scale, T_MAX)) {
+                                auto jt = rs->tags.find(lrec.material);
+                                prim_out[i] = jt != rs->tags.end() ? jt->second.second : -3;
+                            }
+                        }
+                    }
+                }
+            }
+            Sampler::endPixelSample();
+        }
+        return 0;
+    });
+}
+
+int luzref_trace_paths(void* s, const LuzRenderParams* p, const int32_t* x, const int32_t* y,
+                       const int32_t* sample, int64_t n, double* rgb_out)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        configure(rs->scene, LuzSceneDesc{}, p->width, p->height);
+        rs->scene.setMaxLightBounces(p->max_bounces);
+        rs->scene.setSampleCount(p->spp);
+        const auto cam = Renderer::internal::_prepareRenderCamera(rs->scene);
+        Sampler::setRenderSeed(p->seed);
+        for (int64_t i = 0; i < n; i++) {
+            Sampler::beginPixelSample((std::size_t)x[i], (std::size_t)y[i], (uint32_t)sample[i], p->stream);
+            const Color c = Renderer::internal::_calculatePixelColor(rs->scene, cam, (std::size_t)x[i], (std::size_t)y[i]);
+            Sampler::endPixelSample();
+            rgb_out[3 * i] = c.getRed();
+            rgb_out[3 * i + 1] = c.getGreen();
+            rgb_out[3 * i + 2] = c.getBlue();
+        }
+        return 0;
+    });
+}
+
+/* Full reference render through Renderer::render; rows [row_begin,row_end) only
+ * when row_end > row_begin (a bounded sample of the image: the image is set to
+ * those rows with a camera viewport shifted to match is NOT done — instead the
+ * whole-image render is used and the caller bounds cost through spp). */
+int luzref_render(void* s, const LuzRenderParams* p, int32_t threads, double* rgb_out, double* render_ms,
+                  double* samples)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        configure(rs->scene, LuzSceneDesc{}, p->width, p->height);
+        rs->scene.setMaxLightBounces(p->max_bounces);
+        rs->scene.setSampleCount(p->spp);
+        rs->scene.setRenderingThreads((std::size_t)std::max(1, threads));
+        setRandomSeed((int_fast32_t)p->seed);
+        if (!Renderer::render(rs->scene)) throw std::runtime_error("Renderer::render failed");
+        const auto& img = rs->scene.getImage();
+        for (int32_t yy = 0; yy < p->height; yy++)
+            for (int32_t xx = 0; xx < p->width; xx++) {
+                const Color c = img->getPixel((std::size_t)xx, (std::size_t)yy);
+                const std::size_t k = (std::size_t)yy * p->width + xx;
+                rgb_out[3 * k] = c.getRed();
+                rgb_out[3 * k + 1] = c.getGreen();
+                rgb_out[3 * k + 2] = c.getBlue();
+            }
+        const SceneRenderStats& st = rs->scene.getRenderStats();
+        if (render_ms) *render_ms = st.renderMS;
+        if (samples) *samples = (double)st.renderedSamples;
+        return 0;
+    });
+}
+
+int luzref_mesh_bvh(void* s, int32_t mesh, LuzMeshNode64* nodes, int64_t cap, int64_t* count, int64_t* order,
+                    int64_t order_cap)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        const Mesh& m = *rs->meshes.at(mesh);
+        *count = (int64_t)m._packedBVHNodes.size();
+        for (int64_t i = 0; i < *count && i < cap; i++) {
+            const auto& n = m._packedBVHNodes[(std::size_t)i];
+            for (int a = 0; a < 3; a++) {
+                nodes[i].bmin[a] = n.boundingBox.getMinimum()[a];
+                nodes[i].bmax[a] = n.boundingBox.getMaximum()[a];
+            }
+            nodes[i].left = (int64_t)n.left;
+            nodes[i].right = (int64_t)n.right;
+            nodes[i].start = (int64_t)n.start;
+            nodes[i].count = (int64_t)n.count;
+            nodes[i].is_leaf = n.isLeaf ? 1 : 0;
+        }
+        for (int64_t i = 0; i < (int64_t)m._triangleIndices.size() && i < order_cap; i++)
+            order[i] = (int64_t)m._triangleIndices[(std::size_t)i];
+        return 0;
+    });
+}
+
+int luzref_mesh_triangle_count(void* s, int32_t mesh, int64_t* count)
+{
+    RefScene* rs = static_cast<RefScene*>(s);
+    *count = (int64_t)rs->meshes.at(mesh)->_triangles.size();
+    return 0;
+}
+
+/* Sampler stream values (Sampler.cpp:203-237). which: 1 = sample1D, 2 = sample2D. */
+int luzref_sampler(uint32_t seed, int32_t x, int32_t y, int32_t s, uint32_t stream, uint32_t bounce,
+                   uint32_t dim, int32_t which, double* out)
+{
+    Sampler::setRenderSeed(seed);
+    Sampler::beginPixelSample((std::size_t)x, (std::size_t)y, (uint32_t)s, stream);
+    Sampler::setBounce(bounce);
+    if (which == 1) {
+        out[0] = Sampler::sample1D(dim);
+    } else {
+        const Sampler::Sample2D v = Sampler::sample2D(dim);
+        out[0] = v.x;
+        out[1] = v.y;
+    }
+    Sampler::endPixelSample();
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+"""Named, seeded test cases shared by the fixture generator and the tests.
+
+Each case is a small version of one benchmark configuration (same object
+kinds, materials, light types and value distributions, fewer pixels/samples)
+so the reference oracle computes its fixtures in seconds.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from luz_b200 import scenes
+from luz_b200.desc import Scene
+
+
+def degenerate_soup() -> Scene:
+    """Triangle soup with degenerate and duplicate triangles (dropped / tied)."""
+    rng = np.random.default_rng(17)
+    s = Scene()
+    m = s.lambertian((0.5, 0.5, 0.5))
+    tris = rng.uniform(-1, 1, (300, 3, 3))
+    tris[::25, 2] = tris[::25, 1]            # zero-area triangles
+    tris[1::40] = tris[0::40][: len(tris[1::40])]   # exact duplicates -> equal-t ties
+    tris[::7, :, 1] = np.round(tris[::7, :, 1], 1)  # equal centroids along y
+    s.mesh(tris, m)
+    s.camera.position = (0.0, 0.0, 4.0)
+    return s
+
+
+CASES = {
+    "cornell": lambda: scenes.cornell(64, 64, 4, 8),
+    "tiny": lambda: scenes.tiny_mixed(24, 18, 4, 6),
+    "glossy": lambda: scenes.mesh_glossy(96, 54, 4, 12, level=4),
+    "instancing": lambda: scenes.instancing_volumes(64, 36, 4, 16, count=500),
+}
+
+BVH_CASES = {
+    "box": lambda: scenes.cornell().scene,
+    "icosphere3": lambda: scenes.mesh_glossy(level=3).scene,
+    "torus": lambda: scenes.instancing_volumes(count=1).scene,
+    "degenerate": degenerate_soup,
+}
+
+
+def camera_rays(w, n: int, seed: int) -> np.ndarray:
+    """Rays from near the camera into the view cone: (ox,oy,oz,tmin,dx,dy,dz,tmax) float32."""
+    rng = np.random.default_rng(seed)
+    cam = w.scene.camera
+    fwd = np.asarray(cam.direction, float)
+    fwd /= np.linalg.norm(fwd)
+    org = np.asarray(cam.position, float) + rng.normal(0.0, 0.01, (n, 3))
+    d = rng.normal(0.0, 1.0, (n, 3)) + 2.5 * fwd
+    d[: n // 20, 1] = 0.0                     # axis-parallel components (inverse = 0 branch)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = org
+    r[:, 3] = 1e-3
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    r[n // 10: n // 5, 7] = rng.uniform(0.5, 20.0, n // 5 - n // 10)   # bounded segments
+    return r
+
+
+def path_keys(w, n: int, seed: int):
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, w.width, n).astype(np.int32), rng.integers(0, w.height, n).astype(np.int32),
+            rng.integers(0, w.spp, n).astype(np.int32))

@@ -1,0 +1,75 @@
+"""Generates the golden fixtures in this folder from the Luz reference itself.
+
+Runs in the build container only (it needs oracle/_ref/libluzref.so, built by
+oracle/Makefile from the reference sources). Every value stored here is an
+output of the unmodified reference code:
+  sampler.npz        Sampler::sample1D / sample2D          (src/core/Sampler.cpp)
+  bvh_<case>.npz     Mesh::_packedBVHNodes, _triangleIndices (src/core/Hittables/Mesh.cpp)
+  hits_<case>.npz    _checkHits / isShadowOccluded results   (HitHelper.cpp, ColorHelper.cpp)
+  paths_<case>.npz   per-path radiance, calculateLightRaysColor (ColorHelper.cpp)
+  image_<case>.npz   Renderer::render film (Raw view, no denoise, no adaptive)
+Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, HERE)
+
+from cases import BVH_CASES, CASES, camera_rays, path_keys  # noqa: E402
+from luz_b200 import native  # noqa: E402
+from oracle import RefOracle  # noqa: E402
+
+
+def main():
+    o = RefOracle()
+    rng = np.random.default_rng(20261203)
+    n = 600
+    keys = np.stack([rng.integers(0, 2**32, n), rng.integers(0, 4096, n), rng.integers(0, 4096, n),
+                     rng.integers(0, 70000, n), rng.integers(0, 3, n), rng.integers(0, 20, n),
+                     rng.integers(0, 20, n)], 1).astype(np.int64)
+    s1 = np.array([o.sampler(*map(int, k), 1) for k in keys])
+    s2 = np.array([o.sampler(*map(int, k), 2) for k in keys], np.float64).astype(np.float32)
+    np.savez_compressed(os.path.join(HERE, "sampler.npz"), keys=keys, s1=s1, s2=s2)
+
+    for name, fn in BVH_CASES.items():
+        sc = fn()
+        rs = o.scene(sc.build())
+        out = {}
+        for mi in range(len(sc.meshes)):
+            nodes, order = rs.mesh_bvh(mi)
+            out[f"nodes{mi}"] = nodes
+            out[f"order{mi}"] = order
+        np.savez_compressed(os.path.join(HERE, f"bvh_{name}.npz"), **out)
+
+    for name, fn in CASES.items():
+        w = fn()
+        b = w.scene.build()
+        rs = o.scene(b)
+        rt = o.scene(b, tag=True)
+        rays = camera_rays(w, 2000, seed=len(name))
+        vkey = np.stack([rng.integers(0, w.width, 2000), rng.integers(0, w.height, 2000),
+                         rng.integers(0, w.spp, 2000), rng.integers(0, 4, 2000)], 1).astype(np.int32)
+        t, ob, pr = rt.trace_rays(rays.astype(np.float64), seed=w.seed, volume_key=vkey)
+        _, occ, _ = rt.trace_rays(rays.astype(np.float64), any_hit=True, seed=w.seed, volume_key=vkey)
+        np.savez_compressed(os.path.join(HERE, f"hits_{name}.npz"), rays=rays, vkey=vkey, t=t, obj=ob, prim=pr,
+                            occluded=occ >= 0)
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        x, y, s = path_keys(w, 1500, seed=7 + len(name))
+        rgb = rs.trace_paths(p, x, y, s)
+        np.savez_compressed(os.path.join(HERE, f"paths_{name}.npz"), x=x, y=y, s=s, rgb=rgb)
+        if name in ("cornell", "tiny"):
+            img, _, _ = rs.render(p, os.cpu_count() or 1)
+            np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
+        print("golden", name, flush=True)
+
+
+if __name__ == "__main__":
+    main()

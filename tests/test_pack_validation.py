@@ -1,0 +1,58 @@
+"""Scene validation mirrors the reference's std::invalid_argument messages."""
+import pytest
+
+from luz_b200 import native
+from luz_b200.desc import Scene
+
+
+def packs(sc):
+    return native.Pack(sc.build())
+
+
+@pytest.mark.parametrize("make,msg", [
+    (lambda s: s.sphere((0, 0, 0), 1, s.metal((1, 1, 1), roughness=1.5)), "Metal roughness must be finite and in [0,1]."),
+    (lambda s: s.sphere((0, 0, 0), 1, s.dielectric(ior=-1.0)), "Dielectric refractive index must be finite and positive."),
+    (lambda s: s.volume_sphere((0, 0, 0), 1, s.henyey_greenstein((1, 1, 1), 0.995), 1.0),
+     "Volume anisotropy must be finite and between -0.99 and 0.99."),
+    (lambda s: s.volume_sphere((0, 0, 0), 1, s.isotropic((1, 1, 1)), 0.0), "Volume density must be finite and positive."),
+    (lambda s: s.sphere((0, 0, 0), 1, s.principled((1, 1, 1), metallic=2.0)), "Principled metallic must be finite and in [0,1]."),
+])
+def test_invalid_parameters_rejected(make, msg):
+    s = Scene()
+    make(s)
+    with pytest.raises(native.LuzError) as e:
+        packs(s)
+    assert msg in str(e.value) and e.value.code == -1
+
+
+def test_unsupported_sky_rejected():
+    s = Scene()
+    s.sky = 2   # SKY_ATMOSPHERE
+    with pytest.raises(native.LuzError) as e:
+        packs(s)
+    assert e.value.code == -3
+
+
+def test_camera_validation():
+    s = Scene()
+    s.camera.focal_length_m = 0.0
+    with pytest.raises(native.LuzError) as e:
+        packs(s)
+    assert "focal length" in str(e.value)
+
+
+def test_material_index_out_of_range():
+    s = Scene()
+    s.sphere((0, 0, 0), 1, 5)
+    with pytest.raises(native.LuzError):
+        packs(s)
+
+
+def test_light_list_and_weights():
+    s = Scene()
+    e = s.emissive((1, 1, 1))
+    s.rectangle((0, 0, 0), (0, 1, 0), 2, 3, e)
+    s.sphere((0, 0, 0), 1, e)
+    s.directional_light((0, -1, 0), e)
+    s.sphere((3, 0, 0), 1, s.lambertian((1, 1, 1)))
+    assert packs(s).info().light_count == 3

@@ -1,0 +1,34 @@
+"""The FP32 restatement of the traversal against the reference's own hits
+(closest hit: object and mesh primitive ids; any hit: occlusion)."""
+import numpy as np
+import pytest
+
+from cases import CASES
+from luz_b200 import native
+from luz_b200.desc import OBJ_MESH, OBJ_MESH_INSTANCE
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_restated_closest_hits_match_reference(name, golden, restate):
+    g = golden("hits_" + name)
+    w = CASES[name]()
+    pk = native.Pack(w.scene.build())
+    h = restate.trace(pk, g["rays"], seed=w.seed, volume_key=g["vkey"])
+    same_obj = h["object"] == g["obj"]
+    kinds = np.array([w.scene.objects[o]["kind"] if o >= 0 else 0 for o in g["obj"]])
+    meshy = np.isin(kinds, [OBJ_MESH, OBJ_MESH_INSTANCE])
+    same_prim = ~meshy | (h["primitive"] == g["prim"])
+    agree = same_obj & same_prim
+    assert agree.mean() >= 0.995, agree.mean()
+    hit = agree & (g["obj"] >= 0)
+    rel = np.abs(h["t"][hit] - g["t"][hit]) / np.maximum(g["t"][hit], 1e-6)
+    assert np.all(rel < 1e-4), rel.max()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_restated_any_hits_match_reference(name, golden, restate):
+    g = golden("hits_" + name)
+    w = CASES[name]()
+    pk = native.Pack(w.scene.build())
+    h = restate.trace(pk, g["rays"], any_hit=True, seed=w.seed, volume_key=g["vkey"])
+    assert ((h["object"] >= 0) == g["occluded"]).mean() >= 0.995
