@@ -54,7 +54,19 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 
 // ---------------------------------------------------------------------------- extend (closest hit)
 
-__global__ void __launch_bounds__(kBlock) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
+// Resident blocks per SM the register allocator is asked to allow (measured on
+// B200: more resident warps beat the few spills this costs in the traversal).
+#ifndef LUZ_EXTEND_MIN_BLOCKS
+#define LUZ_EXTEND_MIN_BLOCKS 6
+#endif
+#ifndef LUZ_SHADE_MIN_BLOCKS
+#define LUZ_SHADE_MIN_BLOCKS 4
+#endif
+#ifndef LUZ_SHADOW_MIN_BLOCKS
+#define LUZ_SHADOW_MIN_BLOCKS 8
+#endif
+
+__global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     const uint32_t count = C->count[bounce];
     const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
@@ -84,7 +96,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(DScene S, WaveArgs w, PathBuf
 
 // ---------------------------------------------------------------------------- shadow (any hit)
 
-__global__ void __launch_bounds__(kBlock) k_shadow(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
+__global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     const uint32_t count = C->shadow[bounce];
     while (true) {
@@ -114,8 +126,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DScene S, WaveArgs w, PathBuf
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
+__global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
+    const DScene& S = *Sp;
     const uint32_t count = C->count[bounce];
     const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
     uint32_t* nq = (bounce & 1) ? P.queue0 : P.queue1;
@@ -145,6 +158,18 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene S, WaveArgs w, PathBuf 
             }
         }
     }
+}
+
+// Adds one wave's per-bounce queue sizes to the render totals (no host wait per wave).
+__global__ void k_tally(const Ctrl* C, int max_b, unsigned long long* totals)
+{
+    unsigned long long e = 0, s = 0;
+    for (int b = 0; b <= max_b; b++) {
+        e += C->count[b];
+        s += C->shadow[b];
+    }
+    totals[0] += e;
+    totals[1] += s;
 }
 
 __global__ void k_path_color(WaveArgs w, PathBuf P)
@@ -267,6 +292,8 @@ struct luz_gpu_scene {
     int device = 0;
     std::unique_ptr<ScenePack> pack;
     DScene ds{};
+    DScene* dds = nullptr;           // device copy of ds: k_shade reads it through a pointer so that
+                                     // its out-of-line calls pass a reference, not a stack copy
     std::vector<void*> allocs;
     cudaStream_t stream = nullptr;
     // path buffers (grown on demand)
@@ -275,6 +302,7 @@ struct luz_gpu_scene {
     std::vector<void*> pallocs;
     Ctrl* ctrl = nullptr;
     Ctrl* ctrl_host = nullptr;
+    unsigned long long* totals = nullptr;   // device: extension / shadow rays of the current render
     double* film = nullptr;
     int64_t film_pix = 0;
     int sms = 0;
@@ -330,6 +358,8 @@ struct luz_gpu_scene {
         if (ctrl) cudaFree(ctrl);
         if (ctrl_host) cudaFreeHost(ctrl_host);
         if (film) cudaFree(film);
+        if (dds) cudaFree(dds);
+        if (totals) cudaFree(totals);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -376,7 +406,7 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
         k_extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
-        k_shade<<<g_shade, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
         k_shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
@@ -451,7 +481,9 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
         CK(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
     }
     s->ds.counters = counters;
+    CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(s->film, 0, sizeof(double) * 3 * npix, st));
+    CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
     CK(cudaEventRecord(s->ev0, st));
     int64_t launches = 0, waves = 0;
     for (int sb = 0; sb < p->spp; sb += s_wave) {
@@ -468,10 +500,13 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
             k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
             launch_bounces(s, w, st, launches, T);
             k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, s->film);
-            launches += 2;
+            k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
+            launches += 3;
             waves++;
-            finish_wave(s, st, &acc, w.max_bounces);
-            T.collect();
+            if (T.on) {
+                CK(cudaStreamSynchronize(st));
+                T.collect();
+            }
         }
     }
     k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(s->film, npix, (double)p->spp, d_out);
@@ -479,6 +514,15 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaEventSynchronize(s->ev1));
     CK(cudaGetLastError());
+    {
+        unsigned long long tot[2] = {0, 0};
+        uint32_t err = 0;
+        CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+        acc.extension_rays = (double)tot[0];
+        acc.shadow_rays = (double)tot[1];
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->ds.counters = nullptr;
@@ -486,6 +530,7 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
     if (counters) {
         CK(cudaMemcpy(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost));
         cudaFree(counters);
+        CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
     }
     if (stats) {
         *stats = acc;
@@ -569,7 +614,10 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         d.error = err;
         d.counters = nullptr;
         d.k = P.consts;
+        s->dds = dalloc<DScene>(1);
+        CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
         s->ctrl = dalloc<Ctrl>(1);
+        s->totals = dalloc<unsigned long long>(2);
         CK(cudaMallocHost(&s->ctrl_host, sizeof(Ctrl)));
         cudaDeviceProp prop;
         CK(cudaGetDeviceProperties(&prop, device));

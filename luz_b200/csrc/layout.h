@@ -181,6 +181,8 @@ struct GEnv {
     int64_t texel_offset;     // float4 texels
     int64_t cdf_offset;       // double CDF (W*H)
     int64_t pdf_offset;       // double (weight/total)/solidAngle per texel
+    int32_t guide_offset;     // CDF guide tables (lo[K], hi[K] in the index pool), -1 = none
+    int32_t guide_count;
 };
 
 struct GSceneConst {

@@ -1153,7 +1153,24 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         }
         E.total_weight = total;
         E.cdf_offset = (int64_t)S.cdf.size();
+        E.guide_offset = -1;
         if (total > 0.0) {
+            // Guide tables for the device-side std::lower_bound. For bucket b of K:
+            //   lo[b] = first index with cdf >= (b/K) total (1 - eps)
+            //   hi[b] = first index with cdf >= ((b+1)/K) total (1 + eps), plus one
+            // so for any target whose computed bucket is b (even if rounding moved
+            // it across a bucket edge) the lower_bound answer lies in [lo[b], hi[b]).
+            const int32_t K = (int32_t)std::min<int64_t>(65536, std::max<int64_t>(1, WH / 4));
+            const double eps = 1e-9;
+            E.guide_count = K;
+            E.guide_offset = (int32_t)S.index_pool.size();
+            auto first_ge = [&](double thr) {
+                return (int64_t)(std::lower_bound(cdf.begin(), cdf.end(), thr) - cdf.begin());
+            };
+            for (int32_t b = 0; b < K; b++)
+                S.index_pool.push_back((int32_t)std::min<int64_t>(first_ge(((double)b / K) * total * (1.0 - eps)), WH - 1));
+            for (int32_t b = 0; b < K; b++)
+                S.index_pool.push_back((int32_t)std::min<int64_t>(first_ge(((double)(b + 1) / K) * total * (1.0 + eps)) + 1, WH));
             S.cdf.insert(S.cdf.end(), cdf.begin(), cdf.end());
             E.pdf_offset = (int64_t)S.cdf.size();
             for (int64_t k = 0; k < WH; k++)

@@ -81,7 +81,7 @@ __device__ __forceinline__ F3 transform_normal(const GObject& O, F3 n)
 }
 
 // Builds the HitRecord the reference's hit() would fill for THit h on ray r.
-__device__ Hit make_hit(const DScene& S, const TRay& r, const THit& th)
+__device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit& th)
 {
     Hit h;
     const GObject O = S.objects[th.obj];
@@ -153,7 +153,7 @@ __device__ __forceinline__ float wrap01f(float v)
     if (v < 0.0f) v += 1.0f;
     return v;
 }
-__device__ F3 texture_sample(const DScene& S, int32_t ti, float u, float v)
+__device__ __noinline__ F3 texture_sample(const DScene& S, int32_t ti, float u, float v)
 {
     const GTexture T = S.textures[ti];
     u = wrap01f(u);
@@ -390,7 +390,7 @@ __device__ PWeights principled_weights(const GMaterial& m, F3 base)
     }
     return r;
 }
-__device__ F3 principled_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+__device__ __noinline__ F3 principled_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 base = clamp_color01(color_at(S, m, h));
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
@@ -436,7 +436,7 @@ __device__ F3 principled_eval(const DScene& S, const GMaterial& m, const Hit& h,
                                  m.clearcoat * 0.25f);
     return res;
 }
-__device__ float principled_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+__device__ __noinline__ float principled_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 base = clamp_color01(color_at(S, m, h));
     const PWeights W = principled_weights(m, base);
@@ -486,7 +486,7 @@ __device__ __forceinline__ F3 ray_dir_normalized(F3 d)   // Ray::_normalize (inc
 }
 
 // Material::evaluateBSDFCos / scatteringPDF for the BSDF-typed materials.
-__device__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+__device__ __noinline__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
     switch (m.type) {
@@ -503,7 +503,7 @@ __device__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ra
         return F3{0.f, 0.f, 0.f};
     }
 }
-__device__ float bsdf_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+__device__ __noinline__ float bsdf_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
     switch (m.type) {
@@ -551,7 +551,7 @@ __device__ __forceinline__ bool finish_bsdf(const DScene& S, const GMaterial& m,
 }
 
 // Material::scatter for every type on the path; false = no scatter (emitter or failed sample).
-__device__ bool scatter(const DScene& S, const GMaterial& m, const Hit& h, F3 d, const Key& k, Scatter& sr)
+__device__ __noinline__ bool scatter(const DScene& S, const GMaterial& m, const Hit& h, F3 d, const Key& k, Scatter& sr)
 {
     sr.specular = false;
     sr.pdf = PDF_NONE;
@@ -718,7 +718,7 @@ __device__ F3 scatter_bsdfcos(const DScene& S, const Scatter& sr, const GMateria
     return sr.att * scatter_pdf(S, sr, m, h, ray_d, dir);
 }
 // henyeyGreensteinDirection (ColorHelper.cpp:108-140)
-__device__ F3 hg_direction(const Scatter& sr, const Key& k)
+__device__ __noinline__ F3 hg_direction(const Scatter& sr, const Key& k)
 {
     const float pl = len2(sr.phase);
     if (pl <= 0.0f || !isfinite(pl)) return sphere_direction(k, DIM_BSDF_DIRECTION);
@@ -779,7 +779,7 @@ __device__ __forceinline__ void env_dir_to_uv(const GEnv& E, F3 dir, double& u, 
     u = wrap01d(0.5 + (phi / (2.0 * kPiD)) + (E.rotation / 360.0));
     v = clamp01d(0.5 + (asin(y) / kPiD));
 }
-__device__ F3 env_lookup_uv(const DScene& S, double u, double v)
+__device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, double v)
 {
     const GEnv& E = S.k.env;
     u = wrap01d(u);
@@ -806,13 +806,30 @@ __device__ F3 env_lookup_uv(const DScene& S, double u, double v)
     return F3{isfinite(c.x) ? fmaxf(0.f, c.x) : 0.f, isfinite(c.y) ? fmaxf(0.f, c.y) : 0.f,
               isfinite(c.z) ? fmaxf(0.f, c.z) : 0.f};
 }
-__device__ __forceinline__ F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
+__device__ __noinline__ F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
 {
     double u, v;
     env_dir_to_uv(S.k.env, dir, u, v);
     return env_lookup_uv(S, u, v);
 }
-__device__ float env_pdf(const DScene& S, F3 dir)
+__device__ __forceinline__ float env_pdf_uv(const DScene& S, double u, double v)
+{
+    const GEnv& E = S.k.env;
+    if (E.total_weight <= 0.0 || E.pdf_offset < 0) return 1.0f / (4.0f * kPiF);
+    const long long x = min((long long)floor(wrap01d(u) * (double)E.width), (long long)E.width - 1);
+    const long long y = min((long long)floor((1.0 - clamp01d(v)) * (double)E.height), (long long)E.height - 1);
+    return (float)S.cdf[E.pdf_offset + y * E.width + x];
+}
+// EnvironmentMap::sampleDirection and ::pdf of one direction: both start from the same
+// directionToUV(direction), so it is evaluated once.
+__device__ __noinline__ void env_query(const DScene& S, F3 dir, bool want_rad, bool want_pdf, F3& rad, float& pdf)
+{
+    double u, v;
+    env_dir_to_uv(S.k.env, dir, u, v);
+    if (want_rad) rad = env_lookup_uv(S, u, v);
+    if (want_pdf) pdf = env_pdf_uv(S, u, v);
+}
+__device__ __noinline__ float env_pdf(const DScene& S, F3 dir)
 {
     const GEnv& E = S.k.env;
     if (E.total_weight <= 0.0 || E.pdf_offset < 0) return 1.0f / (4.0f * kPiF);
@@ -836,7 +853,7 @@ __device__ __forceinline__ double clamp_sample(double v)
     return v;
 }
 // EnvironmentMap::sample (EnvironmentMap.cpp:468-513)
-__device__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
+__device__ __noinline__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
 {
     const GEnv& E = S.k.env;
     const double sel0 = sample1d(k, DIM_ENVIRONMENT_SELECTION);
@@ -855,7 +872,16 @@ __device__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance,
     const double target = clamp_sample(sel0) * E.total_weight;
     const int64_t n = (int64_t)E.width * E.height;
     const double* cdf = S.cdf + E.cdf_offset;
-    int64_t lo = 0, hi = n;   // lower_bound
+    // std::lower_bound over the CDF, narrowed to the guide-table range of the
+    // target's bucket (the answer provably lies inside it; same result, few loads).
+    int64_t lo = 0, hi = n;
+    if (E.guide_offset >= 0) {
+        const int32_t* g = S.index_pool + E.guide_offset;
+        const double fb = (target / E.total_weight) * (double)E.guide_count;
+        const int64_t b = min(max((int64_t)floor(fb), (int64_t)0), (int64_t)E.guide_count - 1);
+        lo = g[b];
+        hi = g[E.guide_count + b];
+    }
     while (lo < hi) {
         const int64_t mid = (lo + hi) >> 1;
         if (cdf[mid] < target) lo = mid + 1;
@@ -869,8 +895,7 @@ __device__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance,
     const double yy = sin((clamp01d(v) - 0.5) * kPiD);
     const double rr = sqrt(fmax(0.0, 1.0 - yy * yy));
     dir = F3{(float)(rr * cos(phi)), (float)yy, (float)(rr * sin(phi))};
-    radiance = env_radiance(S, dir);
-    pdf = env_pdf(S, dir);
+    env_query(S, dir, true, true, radiance, pdf);
     return pdf > 0.0f && isfinite(pdf);
 }
 
@@ -923,7 +948,7 @@ __device__ int32_t mesh_pick(const DScene& S, const GMesh& M, const Key& k, doub
     return S.index_pool[M.slot_offset + idx];
 }
 
-__device__ bool light_surface_sample(const DScene& S, const GLight& L, F3 origin, const Key& k, LightSample& ls)
+__device__ __noinline__ bool light_surface_sample(const DScene& S, const GLight& L, F3 origin, const Key& k, LightSample& ls)
 {
     ls.valid = false;
     switch (L.kind) {
@@ -1050,7 +1075,7 @@ __device__ bool light_surface_sample(const DScene& S, const GLight& L, F3 origin
 }
 
 // Hittable::pdfValue of light L toward direction vec from origin.
-__device__ float light_pdf_value(const DScene& S, const GLight& L, F3 origin, F3 vec)
+__device__ __noinline__ float light_pdf_value(const DScene& S, const GLight& L, F3 origin, F3 vec)
 {
     VolSample vs{nullptr, 0.0, true};
     switch (L.kind) {
@@ -1122,7 +1147,7 @@ __device__ __forceinline__ float light_select_prob(const DScene& S, int32_t i)
     return (float)(w / S.k.light_total_weight);
 }
 // lightPDFValue (ColorHelper.cpp:233-257)
-__device__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
+__device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
 {
     const int32_t n = S.k.light_count;
     if (n <= 0) return 0.0f;
@@ -1132,7 +1157,7 @@ __device__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
     return sum;
 }
 // selectLightIndex + sampleLight (ColorHelper.cpp:190-231, 925-971)
-__device__ bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
+__device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
 {
     ls.valid = false;
     const int32_t n = S.k.light_count;

@@ -167,7 +167,7 @@ __device__ __forceinline__ bool leaves_opaque(const GMaterial& m, const Hit& h, 
 __device__ __forceinline__ float direct_prob(int bounce) { return bounce < 2 ? 1.0f : 0.5f; }
 
 // relocateSubsurfaceExit (ColorHelper.cpp:428-504)
-__device__ void relocate_subsurface(const DScene& S, const GMaterial& m, Hit& h, Scatter& sr, F3 ray_d, const Key& k)
+__device__ __noinline__ void relocate_subsurface(const DScene& S, const GMaterial& m, Hit& h, Scatter& sr, F3 ray_d, const Key& k)
 {
     if (!sr.subsurface || sr.thin) return;
     const float dl = maxc(sr.ss_radius_m);
@@ -243,14 +243,19 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
 
     if (obj < 0) {   // miss (ColorHelper.cpp:1169-1210)
         float env_mis = 1.0f;
-        if (bounce > 0 && !prev_spec && (flags & PF_PREV_SVIL)) {
+        const bool need_pdf = bounce > 0 && !prev_spec && (flags & PF_PREV_SVIL);
+        const bool need_rad = S.k.sky == 3 && S.k.env.present;
+        F3 env_rad{0.f, 0.f, 0.f};
+        float env_p = 0.0f;
+        if ((need_pdf && S.k.env.lighting) || need_rad) env_query(S, ray.d, need_rad, need_pdf && S.k.env.lighting, env_rad, env_p);
+        if (need_pdf) {
             float ipdf = 0.0f;
-            if (S.k.env.lighting) ipdf = env_pdf(S, ray.d);
+            if (S.k.env.lighting) ipdf = env_p;
             else if (S.k.has_constant_background_light) ipdf = 1.0f / (4.0f * kPiF);
             env_mis = power_heuristic(prev_pdf, ipdf);
         }
         F3 sky;
-        if (S.k.sky == 3 && S.k.env.present) sky = (env_radiance(S, ray.d) * S.k.env.strength) * env_mis;
+        if (need_rad) sky = (env_rad * S.k.env.strength) * env_mis;
         else sky = f3(S.k.background) * env_mis;
         F3 contrib = thr * sky;
         if (bounce > 0 && S.k.has_constant_background_light) contrib = clamp_bg_miss(S, contrib);
@@ -352,7 +357,9 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         }
         const F3 dir = scatter_generate(sr, k);
         if (!leaves_opaque(m, h, dir)) goto done;
-        const float pdf = scatter_pdf(S, sr, m, h, ray.d, dir);
+        // For a BSDF record this is scatteringPDF of the sampled direction with the same
+        // inputs that produced sr.spdf, so the stored value is reused.
+        const float pdf = sr.pdf == PDF_BSDF ? sr.spdf : scatter_pdf(S, sr, m, h, ray.d, dir);
         if (pdf <= 0.0f || !isfinite(pdf)) goto done;
         thr = clamp_ray_color(thr * att);
         if (terminated(thr) || !russian_roulette(thr, bounce, k)) goto done;
