@@ -264,6 +264,27 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
                         const int32_t* x, const int32_t* y, const int32_t* sample,
                         int64_t count, float* rgb_out);
 
+/* Render without allocating device memory.
+ * For callers that cannot call cudaMalloc while they render: a host whose
+ * device memory is owned by its own allocator, or a per-frame loop that must
+ * not take the implicit device synchronisation that cudaMalloc/cudaFree cause.
+ * Same result as luz_gpu_render_device (same kernels, same FP64 film), but the
+ * path state, queues and film live in one file-scope device array of
+ * LUZ_STATIC_SCRATCH_BYTES that every GPU loading this library holds until
+ * process exit; the caller passes the scene (created beforehand), the device
+ * film and the stream. Limits: width*height <= LUZ_STATIC_MAX_PIXELS, otherwise
+ * LUZ_E_LIMIT; flags must be 0. The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture. All calls share the array and it keeps the previous call's
+ * contents: calls whose GPU work overlaps (other streams, other threads) race
+ * on it and must be serialised by the caller.
+ * No counterpart in the reference: the CPU renderer has no device memory. */
+#define LUZ_STATIC_SCRATCH_BYTES (96u << 20)
+#define LUZ_STATIC_WAVE_PATHS    131072
+#define LUZ_STATIC_MAX_PIXELS    2900000
+int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* params,
+                                  float* d_rgb_out, void* stream, LuzRenderStats* stats);
+
 /* Ray batch traversal (test hook and building block): rays are
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) * count, host buffers. any_hit != 0
  * runs the shadow traversal and reports object = 0 (occluded) / -1. The

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -555,7 +556,158 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
 
 }  // namespace
 
+// ---------------------------------------------------------------------------- no-allocation render
+//
+// One file-scope device array holds the path state, queues and film of
+// luz_gpu_render_device_noalloc, so that entry point never allocates. Its
+// layout (256-B aligned sub-arrays) is carved on the host from the array's
+// device address, resolved once per device with cudaGetSymbolAddress.
+
+static __device__ __align__(256) unsigned char g_static_scratch[LUZ_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+struct StaticArena {
+    PathBuf pb{};
+    Ctrl* ctrl = nullptr;
+    unsigned long long* totals = nullptr;
+    double* film = nullptr;
+    int64_t film_pixels = 0;
+};
+
+constexpr std::size_t align256(std::size_t b) { return (b + 255) & ~std::size_t(255); }
+
+StaticArena carve_static(unsigned char* base)
+{
+    const int64_t n = LUZ_STATIC_WAVE_PATHS;
+    std::size_t off = 0;
+    auto take = [&](std::size_t bytes) {
+        unsigned char* p = base + off;
+        off += align256(bytes);
+        return p;
+    };
+    StaticArena A;
+    PathBuf& P = A.pb;
+    P.ray_o = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.ray_d = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.thr = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.rad = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.prev_o = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.pend0 = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.pend1 = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.hit = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.pixel = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
+    P.sample = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
+    P.hit_prim = reinterpret_cast<int32_t*>(take(n * sizeof(int32_t)));
+    P.queue0 = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
+    P.queue1 = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
+    P.sh_o = reinterpret_cast<float4*>(take(2 * n * sizeof(float4)));
+    P.sh_d = reinterpret_cast<float4*>(take(2 * n * sizeof(float4)));
+    P.sh_x = reinterpret_cast<int2*>(take(2 * n * sizeof(int2)));
+    P.color = nullptr;   // used by trace_paths only
+    A.ctrl = reinterpret_cast<Ctrl*>(take(sizeof(Ctrl)));
+    A.totals = reinterpret_cast<unsigned long long*>(take(2 * sizeof(unsigned long long)));
+    A.film = reinterpret_cast<double*>(base + off);
+    A.film_pixels = (int64_t)((LUZ_STATIC_SCRATCH_BYTES - off) / (3 * sizeof(double)));
+    return A;
+}
+
+// Device address of g_static_scratch, per device, resolved on first use with
+// that device current.
+unsigned char* static_scratch_address(int device)
+{
+    static std::mutex mu;
+    static std::vector<unsigned char*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)addr.size() <= device) addr.resize(device + 1, nullptr);
+    if (!addr[device]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_static_scratch));
+        addr[device] = static_cast<unsigned char*>(p);
+    }
+    return addr[device];
+}
+
+int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStream_t st, LuzRenderStats* stats)
+{
+    check_params(p);
+    if (p->flags != 0) throw Status(LUZ_E_UNSUPPORTED, "luz_gpu_render_device_noalloc takes no render flags.");
+    CK(cudaSetDevice(s->device));
+    const StaticArena A = carve_static(static_scratch_address(s->device));
+    const int64_t npix = (int64_t)p->width * p->height;
+    if (npix > LUZ_STATIC_MAX_PIXELS || npix > A.film_pixels)
+        throw Status(LUZ_E_LIMIT, "Image of " + std::to_string(npix) + " pixels exceeds the static film of " +
+                                      std::to_string((long long)LUZ_STATIC_MAX_PIXELS) + " pixels.");
+    WaveArgs w = base_args(s, p);
+    const int64_t target = LUZ_STATIC_WAVE_PATHS;
+    const int s_wave = (int)std::min<int64_t>(p->spp, target);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, target / s_wave));
+    CK(cudaMemsetAsync(A.film, 0, sizeof(double) * 3 * npix, st));
+    CK(cudaMemsetAsync(A.totals, 0, 2 * sizeof(unsigned long long), st));
+    CK(cudaEventRecord(s->ev0, st));
+    int64_t launches = 0, waves = 0;
+    StageTimer T;
+    for (int sb = 0; sb < p->spp; sb += s_wave) {
+        const int sc = std::min(s_wave, p->spp - sb);
+        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
+            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = sb;
+            w.s_count = sc;
+            w.n = pc * sc;
+            w.list_mode = 0;
+            CK(cudaMemsetAsync(A.ctrl, 0, sizeof(Ctrl), st));
+            k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, A.pb, A.ctrl);
+            const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
+            for (int b = 0; b <= w.max_bounces; b++) {
+                k_extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
+                k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, A.pb, A.ctrl, b);
+                k_shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
+                launches += 3;
+            }
+            k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, A.pb, A.film);
+            k_tally<<<1, 1, 0, st>>>(A.ctrl, w.max_bounces, A.totals);
+            launches += 3;
+            waves++;
+        }
+    }
+    k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(A.film, npix, (double)p->spp, d_out);
+    launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    unsigned long long tot[2] = {0, 0};
+    uint32_t err = 0;
+    CK(cudaMemcpy(tot, A.totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = (double)npix * p->spp;
+        stats->extension_rays = (double)tot[0];
+        stats->shadow_rays = (double)tot[1];
+        stats->kernel_launches = launches;
+        stats->waves = waves;
+    }
+    return LUZ_OK;
+}
+
+}  // namespace
+
 extern "C" {
+
+int luz_gpu_render_device_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, void* stream,
+                                  LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !d_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_render_noalloc(s, p, d_out, stream ? (cudaStream_t)stream : s->stream, stats);
+    });
+}
 
 int luz_gpu_last_error(char* buffer, size_t length)
 {

@@ -22,6 +22,7 @@ EXPORTED = [
     "luz_gpu_last_error", "luz_gpu_device_count", "luz_pack_create", "luz_pack_destroy", "luz_pack_info",
     "luz_pack_mesh_bvh", "luz_pack_array", "luz_gpu_scene_create", "luz_gpu_scene_destroy", "luz_gpu_scene_info",
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
+    "luz_gpu_render_device_noalloc",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -59,6 +60,7 @@ def lib():
     L.luz_gpu_render_device.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_trace_paths.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, vp, i64, vp]
     L.luz_gpu_trace_rays.argtypes = [vp, vp, i64, i32, C.c_uint32, vp, vp]
+    L.luz_gpu_render_device_noalloc.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int
     _lib = L
