@@ -285,6 +285,47 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
 int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* params,
                                   float* d_rgb_out, void* stream, LuzRenderStats* stats);
 
+/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
+ * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),
+ * defaults include/luz/Defaults.hpp:12-15 (on, 128, 32, 0.03). */
+typedef struct LuzAdaptiveParams {
+    int32_t  enabled;
+    int32_t  min_samples;         /* > 0 */
+    int32_t  check_interval;      /* > 0 */
+    int32_t  reserved;
+    double   threshold;           /* finite, > 0: relative 95% confidence interval */
+} LuzAdaptiveParams;
+
+/* NFOR inputs (Denoise::NFORBuffers, include/luz/Denoise/NFOR.hpp:23-32), host
+ * buffers, row-major, y = 0 first. Each pointer may be NULL to skip that buffer. */
+#define LUZ_NFOR_FEATURES 11
+typedef struct LuzNforBuffers {
+    double*  color_a;             /* W*H*3: mean of the even samples (stream 1)      */
+    double*  color_b;             /* W*H*3: mean of the odd samples (stream 2)       */
+    double*  color_variance;      /* W*H: variance of the pixel mean, channel average */
+    double*  features_a;          /* W*H*11 */
+    double*  features_b;          /* W*H*11 */
+    double*  feature_variance;    /* W*H*11 */
+} LuzNforBuffers;
+
+/* Render with adaptive sampling and/or NFOR buffers: the _threadRender loop
+ * (src/renderer/Threads.cpp:551-641) with adaptiveSampleConverged (:194-265)
+ * and storeDenoisePixel (:343-372).
+ *   adaptive: NULL or enabled = 0 samples every pixel params->spp times; else a
+ *             pixel stops at the first check point (min_samples, then every
+ *             check_interval samples) where its luminance and RGB confidence
+ *             intervals are within threshold (adaptiveSamplingCanStop, :267-273).
+ *   nfor:     NULL renders on params->stream; else samples alternate between
+ *             sampler streams 1 and 2 (the denoise half buffers, :593-598) and
+ *             the buffers are filled.
+ *   samples_out: NULL or W*H samples used per pixel.
+ * rgb_out is the host film of per-pixel means; stats->samples is the sum of the
+ * samples used (SceneRenderStats::renderedSamples). */
+int luz_gpu_render_ex(luz_gpu_scene* scene, const LuzRenderParams* params,
+                      const LuzAdaptiveParams* adaptive, float* rgb_out,
+                      const LuzNforBuffers* nfor, int32_t* samples_out,
+                      LuzRenderStats* stats);
+
 /* Ray batch traversal (test hook and building block): rays are
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) * count, host buffers. any_hit != 0
  * runs the shadow traversal and reports object = 0 (occluded) / -1. The

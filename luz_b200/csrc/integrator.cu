@@ -67,8 +67,13 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 #define LUZ_SHADOW_MIN_BLOCKS 8
 #endif
 
+// Extend and shadow are instantiated per scene feature set (TF_* bits:
+// instances, volumes); a scene without them runs traversal code without the
+// instance transform or the volume sampler, and skips the per-ray sampler key.
+template <uint32_t F>
 __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
+    LocalStack<true> st;
     const uint32_t count = C->count[bounce];
     const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
     while (true) {
@@ -81,10 +86,13 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
         const uint32_t p = q[i];
         const float4 o = P.ray_o[p], d = P.ray_d[p];
         const TRay r = make_ray_x(F3{o.x, o.y, o.z}, F3{d.x, d.y, d.z}, __float_as_int(o.w), __float_as_int(d.w));
-        const uint32_t pix = P.pixel[p];
-        const Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        Key k{};
+        if constexpr ((F & TF_VOLUME) != 0) {
+            const uint32_t pix = P.pixel[p];
+            k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        }
         VolSample vs{&k, 0.0, false};
-        const THit h = closest_hit(S, r, kTMin, kInf, vs);
+        const THit h = closest_hit<F>(S, r, kTMin, kInf, vs, st);
         P.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.obj));
         P.hit_prim[p] = h.prim;
         if (S.counters) {
@@ -97,8 +105,10 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
 
 // ---------------------------------------------------------------------------- shadow (any hit)
 
+template <uint32_t F>
 __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
+    LocalStack<false> st;
     const uint32_t count = C->shadow[bounce];
     while (true) {
         uint32_t base = 0;
@@ -112,10 +122,13 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene
         const uint32_t p = tag & 0x7fffffffu;
         const int2 x = P.sh_x[i];
         const TRay r = make_ray_x(F3{o.x, o.y, o.z}, F3{d.x, d.y, d.z}, x.x, x.y);
-        const uint32_t pix = P.pixel[p];
-        const Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        Key k{};
+        if constexpr ((F & TF_VOLUME) != 0) {
+            const uint32_t pix = P.pixel[p];
+            k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        }
         VolSample vs{&k, 0.0, false};
-        if (any_hit(S, r, kTMin, o.w, vs)) {
+        if (any_hit<F>(S, r, kTMin, o.w, vs, st)) {
             if (tag & 0x80000000u) P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
             else P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -126,6 +139,10 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene
         }
     }
 }
+
+using TraceKernel = void (*)(DScene, WaveArgs, PathBuf, Ctrl*, int);
+const TraceKernel kExtendKernels[4] = {k_extend<0>, k_extend<1>, k_extend<2>, k_extend<3>};
+const TraceKernel kShadowKernels[4] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>};
 
 __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
@@ -212,8 +229,182 @@ __global__ void k_resolve(const double* film, int64_t npix, double spp, float* o
     }
 }
 
+// ---------------------------------------------------------------------------- adaptive sampling / NFOR
+
+// Per-pixel running sums of _threadRender (Threads.cpp:551-641): the colour sum
+// and square sum (pixelColor / pixelColorSquare, equal to the adaptive
+// accumulator's colorSum / colorSquareSum) and AdaptiveAccumulator's luminance
+// statistics (Threads.cpp:31-53). Samples are added one at a time in sample
+// order, as the reference does, so every sum is the same FP64 sequence.
+struct PixAcc {
+    double c[3], c2[3];
+    double lum, lum2, lmax;
+};
+// DenoiseHalfAccumulator A/B and the feature sums (Threads.cpp:274-290).
+struct PixNfor {
+    double ca[3], cb[3];
+    double fa[LUZ_NFOR_FEATURES], fb[LUZ_NFOR_FEATURES], fs[LUZ_NFOR_FEATURES], fq[LUZ_NFOR_FEATURES];
+    uint32_t na, nb;
+};
+// Finished NFOR buffers on the device, laid out as LuzNforBuffers.
+struct NforOut {
+    double* color_a;
+    double* color_b;
+    double* color_variance;
+    double* features_a;
+    double* features_b;
+    double* feature_variance;
+};
+
+// Adds the wave's samples of each pixel slot, in sample order, to its sums.
+__global__ void k_accumulate_px(WaveArgs w, PathBuf P, PixAcc* acc, PixNfor* nf)
+{
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= w.pix_count) return;
+    const uint32_t pix = w.pix_list[w.pix_begin + j];
+    PixAcc a = acc[pix];
+    double f[LUZ_NFOR_FEATURES];
+    if (nf) {   // setPrimaryCoordinates (ColorHelper.cpp:734-743)
+        const uint32_t x = pix % (uint32_t)w.width, y = pix / (uint32_t)w.width;
+        f[0] = w.width > 1 ? (double)x / ((double)w.width - 1.0) : 0.0;
+        f[1] = w.height > 1 ? (double)y / ((double)w.height - 1.0) : 0.0;
+    }
+    const int64_t b = j * w.s_count;
+    for (int s = 0; s < w.s_count; s++) {
+        const float4 r = P.rad[b + s], pa = P.pend0[b + s], pb = P.pend1[b + s];
+        const F3 cf = clean((F3{r.x, r.y, r.z} + F3{pa.x, pa.y, pa.z}) + F3{pb.x, pb.y, pb.z});
+        const double c[3] = {(double)cf.x, (double)cf.y, (double)cf.z};
+        if (nf) {
+            const float4 g0 = P.feat[3 * (b + s)], g1 = P.feat[3 * (b + s) + 1], g2 = P.feat[3 * (b + s) + 2];
+            f[2] = g0.x; f[3] = g0.y; f[4] = g0.z; f[5] = g0.w;
+            f[6] = g1.x; f[7] = g1.y; f[8] = g1.z; f[9] = g1.w;
+            f[10] = g2.x;
+            PixNfor& n = nf[pix];
+            const bool half_a = ((uint32_t)(w.s_begin + w.sample_offset + s) & 1u) == 0u;
+            double* hc = half_a ? n.ca : n.cb;
+            double* hf = half_a ? n.fa : n.fb;
+            for (int k = 0; k < 3; k++) hc[k] += c[k];
+            if (half_a) n.na++;
+            else n.nb++;
+            for (int k = 0; k < LUZ_NFOR_FEATURES; k++) {   // addDenoiseFeatureSample (Threads.cpp:274-290)
+                hf[k] += f[k];
+                n.fs[k] += f[k];
+                n.fq[k] += f[k] * f[k];
+            }
+        }
+        for (int k = 0; k < 3; k++) {
+            a.c[k] += c[k];
+            a.c2[k] += c[k] * c[k];
+        }
+        // sampleLuminance: ACEScg luminance in FP64 (ColorManagement.cpp:313-320), 0 if not finite.
+        double l = c[0] * 0.2722287168 + c[1] * 0.6740817658 + c[2] * 0.0536895174;
+        if (!isfinite(l)) l = 0.0;
+        a.lum += l;
+        a.lum2 += l * l;
+        a.lmax = a.lmax < l ? l : a.lmax;
+    }
+    acc[pix] = a;
+}
+
+struct AdaptiveRule {
+    uint32_t max_samples;   // scene sample count
+    uint32_t min_samples;   // min(adaptive minimum, sample count)
+    uint32_t interval;
+    uint32_t dark_min;      // darkMinimumSamples (Threads.cpp:182-192)
+    double threshold;
+    int32_t can_stop;       // adaptiveSamplingCanStop (Threads.cpp:267-273)
+};
+
+// sampleMeanVariance (Threads.cpp:150-161); std::max(0, NaN) is 0.
+__device__ __forceinline__ double mean_variance(double sum, double sq, uint32_t count)
+{
+    if (count <= 1) return 0.0;
+    const double n = (double)count;
+    const double var = (sq - (sum * sum / n)) / (n - 1.0);
+    const double v = var / n;
+    return 0.0 < v ? v : 0.0;
+}
+// confidenceInterval95 (Threads.cpp:163-172)
+__device__ __forceinline__ double ci95(double sum, double sq, uint32_t count)
+{
+    const double mv = mean_variance(sum, sq, count);
+    if (!isfinite(mv)) return __longlong_as_double(0x7ff0000000000000ll);
+    return 1.96 * sqrt(mv);
+}
+// channelConverged (Threads.cpp:174-180)
+__device__ __forceinline__ bool channel_converged(double mean, double ci, double threshold)
+{
+    const double am = fabs(mean);
+    const double target = threshold * (am < 0.02 ? 0.02 : am);
+    return ci <= target;
+}
+// adaptiveSampleConverged (Threads.cpp:194-265)
+__device__ bool adaptive_converged(const AdaptiveRule& R, uint32_t used, const PixAcc& a)
+{
+    if (used >= R.max_samples) return true;
+    if (!R.can_stop) return false;
+    if (used < R.min_samples) return false;
+    if ((used - R.min_samples) % R.interval != 0) return false;
+    if (used <= 1) return false;
+    const double n = (double)used;
+    const double lum_mean = a.lum / n;
+    if (a.lmax < 0.02 && used < R.dark_min) return false;
+    const double lci = ci95(a.lum, a.lum2, used);
+    const double rci = ci95(a.c[0], a.c2[0], used);
+    const double gci = ci95(a.c[1], a.c2[1], used);
+    const double bci = ci95(a.c[2], a.c2[2], used);
+    return channel_converged(lum_mean, lci, R.threshold) && channel_converged(a.c[0] / n, rci, R.threshold)
+        && channel_converged(a.c[1] / n, gci, R.threshold) && channel_converged(a.c[2] / n, bci, R.threshold);
+}
+
+// After a round of `used` samples: finished pixels get their mean colour,
+// sample count and NFOR buffers (storeDenoisePixel, Threads.cpp:343-372); the
+// others go to the next active list.
+__global__ void k_converge(AdaptiveRule R, uint32_t used, const uint32_t* act, uint32_t n_act, uint32_t* next,
+                           uint32_t* next_count, const PixAcc* acc, const PixNfor* nf, NforOut out_nf, float* rgb,
+                           int32_t* used_out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_act;
+    const uint32_t pix = valid ? act[i] : 0u;
+    bool done = true;
+    if (valid) {
+        const PixAcc a = acc[pix];
+        done = adaptive_converged(R, used, a);
+        if (done) {
+            const double n = (double)used;
+            for (int k = 0; k < 3; k++) {
+                const double m = a.c[k] / n;
+                rgb[3 * (int64_t)pix + k] = isfinite(m) ? (float)m : 0.0f;   // cleanColor(pixelColor / samplesUsed)
+            }
+            used_out[pix] = (int32_t)used;
+            if (nf) {
+                const PixNfor& f = nf[pix];
+                const int64_t p3 = 3 * (int64_t)pix, pf = (int64_t)LUZ_NFOR_FEATURES * pix;
+                for (int k = 0; k < 3; k++) {   // meanColor with the whole-pixel mean as fallback
+                    out_nf.color_a[p3 + k] = f.na ? f.ca[k] / (double)f.na : a.c[k] / n;
+                    out_nf.color_b[p3 + k] = f.nb ? f.cb[k] / (double)f.nb : a.c[k] / n;
+                }
+                out_nf.color_variance[pix] = (mean_variance(a.c[0], a.c2[0], used) + mean_variance(a.c[1], a.c2[1], used)
+                                              + mean_variance(a.c[2], a.c2[2], used)) / 3.0;
+                for (int k = 0; k < LUZ_NFOR_FEATURES; k++) {
+                    const double fb = f.fs[k] / n;
+                    out_nf.features_a[pf + k] = f.na ? f.fa[k] / (double)f.na : fb;
+                    out_nf.features_b[pf + k] = f.nb ? f.fb[k] / (double)f.nb : fb;
+                    out_nf.feature_variance[pf + k] = mean_variance(f.fs[k], f.fq[k], used);
+                }
+            }
+        }
+    }
+    const uint32_t slot = warp_append(next_count, valid && !done);
+    if (valid && !done) next[slot] = pix;
+}
+
 // ---------------------------------------------------------------------------- ray batches
 
+// luz_gpu_trace_rays: one ray per thread through the traversal instantiation
+// the extend / shadow kernels use for this scene.
+template <uint32_t F>
 __global__ void k_trace_rays(DScene S, const float* rays, int64_t n, int any, uint32_t seed, const int32_t* vkey,
                              LuzHit* out)
 {
@@ -227,11 +418,12 @@ __global__ void k_trace_rays(DScene S, const float* rays, int64_t n, int any, ui
     else k = Key{base_key(seed, 0, 0, 0), 0, 0};
     VolSample vs{&k, 0.0, false};
     LuzHit o;
+    LocalStack<true> st;
     if (any) {
-        const bool occ = any_hit(S, ray, r[3], r[7], vs);
+        const bool occ = any_hit<F>(S, ray, r[3], r[7], vs, st);
         o = LuzHit{0.f, occ ? 0 : -1, 0, 0.f, 0.f};
     } else {
-        const THit h = closest_hit(S, ray, r[3], r[7], vs);
+        const THit h = closest_hit<F>(S, ray, r[3], r[7], vs, st);
         if (h.obj < 0) {
             o = LuzHit{kInf, -1, -1, 0.f, 0.f};
         } else {
@@ -243,6 +435,9 @@ __global__ void k_trace_rays(DScene S, const float* rays, int64_t n, int any, ui
     }
     out[i] = o;
 }
+
+using RayKernel = void (*)(DScene, const float*, int64_t, int, uint32_t, const int32_t*, LuzHit*);
+const RayKernel kTraceRayKernels[4] = {k_trace_rays<0>, k_trace_rays<1>, k_trace_rays<2>, k_trace_rays<3>};
 
 }  // namespace luz
 
@@ -308,6 +503,7 @@ struct luz_gpu_scene {
     int64_t film_pix = 0;
     int sms = 0;
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
+    TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     template <class T> T* up(const std::vector<T>& v)
@@ -328,9 +524,10 @@ struct luz_gpu_scene {
         pallocs.clear();
         cap = 0;
     }
-    void ensure_paths(int64_t n)
+    void ensure_paths(int64_t n, bool feat = false)
     {
-        if (n <= cap) return;
+        if (n <= cap && (!feat || pb.feat)) return;
+        n = std::max(n, cap);
         free_paths();
         pb.ray_o = palloc<float4>(n);
         pb.ray_d = palloc<float4>(n);
@@ -349,6 +546,7 @@ struct luz_gpu_scene {
         pb.sh_d = palloc<float4>(2 * n);
         pb.sh_x = palloc<int2>(2 * n);
         pb.color = palloc<float4>(n);
+        pb.feat = feat ? palloc<float4>(3 * n) : nullptr;
         cap = n;
     }
     ~luz_gpu_scene()
@@ -404,13 +602,13 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
     const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
     for (int b = 0; b <= w.max_bounces; b++) {
         T.mark(st, 0, true);
-        k_extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
         k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
-        k_shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 2, false);
         launches += 3;
     }
@@ -426,7 +624,7 @@ void check_params(const LuzRenderParams* p)
     if (p->max_bounces < 0 || p->max_bounces >= kMaxBounceSlots)
         throw Status(LUZ_E_INVALID, "Max light bounces must be in [0, 255).");
     if (p->flags & ~(LUZ_RENDER_PROFILE | LUZ_RENDER_COUNT))
-        throw Status(LUZ_E_UNSUPPORTED, "Adaptive sampling and NFOR buffers are not on the GPU path.");
+        throw Status(LUZ_E_UNSUPPORTED, "Unknown render flags.");
     if (p->sample_offset < 0) throw Status(LUZ_E_INVALID, "Sample offset must be non-negative.");
 }
 
@@ -554,6 +752,188 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
     return LUZ_OK;
 }
 
+// Device buffers of one luz_gpu_render_ex call, freed on every exit path.
+struct DeviceScratch {
+    std::vector<void*> ptrs;
+    template <class T> T* get(int64_t n, cudaStream_t st)
+    {
+        T* p = dalloc<T>((std::size_t)n);
+        ptrs.push_back(p);
+        CK(cudaMemsetAsync(p, 0, sizeof(T) * (std::size_t)std::max<int64_t>(n, 1), st));
+        return p;
+    }
+    ~DeviceScratch()
+    {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+// Scene::setAdaptive* validation (src/scene/Scene.cpp:193-222).
+void check_adaptive(const LuzAdaptiveParams* a)
+{
+    if (!a || !a->enabled) return;
+    if (a->min_samples <= 0) throw Status(LUZ_E_INVALID, "Adaptive minimum samples must be positive.");
+    if (a->check_interval <= 0) throw Status(LUZ_E_INVALID, "Adaptive check interval must be positive.");
+    if (!std::isfinite(a->threshold) || a->threshold <= 0.0)
+        throw Status(LUZ_E_INVALID, "Adaptive threshold must be positive.");
+}
+
+// The sample counts after which some pixel may stop: every check point
+// adaptiveSampleConverged can pass (min, min + interval, ... > 1) and spp.
+std::vector<uint32_t> round_ends(const AdaptiveRule& R)
+{
+    std::vector<uint32_t> e;
+    if (R.can_stop)
+        for (uint64_t m = R.min_samples; m < R.max_samples; m += R.interval)
+            if (m > 1) e.push_back((uint32_t)m);
+    e.push_back(R.max_samples);
+    return e;
+}
+
+int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptiveParams* ad, float* rgb_out,
+                 const LuzNforBuffers* nfor, int32_t* samples_out, LuzRenderStats* stats)
+{
+    check_params(p);
+    check_adaptive(ad);
+    if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported with adaptive sampling or NFOR buffers.");
+    CK(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    const int64_t npix = (int64_t)p->width * p->height;
+    if (npix > (int64_t)UINT32_MAX) throw Status(LUZ_E_LIMIT, "Image has too many pixels.");
+
+    AdaptiveRule R{};
+    R.max_samples = (uint32_t)p->spp;
+    const bool enabled = ad && ad->enabled;
+    R.can_stop = enabled && ad->min_samples < p->spp;
+    if (R.can_stop) {
+        R.min_samples = (uint32_t)std::min(ad->min_samples, p->spp);
+        R.interval = (uint32_t)ad->check_interval;
+        R.threshold = ad->threshold;
+        const uint64_t dark = std::max<uint64_t>(256u, (uint64_t)R.min_samples + 3ull * R.interval);
+        R.dark_min = (uint32_t)std::min<uint64_t>(R.max_samples, std::max<uint64_t>(R.min_samples, dark));
+    } else {
+        R.min_samples = R.max_samples;
+        R.interval = 1;
+        R.dark_min = R.max_samples;
+    }
+    const std::vector<uint32_t> ends = round_ends(R);
+    const bool want_nfor = nfor != nullptr;
+
+    DeviceScratch D;
+    PixAcc* acc = D.get<PixAcc>(npix, st);
+    PixNfor* nf = want_nfor ? D.get<PixNfor>(npix, st) : nullptr;
+    NforOut nout{};
+    if (want_nfor) {
+        nout.color_a = D.get<double>(3 * npix, st);
+        nout.color_b = D.get<double>(3 * npix, st);
+        nout.color_variance = D.get<double>(npix, st);
+        nout.features_a = D.get<double>(LUZ_NFOR_FEATURES * npix, st);
+        nout.features_b = D.get<double>(LUZ_NFOR_FEATURES * npix, st);
+        nout.feature_variance = D.get<double>(LUZ_NFOR_FEATURES * npix, st);
+    }
+    uint32_t* act[2] = {D.get<uint32_t>(npix, st), D.get<uint32_t>(npix, st)};
+    uint32_t* act_count = D.get<uint32_t>(2, st);
+    float* d_rgb = D.get<float>(3 * npix, st);
+    int32_t* d_used = D.get<int32_t>(npix, st);
+    {
+        std::vector<uint32_t> all((std::size_t)npix);
+        for (int64_t i = 0; i < npix; i++) all[(std::size_t)i] = (uint32_t)i;
+        CK(cudaMemcpyAsync(act[0], all.data(), sizeof(uint32_t) * (std::size_t)npix, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+
+    WaveArgs w = base_args(s, p);
+    w.half_streams = want_nfor ? 1 : 0;
+    w.nfor = want_nfor ? 1 : 0;
+    uint32_t max_round = 0, prev = 0;
+    for (uint32_t e : ends) {
+        max_round = std::max(max_round, e - prev);
+        prev = e;
+    }
+    const int s_wave = (int)std::min<int64_t>(max_round, kWaveTarget);
+    const int64_t n_wave = std::max<int64_t>(s_wave, std::min<int64_t>(npix * s_wave, kWaveTarget));
+    s->ensure_paths(n_wave, want_nfor);
+    CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
+    CK(cudaEventRecord(s->ev0, st));
+
+    StageTimer T;
+    int64_t launches = 0, waves = 0;
+    double samples = 0.0;
+    uint32_t n_act = (uint32_t)npix, done_to = 0;
+    int cur = 0;
+    for (uint32_t e : ends) {
+        if (n_act == 0) break;
+        const int round = (int)(e - done_to);
+        const int sc_max = std::min(round, s_wave);
+        const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(n_act, kWaveTarget / sc_max));
+        w.pix_list = act[cur];
+        for (int sb = 0; sb < round; sb += sc_max) {          // sample chunks in order: sums stay sequential
+            const int sc = std::min(sc_max, round - sb);
+            for (int64_t pb = 0; pb < n_act; pb += pix_wave) {
+                const int64_t pc = std::min<int64_t>(pix_wave, n_act - pb);
+                w.pix_begin = (int32_t)pb;
+                w.pix_count = (int32_t)pc;
+                w.s_begin = (int32_t)done_to + sb;
+                w.s_count = sc;
+                w.n = pc * sc;
+                w.list_mode = 0;
+                CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+                k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
+                launch_bounces(s, w, st, launches, T);
+                k_accumulate_px<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, acc, nf);
+                k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
+                launches += 3;
+                waves++;
+            }
+        }
+        samples += (double)n_act * round;
+        CK(cudaMemsetAsync(act_count, 0, sizeof(uint32_t), st));
+        k_converge<<<(unsigned)((n_act + 127) / 128), 128, 0, st>>>(R, e, act[cur], n_act, act[cur ^ 1], act_count, acc,
+                                                                  nf, nout, d_rgb, d_used);
+        launches++;
+        CK(cudaMemcpyAsync(&n_act, act_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        cur ^= 1;
+        done_to = e;
+    }
+    if (n_act != 0) throw Status(LUZ_E_DEVICE, "Adaptive sampling left pixels unfinished.");
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    unsigned long long tot[2] = {0, 0};
+    uint32_t err = 0;
+    CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    CK(cudaMemcpy(rgb_out, d_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    if (samples_out) CK(cudaMemcpy(samples_out, d_used, sizeof(int32_t) * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    if (want_nfor) {
+        auto down = [&](double* host, const double* dev, int64_t n) {
+            if (host) CK(cudaMemcpy(host, dev, sizeof(double) * (std::size_t)n, cudaMemcpyDeviceToHost));
+        };
+        down(nfor->color_a, nout.color_a, 3 * npix);
+        down(nfor->color_b, nout.color_b, 3 * npix);
+        down(nfor->color_variance, nout.color_variance, npix);
+        down(nfor->features_a, nout.features_a, LUZ_NFOR_FEATURES * npix);
+        down(nfor->features_b, nout.features_b, LUZ_NFOR_FEATURES * npix);
+        down(nfor->feature_variance, nout.feature_variance, LUZ_NFOR_FEATURES * npix);
+    }
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = samples;
+        stats->extension_rays = (double)tot[0];
+        stats->shadow_rays = (double)tot[1];
+        stats->kernel_launches = launches;
+        stats->waves = waves;
+        stats->extend_launches = waves * (p->max_bounces + 1);
+        stats->shadow_launches = waves * (p->max_bounces + 1);
+    }
+    return LUZ_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------- no-allocation render
@@ -661,9 +1041,9 @@ int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, 
             k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, A.pb, A.ctrl);
             const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
             for (int b = 0; b <= w.max_bounces; b++) {
-                k_extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
+                s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
                 k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, A.pb, A.ctrl, b);
-                k_shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
+                s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
                 launches += 3;
             }
             k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, A.pb, A.film);
@@ -774,9 +1154,12 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         cudaDeviceProp prop;
         CK(cudaGetDeviceProperties(&prop, device));
         s->sms = prop.multiProcessorCount;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, k_extend, kBlock, 0));
+        const int feat = P.consts.features & TF_ALL;
+        s->extend = kExtendKernels[feat];
+        s->shadow = kShadowKernels[feat];
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, s->extend, kBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, k_shade, kBlock, 0));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_sh, k_shadow, kBlock, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_sh, s->shadow, kBlock, 0));
         s->occ_ext = std::max(1, s->occ_ext);
         s->occ_shade = std::max(1, s->occ_shade);
         s->occ_sh = std::max(1, s->occ_sh);
@@ -833,6 +1216,15 @@ int luz_gpu_render(luz_gpu_scene* s, const LuzRenderParams* p, float* rgb_out, L
         }
         cudaFree(d);
         return rc;
+    });
+}
+
+int luz_gpu_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptiveParams* adaptive, float* rgb_out,
+                      const LuzNforBuffers* nfor, int32_t* samples_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !rgb_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_render_ex(s, p, adaptive, rgb_out, nfor, samples_out, stats);
     });
 }
 
@@ -909,7 +1301,8 @@ int luz_gpu_trace_rays(luz_gpu_scene* s, const float* rays, int64_t count, int32
         try {
             CK(cudaMemcpyAsync(dr, rays, sizeof(float) * 8 * count, cudaMemcpyHostToDevice, st));
             if (dk) CK(cudaMemcpyAsync(dk, volume_key, sizeof(int32_t) * 4 * count, cudaMemcpyHostToDevice, st));
-            k_trace_rays<<<(unsigned)((count + 127) / 128), 128, 0, st>>>(s->ds, dr, count, any_hit, seed, dk, dh);
+            kTraceRayKernels[s->ds.k.features & TF_ALL]<<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
+                s->ds, dr, count, any_hit, seed, dk, dh);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(out, dh, sizeof(LuzHit) * count, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));

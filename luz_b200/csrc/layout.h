@@ -198,7 +198,7 @@ struct GSceneConst {
     float background_luminance;
     double light_total_weight;
     int32_t light_cdf_offset; // double cumulative weights; -1 = uniform selection
-    int32_t any_can_transmit;
+    int32_t features;         // traversal specialisation: 1 = has instances, 2 = has volumes
     double meters_per_unit;
     GCamera camera;
     GEnv env;

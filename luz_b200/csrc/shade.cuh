@@ -1105,7 +1105,8 @@ __device__ __noinline__ float light_pdf_value(const DScene& S, const GLight& L, 
         const TRay r = make_ray(origin, ray_dir_normalized(vec));
         float closest = kInf, u, v;
         int32_t slot;
-        if (!mesh_closest(S, M, r, kTMin, closest, slot, u, v, -1, vs)) return 0.0f;
+        LocalStack<true> st;
+        if (!mesh_closest(S, M, r, kTMin, closest, slot, u, v, -1, vs, st)) return 0.0f;
         F3 n, gn;
         bool front;
         float tu, tv;
@@ -1122,7 +1123,8 @@ __device__ __noinline__ float light_pdf_value(const DScene& S, const GLight& L, 
         const TRay r = make_ray(origin, ray_dir_normalized(vec));
         float closest = kInf;
         THit th{kInf, -1, 0, 0.f, 0.f};
-        object_closest(S, L.object, r, kTMin, closest, th, vs);
+        LocalStack<true> st;
+        object_closest<TF_ALL>(S, L.object, r, kTMin, closest, th, vs, st);
         if (th.obj < 0) return 0.0f;
         const Hit h = make_hit(S, r, th);
         const float d2 = th.t * th.t * len2(vec);

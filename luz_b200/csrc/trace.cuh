@@ -45,6 +45,13 @@ struct DScene {
 
 enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u };
 
+// Scene features a traversal kernel is instantiated for (GSceneConst.features).
+// A kernel compiled without a feature never meets that object kind in its
+// scene. (Analytic primitives are always compiled in: an instantiation with
+// meshes as its only kind measured 2.3x slower in the any-hit kernel, at 2.4
+// instead of 6.1 active threads per warp instruction.)
+enum TraceFeature : uint32_t { TF_INSTANCE = 1u, TF_VOLUME = 2u, TF_ALL = 3u };
+
 // xobj / xprim name the primitive a secondary ray leaves from. A ray that
 // starts on a planar primitive cannot meet it again at t > 0 in exact
 // arithmetic (the reference's FP64 hits never do, they fall below T_MIN), so
@@ -54,6 +61,7 @@ enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u };
 struct TRay {
     F3 o, d, inv;
     bool zero;
+    bool axis0;      // some inverse-direction component is 0 (axis-parallel ray)
     int32_t xobj, xprim;
 };
 
@@ -70,6 +78,7 @@ __device__ __forceinline__ TRay make_ray(F3 o, F3 d)
     r.d = d;
     r.inv = F3{inv_component(d.x), inv_component(d.y), inv_component(d.z)};
     r.zero = (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f);
+    r.axis0 = r.inv.x == 0.0f || r.inv.y == 0.0f || r.inv.z == 0.0f;
     r.xobj = -1;
     r.xprim = -1;
     return r;
@@ -107,13 +116,27 @@ struct VolSample {
     }
 };
 
-// boxHitDistance / AABB::hit (Mesh.cpp:99-139, BVHNode.cpp:20-60, AABB.cpp:37-71)
+// boxHitDistance / AABB::hit (Mesh.cpp:99-139, BVHNode.cpp:20-60, AABB.cpp:37-71).
+// For a ray with no zero inverse component the per-axis swap and the running
+// max/min are written as selects (same values as the reference's sequence: the
+// early exit on tmax <= tmin is monotone, so testing once at the end is equal).
 __device__ __forceinline__ bool box_hit(const float* mn, const float* mx, const TRay& r, float tmax, float& tnear)
 {
     if (r.zero) return false;
     float tmin = kTMin;
     const float o[3] = {r.o.x, r.o.y, r.o.z};
     const float iv[3] = {r.inv.x, r.inv.y, r.inv.z};
+    if (!r.axis0) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float t0 = (mn[a] - o[a]) * iv[a];
+            const float t1 = (mx[a] - o[a]) * iv[a];
+            tmin = fmaxf(tmin, fminf(t0, t1));
+            tmax = fminf(tmax, fmaxf(t0, t1));
+        }
+        tnear = tmin;
+        return !(tmax <= tmin);
+    }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const float inv = iv[a];
@@ -124,9 +147,9 @@ __device__ __forceinline__ bool box_hit(const float* mn, const float* mx, const 
         float t0 = (mn[a] - o[a]) * inv;
         float t1 = (mx[a] - o[a]) * inv;
         if (inv < 0.0f) {
-            const float s = t0;
+            const float sw = t0;
             t0 = t1;
-            t1 = s;
+            t1 = sw;
         }
         tmin = t0 > tmin ? t0 : tmin;
         tmax = t1 < tmax ? t1 : tmax;
@@ -175,23 +198,41 @@ __device__ __forceinline__ GNode load_node(const GNode* nodes, uint32_t i)
     return n;
 }
 
+// Mesh traversal stack in the thread's local memory: node or leaf reference
+// and near distance per entry; NEAR = false drops the distances (any-hit never
+// prunes on them). (A variant holding the top 8-32 entries in a shared-memory
+// tile, one bank per thread, measured no faster on B200.)
+template <bool NEAR>
+struct LocalStack {
+    uint32_t r[kMeshStack];
+    float n[NEAR ? kMeshStack : 1];
+    __device__ __forceinline__ void set(int d, uint32_t ref, float near)
+    {
+        r[d] = ref;
+        if constexpr (NEAR) n[d] = near;
+    }
+    __device__ __forceinline__ uint32_t ref(int d) const { return r[d]; }
+    __device__ __forceinline__ float near(int d) const
+    {
+        if constexpr (NEAR) return n[d];
+        else return 0.0f;
+    }
+};
+
 // Mesh::hit — closest triangle; closest is updated in place.
-__device__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
-                             int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs)
+template <class Stk>
+__device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
+                                             int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs, Stk& st)
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, closest, root_near)) return false;
-    uint32_t sref[kMeshStack];
-    float snear[kMeshStack];
     int sp = 0;
-    sref[sp] = (uint32_t)M.root_ref;
-    snear[sp] = root_near;
-    sp++;
+    st.set(sp++, (uint32_t)M.root_ref, root_near);
     bool hit = false;
     while (sp > 0) {
         sp--;
-        const uint32_t ref = sref[sp];
-        if (snear[sp] >= closest) continue;
+        const uint32_t ref = st.ref(sp);
+        if (st.near(sp) >= closest) continue;
         if (ref & kLeafBit) {
             const uint32_t first = (ref & 0x7fffffffu) >> 3;
             const uint32_t cnt = (ref & 7u) + 1u;
@@ -221,32 +262,35 @@ __device__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, flo
         }
         if (hl && hr) {
             if (ln < rn) {
-                sref[sp] = n.rref; snear[sp] = rn; sp++;
-                sref[sp] = n.lref; snear[sp] = ln; sp++;
+                st.set(sp++, n.rref, rn);
+                st.set(sp++, n.lref, ln);
             } else {
-                sref[sp] = n.lref; snear[sp] = ln; sp++;
-                sref[sp] = n.rref; snear[sp] = rn; sp++;
+                st.set(sp++, n.lref, ln);
+                st.set(sp++, n.rref, rn);
             }
         } else if (hl) {
-            sref[sp] = n.lref; snear[sp] = ln; sp++;
+            st.set(sp++, n.lref, ln);
         } else if (hr) {
-            sref[sp] = n.rref; snear[sp] = rn; sp++;
+            st.set(sp++, n.rref, rn);
         }
     }
     return hit;
 }
 
 // Mesh::hitAny
-__device__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax, int32_t skip,
-                         VolSample& vs)
+template <class Stk>
+__device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
+                                         int32_t skip, VolSample& vs, Stk& st)
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, tmax, root_near)) return false;
-    uint32_t sref[kMeshStack];
     int sp = 0;
-    sref[sp++] = (uint32_t)M.root_ref;
+    st.set(sp++, (uint32_t)M.root_ref, 0.f);
+    // One exit at the loop's end (no return from inside the leaf loop), so the
+    // warp reconverges once per popped entry.
+    bool hit = false;
     while (sp > 0) {
-        const uint32_t ref = sref[--sp];
+        const uint32_t ref = st.ref(--sp);
         if (ref & kLeafBit) {
             const uint32_t first = (ref & 0x7fffffffu) >> 3;
             const uint32_t cnt = (ref & 7u) + 1u;
@@ -255,8 +299,12 @@ __device__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float t
                 const GTri T = load_tri(S.tris, i);
                 vs.tris++;
                 float t, u, v;
-                if (tri_test(T, r, tmin, tmax, t, u, v)) return true;
+                if (tri_test(T, r, tmin, tmax, t, u, v)) {
+                    hit = true;
+                    break;
+                }
             }
+            if (hit) break;
             continue;
         }
         const GNode n = load_node(S.nodes, ref);
@@ -266,23 +314,23 @@ __device__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float t
         const bool hr = box_hit(n.rmin, n.rmax, r, tmax, rn);
         if (sp + 2 > kMeshStack) {
             atomicOr(S.error, ERR_MESH_STACK);
-            return false;
+            break;
         }
         if (hl && hr) {
             if (ln < rn) {
-                sref[sp++] = n.rref;
-                sref[sp++] = n.lref;
+                st.set(sp++, n.rref, 0.f);
+                st.set(sp++, n.lref, 0.f);
             } else {
-                sref[sp++] = n.lref;
-                sref[sp++] = n.rref;
+                st.set(sp++, n.lref, 0.f);
+                st.set(sp++, n.rref, 0.f);
             }
         } else if (hl) {
-            sref[sp++] = n.lref;
+            st.set(sp++, n.lref, 0.f);
         } else if (hr) {
-            sref[sp++] = n.rref;
+            st.set(sp++, n.rref, 0.f);
         }
     }
-    return false;
+    return hit;
 }
 
 // Rectangle::hit geometric test (Rectangle.cpp:212-249); returns t.
@@ -448,8 +496,9 @@ __device__ bool volume_distance(const GObject& O, const TRay& r, float tmin, flo
 }
 
 // One object's closest hit; updates closest/hit when it wins.
+template <uint32_t F, class Stk>
 __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, const TRay& r, float tmin, float& closest,
-                                               THit& h, VolSample& vs)
+                                               THit& h, VolSample& vs, Stk& st)
 {
     const GObject O = S.objects[oi];
     vs.top++;
@@ -484,18 +533,19 @@ __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, cons
     case OK_MESH: {
         int32_t slot;
         float u, v;
-        if (mesh_closest(S, S.meshes[O.aux], r, tmin, closest, slot, u, v, src ? r.xprim : -1, vs))
+        if (mesh_closest(S, S.meshes[O.aux], r, tmin, closest, slot, u, v, src ? r.xprim : -1, vs, st))
             h = THit{closest, oi, slot, u, v};
         break;
     }
     case OK_INSTANCE: {
+        if constexpr (!(F & TF_INSTANCE)) break;
         TRay lr;
         float s;
         if (!local_ray(O, r, lr, s)) break;
         float lc = closest * s;
         int32_t slot;
         float u, v;
-        if (!mesh_closest(S, S.meshes[O.aux], lr, tmin * s, lc, slot, u, v, src ? r.xprim : -1, vs)) break;
+        if (!mesh_closest(S, S.meshes[O.aux], lr, tmin * s, lc, slot, u, v, src ? r.xprim : -1, vs, st)) break;
         const float wt = lc / s;
         if (!isfinite(wt) || wt < tmin || wt > closest) break;
         closest = wt;
@@ -503,6 +553,7 @@ __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, cons
         break;
     }
     case OK_VOLUME:
+        if constexpr (!(F & TF_VOLUME)) break;
         if (volume_distance(O, r, tmin, closest, vs, t)) {
             closest = t;
             h = THit{t, oi, 0, 0.f, 0.f};
@@ -513,7 +564,9 @@ __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, cons
     }
 }
 
-__device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TRay& r, float tmin, float tmax, VolSample& vs)
+template <uint32_t F, class Stk>
+__device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TRay& r, float tmin, float tmax, VolSample& vs,
+                                           Stk& st)
 {
     const GObject O = S.objects[oi];
     vs.top++;
@@ -531,14 +584,16 @@ __device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TR
     case OK_PLANE:
         return !src && plane_test(O, r, tmin, tmax, t);
     case OK_MESH:
-        return mesh_any(S, S.meshes[O.aux], r, tmin, tmax, src ? r.xprim : -1, vs);
+        return mesh_any(S, S.meshes[O.aux], r, tmin, tmax, src ? r.xprim : -1, vs, st);
     case OK_INSTANCE: {
+        if constexpr (!(F & TF_INSTANCE)) return false;
         TRay lr;
         float s;
         if (!local_ray(O, r, lr, s)) return false;
-        return mesh_any(S, S.meshes[O.aux], lr, tmin * s, tmax * s, src ? r.xprim : -1, vs);
+        return mesh_any(S, S.meshes[O.aux], lr, tmin * s, tmax * s, src ? r.xprim : -1, vs, st);
     }
     case OK_VOLUME:
+        if constexpr (!(F & TF_VOLUME)) return false;
         return volume_distance(O, r, tmin, tmax, vs, t);
     default:
         return false;
@@ -560,12 +615,13 @@ __device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TR
     } while (0)
 
 // Renderer::internal::_checkHits with explicit [tmin, tmax].
-__device__ THit closest_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs)
+template <uint32_t F, class Stk>
+__device__ __forceinline__ THit closest_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs, Stk& st)
 {
     THit h{kInf, -1, 0, 0.f, 0.f};
     float closest = tmax;
     if (S.k.accel_kind == 2) {
-        object_closest(S, S.k.accel_object, r, tmin, closest, h, vs);
+        object_closest<F>(S, S.k.accel_object, r, tmin, closest, h, vs, st);
     } else if (S.k.accel_kind == 1) {
         uint32_t sref[kTopStack];
         float snear[kTopStack];
@@ -579,7 +635,7 @@ __device__ THit closest_hit(const DScene& S, const TRay& r, float tmin, float tm
             const int32_t idx = (int32_t)(e & 0x3fffffffu);
             if (kind >= 2) {
                 if (kind == 2 && near >= closest) continue;
-                object_closest(S, idx, r, tmin, closest, h, vs);
+                object_closest<F>(S, idx, r, tmin, closest, h, vs, st);
                 continue;
             }
             const GTopNode N = S.top_nodes[idx];
@@ -638,16 +694,19 @@ __device__ THit closest_hit(const DScene& S, const TRay& r, float tmin, float tm
             }
         }
     }
-    for (int i = 0; i < S.k.unaccel_count; i++) object_closest(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, closest, h, vs);
+    for (int i = 0; i < S.k.unaccel_count; i++)
+        object_closest<F>(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, closest, h, vs, st);
     return h;
 }
 
 // isShadowOccluded body with explicit [tmin, tmax] (tmax <= T_MIN -> not occluded).
-__device__ bool any_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs)
+template <uint32_t F, class Stk>
+__device__ __forceinline__ bool any_hit(const DScene& S, const TRay& r, float tmin, float tmax, VolSample& vs, Stk& st)
 {
     if (tmax <= kTMin) return false;
+    bool occ = false;
     if (S.k.accel_kind == 2) {
-        if (object_any(S, S.k.accel_object, r, tmin, tmax, vs)) return true;
+        occ = object_any<F>(S, S.k.accel_object, r, tmin, tmax, vs, st);
     } else if (S.k.accel_kind == 1) {
         uint32_t sref[kTopStack];
         float snear[kTopStack];
@@ -659,7 +718,10 @@ __device__ bool any_hit(const DScene& S, const TRay& r, float tmin, float tmax, 
             const uint32_t kind = e >> 30;
             const int32_t idx = (int32_t)(e & 0x3fffffffu);
             if (kind >= 2) {
-                if (object_any(S, idx, r, tmin, tmax, vs)) return true;
+                if (object_any<F>(S, idx, r, tmin, tmax, vs, st)) {
+                    occ = true;
+                    break;
+                }
                 continue;
             }
             const GTopNode N = S.top_nodes[idx];
@@ -680,9 +742,9 @@ __device__ bool any_hit(const DScene& S, const TRay& r, float tmin, float tmax, 
             }
         }
     }
-    for (int i = 0; i < S.k.unaccel_count; i++)
-        if (object_any(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, tmax, vs)) return true;
-    return false;
+    for (int i = 0; i < S.k.unaccel_count && !occ; i++)
+        occ = object_any<F>(S, S.index_pool[S.k.unaccel_offset + i], r, tmin, tmax, vs, st);
+    return occ;
 }
 
 }  // namespace luz

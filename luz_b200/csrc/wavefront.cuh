@@ -33,6 +33,7 @@ struct PathBuf {
     float4* sh_d;      // xyz direction, w path | slot << 31 (bits)
     int2* sh_x;        // source primitive excluded from the shadow ray
     float4* color;     // per-path final colour
+    float4* feat;      // NFOR primary-vertex features 2..10, 3 float4 per path (NULL unless requested)
 };
 
 struct WaveArgs {
@@ -47,6 +48,9 @@ struct WaveArgs {
     const int32_t* list_y;
     const int32_t* list_s;
     int32_t list_mode;
+    const uint32_t* pix_list;     // pixel of each pixel slot (adaptive rounds); NULL = pix_begin + slot
+    int32_t half_streams;         // NFOR: sample s runs on sampler stream 1 + s % 2
+    int32_t nfor;                 // store primary features in PathBuf.feat
     GCamera cam;
 };
 
@@ -60,7 +64,8 @@ __device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint3
         s = (uint32_t)w.list_s[p];
         return;
     }
-    const uint32_t pix = (uint32_t)w.pix_begin + p / (uint32_t)w.s_count;
+    const uint32_t slot = (uint32_t)w.pix_begin + p / (uint32_t)w.s_count;
+    const uint32_t pix = w.pix_list ? w.pix_list[slot] : slot;
     s = (uint32_t)(w.s_begin + w.sample_offset) + p % (uint32_t)w.s_count;
     x = pix % (uint32_t)w.width;
     y = pix / (uint32_t)w.width;
@@ -68,7 +73,9 @@ __device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint3
 
 __device__ __forceinline__ Key path_key(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, uint32_t bounce)
 {
-    return Key{base_key(w.seed, x, y, w.stream), s, bounce};
+    // _threadRender with denoise buffers: beginPixelSample(x, y, s, s % 2 + 1) (Threads.cpp:593-598).
+    const uint32_t stream = w.half_streams ? 1u + (s & 1u) : w.stream;
+    return Key{base_key(w.seed, x, y, stream), s, bounce};
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -192,7 +199,8 @@ __device__ __noinline__ void relocate_subsurface(const DScene& S, const GMateria
     const float probe = fmaxf(radius + (4.0f * dl / mpu), 16.0f * kTMin);
     const TRay pr = make_ray(cand + n * probe, ray_dir_normalized(n * -1.0f));
     VolSample vs{&k, 0.0, false};
-    const THit th = closest_hit(S, pr, kTMin, kInf, vs);
+    LocalStack<true> st;
+    const THit th = closest_hit<TF_ALL>(S, pr, kTMin, kInf, vs, st);
     if (th.obj < 0) return;
     const Hit eh = make_hit(S, pr, th);
     if (eh.material != h.material || eh.t <= kTMin || eh.t > (2.0f * probe + kTMin)) return;
@@ -215,6 +223,40 @@ struct ShadeOut {
     F3 sh_o[2], sh_d[2];
     float sh_t[2];
 };
+
+// NFOR primary-vertex features (primaryMissFeatures / primaryHitFeatures,
+// src/renderer/ColorHelper.cpp:725-799), entries 2..10; entries 0 and 1 (the
+// pixel coordinates) are formed in FP64 when the samples are accumulated.
+__device__ __forceinline__ float nfor_channel(float v)
+{
+    if (!isfinite(v) || v <= 0.0f) return 0.0f;
+    return (float)fmin(1.0, log1p((double)v) / log1p(1.0e12));   // D_MAX_RAY_COLOR_LUMINANCE
+}
+__device__ __noinline__ void store_miss_features(const PathBuf& P, uint32_t p, F3 sky)
+{
+    P.feat[3 * p] = make_float4(0.0f, 1.0f, 0.5f, 0.5f);
+    P.feat[3 * p + 1] = make_float4(0.5f, nfor_channel(sky.x), nfor_channel(sky.y), nfor_channel(sky.z));
+    P.feat[3 * p + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+__device__ __noinline__ void store_hit_features(const DScene& S, const PathBuf& P, uint32_t p, const Hit& h,
+                                                const GMaterial& m)
+{
+    double nx = h.n.x, ny = h.n.y, nz = h.n.z;
+    const double l2 = nx * nx + ny * ny + nz * nz;
+    if (l2 > 0.0) {
+        const double l = sqrt(l2);
+        nx /= l;
+        ny /= l;
+        nz /= l;
+    }
+    const double t = h.t;
+    const F3 albedo = color_at(S, m, h);
+    P.feat[3 * p] = make_float4(1.0f, t > 0.0 ? (float)(t / (1.0 + t)) : 0.0f, (float)(nx * 0.5 + 0.5),
+                                (float)(ny * 0.5 + 0.5));
+    P.feat[3 * p + 1] = make_float4((float)(nz * 0.5 + 0.5), nfor_channel(albedo.x), nfor_channel(albedo.y),
+                                    nfor_channel(albedo.z));
+    P.feat[3 * p + 2] = make_float4((float)((double)m.type / (double)MT_PRINCIPLED), 0.0f, 0.0f, 0.0f);
+}
 
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
@@ -257,6 +299,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         F3 sky;
         if (need_rad) sky = (env_rad * S.k.env.strength) * env_mis;
         else sky = f3(S.k.background) * env_mis;
+        if (bounce == 0 && w.nfor) store_miss_features(P, p, sky);   // env_mis is 1 at bounce 0
         F3 contrib = thr * sky;
         if (bounce > 0 && S.k.has_constant_background_light) contrib = clamp_bg_miss(S, contrib);
         rad = rad + clamp_ray_color(contrib);
@@ -266,6 +309,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         THit th{h4.x, obj, P.hit_prim[p], h4.y, h4.z};
         Hit h = make_hit(S, ray, th);
         const GMaterial m = S.materials[h.material];
+        if (bounce == 0 && w.nfor) store_hit_features(S, P, p, h, m);
         const F3 emitted = m.type == MT_EMISSIVE ? f3(m.color) : F3{0.f, 0.f, 0.f};
         Scatter sr;
         if (!scatter(S, m, h, ray.d, k, sr)) {

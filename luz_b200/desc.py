@@ -113,6 +113,21 @@ class RenderStats(C.Structure):
     ]
 
 
+class AdaptiveParams(C.Structure):
+    """LuzAdaptiveParams: Scene adaptive settings (src/scene/Scene.cpp:183-222)."""
+    _fields_ = [("enabled", C.c_int32), ("min_samples", C.c_int32), ("check_interval", C.c_int32),
+                ("reserved", C.c_int32), ("threshold", C.c_double)]
+
+
+NFOR_FEATURES = 11
+
+
+class NforBuffers(C.Structure):
+    """LuzNforBuffers: host pointers of the Denoise::NFORBuffers arrays."""
+    _fields_ = [("color_a", C.c_void_p), ("color_b", C.c_void_p), ("color_variance", C.c_void_p),
+                ("features_a", C.c_void_p), ("features_b", C.c_void_p), ("feature_variance", C.c_void_p)]
+
+
 class Hit(C.Structure):
     _fields_ = [("t", C.c_float), ("object", C.c_int32), ("primitive", C.c_int32), ("u", C.c_float), ("v", C.c_float)]
 

@@ -22,7 +22,7 @@ EXPORTED = [
     "luz_gpu_last_error", "luz_gpu_device_count", "luz_pack_create", "luz_pack_destroy", "luz_pack_info",
     "luz_pack_mesh_bvh", "luz_pack_array", "luz_gpu_scene_create", "luz_gpu_scene_destroy", "luz_gpu_scene_info",
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
-    "luz_gpu_render_device_noalloc",
+    "luz_gpu_render_device_noalloc", "luz_gpu_render_ex",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -61,6 +61,8 @@ def lib():
     L.luz_gpu_trace_paths.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, vp, i64, vp]
     L.luz_gpu_trace_rays.argtypes = [vp, vp, i64, i32, C.c_uint32, vp, vp]
     L.luz_gpu_render_device_noalloc.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_render_ex.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams), vp,
+                                    C.POINTER(D.NforBuffers), vp, C.POINTER(D.RenderStats)]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int
     _lib = L
@@ -78,6 +80,11 @@ def device_count() -> int:
     n = C.c_int32(0)
     _check(lib().luz_gpu_device_count(C.byref(n)))
     return n.value
+
+
+def adaptive(min_samples=128, check_interval=32, threshold=0.03, enabled=True) -> D.AdaptiveParams:
+    """Adaptive sampling settings; the defaults are the reference's (include/luz/Defaults.hpp:12-15)."""
+    return D.AdaptiveParams(1 if enabled else 0, int(min_samples), int(check_interval), 0, float(threshold))
 
 
 def params(width, height, spp, max_bounces, seed, stream=0, sample_offset=0) -> D.RenderParams:
@@ -157,6 +164,26 @@ class GpuScene:
         st = D.RenderStats()
         _check(lib().luz_gpu_render(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
         return out, st
+
+    def render_ex(self, p: D.RenderParams, adaptive: Optional[D.AdaptiveParams] = None, nfor: bool = False):
+        """luz_gpu_render_ex: film, samples used per pixel, NFOR buffers (dict, or None) and stats."""
+        h, w = p.height, p.width
+        out = np.zeros((h, w, 3), np.float32)
+        used = np.zeros((h, w), np.int32)
+        st = D.RenderStats()
+        bufs = None
+        nb = None
+        if nfor:
+            bufs = {"color_a": np.zeros((h, w, 3)), "color_b": np.zeros((h, w, 3)),
+                    "color_variance": np.zeros((h, w)),
+                    "features_a": np.zeros((h, w, D.NFOR_FEATURES)), "features_b": np.zeros((h, w, D.NFOR_FEATURES)),
+                    "feature_variance": np.zeros((h, w, D.NFOR_FEATURES))}
+            nb = D.NforBuffers(*[bufs[k].ctypes.data for k in ("color_a", "color_b", "color_variance", "features_a",
+                                                                 "features_b", "feature_variance")])
+        _check(lib().luz_gpu_render_ex(self.h, C.byref(p), C.byref(adaptive) if adaptive is not None else None,
+                                       out.ctypes.data, C.byref(nb) if nb is not None else None, used.ctypes.data,
+                                       C.byref(st)))
+        return out, used, bufs, st
 
     def render_device(self, p: D.RenderParams, out_ptr: int, stream: int = 0) -> D.RenderStats:
         st = D.RenderStats()
