@@ -45,6 +45,9 @@ class RefOracle:
         L.luzref_trace_rays.argtypes = [vp, vp, C.c_int64, C.c_int32, C.c_uint32, vp, vp, vp, vp]
         L.luzref_trace_paths.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp]
         L.luzref_render.argtypes = [vp, vp, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.luzref_trace_samples.argtypes = [vp, vp, C.c_int32, vp, vp, vp, C.c_int64, vp, vp]
+        L.luzref_render_pixels.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, vp, vp,
+                                           C.c_int64, vp, vp, vp]
         L.luzref_mesh_bvh.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int64), vp, C.c_int64]
         L.luzref_mesh_triangle_count.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64)]
         L.luzref_sampler.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32,
@@ -111,6 +114,39 @@ class RefScene:
         self.o._check(self.o.lib.luzref_render(self.h, C.addressof(params), threads, out.ctypes.data,
                                                C.byref(ms), C.byref(ns)))
         return out, ms.value, ns.value
+
+    def trace_samples(self, params, x, y, s, half_streams=False):
+        """Per-sample colour (before cleanColor) and primary features (_calculatePixelSample)."""
+        x = np.ascontiguousarray(x, dtype=np.int32)
+        y = np.ascontiguousarray(y, dtype=np.int32)
+        s = np.ascontiguousarray(s, dtype=np.int32)
+        rgb = np.zeros((x.shape[0], 3), np.float64)
+        feat = np.zeros((x.shape[0], 11), np.float64)
+        self.o._check(self.o.lib.luzref_trace_samples(self.h, C.addressof(params), 1 if half_streams else 0,
+                                                      x.ctypes.data, y.ctypes.data, s.ctypes.data, x.shape[0],
+                                                      rgb.ctypes.data, feat.ctypes.data))
+        return rgb, feat
+
+    def render_pixels(self, params, x, y, adaptive=None, nfor=False):
+        """_threadRender for the listed pixels (Threads.cpp:551-641). adaptive: None or a dict
+        with min_samples, check_interval, threshold. Returns rgb (n,3), samples used (n,) and,
+        with nfor, a dict of the NFORBuffers entries of each pixel."""
+        x = np.ascontiguousarray(x, dtype=np.int32)
+        y = np.ascontiguousarray(y, dtype=np.int32)
+        n = x.shape[0]
+        rgb = np.zeros((n, 3), np.float64)
+        used = np.zeros(n, np.int32)
+        nf = np.zeros((n, 40), np.float64)
+        a = adaptive or {}
+        self.o._check(self.o.lib.luzref_render_pixels(
+            self.h, C.addressof(params), 1 if adaptive else 0, int(a.get("min_samples", 1)),
+            int(a.get("check_interval", 1)), float(a.get("threshold", 1.0)), 1 if nfor else 0, x.ctypes.data,
+            y.ctypes.data, n, rgb.ctypes.data, used.ctypes.data, nf.ctypes.data if nfor else None))
+        bufs = None
+        if nfor:
+            bufs = {"color_a": nf[:, 0:3], "color_b": nf[:, 3:6], "color_variance": nf[:, 6],
+                    "features_a": nf[:, 7:18], "features_b": nf[:, 18:29], "feature_variance": nf[:, 29:40]}
+        return rgb, used, bufs
 
     def mesh_bvh(self, mesh: int):
         from luz_b200.desc import NODE64_DTYPE

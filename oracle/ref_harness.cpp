@@ -39,6 +39,7 @@
 #include "EnvironmentMap.hpp"
 #include "Texture.hpp"
 #include "Sampler.hpp"
+#include "Denoise/NFOR.hpp"
 #include "Random.hpp"
 #include "Defaults.hpp"
 #include "Transform.hpp"
@@ -467,6 +468,93 @@ int luzref_render(void* s, const LuzRenderParams* p, int32_t threads, double* rg
         const SceneRenderStats& st = rs->scene.getRenderStats();
         if (render_ms) *render_ms = st.renderMS;
         if (samples) *samples = (double)st.renderedSamples;
+        return 0;
+    });
+}
+
+/* _calculatePixelSample (src/renderer/ColorHelper.cpp:1119-1126) for explicit
+ * (x, y, sample): colour (before cleanColor) and the 11 primary features. The
+ * sampler stream is params->stream, or 1 + sample % 2 when half_streams != 0
+ * (the denoise half buffers, Threads.cpp:593-598). */
+int luzref_trace_samples(void* s, const LuzRenderParams* p, int32_t half_streams, const int32_t* x,
+                         const int32_t* y, const int32_t* sample, int64_t n, double* rgb_out, double* feat_out)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        configure(rs->scene, LuzSceneDesc{}, p->width, p->height);
+        rs->scene.setMaxLightBounces(p->max_bounces);
+        rs->scene.setSampleCount(p->spp);
+        const auto cam = Renderer::internal::_prepareRenderCamera(rs->scene);
+        Sampler::setRenderSeed(p->seed);
+        for (int64_t i = 0; i < n; i++) {
+            const uint32_t st = half_streams ? 1u + ((uint32_t)sample[i] % 2u) : p->stream;
+            Sampler::beginPixelSample((std::size_t)x[i], (std::size_t)y[i], (uint32_t)sample[i], st);
+            const Renderer::internal::RenderSample r =
+                Renderer::internal::_calculatePixelSample(rs->scene, cam, (std::size_t)x[i], (std::size_t)y[i]);
+            Sampler::endPixelSample();
+            rgb_out[3 * i] = r.color.getRed();
+            rgb_out[3 * i + 1] = r.color.getGreen();
+            rgb_out[3 * i + 2] = r.color.getBlue();
+            for (int f = 0; f < 11; f++) feat_out[11 * i + f] = r.features[(std::size_t)f];
+        }
+        return 0;
+    });
+}
+
+/* _threadRender (src/renderer/Threads.cpp:551-641) for listed pixels with the
+ * scene's adaptive settings and, when nfor != 0, its denoise buffers
+ * (Scene::initializeDenoiseBuffers). Per pixel: rgb_out[3] (the stored pixel),
+ * used_out (samples used) and, when nfor_out is given, 40 doubles laid out as
+ * colorA[3], colorB[3], colorVariance, featuresA[11], featuresB[11],
+ * featureVariance[11] (storeDenoisePixel, :343-372). */
+int luzref_render_pixels(void* s, const LuzRenderParams* p, int32_t adaptive, int32_t min_samples,
+                         int32_t check_interval, double threshold, int32_t nfor, const int32_t* x,
+                         const int32_t* y, int64_t n, double* rgb_out, int32_t* used_out, double* nfor_out)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        Scene& scene = rs->scene;
+        configure(scene, LuzSceneDesc{}, p->width, p->height);
+        scene.setMaxLightBounces(p->max_bounces);
+        scene.setSampleCount(p->spp);
+        scene.setAdaptiveSampling(adaptive != 0);
+        if (adaptive) {
+            scene.setAdaptiveMinSamples(min_samples);
+            scene.setAdaptiveCheckInterval(check_interval);
+            scene.setAdaptiveThreshold(threshold);
+        }
+        if (nfor) scene.initializeDenoiseBuffers((std::size_t)p->width, (std::size_t)p->height);
+        else scene.clearDenoiseBuffers();
+        const auto cam = Renderer::internal::_prepareRenderCamera(scene);
+        Sampler::setRenderSeed(p->seed);
+        for (int64_t i = 0; i < n; i++) {
+            const std::size_t px = (std::size_t)x[i], py = (std::size_t)y[i];
+            used_out[i] = (int32_t)Renderer::internal::_threadRender(scene, cam, px, py);
+            const Color c = scene.getImage()->getPixel(px, py);
+            rgb_out[3 * i] = c.getRed();
+            rgb_out[3 * i + 1] = c.getGreen();
+            rgb_out[3 * i + 2] = c.getBlue();
+            if (nfor && nfor_out) {
+                const Denoise::NFORBuffers* b = scene.getDenoiseBuffers();
+                const std::size_t k = b->index(px, py);
+                double* o = nfor_out + 40 * i;
+                const Color ca = b->colorA[k], cb = b->colorB[k];
+                o[0] = ca.getRed();
+                o[1] = ca.getGreen();
+                o[2] = ca.getBlue();
+                o[3] = cb.getRed();
+                o[4] = cb.getGreen();
+                o[5] = cb.getBlue();
+                o[6] = b->colorVariance[k];
+                for (int f = 0; f < 11; f++) {
+                    o[7 + f] = b->featuresA[k][(std::size_t)f];
+                    o[18 + f] = b->featuresB[k][(std::size_t)f];
+                    o[29 + f] = b->featureVariance[k][(std::size_t)f];
+                }
+            }
+        }
+        scene.clearDenoiseBuffers();
+        scene.setAdaptiveSampling(false);
         return 0;
     });
 }

@@ -33,6 +33,15 @@ CASES = {
     "instancing": lambda: scenes.instancing_volumes(64, 36, 4, 16, count=500),
 }
 
+# Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.
+ADAPTIVE_CASES = {
+    "cornell_adaptive": (lambda: scenes.cornell(32, 32, 128, 8),
+                         dict(min_samples=16, check_interval=16, threshold=0.25), False),
+    "tiny_nfor": (lambda: scenes.tiny_mixed(24, 18, 8, 6), None, True),
+    "tiny_adaptive_nfor": (lambda: scenes.tiny_mixed(24, 18, 48, 6),
+                           dict(min_samples=8, check_interval=8, threshold=0.15), True),
+}
+
 BVH_CASES = {
     "box": lambda: scenes.cornell().scene,
     "icosphere3": lambda: scenes.mesh_glossy(level=3).scene,

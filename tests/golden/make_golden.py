@@ -8,7 +8,9 @@ output of the unmodified reference code:
   hits_<case>.npz    _checkHits / isShadowOccluded results   (HitHelper.cpp, ColorHelper.cpp)
   paths_<case>.npz   per-path radiance, calculateLightRaysColor (ColorHelper.cpp)
   image_<case>.npz   Renderer::render film (Raw view, no denoise, no adaptive)
-Usage: python tests/golden/make_golden.py
+  adaptive_<case>.npz _threadRender with adaptive sampling and/or NFOR buffers
+                     (src/renderer/Threads.cpp:551-641): film, samples used, NFORBuffers
+Usage: python tests/golden/make_golden.py [adaptive]   (adaptive: only the adaptive_* files)
 """
 from __future__ import annotations
 
@@ -23,13 +25,30 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import BVH_CASES, CASES, camera_rays, path_keys  # noqa: E402
+from cases import ADAPTIVE_CASES, BVH_CASES, CASES, camera_rays, path_keys  # noqa: E402
 from luz_b200 import native  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
 
+def adaptive_fixtures(o):
+    for name, (fn, ad, nfor) in ADAPTIVE_CASES.items():
+        w = fn()
+        rs = o.scene(w.scene.build())
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        yy, xx = np.mgrid[0:w.height, 0:w.width]
+        rgb, used, bufs = rs.render_pixels(p, xx.ravel(), yy.ravel(), ad, nfor)
+        out = {"rgb": rgb.reshape(w.height, w.width, 3), "used": used.reshape(w.height, w.width)}
+        for k, v in (bufs or {}).items():
+            out[k] = v.reshape((w.height, w.width) + v.shape[1:])
+        np.savez_compressed(os.path.join(HERE, f"adaptive_{name}.npz"), **out)
+        print("golden", name, flush=True)
+
+
 def main():
     o = RefOracle()
+    if sys.argv[1:] == ["adaptive"]:
+        adaptive_fixtures(o)
+        return
     rng = np.random.default_rng(20261203)
     n = 600
     keys = np.stack([rng.integers(0, 2**32, n), rng.integers(0, 4096, n), rng.integers(0, 4096, n),
@@ -69,6 +88,7 @@ def main():
             img, _, _ = rs.render(p, os.cpu_count() or 1)
             np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
         print("golden", name, flush=True)
+    adaptive_fixtures(o)
 
 
 if __name__ == "__main__":
