@@ -314,10 +314,47 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """--workload batch48: 48 independent scenes (scenes.batch_workloads) rendered one
+    luz_gpu_render after another, then as one luz_gpu_batch_render call. Host wall clock
+    around the calls (host films, device->host copies included): an end-to-end figure."""
+    from luz_b200 import native, scenes
+    ws = scenes.batch_workloads(48)
+    gs = [native.GpuScene(w.scene.build()) for w in ws]
+    ps = [native.params(w.width, w.height, w.spp, w.max_bounces, w.seed) for w in ws]
+    samples = float(sum(w.width * w.height * w.spp for w in ws))
+    for _ in range(max(1, args.warmup)):
+        native.batch_render(gs, ps)
+    t_seq, t_bat = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for g, p in zip(gs, ps):
+            g.render(p)
+        t_seq.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        native.batch_render(gs, ps)
+        t_bat.append(time.perf_counter() - t0)
+    tb, ts = statistics.median(t_bat), statistics.median(t_seq)
+    out = {"metric": METRIC, "value": samples / tb / 1e6, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": tb * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+           "timing": "host wall clock around the C ABI calls (e2e, host films)",
+           "config": {"workload": "batch48: 48 scenes, 1e3-1e6 triangles, 128^2-1024^2, 4-256 spp, depth 4-16",
+                      "samples_per_step": samples,
+                      "triangles": int(sum(g.info().mesh_triangles for g in gs))},
+           "sequential": {"value": samples / ts / 1e6, "unit": UNIT, "ms_per_step": ts * 1e3},
+           "batch_speedup": ts / tb}
+    print(json.dumps(out), flush=True)
+    for g in gs:
+        g.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch48":
+        run_batch(args)
     else:
         run_ours(args)
 

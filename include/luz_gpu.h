@@ -285,7 +285,17 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
 int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* params,
                                   float* d_rgb_out, void* stream, LuzRenderStats* stats);
 
-/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
+/* Many independent renders in one call (a batch of scenes, one result each).
+ * Every scene renders on its own stream: all device memory is taken first,
+ * then the waves of every scene are queued, so small scenes overlap on the GPU
+ * instead of each waiting for the previous one. Each result equals
+ * luz_gpu_render(scenes[i], &params[i], rgb_out[i], &stats[i]) bit for bit.
+ * A handle may appear once per batch; params[i].flags must be 0; stats may be
+ * NULL. No counterpart in the reference (it renders one scene per process). */
+int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
+                         float* const* rgb_out, LuzRenderStats* stats);
+
+/* Adaptive sampling settings:/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
  * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),
  * defaults include/luz/Defaults.hpp:12-15 (on, 128, 32, 0.03). */
 typedef struct LuzAdaptiveParams {

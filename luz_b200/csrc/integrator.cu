@@ -67,6 +67,31 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 #define LUZ_SHADOW_MIN_BLOCKS 8
 #endif
 
+// Appends path p to the segment of its shade class; the lanes of vmask with the
+// same class share one atomic (match.any).
+__device__ __forceinline__ void bin_append(uint32_t* bin_count, const PathBuf& P, unsigned vmask, uint32_t cls,
+                                           uint32_t p)
+{
+    const unsigned peers = __match_any_sync(vmask, cls);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(&bin_count[cls], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    P.bins[cls * P.bin_stride + base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = p;
+}
+
+// Path of shade slot i: slots run through the class segments in class order.
+__device__ __forceinline__ uint32_t binned_path(const PathBuf& P, const uint32_t* bin, uint32_t i)
+{
+    uint32_t k = 0, start = 0;
+    while (k < kShadeClasses - 1 && i >= start + bin[k]) {
+        start += bin[k];
+        k++;
+    }
+    return P.bins[k * P.bin_stride + (i - start)];
+}
+
 // Extend and shadow are instantiated per scene feature set (TF_* bits:
 // instances, volumes); a scene without them runs traversal code without the
 // instance transform or the volume sampler, and skips the per-ray sampler key.
@@ -82,6 +107,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= count) break;
         const uint32_t i = base + lane_id();
+        const unsigned vmask = __ballot_sync(0xffffffffu, i < count);
         if (i >= count) continue;
         const uint32_t p = q[i];
         const float4 o = P.ray_o[p], d = P.ray_d[p];
@@ -95,6 +121,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
         const THit h = closest_hit<F>(S, r, kTMin, kInf, vs, st);
         P.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.obj));
         P.hit_prim[p] = h.prim;
+        if (P.bins) bin_append(C->bin[bounce], P, vmask, h.obj < 0 ? 0u : (uint32_t)S.obj_class[h.obj], p);
         if (S.counters) {
             atomicAdd(&S.counters[0], (unsigned long long)vs.nodes);
             atomicAdd(&S.counters[1], (unsigned long long)vs.tris);
@@ -160,7 +187,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DS
         o.sh[0] = o.sh[1] = false;
         uint32_t p = 0;
         if (valid) {
-            p = q[i];
+            p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
             shade_path(S, w, P, p, bounce, o);
         }
         __syncwarp();
@@ -547,6 +574,8 @@ struct luz_gpu_scene {
         pb.sh_x = palloc<int2>(2 * n);
         pb.color = palloc<float4>(n);
         pb.feat = feat ? palloc<float4>(3 * n) : nullptr;
+        pb.bins = palloc<uint32_t>(kShadeClasses * n);
+        pb.bin_stride = (uint32_t)n;
         cap = n;
     }
     ~luz_gpu_scene()
@@ -656,39 +685,61 @@ void finish_wave(luz_gpu_scene* s, cudaStream_t st, LuzRenderStats* acc, int max
     if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
 }
 
-int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStream_t st, LuzRenderStats* stats)
+// One render split in three phases so that a batch can allocate for every
+// scene first (cudaFree synchronises the device), then enqueue every scene on
+// its own stream, then wait: render_prepare / render_enqueue / render_finish.
+struct RenderJob {
+    luz_gpu_scene* s = nullptr;
+    const LuzRenderParams* p = nullptr;
+    float* d_out = nullptr;
+    cudaStream_t st = nullptr;
+    WaveArgs w{};
+    int64_t npix = 0, pix_wave = 0;
+    int s_wave = 0;
+    StageTimer T;
+    unsigned long long* counters = nullptr;
+    int64_t launches = 0, waves = 0;
+};
+
+void render_prepare(RenderJob& J)
 {
+    const LuzRenderParams* p = J.p;
+    luz_gpu_scene* s = J.s;
     check_params(p);
     CK(cudaSetDevice(s->device));
-    WaveArgs w = base_args(s, p);
-    const int64_t npix = (int64_t)p->width * p->height;
-    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, kWaveTarget / 1));
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
-    const int64_t n_wave = pix_wave * s_wave;
-    s->ensure_paths(n_wave);
-    if (s->film_pix < npix) {
+    J.w = base_args(s, p);
+    J.npix = (int64_t)p->width * p->height;
+    J.s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
+    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, kWaveTarget / J.s_wave));
+    s->ensure_paths(J.pix_wave * J.s_wave);
+    if (s->film_pix < J.npix) {
         if (s->film) cudaFree(s->film);
-        s->film = dalloc<double>((std::size_t)(3 * npix));
-        s->film_pix = npix;
+        s->film = nullptr;
+        s->film_pix = 0;
+        s->film = dalloc<double>((std::size_t)(3 * J.npix));
+        s->film_pix = J.npix;
     }
-    LuzRenderStats acc{};
-    StageTimer T;
-    T.on = (p->flags & LUZ_RENDER_PROFILE) != 0;
-    unsigned long long* counters = nullptr;
-    if (p->flags & LUZ_RENDER_COUNT) {
-        counters = dalloc<unsigned long long>(8);
-        CK(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
-    }
-    s->ds.counters = counters;
+    J.T.on = (p->flags & LUZ_RENDER_PROFILE) != 0;
+    if (p->flags & LUZ_RENDER_COUNT) J.counters = dalloc<unsigned long long>(8);
+}
+
+void render_enqueue(RenderJob& J)
+{
+    luz_gpu_scene* s = J.s;
+    const LuzRenderParams* p = J.p;
+    const cudaStream_t st = J.st;
+    WaveArgs& w = J.w;
+    CK(cudaSetDevice(s->device));
+    if (J.counters) CK(cudaMemsetAsync(J.counters, 0, 8 * sizeof(unsigned long long), st));
+    s->ds.counters = J.counters;
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(s->film, 0, sizeof(double) * 3 * npix, st));
+    CK(cudaMemsetAsync(s->film, 0, sizeof(double) * 3 * J.npix, st));
     CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
     CK(cudaEventRecord(s->ev0, st));
-    int64_t launches = 0, waves = 0;
-    for (int sb = 0; sb < p->spp; sb += s_wave) {
-        const int sc = std::min(s_wave, p->spp - sb);
-        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
-            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+    for (int sb = 0; sb < p->spp; sb += J.s_wave) {
+        const int sc = std::min(J.s_wave, p->spp - sb);
+        for (int64_t pb = 0; pb < J.npix; pb += J.pix_wave) {
+            const int64_t pc = std::min<int64_t>(J.pix_wave, J.npix - pb);
             w.pix_begin = (int32_t)pb;
             w.pix_count = (int32_t)pc;
             w.s_begin = sb;
@@ -697,22 +748,31 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
             w.list_mode = 0;
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, launches, T);
+            launch_bounces(s, w, st, J.launches, J.T);
             k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, s->film);
             k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
-            launches += 3;
-            waves++;
-            if (T.on) {
+            J.launches += 3;
+            J.waves++;
+            if (J.T.on) {
                 CK(cudaStreamSynchronize(st));
-                T.collect();
+                J.T.collect();
             }
         }
     }
-    k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(s->film, npix, (double)p->spp, d_out);
-    launches++;
+    k_resolve<<<(unsigned)((J.npix + 255) / 256), 256, 0, st>>>(s->film, J.npix, (double)p->spp, J.d_out);
+    J.launches++;
+    CK(cudaGetLastError());
     CK(cudaEventRecord(s->ev1, st));
+}
+
+void render_finish(RenderJob& J, LuzRenderStats* stats)
+{
+    luz_gpu_scene* s = J.s;
+    const LuzRenderParams* p = J.p;
+    CK(cudaSetDevice(s->device));
     CK(cudaEventSynchronize(s->ev1));
     CK(cudaGetLastError());
+    LuzRenderStats acc{};
     {
         unsigned long long tot[2] = {0, 0};
         uint32_t err = 0;
@@ -726,28 +786,49 @@ int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStre
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->ds.counters = nullptr;
     unsigned long long cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (counters) {
-        CK(cudaMemcpy(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost));
-        cudaFree(counters);
+    if (J.counters) {
+        CK(cudaMemcpy(cnt, J.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+        cudaFree(J.counters);
+        J.counters = nullptr;
         CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
     }
     if (stats) {
         *stats = acc;
         stats->render_ms = ms;
-        stats->samples = (double)npix * p->spp;
-        stats->kernel_launches = launches;
-        stats->waves = waves;
-        stats->extend_ms = T.ms[0];
-        stats->shade_ms = T.ms[1];
-        stats->shadow_ms = T.ms[2];
-        stats->extend_launches = waves * (p->max_bounces + 1);
-        stats->shadow_launches = waves * (p->max_bounces + 1);
+        stats->samples = (double)J.npix * p->spp;
+        stats->kernel_launches = J.launches;
+        stats->waves = J.waves;
+        stats->extend_ms = J.T.ms[0];
+        stats->shade_ms = J.T.ms[1];
+        stats->shadow_ms = J.T.ms[2];
+        stats->extend_launches = J.waves * (p->max_bounces + 1);
+        stats->shadow_launches = J.waves * (p->max_bounces + 1);
         stats->ext_nodes = (double)cnt[0];
         stats->ext_tris = (double)cnt[1];
         stats->ext_top = (double)cnt[2];
         stats->sh_nodes = (double)cnt[3];
         stats->sh_tris = (double)cnt[4];
         stats->sh_top = (double)cnt[5];
+    }
+}
+
+int do_render(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, cudaStream_t st, LuzRenderStats* stats)
+{
+    RenderJob J;
+    J.s = s;
+    J.p = p;
+    J.d_out = d_out;
+    J.st = st;
+    try {
+        render_prepare(J);
+        render_enqueue(J);
+        render_finish(J, stats);
+    } catch (...) {
+        if (J.counters) {
+            cudaFree(J.counters);
+            s->ds.counters = nullptr;
+        }
+        throw;
     }
     return LUZ_OK;
 }
@@ -1140,6 +1221,7 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         d.cdf = s->up(P.cdf);
         d.index_pool = s->up(P.index_pool);
         d.env_texels = reinterpret_cast<const float4*>(s->up(P.env_texels));
+        d.obj_class = s->up(P.obj_class);
         uint32_t* err = dalloc<uint32_t>(1);
         CK(cudaMemset(err, 0, sizeof(uint32_t)));
         s->allocs.push_back(err);
@@ -1216,6 +1298,67 @@ int luz_gpu_render(luz_gpu_scene* s, const LuzRenderParams* p, float* rgb_out, L
         }
         cudaFree(d);
         return rc;
+    });
+}
+
+int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
+                         float* const* rgb_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (count < 0) throw Status(LUZ_E_INVALID, "Batch size must be non-negative.");
+        if (count == 0) return LUZ_OK;
+        if (!scenes || !params || !rgb_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        for (int32_t i = 0; i < count; i++) {
+            if (!scenes[i] || !rgb_out[i]) throw Status(LUZ_E_INVALID, "NULL argument.");
+            if (params[i].flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in a batch.");
+            for (int32_t j = 0; j < i; j++)
+                if (scenes[j] == scenes[i])
+                    throw Status(LUZ_E_INVALID, "A scene handle appears twice in one batch.");
+        }
+        std::vector<RenderJob> jobs((std::size_t)count);
+        std::vector<float*> outs((std::size_t)count, nullptr);
+        auto release = [&] {
+            for (int32_t i = 0; i < count; i++)
+                if (outs[(std::size_t)i]) {
+                    cudaSetDevice(scenes[i]->device);
+                    cudaFree(outs[(std::size_t)i]);
+                }
+        };
+        try {
+            for (int32_t i = 0; i < count; i++) {   // every allocation before any work is queued
+                RenderJob& J = jobs[(std::size_t)i];
+                J.s = scenes[i];
+                J.p = &params[i];
+                J.st = scenes[i]->stream;
+                render_prepare(J);
+                outs[(std::size_t)i] = dalloc<float>((std::size_t)(3 * J.npix));
+                J.d_out = outs[(std::size_t)i];
+            }
+            for (RenderJob& J : jobs) render_enqueue(J);
+            for (int32_t i = 0; i < count; i++) {
+                RenderJob& J = jobs[(std::size_t)i];
+                CK(cudaSetDevice(J.s->device));
+                CK(cudaMemcpyAsync(rgb_out[i], J.d_out, sizeof(float) * 3 * (std::size_t)J.npix, cudaMemcpyDeviceToHost,
+                                   J.st));
+            }
+            for (int32_t i = 0; i < count; i++) {
+                RenderJob& J = jobs[(std::size_t)i];
+                CK(cudaSetDevice(J.s->device));
+                CK(cudaStreamSynchronize(J.st));
+                render_finish(J, stats ? &stats[i] : nullptr);
+            }
+        } catch (...) {
+            for (RenderJob& J : jobs) {
+                if (J.s) {
+                    cudaSetDevice(J.s->device);
+                    cudaStreamSynchronize(J.st);
+                }
+            }
+            release();
+            throw;
+        }
+        release();
+        return LUZ_OK;
     });
 }
 

@@ -1179,6 +1179,14 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
             E.pdf_offset = -1;
         }
     }
+    // Shade binning: the material type (1..7) a hit on each object shades with
+    // (make_hit: a mesh shades with its mesh's material, every other kind with its own).
+    S.obj_class.assign(S.objects.size(), 0);
+    for (std::size_t i = 0; i < S.objects.size(); i++) {
+        const GObject& o = S.objects[i];
+        const int32_t mat = o.kind == OK_MESH ? S.meshes[(std::size_t)o.aux].material : o.material;
+        if (mat >= 0 && (std::size_t)mat < S.materials.size()) S.obj_class[i] = (uint8_t)S.materials[(std::size_t)mat].type;
+    }
     // Traversal kernel specialisation (TraceFeature bits: 1 instances, 2 volumes).
     K.features = 0;
     for (const GObject& o : S.objects) {

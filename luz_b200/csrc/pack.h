@@ -57,6 +57,7 @@ struct ScenePack {
     std::vector<double> cdf;                 // all double CDF / pdf pools
     std::vector<int32_t> index_pool;         // unaccelerated object list, slot maps
     std::vector<float> env_texels;           // float4 per texel
+    std::vector<uint8_t> obj_class;          // per GObject: material type a hit on it shades (shade binning)
     GSceneConst consts{};
     LuzCameraDesc camera{};
     std::vector<int32_t> object_of_desc;     // desc object -> GObject index (-1 = none)

@@ -38,6 +38,7 @@ struct DScene {
     const double* cdf;
     const int32_t* index_pool;
     const float4* env_texels;
+    const uint8_t* obj_class;  // material type a hit on each object shades with (shade binning)
     uint32_t* error;          // device error word (bit flags)
     unsigned long long* counters;   // LUZ_RENDER_COUNT: ext nodes/tris/top, shadow nodes/tris/top
     GSceneConst k;

@@ -7,12 +7,14 @@ namespace luz {
 
 constexpr int kMaxBounceSlots = 256;
 constexpr int kBlock = 128;
+constexpr int kShadeClasses = 8;            // 0 = miss, 1..7 = material type of the hit
 
 struct Ctrl {
     uint32_t count[kMaxBounceSlots + 2];    // extension queue size entering bounce b
     uint32_t shadow[kMaxBounceSlots + 2];   // shadow rays emitted at bounce b
     uint32_t fetch_ext[kMaxBounceSlots + 2];
     uint32_t fetch_sh[kMaxBounceSlots + 2];
+    uint32_t bin[kMaxBounceSlots + 2][kShadeClasses];   // paths of bounce b per shade class
 };
 
 struct PathBuf {
@@ -34,6 +36,9 @@ struct PathBuf {
     int2* sh_x;        // source primitive excluded from the shadow ray
     float4* color;     // per-path final colour
     float4* feat;      // NFOR primary-vertex features 2..10, 3 float4 per path (NULL unless requested)
+    uint32_t* bins;    // kShadeClasses segments of bin_stride paths, filled by extend in hit-class order
+                       // (NULL: shade reads the extension queue as it is)
+    uint32_t bin_stride;
 };
 
 struct WaveArgs {

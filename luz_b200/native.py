@@ -22,7 +22,7 @@ EXPORTED = [
     "luz_gpu_last_error", "luz_gpu_device_count", "luz_pack_create", "luz_pack_destroy", "luz_pack_info",
     "luz_pack_mesh_bvh", "luz_pack_array", "luz_gpu_scene_create", "luz_gpu_scene_destroy", "luz_gpu_scene_info",
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
-    "luz_gpu_render_device_noalloc", "luz_gpu_render_ex",
+    "luz_gpu_render_device_noalloc", "luz_gpu_render_ex", "luz_gpu_batch_render",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -63,6 +63,7 @@ def lib():
     L.luz_gpu_render_device_noalloc.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_render_ex.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams), vp,
                                     C.POINTER(D.NforBuffers), vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_batch_render.argtypes = [vp, vp, i32, vp, vp]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int
     _lib = L
@@ -206,6 +207,21 @@ class GpuScene:
         _check(lib().luz_gpu_trace_rays(self.h, rays.ctypes.data, rays.shape[0], 1 if any_hit else 0, seed,
                                         None if vk is None else vk.ctypes.data, out.ctypes.data))
         return out
+
+
+def batch_render(scenes, plist):
+    """luz_gpu_batch_render: renders every (scene, params) pair concurrently; returns the
+    films (H x W x 3 each) and the per-scene stats."""
+    n = len(scenes)
+    if len(plist) != n:
+        raise ValueError("one RenderParams per scene")
+    handles = (C.c_void_p * n)(*[g.h.value for g in scenes])
+    ps = (D.RenderParams * n)(*plist)
+    outs = [np.zeros((p.height, p.width, 3), np.float32) for p in plist]
+    optrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+    stats = (D.RenderStats * n)()
+    _check(lib().luz_gpu_batch_render(handles, ps, n, optrs, stats))
+    return outs, list(stats)
 
 
 def render(scene: D.Scene, width: int, height: int, spp: int, max_bounces: int, seed: int, device: int = 0,

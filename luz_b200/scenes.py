@@ -270,6 +270,24 @@ def tiny_mixed(width: int = 24, height: int = 18, spp: int = 4, max_bounces: int
     return Workload("tiny_mixed", s, width, height, spp, max_bounces)
 
 
+def batch_workloads(count: int = 48, seed: int = 4242) -> list:
+    """Many independent scenes for luz_gpu_batch_render: triangle counts log-uniform in
+    [1e3, 1e6] (displaced icospheres of the nearest level), square images with sides
+    log-uniform in [128, 1024], spp log-uniform in [4, 256], max depth uniform in [4, 16]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        tris = float(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        level = int(np.clip(np.round(np.log(tris / 20.0) / np.log(4.0)), 3, 8))
+        side = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        spp = int(np.exp(rng.uniform(np.log(4), np.log(256))))
+        depth = int(rng.integers(4, 17))
+        w = mesh_glossy(side, side, spp, depth, level=level, seed=seed + i)
+        w.name = f"batch{i}"
+        out.append(w)
+    return out
+
+
 WORKLOADS = {
     "cornell": cornell,
     "mesh_glossy": mesh_glossy,

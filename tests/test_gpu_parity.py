@@ -147,3 +147,22 @@ def test_full_size_instancing_frame_properties():
         assert g.info().top_leaf_objects >= 100_000
     finally:
         g.close()
+
+
+@pytest.mark.gpu
+def test_batch_render_equals_individual_renders():
+    """luz_gpu_batch_render: scenes of different sizes rendered concurrently give
+    exactly the films and ray counts of one-at-a-time renders."""
+    ws = [scenes.cornell(48, 40, 3, 8), scenes.tiny_mixed(24, 18, 5, 6),
+          scenes.mesh_glossy(64, 36, 2, 12, level=4), scenes.instancing_volumes(40, 30, 2, 16, count=300)]
+    gs = [native.GpuScene(w.scene.build()) for w in ws]
+    ps = [native.params(w.width, w.height, w.spp, w.max_bounces, w.seed) for w in ws]
+    imgs, stats = native.batch_render(gs, ps)
+    for g, p, img, st in zip(gs, ps, imgs, stats):
+        ref, rst = g.render(p)
+        assert np.array_equal(img, ref)
+        assert st.extension_rays == rst.extension_rays and st.shadow_rays == rst.shadow_rays
+    with pytest.raises(native.LuzError) as e:
+        native.batch_render([gs[0], gs[0]], [ps[0], ps[0]])
+    assert e.value.code == -1
+    assert native.batch_render([], []) == ([], [])
