@@ -126,11 +126,13 @@ def measured_peak():
 
 
 def profile_traffic():
-    """dram bytes per k_extend launch from the committed ncu summary (profiles/), if any."""
-    p = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
+    """DRAM bytes per extension ray of k_extend, from the committed ncu summary (profiles/)."""
+    import re
+    p = os.path.join(ROOT, "profiles", "launches_mesh_glossy_2spp.md")
     if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
+        m = re.search(r"DRAM bytes per extension ray: ([0-9.]+)", open(p).read())
+        if m:
+            return float(m.group(1))
     return None
 
 
@@ -250,12 +252,12 @@ def run_ours(args):
 
     # end to end through the C ABI with a host film (device -> host copy in the timed region)
     e2e_ms = []
-    host = None
+    host = torch.empty((w.height, w.width, 3), dtype=torch.float32, pin_memory=True).numpy()
     for i in range(max(1, min(args.steps, 3))):
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        host, _ = g.render(p)
+        host, _ = g.render(p, out=host)
         if dist is not None:
             ht = torch.from_numpy(host).cuda()
             dist.all_reduce(ht)
@@ -282,9 +284,7 @@ def run_ours(args):
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9 if launch_ms > 0 else None
     peak, peak_kind = measured_peak()
     tr = profile_traffic()
-    traffic = None
-    if tr:
-        traffic = tr.get("bytes_per_launch")
+    traffic = tr * ext_rays / max(1, prof.extend_launches) if tr else None
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -292,7 +292,8 @@ def run_ours(args):
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
                "config": config_of(w, world),
                "e2e": {"value": samples_all / e2 / 1e3, "unit": UNIT, "h2d_bytes_per_step": 32,
-                       "d2h_bytes_per_step": npix * 3 * 4},
+                       "d2h_bytes_per_step": npix * 3 * 4, "ms_per_step": [round(x, 2) for x in e2e_ms],
+                       "host_film": "pinned"},
                "gpu_launches": int(launches),
                "clocks": clk,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -300,7 +301,9 @@ def run_ours(args):
                             "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
                             "algorithmic_bytes_per_ray": alg_bytes / max(1.0, ext_rays),
                             "rays_per_launch": ext_rays / max(1, prof.extend_launches),
-                            "launch_ms": launch_ms},
+                            "launch_ms": launch_ms,
+                            "traffic_source": "ncu dram bytes per extension ray (profiles/launches_mesh_glossy_2spp.md)"
+                                              " x rays per launch"},
                "stages_ms": {"extend": timed.extend_ms, "shade": timed.shade_ms, "shadow": timed.shadow_ms,
                              "total": timed.render_ms},
                "mrays_per_s": (timed.extension_rays + timed.shadow_rays) / timed.render_ms / 1e3 * world}
@@ -349,12 +352,48 @@ def run_batch(args):
         g.close()
 
 
+def run_adjoint(args):
+    """--workload adjoint_c3: albedo-texture gradient of the textured Cornell box (256x256,
+    64 spp, depth 8, 32x32 back-wall texture): Madjoint paths/s = W*H*spp paths replayed per
+    second of luz_gpu_adjoint_backward (both passes), device time from the call's CUDA events."""
+    from luz_b200 import native, scenes
+    w = scenes.cornell_textured(256, 256, 64, 8)
+    g = native.GpuScene(w.scene.build())
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    tex = np.array(w.scene.textures[0])
+    target = scenes.checker_texture()
+    tg = native.GpuScene(scenes.cornell_textured(256, 256, 64, 8, texture=target).scene.build())
+    goal, _ = tg.render(native.params(w.width, w.height, 1024, w.max_bounces, w.seed))
+    for _ in range(max(1, args.warmup)):
+        img, _ = g.adjoint_forward(p, 0, tex)
+        g.adjoint_backward(p, 0, 2.0 * (img - goal) / img.size, tex.shape)
+    fw, bw = [], []
+    for _ in range(args.steps):
+        img, sf = g.adjoint_forward(p, 0, tex)
+        grad, sb = g.adjoint_backward(p, 0, 2.0 * (img - goal) / img.size, tex.shape)
+        fw.append(sf.render_ms)
+        bw.append(sb.render_ms)
+    paths = float(w.width * w.height * w.spp)
+    ms = float(np.mean(bw))
+    out = {"metric": "Madjoint paths/s", "value": paths / ms / 1e3, "unit": "Mpaths/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+           "config": {"workload": "adjoint_c3: textured Cornell 256x256 64spp depth8, 32x32 albedo texture",
+                      "loss": "mean squared error to the 1024-spp checker render"},
+           "forward_ms": float(np.mean(fw)), "grad_norm": float(np.linalg.norm(grad))}
+    print(json.dumps(out), flush=True)
+    g.close()
+    tg.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch48":
         run_batch(args)
+    elif args.workload == "adjoint_c3":
+        run_adjoint(args)
     else:
         run_ours(args)
 

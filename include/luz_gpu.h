@@ -295,6 +295,25 @@ int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* p
 int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
                          float* const* rgb_out, LuzRenderStats* stats);
 
+/* ---- differentiation (albedo textures) ------------------------------------
+ * No counterpart in the reference (it has no gradients); the oracle is central
+ * finite differences of renders with common random numbers. */
+/* Replaces the texels of texture `texture` (its width*height*3 RGB, row 0 =
+ * top, as in LuzTextureDesc) in the device scene. */
+int luz_gpu_scene_set_texture(luz_gpu_scene* scene, int32_t texture, const double* rgb);
+/* Forward pass: set the texture's texels, then luz_gpu_render. */
+int luz_gpu_adjoint_forward(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t texture,
+                            const double* texels, float* rgb_out, LuzRenderStats* stats);
+/* Backward pass: dLoss/dtexel (texture width*height*3, host) for the film of
+ * `params` and dLoss/dpixel = adjoint_rgb (W*H*3, host), by path replay: the
+ * paths are traced once for their radiance and once more to spread each
+ * textured Lambertian vertex's share of it over the bilinear texel weights.
+ * Russian roulette's survival probabilities are treated as constants. Only
+ * Lambertian materials may use the texture (else LUZ_E_UNSUPPORTED).
+ * stats->samples counts the paths replayed. */
+int luz_gpu_adjoint_backward(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t texture,
+                             const float* adjoint_rgb, double* grad_out, LuzRenderStats* stats);
+
 /* Adaptive sampling settings:/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
  * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),
  * defaults include/luz/Defaults.hpp:12-15 (on, 128, 32, 0.03). */

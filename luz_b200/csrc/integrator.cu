@@ -528,6 +528,8 @@ struct luz_gpu_scene {
     unsigned long long* totals = nullptr;   // device: extension / shadow rays of the current render
     double* film = nullptr;
     int64_t film_pix = 0;
+    float* out_dev = nullptr;        // luz_gpu_render: device film of per-pixel means
+    int64_t out_cap = 0;
     int sms = 0;
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
     TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
@@ -582,6 +584,7 @@ struct luz_gpu_scene {
     {
         cudaSetDevice(device);
         free_paths();
+        if (out_dev) cudaFree(out_dev);
         for (void* p : allocs) cudaFree(p);
         if (ctrl) cudaFree(ctrl);
         if (ctrl_host) cudaFreeHost(ctrl_host);
@@ -1015,6 +1018,95 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     return LUZ_OK;
 }
 
+// Replaces the texels of one texture on the device (same size).
+void set_texture(luz_gpu_scene* s, int32_t texture, const double* rgb)
+{
+    const ScenePack& P = *s->pack;
+    if (texture < 0 || (std::size_t)texture >= P.textures.size()) throw Status(LUZ_E_INVALID, "Texture index out of range.");
+    if (!rgb) throw Status(LUZ_E_INVALID, "NULL argument.");
+    const GTexture& T = P.textures[(std::size_t)texture];
+    const int64_t n = (int64_t)T.width * T.height;
+    std::vector<float4> tx((std::size_t)n);
+    for (int64_t k = 0; k < n; k++)
+        tx[(std::size_t)k] = make_float4((float)rgb[3 * k], (float)rgb[3 * k + 1], (float)rgb[3 * k + 2], 0.f);
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpy(const_cast<float4*>(s->ds.texels) + T.offset, tx.data(), sizeof(float4) * (std::size_t)n,
+                  cudaMemcpyHostToDevice));
+}
+
+int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t texture, const float* adj_rgb,
+                        double* grad_out, LuzRenderStats* stats)
+{
+    check_params(p);
+    if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in the adjoint pass.");
+    const ScenePack& PK = *s->pack;
+    if (texture < 0 || (std::size_t)texture >= PK.textures.size()) throw Status(LUZ_E_INVALID, "Texture index out of range.");
+    for (const GMaterial& m : PK.materials)
+        if (m.texture == texture && m.type != MT_LAMBERTIAN)
+            throw Status(LUZ_E_UNSUPPORTED, "Texture gradients are defined for Lambertian albedo textures only.");
+    CK(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    const GTexture& T = PK.textures[(std::size_t)texture];
+    const int64_t npix = (int64_t)p->width * p->height, ntex = (int64_t)T.width * T.height;
+    DeviceScratch D;
+    float* d_adj = D.get<float>(3 * npix, st);
+    double* d_grad = D.get<double>(3 * ntex, st);
+    CK(cudaMemcpyAsync(d_adj, adj_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyHostToDevice, st));
+    WaveArgs w = base_args(s, p);
+    w.grad_texture = texture;
+    w.adj_rgb = d_adj;
+    w.grad = d_grad;
+    w.inv_spp = 1.0 / (double)p->spp;
+    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
+    s->ensure_paths(pix_wave * s_wave);
+    CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(s->ev0, st));
+    StageTimer T0;
+    int64_t launches = 0, waves = 0;
+    for (int sb = 0; sb < p->spp; sb += s_wave) {
+        const int sc = std::min(s_wave, p->spp - sb);
+        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
+            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = sb;
+            w.s_count = sc;
+            w.n = pc * sc;
+            const unsigned grid = (unsigned)((w.n + kBlock - 1) / kBlock);
+            for (int pass = 0; pass < 2; pass++) {   // 0: radiance of every path; 1: replay with gradients
+                w.adjoint = pass;
+                CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+                k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
+                launch_bounces(s, w, st, launches, T0);
+                launches++;
+                if (pass == 0) {
+                    k_path_color<<<grid, kBlock, 0, st>>>(w, s->pb);
+                    launches++;
+                }
+            }
+            waves++;
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    uint32_t err = 0;
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    CK(cudaMemcpy(grad_out, d_grad, sizeof(double) * 3 * (std::size_t)ntex, cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = (double)npix * p->spp;
+        stats->kernel_launches = launches;
+        stats->waves = waves;
+    }
+    return LUZ_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------- no-allocation render
@@ -1287,16 +1379,16 @@ int luz_gpu_render(luz_gpu_scene* s, const LuzRenderParams* p, float* rgb_out, L
         check_params(p);
         CK(cudaSetDevice(s->device));
         const int64_t npix = (int64_t)p->width * p->height;
-        float* d = dalloc<float>((std::size_t)(3 * npix));
-        int rc = LUZ_OK;
-        try {
-            rc = do_render(s, p, d, s->stream, stats);
-            CK(cudaMemcpy(rgb_out, d, sizeof(float) * 3 * npix, cudaMemcpyDeviceToHost));
-        } catch (...) {
-            cudaFree(d);
-            throw;
+        if (s->out_cap < npix) {   // device copy of the film, kept between calls
+            if (s->out_dev) cudaFree(s->out_dev);
+            s->out_dev = nullptr;
+            s->out_cap = 0;
+            s->out_dev = dalloc<float>((std::size_t)(3 * npix));
+            s->out_cap = npix;
         }
-        cudaFree(d);
+        const int rc = do_render(s, p, s->out_dev, s->stream, stats);
+        CK(cudaMemcpyAsync(rgb_out, s->out_dev, sizeof(float) * 3 * npix, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
         return rc;
     });
 }
@@ -1359,6 +1451,36 @@ int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* pa
         }
         release();
         return LUZ_OK;
+    });
+}
+
+int luz_gpu_scene_set_texture(luz_gpu_scene* s, int32_t texture, const double* rgb)
+{
+    return guard([&] {
+        if (!s) throw Status(LUZ_E_INVALID, "NULL argument.");
+        set_texture(s, texture, rgb);
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_adjoint_forward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t texture, const double* texels,
+                            float* rgb_out, LuzRenderStats* stats)
+{
+    if (!s || !texels) {
+        set_error("NULL argument.");
+        return LUZ_E_INVALID;
+    }
+    const int rc = luz_gpu_scene_set_texture(s, texture, texels);
+    if (rc != LUZ_OK) return rc;
+    return luz_gpu_render(s, p, rgb_out, stats);
+}
+
+int luz_gpu_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t texture, const float* adjoint_rgb,
+                             double* grad_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !adjoint_rgb || !grad_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_adjoint_backward(s, p, texture, adjoint_rgb, grad_out, stats);
     });
 }
 

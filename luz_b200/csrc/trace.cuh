@@ -227,53 +227,66 @@ __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, co
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, closest, root_near)) return false;
+    // The entry about to be visited stays in registers (ref, near): a node
+    // visit pushes only the far child and moves on to the near one, which is
+    // the reference's push-far, push-near, pop-near sequence without the round
+    // trip through the stack. sp counts the same entries as the reference's
+    // stack after its pop, so the overflow check fires at the same depth.
+    uint32_t ref = (uint32_t)M.root_ref;
+    float near = root_near;
     int sp = 0;
-    st.set(sp++, (uint32_t)M.root_ref, root_near);
     bool hit = false;
-    while (sp > 0) {
-        sp--;
-        const uint32_t ref = st.ref(sp);
-        if (st.near(sp) >= closest) continue;
-        if (ref & kLeafBit) {
-            const uint32_t first = (ref & 0x7fffffffu) >> 3;
-            const uint32_t cnt = (ref & 7u) + 1u;
-            for (uint32_t i = first; i < first + cnt; i++) {
-                if ((int32_t)i == skip) continue;
-                const GTri T = load_tri(S.tris, i);
-                vs.tris++;
-                float t, u, v;
-                if (tri_test(T, r, tmin, closest, t, u, v)) {
-                    closest = t;
-                    slot = (int32_t)i;
-                    bu = u;
-                    bv = v;
-                    hit = true;
+    while (true) {
+        if (!(near >= closest)) {
+            if (ref & kLeafBit) {
+                const uint32_t first = (ref & 0x7fffffffu) >> 3;
+                const uint32_t cnt = (ref & 7u) + 1u;
+                for (uint32_t i = first; i < first + cnt; i++) {
+                    if ((int32_t)i == skip) continue;
+                    const GTri T = load_tri(S.tris, i);
+                    vs.tris++;
+                    float t, u, v;
+                    if (tri_test(T, r, tmin, closest, t, u, v)) {
+                        closest = t;
+                        slot = (int32_t)i;
+                        bu = u;
+                        bv = v;
+                        hit = true;
+                    }
+                }
+            } else {
+                const GNode n = load_node(S.nodes, ref);
+                vs.nodes++;
+                float ln = 0.f, rn = 0.f;
+                const bool hl = box_hit(n.lmin, n.lmax, r, closest, ln);
+                const bool hr = box_hit(n.rmin, n.rmax, r, closest, rn);
+                if (sp + 2 > kMeshStack) {
+                    atomicOr(S.error, ERR_MESH_STACK);
+                    break;
+                }
+                if (hl && hr) {
+                    if (ln < rn) {
+                        st.set(sp++, n.rref, rn);
+                        ref = n.lref;
+                        near = ln;
+                    } else {
+                        st.set(sp++, n.lref, ln);
+                        ref = n.rref;
+                        near = rn;
+                    }
+                    continue;
+                }
+                if (hl || hr) {
+                    ref = hl ? n.lref : n.rref;
+                    near = hl ? ln : rn;
+                    continue;
                 }
             }
-            continue;
         }
-        const GNode n = load_node(S.nodes, ref);
-        vs.nodes++;
-        float ln = 0.f, rn = 0.f;
-        const bool hl = box_hit(n.lmin, n.lmax, r, closest, ln);
-        const bool hr = box_hit(n.rmin, n.rmax, r, closest, rn);
-        if (sp + 2 > kMeshStack) {
-            atomicOr(S.error, ERR_MESH_STACK);
-            return hit;
-        }
-        if (hl && hr) {
-            if (ln < rn) {
-                st.set(sp++, n.rref, rn);
-                st.set(sp++, n.lref, ln);
-            } else {
-                st.set(sp++, n.lref, ln);
-                st.set(sp++, n.rref, rn);
-            }
-        } else if (hl) {
-            st.set(sp++, n.lref, ln);
-        } else if (hr) {
-            st.set(sp++, n.rref, rn);
-        }
+        if (sp == 0) break;
+        sp--;
+        ref = st.ref(sp);
+        near = st.near(sp);
     }
     return hit;
 }
@@ -285,13 +298,11 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, tmax, root_near)) return false;
+    // Same register-held next entry as mesh_closest.
+    uint32_t ref = (uint32_t)M.root_ref;
     int sp = 0;
-    st.set(sp++, (uint32_t)M.root_ref, 0.f);
-    // One exit at the loop's end (no return from inside the leaf loop), so the
-    // warp reconverges once per popped entry.
     bool hit = false;
-    while (sp > 0) {
-        const uint32_t ref = st.ref(--sp);
+    while (true) {
         if (ref & kLeafBit) {
             const uint32_t first = (ref & 0x7fffffffu) >> 3;
             const uint32_t cnt = (ref & 7u) + 1u;
@@ -306,30 +317,29 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
                 }
             }
             if (hit) break;
-            continue;
-        }
-        const GNode n = load_node(S.nodes, ref);
-        vs.nodes++;
-        float ln = 0.f, rn = 0.f;
-        const bool hl = box_hit(n.lmin, n.lmax, r, tmax, ln);
-        const bool hr = box_hit(n.rmin, n.rmax, r, tmax, rn);
-        if (sp + 2 > kMeshStack) {
-            atomicOr(S.error, ERR_MESH_STACK);
-            break;
-        }
-        if (hl && hr) {
-            if (ln < rn) {
-                st.set(sp++, n.rref, 0.f);
-                st.set(sp++, n.lref, 0.f);
-            } else {
-                st.set(sp++, n.lref, 0.f);
-                st.set(sp++, n.rref, 0.f);
+        } else {
+            const GNode n = load_node(S.nodes, ref);
+            vs.nodes++;
+            float ln = 0.f, rn = 0.f;
+            const bool hl = box_hit(n.lmin, n.lmax, r, tmax, ln);
+            const bool hr = box_hit(n.rmin, n.rmax, r, tmax, rn);
+            if (sp + 2 > kMeshStack) {
+                atomicOr(S.error, ERR_MESH_STACK);
+                break;
             }
-        } else if (hl) {
-            st.set(sp++, n.lref, 0.f);
-        } else if (hr) {
-            st.set(sp++, n.rref, 0.f);
+            if (hl && hr) {
+                const bool lfirst = ln < rn;
+                st.set(sp++, lfirst ? n.rref : n.lref, 0.f);
+                ref = lfirst ? n.lref : n.rref;
+                continue;
+            }
+            if (hl || hr) {
+                ref = hl ? n.lref : n.rref;
+                continue;
+            }
         }
+        if (sp == 0) break;
+        ref = st.ref(--sp);
     }
     return hit;
 }

@@ -56,6 +56,11 @@ struct WaveArgs {
     const uint32_t* pix_list;     // pixel of each pixel slot (adaptive rounds); NULL = pix_begin + slot
     int32_t half_streams;         // NFOR: sample s runs on sampler stream 1 + s % 2
     int32_t nfor;                 // store primary features in PathBuf.feat
+    int32_t adjoint;              // replay pass of luz_gpu_adjoint_backward
+    int32_t grad_texture;         // texture whose texel gradient is accumulated
+    const float* adj_rgb;         // dLoss/dPixel, W*H*3
+    double* grad;                 // dLoss/dTexel, texture W*H*3
+    double inv_spp;
     GCamera cam;
 };
 
@@ -263,6 +268,48 @@ __device__ __noinline__ void store_hit_features(const DScene& S, const PathBuf& 
     P.feat[3 * p + 2] = make_float4((float)((double)m.type / (double)MT_PRINCIPLED), 0.0f, 0.0f, 0.0f);
 }
 
+// Path replay gradient of a Lambertian albedo texture (luz_gpu_adjoint_backward).
+// Everything the path gathers from this vertex on (its NEE and every later
+// vertex) carries the vertex's albedo = colour * clamp01(bilinear(texels)) as
+// one factor per channel, so with L the path's final radiance (stored by the
+// first pass) and `before` what it had gathered before this vertex:
+//   dL/dtexel = (L - before) / bilinear(u, v) * (bilinear weight of the texel)
+// per channel, zero where the clamp is active. The pixel's film is the mean of
+// cleanColor(L) over its samples, so each path adds adj(pixel) / spp times that.
+// Russian roulette's survival probability is held fixed (not differentiated).
+__device__ __noinline__ void adjoint_texture(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
+                                             const Hit& h, F3 before)
+{
+    const float4 L = P.color[p];
+    const uint32_t pix = P.pixel[p];
+    const GTexture T = S.textures[w.grad_texture];
+    const float u = wrap01f(h.u), v = wrap01f(h.v);
+    const float x = u * (float)(T.width - 1);
+    const float y = (1.0f - v) * (float)(T.height - 1);
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    const int x1 = min(x0 + 1, T.width - 1), y1 = min(y0 + 1, T.height - 1);
+    const float tx = x - (float)x0, ty = y - (float)y0;
+    const float4 c00 = __ldg(S.texels + T.offset + y0 * T.width + x0);
+    const float4 c10 = __ldg(S.texels + T.offset + y0 * T.width + x1);
+    const float4 c01 = __ldg(S.texels + T.offset + y1 * T.width + x0);
+    const float4 c11 = __ldg(S.texels + T.offset + y1 * T.width + x1);
+    const F3 top = (F3{c00.x, c00.y, c00.z} * (1.0f - tx)) + (F3{c10.x, c10.y, c10.z} * tx);
+    const F3 bot = (F3{c01.x, c01.y, c01.z} * (1.0f - tx)) + (F3{c11.x, c11.y, c11.z} * tx);
+    const F3 raw = (top * (1.0f - ty)) + (bot * ty);
+    const double wt[4] = {(double)((1.0f - tx) * (1.0f - ty)), (double)(tx * (1.0f - ty)), (double)((1.0f - tx) * ty),
+                          (double)(tx * ty)};
+    const int idx[4] = {y0 * T.width + x0, y0 * T.width + x1, y1 * T.width + x0, y1 * T.width + x1};
+    const float Lc[3] = {L.x, L.y, L.z}, bc[3] = {before.x, before.y, before.z}, rc[3] = {raw.x, raw.y, raw.z};
+    for (int ch = 0; ch < 3; ch++) {
+        if (!(rc[ch] > 0.0f && rc[ch] < 1.0f) || !isfinite(Lc[ch])) continue;
+        const double g = (double)w.adj_rgb[3 * (int64_t)pix + ch] * w.inv_spp * ((double)Lc[ch] - (double)bc[ch])
+                       / (double)rc[ch];
+        if (g == 0.0 || !isfinite(g)) continue;
+        for (int q = 0; q < 4; q++)
+            if (wt[q] != 0.0) atomicAdd(&w.grad[3 * (int64_t)idx[q] + ch], g * wt[q]);
+    }
+}
+
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
     out.cont = false;
@@ -346,6 +393,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
             goto done;
         }
         rad = rad + thr * emitted;
+        if (w.adjoint && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture) adjoint_texture(S, w, P, p, h, rad);
         if (terminated(thr * att)) goto done;
         if (S.k.light_count > 0) {   // estimateDirectLighting (ColorHelper.cpp:973-1033)
             const float prob = direct_prob(bounce);

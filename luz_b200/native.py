@@ -23,6 +23,7 @@ EXPORTED = [
     "luz_pack_mesh_bvh", "luz_pack_array", "luz_gpu_scene_create", "luz_gpu_scene_destroy", "luz_gpu_scene_info",
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
     "luz_gpu_render_device_noalloc", "luz_gpu_render_ex", "luz_gpu_batch_render",
+    "luz_gpu_scene_set_texture", "luz_gpu_adjoint_forward", "luz_gpu_adjoint_backward",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -64,6 +65,9 @@ def lib():
     L.luz_gpu_render_ex.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams), vp,
                                     C.POINTER(D.NforBuffers), vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_batch_render.argtypes = [vp, vp, i32, vp, vp]
+    L.luz_gpu_scene_set_texture.argtypes = [vp, i32, vp]
+    L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int
     _lib = L
@@ -160,8 +164,12 @@ class GpuScene:
         _check(lib().luz_gpu_scene_info(self.h, C.byref(i)))
         return i
 
-    def render(self, p: D.RenderParams) -> Tuple[np.ndarray, D.RenderStats]:
-        out = np.zeros((p.height, p.width, 3), np.float32)
+    def render(self, p: D.RenderParams, out: Optional[np.ndarray] = None) -> Tuple[np.ndarray, D.RenderStats]:
+        """luz_gpu_render into `out` (H x W x 3 float32, C-contiguous, e.g. pinned) or a new array."""
+        if out is None:
+            out = np.zeros((p.height, p.width, 3), np.float32)
+        elif out.dtype != np.float32 or out.shape != (p.height, p.width, 3) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (height, width, 3)")
         st = D.RenderStats()
         _check(lib().luz_gpu_render(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
         return out, st
@@ -185,6 +193,27 @@ class GpuScene:
                                        out.ctypes.data, C.byref(nb) if nb is not None else None, used.ctypes.data,
                                        C.byref(st)))
         return out, used, bufs, st
+
+    def set_texture(self, texture: int, rgb: np.ndarray):
+        rgb = np.ascontiguousarray(rgb, np.float64)
+        _check(lib().luz_gpu_scene_set_texture(self.h, int(texture), rgb.ctypes.data))
+
+    def adjoint_forward(self, p: D.RenderParams, texture: int, texels: np.ndarray):
+        texels = np.ascontiguousarray(texels, np.float64)
+        out = np.zeros((p.height, p.width, 3), np.float32)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_adjoint_forward(self.h, C.byref(p), int(texture), texels.ctypes.data, out.ctypes.data,
+                                             C.byref(st)))
+        return out, st
+
+    def adjoint_backward(self, p: D.RenderParams, texture: int, adjoint_rgb: np.ndarray, tex_shape):
+        """dLoss/dtexel (tex_shape = (height, width, 3)) for dLoss/dpixel = adjoint_rgb (H x W x 3)."""
+        adj = np.ascontiguousarray(adjoint_rgb, np.float32)
+        grad = np.zeros(tex_shape, np.float64)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_adjoint_backward(self.h, C.byref(p), int(texture), adj.ctypes.data, grad.ctypes.data,
+                                              C.byref(st)))
+        return grad, st
 
     def render_device(self, p: D.RenderParams, out_ptr: int, stream: int = 0) -> D.RenderStats:
         st = D.RenderStats()

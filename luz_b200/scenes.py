@@ -151,6 +151,28 @@ def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int
     return Workload("cornell", s, width, height, spp, max_bounces)
 
 
+def checker_texture(size: int = 32, squares: int = 4, lo: float = 0.2, hi: float = 0.8) -> np.ndarray:
+    """size x size x 3 checker of `squares` x `squares` cells (the target of the albedo fit)."""
+    c = (np.arange(size) * squares // size)
+    return np.where(((c[:, None] + c[None, :]) % 2)[..., None] == 0, hi, lo) * np.ones((1, 1, 3))
+
+
+def cornell_textured(width: int = 256, height: int = 256, spp: int = 64, max_bounces: int = 8,
+                     texture: np.ndarray = None, seed: int = 31) -> Workload:
+    """The Cornell box with its back wall's albedo given by a 32 x 32 texture on a white
+    (1, 1, 1) Lambertian (Material::setTexture): the differentiation workload. The
+    texture starts uniform in [0.2, 0.8] unless given; it is texture 0 of the scene."""
+    w = cornell(width, height, spp, max_bounces)
+    s = w.scene
+    if texture is None:
+        texture = np.random.default_rng(seed).uniform(0.2, 0.8, (32, 32, 3))
+    t = s.texture(texture)
+    wall = s.lambertian((1.0, 1.0, 1.0), texture=t)
+    back = [o for o in s.objects if tuple(o["position"]) == (277.5, 277.5, 555.0)]
+    back[0]["material"] = wall
+    return Workload("cornell_textured", s, width, height, spp, max_bounces)
+
+
 def sky_environment(width: int = 1024, height: int = 512, seed: int = 7, sun_peak: float = 5.0e4,
                     sun_diameter_deg: float = 0.5):
     """Equirect RGB sky: zenith-to-horizon gradient, dark ground, seeded sun lobe.

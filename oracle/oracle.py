@@ -11,8 +11,10 @@ module, as the checker. The product (luz_b200) never does.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
+import sys
 from typing import Optional
 
 import numpy as np
@@ -23,6 +25,21 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 def _path(name: str) -> str:
     return os.path.join(REF_DIR, name)
+
+
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """The reference's renderer prints its render statistics on stdout (std::cout); a
+    caller whose stdout carries machine-read output moves them to stderr."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        C.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def reference_available(fast: bool = False) -> bool:
@@ -111,8 +128,10 @@ class RefScene:
         out = np.zeros((params.height, params.width, 3), np.float64)
         ms = C.c_double()
         ns = C.c_double()
-        self.o._check(self.o.lib.luzref_render(self.h, C.addressof(params), threads, out.ctypes.data,
-                                               C.byref(ms), C.byref(ns)))
+        with stdout_to_stderr():
+            rc = self.o.lib.luzref_render(self.h, C.addressof(params), threads, out.ctypes.data, C.byref(ms),
+                                          C.byref(ns))
+        self.o._check(rc)
         return out, ms.value, ns.value
 
     def trace_samples(self, params, x, y, s, half_streams=False):

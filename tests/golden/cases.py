@@ -42,6 +42,17 @@ ADAPTIVE_CASES = {
                            dict(min_samples=8, check_interval=8, threshold=0.15), True),
 }
 
+# Differentiation case: textured Cornell box (texture 0 = back-wall albedo), depth 2
+# (no Russian roulette, so finite differences with common random numbers are exact
+# up to rounding), a seeded adjoint image and the texel channels checked.
+def adjoint_case():
+    w = scenes.cornell_textured(48, 48, 16, 2)
+    rng = np.random.default_rng(77)
+    adj = rng.normal(0.0, 1.0, (w.height, w.width, 3)).astype(np.float32)
+    picks = np.stack([rng.integers(0, 32, 8), rng.integers(0, 32, 8), rng.integers(0, 3, 8)], 1)
+    return w, adj, picks
+
+
 BVH_CASES = {
     "box": lambda: scenes.cornell().scene,
     "icosphere3": lambda: scenes.mesh_glossy(level=3).scene,

@@ -10,7 +10,10 @@ output of the unmodified reference code:
   image_<case>.npz   Renderer::render film (Raw view, no denoise, no adaptive)
   adaptive_<case>.npz _threadRender with adaptive sampling and/or NFOR buffers
                      (src/renderer/Threads.cpp:551-641): film, samples used, NFORBuffers
-Usage: python tests/golden/make_golden.py [adaptive]   (adaptive: only the adaptive_* files)
+  adjoint_cornell.npz central differences of the reference's film functional
+                     sum(adjoint * film) with respect to chosen texel channels
+                     (the reference has no gradients; common random numbers: same seed)
+Usage: python tests/golden/make_golden.py [adaptive|adjoint]   (only those files)
 """
 from __future__ import annotations
 
@@ -25,7 +28,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import ADAPTIVE_CASES, BVH_CASES, CASES, camera_rays, path_keys  # noqa: E402
+from cases import ADAPTIVE_CASES, BVH_CASES, CASES, adjoint_case, camera_rays, path_keys  # noqa: E402
 from luz_b200 import native  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
@@ -44,10 +47,42 @@ def adaptive_fixtures(o):
         print("golden", name, flush=True)
 
 
+def adjoint_fixture(o, h=0.05):
+    w, adj, picks = adjoint_case()
+    tex0 = np.array(w.scene.textures[0])
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    yy, xx = np.mgrid[0:w.height, 0:w.width]
+    S = w.spp
+    x = np.repeat(xx.ravel(), S)
+    y = np.repeat(yy.ravel(), S)
+    s = np.tile(np.arange(S), w.width * w.height)
+
+    def loss(tex):
+        w.scene.textures[0] = tex
+        rs = o.scene(w.scene.build())
+        c = rs.trace_paths(p, x, y, s)
+        c = np.where(np.isfinite(c), c, 0.0).reshape(w.height, w.width, S, 3).mean(axis=2)
+        return float((adj.astype(np.float64) * c).sum())
+
+    fd = []
+    for ty, tx, ch in picks:
+        tp, tm = tex0.copy(), tex0.copy()
+        tp[ty, tx, ch] += h
+        tm[ty, tx, ch] -= h
+        fd.append((loss(tp) - loss(tm)) / (2.0 * h))
+    w.scene.textures[0] = tex0
+    np.savez_compressed(os.path.join(HERE, "adjoint_cornell.npz"), adj=adj, texture=tex0, picks=picks,
+                        fd=np.array(fd), h=h)
+    print("golden adjoint_cornell", flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
         adaptive_fixtures(o)
+        return
+    if sys.argv[1:] == ["adjoint"]:
+        adjoint_fixture(o)
         return
     rng = np.random.default_rng(20261203)
     n = 600
@@ -89,6 +124,7 @@ def main():
             np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
         print("golden", name, flush=True)
     adaptive_fixtures(o)
+    adjoint_fixture(o)
 
 
 if __name__ == "__main__":
