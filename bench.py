@@ -278,7 +278,7 @@ def run_ours(args):
     timed = g.render_device(pt, film.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     ext_rays = prof.extension_rays
-    alg_bytes = 64.0 * prof.ext_nodes + 48.0 * prof.ext_tris + 32.0 * prof.ext_top + 64.0 * ext_rays
+    alg_bytes = 160.0 * prof.ext_nodes + 48.0 * prof.ext_tris + 32.0 * prof.ext_top + 64.0 * ext_rays
     launch_ms = timed.extend_ms / max(1, timed.extend_launches)
     bytes_per_launch = alg_bytes / max(1, prof.extend_launches)
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9 if launch_ms > 0 else None

@@ -1300,7 +1300,7 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         d.objects = s->up(P.objects);
         d.top_nodes = s->up(P.top_nodes);
         d.top_children = s->up(P.top_children);
-        d.nodes = s->up(P.nodes);
+        d.nodes4 = s->up(P.nodes4);
         d.tris = s->up(P.tris);
         d.tri_shade = s->up(P.tri_shade);
         d.vnormals = s->up(P.vnormals);

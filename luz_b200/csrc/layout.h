@@ -17,6 +17,9 @@ namespace luz {
 // T_MIN of include/luz/Defaults.hpp:18 as the nearest float.
 constexpr float kTMin = 0.001f;
 constexpr int kMeshStack = 128;        // MESH_BVH_STACK_SIZE, src/core/Hittables/Mesh.cpp:17
+// Device stack of the collapsed (4-wide) mesh BVH: a node visit pushes up to 3
+// entries, for at most 63 collapsed levels of a depth-126 binary tree.
+constexpr int kMeshStack4 = 192;
 constexpr int kTopStack = 96;
 constexpr uint32_t kLeafBit = 0x80000000u;
 
@@ -79,6 +82,21 @@ struct alignas(16) GNode {
     uint32_t pad0, pad1;
 };
 
+// Collapsed mesh BVH node (160 B): a binary node N together with its two
+// children L and R. It holds the boxes of L and R and of up to four
+// grandchildren: slots 0-1 are L's children (or L itself, slot 1 empty, when L
+// is a leaf), slots 2-3 are R's. A traversal step over it visits exactly the
+// entries the binary near-first traversal would visit after N, L and R, in the
+// same order (see trace.cuh). ref: node4 index, leaf ref, or kEmptySlot.
+constexpr uint32_t kEmptySlot = 0xffffffffu;
+struct alignas(16) GNode4 {
+    float lmin[3], lmax[3];
+    float rmin[3], rmax[3];
+    float cmin[4][3];
+    float cmax[4][3];
+    uint32_t ref[4];
+};
+
 // Triangle in leaf order: v0, e1 = v1 - v0, e2 = v2 - v0 (edges formed in double
 // as Triangle::_updateCache does, src/core/Hittables/Triangle.cpp:94-126).
 struct alignas(16) GTri {
@@ -110,6 +128,8 @@ struct alignas(16) GMesh {
     int32_t material;
     int32_t depth;
     double total_area;
+    int32_t node4_offset;     // first GNode4 of this mesh; -1 when the root is a leaf
+    int32_t root4_ref;        // root reference in the collapsed BVH (node4 index or leaf ref)
 };
 
 // Materials (src/core/Materials/*). 144 B.

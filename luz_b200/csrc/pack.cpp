@@ -560,7 +560,7 @@ int64_t ScenePack::device_bytes() const
 {
     return (int64_t)(rects.size() * sizeof(GRect) + objects.size() * sizeof(GObject)
                      + top_nodes.size() * sizeof(GTopNode) + top_children.size() * sizeof(GTopChild)
-                     + nodes.size() * sizeof(GNode) + tris.size() * sizeof(GTri) + tri_shade.size() * sizeof(GTriShade)
+                     + nodes4.size() * sizeof(GNode4) + tris.size() * sizeof(GTri) + tri_shade.size() * sizeof(GTriShade)
                      + vnormals.size() * 4 + vuvs.size() * 4 + meshes.size() * sizeof(GMesh)
                      + materials.size() * sizeof(GMaterial) + textures.size() * sizeof(GTexture) + texels.size() * 4
                      + lights.size() * sizeof(GLight) + cdf.size() * 8 + index_pool.size() * 4 + env_texels.size() * 4);
@@ -701,6 +701,57 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
             }
             g.node_offset = cnt > 0 ? base : -1;
             g.root_ref = (int32_t)ref_of(0);
+            // Collapse every other level: one GNode4 per binary node N whose
+            // children are visited together with it (preorder, parent first).
+            g.node4_offset = -1;
+            g.root4_ref = g.root_ref;
+            if (cnt > 0) {
+                g.node4_offset = (int32_t)S.nodes4.size();
+                std::function<uint32_t(uint32_t)> collapse = [&](uint32_t bn) -> uint32_t {
+                    const GNode b = S.nodes[bn];
+                    const uint32_t qi = (uint32_t)S.nodes4.size();
+                    S.nodes4.push_back(GNode4{});
+                    GNode4 q{};
+                    for (int a = 0; a < 3; a++) {
+                        q.lmin[a] = b.lmin[a];
+                        q.lmax[a] = b.lmax[a];
+                        q.rmin[a] = b.rmin[a];
+                        q.rmax[a] = b.rmax[a];
+                    }
+                    uint32_t sub[4] = {kEmptySlot, kEmptySlot, kEmptySlot, kEmptySlot};
+                    for (int s = 0; s < 2; s++) {
+                        const uint32_t c = s ? b.rref : b.lref;
+                        const float* cmn = s ? b.rmin : b.lmin;
+                        const float* cmx = s ? b.rmax : b.lmax;
+                        if (c & kLeafBit) {
+                            q.ref[2 * s] = c;
+                            q.ref[2 * s + 1] = kEmptySlot;
+                            for (int a = 0; a < 3; a++) {
+                                q.cmin[2 * s][a] = cmn[a];
+                                q.cmax[2 * s][a] = cmx[a];
+                                q.cmin[2 * s + 1][a] = 0.f;
+                                q.cmax[2 * s + 1][a] = 0.f;
+                            }
+                            continue;
+                        }
+                        const GNode cn = S.nodes[c];
+                        for (int k = 0; k < 2; k++) {
+                            const uint32_t gc = k ? cn.rref : cn.lref;
+                            for (int a = 0; a < 3; a++) {
+                                q.cmin[2 * s + k][a] = k ? cn.rmin[a] : cn.lmin[a];
+                                q.cmax[2 * s + k][a] = k ? cn.rmax[a] : cn.lmax[a];
+                            }
+                            q.ref[2 * s + k] = gc;
+                            if (!(gc & kLeafBit)) sub[2 * s + k] = gc;
+                        }
+                    }
+                    for (int k = 0; k < 4; k++)
+                        if (sub[k] != kEmptySlot) q.ref[k] = collapse(sub[k]);
+                    S.nodes4[qi] = q;
+                    return qi;
+                };
+                g.root4_ref = (int32_t)collapse((uint32_t)g.root_ref);
+            }
             // triangles in leaf order
             const bool vn = !mb.vn.empty();
             const bool uv = !mb.uv.empty();

@@ -44,7 +44,8 @@ struct ScenePack {
     std::vector<GObject> objects;
     std::vector<GTopNode> top_nodes;
     std::vector<GTopChild> top_children;
-    std::vector<GNode> nodes;
+    std::vector<GNode> nodes;                // binary mesh BVH (host: restatement and layout dumps)
+    std::vector<GNode4> nodes4;              // collapsed 4-wide mesh BVH (device traversal)
     std::vector<GTri> tris;
     std::vector<GTriShade> tri_shade;
     std::vector<float> vnormals;             // 9 floats per tri (leaf order) for meshes with normals

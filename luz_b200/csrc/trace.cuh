@@ -25,7 +25,7 @@ struct DScene {
     const GObject* objects;
     const GTopNode* top_nodes;
     const GTopChild* top_children;
-    const GNode* nodes;
+    const GNode4* nodes4;      // collapsed mesh BVH
     const GTri* tris;
     const GTriShade* tri_shade;
     const float* vnormals;
@@ -187,16 +187,81 @@ __device__ __forceinline__ GTri load_tri(const GTri* tris, uint32_t i)
     t.e2[0] = c.x; t.e2[1] = c.y; t.e2[2] = c.z; t.pad = 0;
     return t;
 }
-__device__ __forceinline__ GNode load_node(const GNode* nodes, uint32_t i)
+__device__ __forceinline__ GNode4 load_node4(const GNode4* nodes, uint32_t i)
 {
     const float4* p = reinterpret_cast<const float4*>(nodes + i);
-    const float4 a = ld4(p), b = ld4(p + 1), c = ld4(p + 2), d = ld4(p + 3);
-    GNode n;
-    n.lmin[0] = a.x; n.lmin[1] = a.y; n.lmin[2] = a.z; n.lmax[0] = a.w;
-    n.lmax[1] = b.x; n.lmax[2] = b.y; n.rmin[0] = b.z; n.rmin[1] = b.w;
-    n.rmin[2] = c.x; n.rmax[0] = c.y; n.rmax[1] = c.z; n.rmax[2] = c.w;
-    n.lref = __float_as_uint(d.x); n.rref = __float_as_uint(d.y);
+    float4 v[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) v[k] = ld4(p + k);
+    GNode4 n;
+    float* f = reinterpret_cast<float*>(&n);
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        f[4 * k] = v[k].x;
+        f[4 * k + 1] = v[k].y;
+        f[4 * k + 2] = v[k].z;
+        f[4 * k + 3] = v[k].w;
+    }
     return n;
+}
+
+// Visit order of a collapsed node's entries, as the binary near-first
+// traversal (Mesh::hit, Mesh.cpp:578-660) would reach them: the nearer of L
+// and R first (ties: R), and within each the nearer child first (ties: the
+// right one). ha/na: acceptance and entry distance of the four slots and of
+// L, R. Returns the number of entries written to er/en in visit order.
+//
+// Testing all boxes at N's visit instead of at L's and R's gives the same
+// visits: L is visited right after N (nothing changes `closest` in between),
+// and an entry of R's side that the binary traversal would reject later,
+// because `closest` shrank meanwhile, has near >= closest by then and is
+// pruned when popped. Child boxes lie inside their parent's (the node boxes
+// are unions of their triangles' boxes, rounded outward), so a grandchild's
+// entry distance is never below its parent's and a grandchild of a rejected
+// child is itself rejected.
+__device__ __forceinline__ int node4_order(const GNode4& n, bool hl, float nl, bool hr, float nr, const bool* ha,
+                                           const float* na, uint32_t* er, float* en)
+{
+    int ne = 0;
+    auto add = [&](int k) {
+        er[ne] = n.ref[k];
+        en[ne] = na[k];
+        ne++;
+    };
+    auto side = [&](int s) {
+        const int a = 2 * s, b = 2 * s + 1;
+        if (n.ref[b] == kEmptySlot) {       // leaf child: slot a is the leaf itself
+            if (ha[a]) add(a);
+            return;
+        }
+        if (ha[a] && ha[b]) {
+            if (na[a] < na[b]) {
+                add(a);
+                add(b);
+            } else {
+                add(b);
+                add(a);
+            }
+        } else if (ha[a]) {
+            add(a);
+        } else if (ha[b]) {
+            add(b);
+        }
+    };
+    if (hl && hr) {
+        if (nl < nr) {
+            side(0);
+            side(1);
+        } else {
+            side(1);
+            side(0);
+        }
+    } else if (hl) {
+        side(0);
+    } else if (hr) {
+        side(1);
+    }
+    return ne;
 }
 
 // Mesh traversal stack in the thread's local memory: node or leaf reference
@@ -205,8 +270,8 @@ __device__ __forceinline__ GNode load_node(const GNode* nodes, uint32_t i)
 // tile, one bank per thread, measured no faster on B200.)
 template <bool NEAR>
 struct LocalStack {
-    uint32_t r[kMeshStack];
-    float n[NEAR ? kMeshStack : 1];
+    uint32_t r[kMeshStack4];
+    float n[NEAR ? kMeshStack4 : 1];
     __device__ __forceinline__ void set(int d, uint32_t ref, float near)
     {
         r[d] = ref;
@@ -227,12 +292,11 @@ __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, co
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, closest, root_near)) return false;
-    // The entry about to be visited stays in registers (ref, near): a node
-    // visit pushes only the far child and moves on to the near one, which is
-    // the reference's push-far, push-near, pop-near sequence without the round
-    // trip through the stack. sp counts the same entries as the reference's
-    // stack after its pop, so the overflow check fires at the same depth.
-    uint32_t ref = (uint32_t)M.root_ref;
+    // Walks the collapsed BVH. The entry about to be visited stays in
+    // registers (ref, near); a node visit pushes the other accepted entries in
+    // reverse visit order. Pruning (near >= closest) happens when an entry is
+    // reached, as in the reference.
+    uint32_t ref = (uint32_t)M.root4_ref;
     float near = root_near;
     int sp = 0;
     bool hit = false;
@@ -255,30 +319,29 @@ __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, co
                     }
                 }
             } else {
-                const GNode n = load_node(S.nodes, ref);
+                const GNode4 n = load_node4(S.nodes4, ref);
                 vs.nodes++;
-                float ln = 0.f, rn = 0.f;
-                const bool hl = box_hit(n.lmin, n.lmax, r, closest, ln);
-                const bool hr = box_hit(n.rmin, n.rmax, r, closest, rn);
-                if (sp + 2 > kMeshStack) {
+                float nl = 0.f, nr = 0.f;
+                const bool hl = box_hit(n.lmin, n.lmax, r, closest, nl);
+                const bool hr = box_hit(n.rmin, n.rmax, r, closest, nr);
+                bool ha[4];
+                float na[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    na[k] = 0.f;
+                    ha[k] = n.ref[k] != kEmptySlot && box_hit(n.cmin[k], n.cmax[k], r, closest, na[k]);
+                }
+                uint32_t er[4];
+                float en[4];
+                const int ne = node4_order(n, hl, nl, hr, nr, ha, na, er, en);
+                if (sp + ne > kMeshStack4) {
                     atomicOr(S.error, ERR_MESH_STACK);
                     break;
                 }
-                if (hl && hr) {
-                    if (ln < rn) {
-                        st.set(sp++, n.rref, rn);
-                        ref = n.lref;
-                        near = ln;
-                    } else {
-                        st.set(sp++, n.lref, ln);
-                        ref = n.rref;
-                        near = rn;
-                    }
-                    continue;
-                }
-                if (hl || hr) {
-                    ref = hl ? n.lref : n.rref;
-                    near = hl ? ln : rn;
+                if (ne > 0) {
+                    for (int e = ne - 1; e >= 1; e--) st.set(sp++, er[e], en[e]);
+                    ref = er[0];
+                    near = en[0];
                     continue;
                 }
             }
@@ -298,8 +361,8 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
 {
     float root_near;
     if (!box_hit(M.bmin, M.bmax, r, tmax, root_near)) return false;
-    // Same register-held next entry as mesh_closest.
-    uint32_t ref = (uint32_t)M.root_ref;
+    // Same walk as mesh_closest without pruning (any accepted entry may hold an occluder).
+    uint32_t ref = (uint32_t)M.root4_ref;
     int sp = 0;
     bool hit = false;
     while (true) {
@@ -318,23 +381,28 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
             }
             if (hit) break;
         } else {
-            const GNode n = load_node(S.nodes, ref);
+            const GNode4 n = load_node4(S.nodes4, ref);
             vs.nodes++;
-            float ln = 0.f, rn = 0.f;
-            const bool hl = box_hit(n.lmin, n.lmax, r, tmax, ln);
-            const bool hr = box_hit(n.rmin, n.rmax, r, tmax, rn);
-            if (sp + 2 > kMeshStack) {
+            float nl = 0.f, nr = 0.f;
+            const bool hl = box_hit(n.lmin, n.lmax, r, tmax, nl);
+            const bool hr = box_hit(n.rmin, n.rmax, r, tmax, nr);
+            bool ha[4];
+            float na[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                na[k] = 0.f;
+                ha[k] = n.ref[k] != kEmptySlot && box_hit(n.cmin[k], n.cmax[k], r, tmax, na[k]);
+            }
+            uint32_t er[4];
+            float en[4];
+            const int ne = node4_order(n, hl, nl, hr, nr, ha, na, er, en);
+            if (sp + ne > kMeshStack4) {
                 atomicOr(S.error, ERR_MESH_STACK);
                 break;
             }
-            if (hl && hr) {
-                const bool lfirst = ln < rn;
-                st.set(sp++, lfirst ? n.rref : n.lref, 0.f);
-                ref = lfirst ? n.lref : n.rref;
-                continue;
-            }
-            if (hl || hr) {
-                ref = hl ? n.lref : n.rref;
+            if (ne > 0) {
+                for (int e = ne - 1; e >= 1; e--) st.set(sp++, er[e], 0.f);
+                ref = er[0];
                 continue;
             }
         }
