@@ -52,6 +52,7 @@ extern "C" {
 
 /* Sky types: values equal enum SkyTypes (include/luz/SkyTypes.hpp). */
 #define LUZ_SKY_NONE         0
+#define LUZ_SKY_LINEAR       1   /* white-to-blue gradient, Atmospherics.cpp:44-53 */
 #define LUZ_SKY_ENVIRONMENT  3
 
 /* Scene object kinds (one per reference Hittable class on the path). */
@@ -150,7 +151,7 @@ typedef struct LuzSceneDesc {
     const LuzTextureDesc* textures;
     const LuzMeshDesc* meshes;
     int32_t object_count;         /* objects in Scene::addHittable order            */
-    int32_t sky;                  /* LUZ_SKY_NONE or LUZ_SKY_ENVIRONMENT            */
+    int32_t sky;                  /* LUZ_SKY_NONE, LUZ_SKY_LINEAR or LUZ_SKY_ENVIRONMENT */
     const LuzObjectDesc* objects;
     LuzCameraDesc camera;
     LuzEnvironmentDesc environment;
@@ -159,7 +160,7 @@ typedef struct LuzSceneDesc {
 } LuzSceneDesc;
 
 /* Render settings: the parts of Scene that Renderer::render reads for the
- * sample loop. Adaptive sampling and NFOR buffers are not on this path;
+ * sample loop (adaptive sampling and NFOR buffers: luz_gpu_render_ex);
  * stream selects the Sampler stream (0 = no denoise, Threads.cpp:565).
  * sample_offset shifts the sample indices (resume). flags may hold
  * LUZ_RENDER_PROFILE (per-stage device times) and LUZ_RENDER_COUNT (BVH node /

@@ -48,6 +48,7 @@ struct alignas(16) GObject {
     int32_t material;
     int32_t aux;      // rect index (RECT/CUBE first face), mesh index (MESH/INSTANCE), boundary kind (VOLUME)
     int32_t id;       // index in LuzSceneDesc.objects
+    // RECT: texture coordinates uv0..uv3 (x, y) in f[0..7], f[8] = 1 when set
     // SPHERE: c[3], r, visible
     // PLANE: y, n[3]
     // INSTANCE: pos[3], scale[3], cx, sx, cy, sy, cz, sz

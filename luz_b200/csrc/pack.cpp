@@ -810,9 +810,15 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         switch (o.kind) {
         case LUZ_OBJ_RECTANGLE: {
             mat_type(o.material);
-            if (o.has_uvs) unsupported("Rectangle texture coordinates are not on the GPU path.");
             RectBasis rb;
             g.kind = OK_RECT;
+            if (o.has_uvs) {   // Rectangle::setTextureCoordinates: corners uv0..uv3 (x, y used)
+                for (int c = 0; c < 4; c++) {
+                    g.f[2 * c] = (float)o.uv[3 * c];
+                    g.f[2 * c + 1] = (float)o.uv[3 * c + 1];
+                }
+                g.f[8] = 1.0f;
+            }
             if (o.size[0] <= 0.0 || o.size[1] <= 0.0 || !rect_basis(o, rb)) {
                 hittable = false;   // Rectangle::hit returns false; no bounding box
                 g.aux = -1;
@@ -1149,8 +1155,8 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
     }
 
     // sky / environment
-    if (d->sky != LUZ_SKY_NONE && d->sky != LUZ_SKY_ENVIRONMENT)
-        unsupported("Only SKY_NONE and SKY_ENVIRONMENT skies are on the GPU path.");
+    if (d->sky != LUZ_SKY_NONE && d->sky != LUZ_SKY_LINEAR && d->sky != LUZ_SKY_ENVIRONMENT)
+        unsupported("Only SKY_NONE, SKY_LINEAR and SKY_ENVIRONMENT skies are on the GPU path (not SKY_ATMOSPHERE).");
     K.sky = d->sky;
     for (int a = 0; a < 3; a++) K.background[a] = (float)d->background[a];
     K.background_luminance = (float)luminance(d->background);

@@ -101,6 +101,13 @@ __device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit&
         const F3 dd = h.p - f3(R.p);
         h.u = (dot(dd, f3(R.wa)) / R.w) + 0.5f;
         h.v = (dot(dd, f3(R.ha)) / R.h) + 0.5f;
+        if (O.kind == OK_RECT && O.f[8] != 0.0f) {   // Rectangle::_uvAt: bilinear corners (Rectangle.cpp:64-70, 154-161)
+            const float u = h.u, v = h.v;
+            const float bu = (O.f[0] * (1.0f - u)) + (O.f[2] * u), bv = (O.f[1] * (1.0f - u)) + (O.f[3] * u);
+            const float tu = (O.f[6] * (1.0f - u)) + (O.f[4] * u), tv = (O.f[7] * (1.0f - u)) + (O.f[5] * u);
+            h.u = (bu * (1.0f - v)) + (tu * v);
+            h.v = (bv * (1.0f - v)) + (tv * v);
+        }
         break;
     }
     case OK_SPHERE: {

@@ -349,8 +349,14 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
             env_mis = power_heuristic(prev_pdf, ipdf);
         }
         F3 sky;
-        if (need_rad) sky = (env_rad * S.k.env.strength) * env_mis;
-        else sky = f3(S.k.background) * env_mis;
+        if (S.k.sky == 1) {   // SKY_LINEAR: _calculateSkyInterpolation (Atmospherics.cpp:44-53), skyline 0.5
+            const float tl = 0.5f * ((ray.d.y / sqrtf(len2(ray.d))) + 1.0f);
+            sky = (F3{1.0f, 1.0f, 1.0f} * (1.0f - tl)) + (F3{0.5f, 0.7f, 1.0f} * tl);
+        } else if (need_rad) {
+            sky = (env_rad * S.k.env.strength) * env_mis;
+        } else {
+            sky = f3(S.k.background) * env_mis;
+        }
         if (bounce == 0 && w.nfor) store_miss_features(P, p, sky);   // env_mis is 1 at bounce 0
         F3 contrib = thr * sky;
         if (bounce > 0 && S.k.has_constant_background_light) contrib = clamp_bg_miss(S, contrib);

@@ -23,7 +23,7 @@ MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
 OBJ_RECTANGLE, OBJ_SPHERE, OBJ_CUBE, OBJ_PLANE = 1, 2, 3, 4
 OBJ_MESH, OBJ_MESH_INSTANCE, OBJ_VOLUME, OBJ_DIRECTIONAL_LIGHT = 5, 6, 7, 8
 
-SKY_NONE, SKY_ENVIRONMENT = 0, 3
+SKY_NONE, SKY_LINEAR, SKY_ENVIRONMENT = 0, 1, 3
 
 D3 = C.c_double * 3
 D12 = C.c_double * 12
@@ -240,10 +240,14 @@ class Scene:
         self.objects.append(o)
         return len(self.objects) - 1
 
-    def rectangle(self, position, normal, width, height, material, width_axis=None, height_axis=None):
+    def rectangle(self, position, normal, width, height, material, width_axis=None, height_axis=None, uvs=None):
+        """uvs: optional corner texture coordinates ((u0,v0), (u1,v1), (u2,v2), (u3,v3))
+        (Rectangle::setTextureCoordinates)."""
         kw = {}
         if width_axis is not None:
             kw = dict(has_axes=1, width_axis=width_axis, height_axis=height_axis)
+        if uvs is not None:
+            kw.update(has_uvs=1, uv=tuple(float(c) for uv in uvs for c in (uv[0], uv[1], 0.0)))
         return self._obj(kind=OBJ_RECTANGLE, position=position, orientation=normal, size=(width, height, 0),
                          material=material, **kw)
 

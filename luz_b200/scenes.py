@@ -23,7 +23,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .desc import Camera, Scene
+from .desc import SKY_LINEAR, Camera, Scene
 
 
 @dataclass
@@ -149,6 +149,39 @@ def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int
     s.camera = _pinhole((278.0, 278.0, -800.0), (278.0, 278.0, 0.0), 40.0, width / height)
     s.background = (0.0, 0.0, 0.0)
     return Workload("cornell", s, width, height, spp, max_bounces)
+
+
+def spheres_linear_sky(width: int = 64, height: int = 36, spp: int = 4, max_bounces: int = 12,
+                       count: int = 40, seed: int = 9) -> Workload:
+    """Spheres on a ground sphere under the linear sky (SKY_LINEAR), the kind of scene of
+    the reference's ray-tracing-in-one-weekend example: Lambertian, sharp and rough metal,
+    smooth and rough glass."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    s.sky = SKY_LINEAR
+    s.sphere((0.0, -1000.0, 0.0), 1000.0, s.lambertian((0.5, 0.5, 0.5)))
+    s.sphere((0.0, 1.0, 0.0), 1.0, s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.0))
+    s.sphere((-4.0, 1.0, 0.0), 1.0, s.lambertian((0.4, 0.2, 0.1)))
+    s.sphere((4.0, 1.0, 0.0), 1.0, s.metal((0.7, 0.6, 0.5), roughness=0.0))
+    # a textured panel with explicit corner texture coordinates (rotated, tiled mapping)
+    tex = s.texture(checker_texture(16, 4, 0.15, 0.85) * np.array([1.0, 0.8, 0.6]))
+    s.rectangle((-6.0, 2.0, -4.0), (0.6, 0.0, 0.8), 6.0, 4.0, s.lambertian((1.0, 1.0, 1.0), texture=tex),
+                uvs=((0.0, 0.0), (2.0, 0.5), (1.5, 2.5), (-0.5, 2.0)))
+    for _ in range(count):
+        c = (rng.uniform(-8, 8), 0.2, rng.uniform(-8, 8))
+        k = rng.random()
+        if k < 0.6:
+            m = s.lambertian(tuple(rng.uniform(0.05, 0.9, 3)))
+        elif k < 0.85:
+            m = s.metal(tuple(rng.uniform(0.5, 1.0, 3)), roughness=float(rng.uniform(0.0, 0.5)))
+        else:
+            m = s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=float(rng.choice([0.0, 0.1])))
+        s.sphere(c, 0.2, m)
+    s.camera = Camera(position=(13.0, 2.0, 3.0), direction=(-13.0, -2.0, -3.0), up=(0.0, 1.0, 0.0),
+                      focal_length_m=0.050, sensor_width_m=0.036, sensor_height_m=0.02025, f_number=16.0,
+                      focus_distance_m=10.0)
+    s.background = (0.0, 0.0, 0.0)
+    return Workload("spheres_linear_sky", s, width, height, spp, max_bounces)
 
 
 def checker_texture(size: int = 32, squares: int = 4, lo: float = 0.2, hi: float = 0.8) -> np.ndarray:

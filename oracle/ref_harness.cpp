@@ -278,7 +278,7 @@ RefScene* build(const LuzSceneDesc* d, int tag)
     scene.addCamera(cam);
     scene.setMetersPerUnit(d->meters_per_unit);
     scene.setBackgroundColor(col(d->background));
-    scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT : SKY_NONE);
+    scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT : d->sky == LUZ_SKY_LINEAR ? SKY_LINEAR : SKY_NONE);
     if (d->environment.width > 0) {
         const LuzEnvironmentDesc& e = d->environment;
         std::vector<Color> px((std::size_t)e.width * e.height);

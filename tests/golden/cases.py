@@ -31,6 +31,7 @@ CASES = {
     "tiny": lambda: scenes.tiny_mixed(24, 18, 4, 6),
     "glossy": lambda: scenes.mesh_glossy(96, 54, 4, 12, level=4),
     "instancing": lambda: scenes.instancing_volumes(64, 36, 4, 16, count=500),
+    "linear_sky": lambda: scenes.spheres_linear_sky(64, 36, 4, 12),
 }
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.

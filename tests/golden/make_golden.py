@@ -13,12 +13,13 @@ output of the unmodified reference code:
   adjoint_cornell.npz central differences of the reference's film functional
                      sum(adjoint * film) with respect to chosen texel channels
                      (the reference has no gradients; common random numbers: same seed)
-Usage: python tests/golden/make_golden.py [adaptive|adjoint]   (only those files)
+Usage: python tests/golden/make_golden.py [adaptive | adjoint | cases <name>...]   (only those files)
 """
 from __future__ import annotations
 
 import os
 import sys
+import zlib
 
 import numpy as np
 
@@ -76,6 +77,33 @@ def adjoint_fixture(o, h=0.05):
     print("golden adjoint_cornell", flush=True)
 
 
+def case_fixtures(o, only=None):
+    """hits_/paths_/image_<case>.npz; each case draws from its own seeded generator."""
+    for name, fn in CASES.items():
+        if only is not None and name not in only:
+            continue
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        w = fn()
+        b = w.scene.build()
+        rs = o.scene(b)
+        rt = o.scene(b, tag=True)
+        rays = camera_rays(w, 2000, seed=len(name))
+        vkey = np.stack([rng.integers(0, w.width, 2000), rng.integers(0, w.height, 2000),
+                         rng.integers(0, w.spp, 2000), rng.integers(0, 4, 2000)], 1).astype(np.int32)
+        t, ob, pr = rt.trace_rays(rays.astype(np.float64), seed=w.seed, volume_key=vkey)
+        _, occ, _ = rt.trace_rays(rays.astype(np.float64), any_hit=True, seed=w.seed, volume_key=vkey)
+        np.savez_compressed(os.path.join(HERE, f"hits_{name}.npz"), rays=rays, vkey=vkey, t=t, obj=ob, prim=pr,
+                            occluded=occ >= 0)
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        x, y, s = path_keys(w, 1500, seed=7 + len(name))
+        rgb = rs.trace_paths(p, x, y, s)
+        np.savez_compressed(os.path.join(HERE, f"paths_{name}.npz"), x=x, y=y, s=s, rgb=rgb)
+        if name in ("cornell", "tiny"):
+            img, _, _ = rs.render(p, os.cpu_count() or 1)
+            np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
+        print("golden", name, flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -83,6 +111,9 @@ def main():
         return
     if sys.argv[1:] == ["adjoint"]:
         adjoint_fixture(o)
+        return
+    if sys.argv[1:2] == ["cases"]:     # cases <name>...: only the per-case files of those cases
+        case_fixtures(o, sys.argv[2:])
         return
     rng = np.random.default_rng(20261203)
     n = 600
@@ -103,26 +134,7 @@ def main():
             out[f"order{mi}"] = order
         np.savez_compressed(os.path.join(HERE, f"bvh_{name}.npz"), **out)
 
-    for name, fn in CASES.items():
-        w = fn()
-        b = w.scene.build()
-        rs = o.scene(b)
-        rt = o.scene(b, tag=True)
-        rays = camera_rays(w, 2000, seed=len(name))
-        vkey = np.stack([rng.integers(0, w.width, 2000), rng.integers(0, w.height, 2000),
-                         rng.integers(0, w.spp, 2000), rng.integers(0, 4, 2000)], 1).astype(np.int32)
-        t, ob, pr = rt.trace_rays(rays.astype(np.float64), seed=w.seed, volume_key=vkey)
-        _, occ, _ = rt.trace_rays(rays.astype(np.float64), any_hit=True, seed=w.seed, volume_key=vkey)
-        np.savez_compressed(os.path.join(HERE, f"hits_{name}.npz"), rays=rays, vkey=vkey, t=t, obj=ob, prim=pr,
-                            occluded=occ >= 0)
-        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
-        x, y, s = path_keys(w, 1500, seed=7 + len(name))
-        rgb = rs.trace_paths(p, x, y, s)
-        np.savez_compressed(os.path.join(HERE, f"paths_{name}.npz"), x=x, y=y, s=s, rgb=rgb)
-        if name in ("cornell", "tiny"):
-            img, _, _ = rs.render(p, os.cpu_count() or 1)
-            np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
-        print("golden", name, flush=True)
+    case_fixtures(o)
     adaptive_fixtures(o)
     adjoint_fixture(o)
 
