@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LUZ_GPU_ABI_VERSION 1
+#define LUZ_GPU_ABI_VERSION 2
 
 /* status codes */
 #define LUZ_OK            0
@@ -49,6 +49,8 @@ extern "C" {
 #define LUZ_MAT_ISOTROPIC          5
 #define LUZ_MAT_HENYEY_GREENSTEIN  6
 #define LUZ_MAT_PRINCIPLED         7
+#define LUZ_MAT_GLOSSY             8
+#define LUZ_MAT_DIFFUSE_GLOSSY     9
 
 /* Sky types: values equal enum SkyTypes (include/luz/SkyTypes.hpp). */
 #define LUZ_SKY_NONE         0
@@ -67,7 +69,8 @@ extern "C" {
 
 /* Material parameters; which fields are read depends on type, exactly as the
  * reference constructors/setters (Lambertian.cpp, Metal.cpp, Dielectric.cpp,
- * Emissive.cpp, Isotropic.cpp, HenyeyGreenstein.cpp, Principled.cpp). */
+ * Emissive.cpp, Isotropic.cpp, HenyeyGreenstein.cpp, Principled.cpp,
+ * Glossy.cpp, DiffuseGlossy.cpp). */
 typedef struct LuzMaterialDesc {
     int32_t type;                 /* LUZ_MAT_*                                     */
     int32_t texture;              /* -1 or index into LuzSceneDesc.textures         */
@@ -84,6 +87,8 @@ typedef struct LuzMaterialDesc {
     double  subsurface_radius[3];
     double  subsurface_scale;
     double  subsurface_color[3];
+    double  glossy_color[3];      /* DiffuseGlossy glossy colour (color = diffuse colour) */
+    double  glossy_weight;        /* DiffuseGlossy glossy weight; roughness = glossy roughness */
 } LuzMaterialDesc;
 
 /* Bilinear albedo texture (src/core/Texture.cpp:142-172): width*height RGB, row 0 = top. */

@@ -133,10 +133,10 @@ struct alignas(16) GMesh {
     int32_t root4_ref;        // root reference in the collapsed BVH (node4 index or leaf ref)
 };
 
-// Materials (src/core/Materials/*). 144 B.
+// Materials (src/core/Materials/*). 160 B.
 enum MatType : int32_t {
     MT_LAMBERTIAN = 1, MT_METAL = 2, MT_DIELECTRIC = 3, MT_EMISSIVE = 4, MT_ISOTROPIC = 5, MT_HG = 6,
-    MT_PRINCIPLED = 7
+    MT_PRINCIPLED = 7, MT_GLOSSY = 8, MT_DIFFUSE_GLOSSY = 9
 };
 enum MatFlags : int32_t {
     MF_CONDUCTOR = 1, MF_THIN = 2, MF_SMOOTH_FULL_TRANSMISSION = 4, MF_CAN_TRANSMIT = 8, MF_ABSORPTION = 16
@@ -159,6 +159,8 @@ struct alignas(16) GMaterial {
     float absorption[3], pad5;
     float ss_radius_m[3], pad6;  // subsurface radius * scale (metres)
     float ss_color[3], pad7;     // clampColor01(subsurface colour)
+    float gcolor[3];             // DiffuseGlossy glossy colour
+    float gweight;               // DiffuseGlossy glossy weight
 };
 
 struct GTexture {

@@ -113,7 +113,9 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
         g.absorption[a] = (float)m.absorption[a];
         g.ss_radius_m[a] = (float)(m.subsurface_radius[a] * m.subsurface_scale);
         g.ss_color[a] = (float)clamp01(m.subsurface_color[a]);
+        g.gcolor[a] = (float)m.glossy_color[a];
     }
+    g.gweight = (float)m.glossy_weight;
     g.roughness = (float)m.roughness;
     g.alpha = (float)roughness_to_alpha(m.roughness);
     g.clearcoat_alpha = (float)roughness_to_alpha(m.clearcoat_roughness);
@@ -180,6 +182,13 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
         if (m.metallic <= 1e-6 && m.roughness <= 1e-4 && m.transmission >= 1.0 - 1e-6 && m.clearcoat <= 1e-6
             && m.sheen <= 1e-6 && m.subsurface <= 1e-6)
             g.flags |= MF_SMOOTH_FULL_TRANSMISSION;
+        break;
+    case LUZ_MAT_GLOSSY:
+        check_unit(m.roughness, "Glossy roughness");
+        break;
+    case LUZ_MAT_DIFFUSE_GLOSSY:
+        check_unit(m.glossy_weight, "Diffuse-glossy weight");
+        check_unit(m.roughness, "Diffuse-glossy roughness");
         break;
     default:
         unsupported("Material type " + std::to_string(m.type) + " is not on the GPU path.");

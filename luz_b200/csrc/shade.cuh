@@ -506,6 +506,14 @@ __device__ __noinline__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const 
     }
     case MT_PRINCIPLED:
         return principled_eval(S, m, h, ray_d, dir);
+    case MT_GLOSSY:   // Glossy::evaluateBSDFCos (Glossy.cpp:86-100): GGX lobe tinted by the colour, no Fresnel
+        return ggx_reflection_bsdfcos(clamp_color01(color_at(S, m, h)), h.n, view, dir, m.alpha);
+    case MT_DIFFUSE_GLOSSY: {   // DiffuseGlossy::evaluateBSDFCos (DiffuseGlossy.cpp:144-160)
+        const float nol = dot(h.n, dir);
+        const F3 diffuse = nol <= 0.0f ? F3{0.f, 0.f, 0.f} : clamp_color01(color_at(S, m, h)) * (nol / kPiF);
+        const F3 glossy = ggx_reflection_bsdfcos(clamp_color01(f3(m.gcolor)), h.n, view, dir, m.alpha);
+        return (diffuse * (1.0f - m.gweight)) + (glossy * m.gweight);
+    }
     default:
         return F3{0.f, 0.f, 0.f};
     }
@@ -522,6 +530,13 @@ __device__ __noinline__ float bsdf_pdf(const DScene& S, const GMaterial& m, cons
     }
     case MT_PRINCIPLED:
         return principled_pdf(S, m, h, ray_d, dir);
+    case MT_GLOSSY:
+        return ggx_reflection_pdf(h.n, view, dir, m.alpha);
+    case MT_DIFFUSE_GLOSSY: {   // DiffuseGlossy::scatteringPDF (DiffuseGlossy.cpp:162-176)
+        const float c = dot(h.n, dir);
+        const float dp = c <= 0.0f ? 0.0f : c / kPiF;
+        return (dp * (1.0f - m.gweight)) + (ggx_reflection_pdf(h.n, view, dir, m.alpha) * m.gweight);
+    }
     case MT_LAMBERTIAN: {
         const float c = dot(h.n, dir);
         return c < 0.0f ? 0.0f : c / kPiF;
@@ -623,6 +638,14 @@ __device__ __noinline__ bool scatter(const DScene& S, const GMaterial& m, const 
         F3 dir;
         if (!can || sample1d(k, DIM_MATERIAL_DECISION) < (double)F) dir = reflect(d, hv);
         else dir = refr;
+        return finish_bsdf(S, m, h, d, dir, sr);
+    }
+    case MT_GLOSSY:   // Glossy::scatter (Glossy.cpp:68-84)
+        return finish_bsdf(S, m, h, d, ggx_reflection_sample(d, h.n, m.alpha, k), sr);
+    case MT_DIFFUSE_GLOSSY: {   // DiffuseGlossy::scatter (DiffuseGlossy.cpp:118-142)
+        F3 dir;
+        if (sample1d(k, DIM_MATERIAL_DECISION) < (double)m.gweight) dir = ggx_reflection_sample(d, h.n, m.alpha, k);
+        else dir = onb_local(make_onb(h.n), cosine_hemisphere(k, DIM_BSDF_DIRECTION));
         return finish_bsdf(S, m, h, d, dir, sr);
     }
     case MT_PRINCIPLED: {

@@ -7,7 +7,7 @@ namespace luz {
 
 constexpr int kMaxBounceSlots = 256;
 constexpr int kBlock = 128;
-constexpr int kShadeClasses = 8;            // 0 = miss, 1..7 = material type of the hit
+constexpr int kShadeClasses = 10;           // 0 = miss, 1..9 = material type of the hit
 
 struct Ctrl {
     uint32_t count[kMaxBounceSlots + 2];    // extension queue size entering bounce b

@@ -15,10 +15,11 @@ from typing import List, Optional
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE = 1, 2, 3, 4
 MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
+MAT_GLOSSY, MAT_DIFFUSE_GLOSSY = 8, 9
 
 OBJ_RECTANGLE, OBJ_SPHERE, OBJ_CUBE, OBJ_PLANE = 1, 2, 3, 4
 OBJ_MESH, OBJ_MESH_INSTANCE, OBJ_VOLUME, OBJ_DIRECTIONAL_LIGHT = 5, 6, 7, 8
@@ -38,6 +39,7 @@ class MaterialDesc(C.Structure):
         ("metallic", C.c_double), ("transmission", C.c_double), ("clearcoat", C.c_double),
         ("clearcoat_roughness", C.c_double), ("sheen", C.c_double), ("subsurface", C.c_double),
         ("subsurface_radius", D3), ("subsurface_scale", C.c_double), ("subsurface_color", D3),
+        ("glossy_color", D3), ("glossy_weight", C.c_double),
     ]
 
 
@@ -196,7 +198,8 @@ class Scene:
                  anisotropy=0.0, conductor=0, subsurface_method=0, eta=(1.0, 1.0, 1.0), k=(0.0, 0.0, 0.0),
                  absorption=(0.0, 0.0, 0.0), metallic=0.0, transmission=0.0, clearcoat=0.0,
                  clearcoat_roughness=0.03, sheen=0.0, subsurface=0.0, subsurface_radius=(1.0, 1.0, 1.0),
-                 subsurface_scale=0.001, subsurface_color=(1.0, 1.0, 1.0))
+                 subsurface_scale=0.001, subsurface_color=(1.0, 1.0, 1.0), glossy_color=(1.0, 1.0, 1.0),
+                 glossy_weight=0.5)
         m.update(kw)
         self.materials.append(m)
         return len(self.materials) - 1
@@ -208,6 +211,13 @@ class Scene:
         if eta is not None:
             return self._mat(type=MAT_METAL, color=(1.0, 1.0, 1.0), roughness=roughness, conductor=1, eta=eta, k=k)
         return self._mat(type=MAT_METAL, color=color, roughness=roughness)
+
+    def glossy(self, color=(1.0, 1.0, 1.0), roughness=0.0):
+        return self._mat(type=MAT_GLOSSY, color=color, roughness=roughness)
+
+    def diffuse_glossy(self, diffuse=(0.6, 0.6, 0.6), glossy=(1.0, 1.0, 1.0), weight=0.5, roughness=0.0):
+        return self._mat(type=MAT_DIFFUSE_GLOSSY, color=diffuse, glossy_color=glossy, glossy_weight=weight,
+                         roughness=roughness)
 
     def dielectric(self, color=(1.0, 1.0, 1.0), ior=1.52, roughness=0.0, absorption=(0.0, 0.0, 0.0)):
         return self._mat(type=MAT_DIELECTRIC, color=color, ior=ior, roughness=roughness, absorption=absorption)

@@ -154,8 +154,8 @@ def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int
 def spheres_linear_sky(width: int = 64, height: int = 36, spp: int = 4, max_bounces: int = 12,
                        count: int = 40, seed: int = 9) -> Workload:
     """Spheres on a ground sphere under the linear sky (SKY_LINEAR), the kind of scene of
-    the reference's ray-tracing-in-one-weekend example: Lambertian, sharp and rough metal,
-    smooth and rough glass."""
+    the reference's ray-tracing-in-one-weekend example: Lambertian, Glossy, DiffuseGlossy,
+    sharp and rough metal, smooth and rough glass, and a UV-mapped textured panel."""
     rng = np.random.default_rng(seed)
     s = Scene()
     s.sky = SKY_LINEAR
@@ -167,11 +167,18 @@ def spheres_linear_sky(width: int = 64, height: int = 36, spp: int = 4, max_boun
     tex = s.texture(checker_texture(16, 4, 0.15, 0.85) * np.array([1.0, 0.8, 0.6]))
     s.rectangle((-6.0, 2.0, -4.0), (0.6, 0.0, 0.8), 6.0, 4.0, s.lambertian((1.0, 1.0, 1.0), texture=tex),
                 uvs=((0.0, 0.0), (2.0, 0.5), (1.5, 2.5), (-0.5, 2.0)))
+    s.sphere((-2.0, 0.6, 2.5), 0.6, s.glossy((0.9, 0.7, 0.4), roughness=0.2))
+    s.sphere((2.0, 0.6, 2.5), 0.6, s.diffuse_glossy((0.2, 0.4, 0.8), (1.0, 1.0, 1.0), weight=0.4, roughness=0.1))
     for _ in range(count):
         c = (rng.uniform(-8, 8), 0.2, rng.uniform(-8, 8))
         k = rng.random()
-        if k < 0.6:
+        if k < 0.4:
             m = s.lambertian(tuple(rng.uniform(0.05, 0.9, 3)))
+        elif k < 0.55:
+            m = s.glossy(tuple(rng.uniform(0.3, 1.0, 3)), roughness=float(rng.uniform(0.0, 0.6)))
+        elif k < 0.7:
+            m = s.diffuse_glossy(tuple(rng.uniform(0.05, 0.9, 3)), tuple(rng.uniform(0.5, 1.0, 3)),
+                                 weight=float(rng.uniform(0.1, 0.9)), roughness=float(rng.uniform(0.0, 0.5)))
         elif k < 0.85:
             m = s.metal(tuple(rng.uniform(0.5, 1.0, 3)), roughness=float(rng.uniform(0.0, 0.5)))
         else:

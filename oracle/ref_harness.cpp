@@ -50,6 +50,8 @@
 #include "Materials/Isotropic.hpp"
 #include "Materials/HenyeyGreenstein.hpp"
 #include "Materials/Principled.hpp"
+#include "Materials/Glossy.hpp"
+#include "Materials/DiffuseGlossy.hpp"
 #include "Hittables/Rectangle.hpp"
 #include "Hittables/Sphere.hpp"
 #include "Hittables/Cube.hpp"
@@ -128,6 +130,10 @@ std::shared_ptr<Material> make_material(const LuzMaterialDesc& m, const std::vec
         out = p;
         break;
     }
+    case LUZ_MAT_GLOSSY: out = std::make_shared<Glossy>(col(m.color), m.roughness); break;
+    case LUZ_MAT_DIFFUSE_GLOSSY:
+        out = std::make_shared<DiffuseGlossy>(col(m.color), col(m.glossy_color), m.glossy_weight, m.roughness);
+        break;
     default: throw std::invalid_argument("unknown material type");
     }
     if (m.texture >= 0) {

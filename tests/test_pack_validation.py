@@ -16,6 +16,10 @@ def packs(sc):
      "Volume anisotropy must be finite and between -0.99 and 0.99."),
     (lambda s: s.volume_sphere((0, 0, 0), 1, s.isotropic((1, 1, 1)), 0.0), "Volume density must be finite and positive."),
     (lambda s: s.sphere((0, 0, 0), 1, s.principled((1, 1, 1), metallic=2.0)), "Principled metallic must be finite and in [0,1]."),
+    (lambda s: s.sphere((0, 0, 0), 1, s.glossy((1, 1, 1), roughness=-0.1)), "Glossy roughness must be finite and in [0,1]."),
+    (lambda s: s.sphere((0, 0, 0), 1, s.diffuse_glossy(weight=1.5)), "Diffuse-glossy weight must be finite and in [0,1]."),
+    (lambda s: s.sphere((0, 0, 0), 1, s.diffuse_glossy(roughness=float("nan"))),
+     "Diffuse-glossy roughness must be finite and in [0,1]."),
 ])
 def test_invalid_parameters_rejected(make, msg):
     s = Scene()
