@@ -127,7 +127,24 @@ typedef struct LuzObjectDesc {
     int32_t has_uvs;              /* rect: optional uv0..uv3                        */
     int32_t _pad;
     double  uv[12];
+    int32_t ies;                  /* sphere: -1 or index into LuzSceneDesc.ies      */
+    int32_t _pad2;
+    double  ies_direction[3];     /* Sphere::setIESProfile vertical axis            */
+    double  ies_rotation_degrees; /* Sphere::setIESProfile horizontal rotation      */
 } LuzObjectDesc;
+
+/* IES photometric profile (IESProfile, src/core/IESProfile.cpp): angles in
+ * degrees, each strictly increasing; candela[h * vertical_count + v], the
+ * file's candela multiplier already applied. Scales the emission of the sphere
+ * lights that use it when they are sampled for direct lighting
+ * (Sphere::sampleLight, src/core/Hittables/Sphere.cpp:451-460). */
+typedef struct LuzIesDesc {
+    int32_t vertical_count;
+    int32_t horizontal_count;
+    const double* vertical_deg;
+    const double* horizontal_deg;
+    const double* candela;
+} LuzIesDesc;
 
 /* Camera (src/core/Camera.cpp); thin lens unless pinhole != 0. */
 typedef struct LuzCameraDesc {
@@ -162,6 +179,9 @@ typedef struct LuzSceneDesc {
     LuzEnvironmentDesc environment;
     double  background[3];
     double  meters_per_unit;
+    int32_t ies_count;
+    int32_t _pad;
+    const LuzIesDesc* ies;
 } LuzSceneDesc;
 
 /* Render settings: the parts of Scene that Renderer::render reads for the

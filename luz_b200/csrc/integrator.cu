@@ -45,7 +45,6 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
     P.ray_d[p] = make_float4((float)d[0], (float)d[1], (float)d[2], __int_as_float(-1));
     P.thr[p] = make_float4(1.f, 1.f, 1.f, 0.f);
     P.rad[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(PF_PREV_SPECULAR));
-    P.prev_o[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     P.pixel[p] = y * (uint32_t)w.width + x;
@@ -562,7 +561,6 @@ struct luz_gpu_scene {
         pb.ray_d = palloc<float4>(n);
         pb.thr = palloc<float4>(n);
         pb.rad = palloc<float4>(n);
-        pb.prev_o = palloc<float4>(n);
         pb.pend0 = palloc<float4>(n);
         pb.pend1 = palloc<float4>(n);
         pb.pixel = palloc<uint32_t>(n);
@@ -1145,7 +1143,6 @@ StaticArena carve_static(unsigned char* base)
     P.ray_d = reinterpret_cast<float4*>(take(n * sizeof(float4)));
     P.thr = reinterpret_cast<float4*>(take(n * sizeof(float4)));
     P.rad = reinterpret_cast<float4*>(take(n * sizeof(float4)));
-    P.prev_o = reinterpret_cast<float4*>(take(n * sizeof(float4)));
     P.pend0 = reinterpret_cast<float4*>(take(n * sizeof(float4)));
     P.pend1 = reinterpret_cast<float4*>(take(n * sizeof(float4)));
     P.hit = reinterpret_cast<float4*>(take(n * sizeof(float4)));
@@ -1310,6 +1307,7 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         d.textures = s->up(P.textures);
         d.texels = reinterpret_cast<const float4*>(s->up(P.texels));
         d.lights = s->up(P.lights);
+        d.ies = s->up(P.ies);
         d.cdf = s->up(P.cdf);
         d.index_pool = s->up(P.index_pool);
         d.env_texels = reinterpret_cast<const float4*>(s->up(P.env_texels));

@@ -181,6 +181,20 @@ struct alignas(16) GLight {
     double area;             // surface area used by pdfValue / sampleLight
     int32_t uniform;         // INSTANCE: uniform area scale
     int32_t mesh;
+    int32_t ies;             // SPHERE: -1 or GIes index
+    int32_t pad;
+    double ies_axis[3];      // Sphere::setIESProfile vertical axis and horizontal rotation
+    double ies_rotation;
+};
+
+// IES profile: angles and candela values in the double pool (vertical
+// angles, then horizontal angles, then candela[h * nv + v]); mean candela
+// = integrated flux / 4 pi (IESProfile::load, IESProfile.cpp:218-223).
+struct alignas(16) GIes {
+    int32_t nv, nh;
+    int32_t offset;
+    int32_t pad;
+    double mean_candela;
 };
 
 // Camera prepared in double (Renderer::internal::_prepareRenderCamera,

@@ -100,6 +100,58 @@ void check_unit(double v, const char* label)
     if (!std::isfinite(v) || v < 0.0 || v > 1.0) invalid(std::string(label) + " must be finite and in [0,1].");
 }
 
+// IESProfile::candelaAt (IESProfile.cpp:231-299): bilinear in (vertical,
+// horizontal) degrees, zero outside the vertical range, horizontal angles
+// wrapped to [0, 360) and closed over the last interval.
+double ies_candela(const double* va, int nv, const double* ha, int nh, const double* cd, double vdeg, double hdeg)
+{
+    if (nv <= 0 || nh <= 0 || !std::isfinite(vdeg)) return 0.0;
+    if (vdeg < va[0] || vdeg > va[nv - 1]) return 0.0;
+    int v0 = 0;
+    while (v0 + 1 < nv && va[v0 + 1] < vdeg) v0++;
+    const int v1 = std::min(v0 + 1, nv - 1);
+    const double vspan = va[v1] - va[v0];
+    const double vt = vspan > 0.0 ? (vdeg - va[v0]) / vspan : 0.0;
+    int h0 = 0, h1 = 0;
+    double ht = 0.0;
+    if (nh > 1) {
+        double hz = std::isfinite(hdeg) ? std::fmod(hdeg, 360.0) : 0.0;
+        if (hz < 0.0) hz += 360.0;
+        const double first = ha[0], last = ha[nh - 1];
+        if (hz < first) hz += 360.0;
+        if (hz > last && last >= 360.0) hz = std::min(hz, last);
+        while (h0 + 1 < nh && ha[h0 + 1] < hz) h0++;
+        if (h0 + 1 < nh) {
+            h1 = h0 + 1;
+            const double hspan = ha[h1] - ha[h0];
+            ht = hspan > 0.0 ? (hz - ha[h0]) / hspan : 0.0;
+        } else {
+            h1 = 0;
+            const double hspan = (first + 360.0) - ha[h0];
+            ht = hspan > 0.0 ? (hz - ha[h0]) / hspan : 0.0;
+        }
+    }
+    auto lerp = [](double a, double b, double t) { return a * (1.0 - t) + b * t; };
+    return lerp(lerp(cd[h0 * nv + v0], cd[h0 * nv + v1], vt), lerp(cd[h1 * nv + v0], cd[h1 * nv + v1], vt), ht);
+}
+
+// integrateTotalLumens (IESProfile.cpp:111-131): midpoint rule on 180 x 360 cells.
+double ies_flux(const double* va, int nv, const double* ha, int nh, const double* cd)
+{
+    const double dth = kPi / 180.0, dph = (2.0 * kPi) / 360.0;
+    double total = 0.0;
+    for (int v = 0; v < 180; v++) {
+        const double th = ((double)v + 0.5) * dth;
+        const double vdeg = th * (180.0 / kPi);
+        const double st = std::sin(th);
+        for (int h = 0; h < 360; h++) {
+            const double hdeg = ((double)h + 0.5) * 360.0 / 360.0;
+            total += ies_candela(va, nv, ha, nh, cd, vdeg, hdeg) * st * dth * dph;
+        }
+    }
+    return total;
+}
+
 GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
 {
     GMaterial g{};
@@ -649,6 +701,33 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         S.textures.push_back(g);
     }
     for (int i = 0; i < d->material_count; i++) S.materials.push_back(pack_material(d->materials[i], d->texture_count));
+    // IES profiles (IESProfile::load checks, IESProfile.cpp:186-223)
+    if (d->ies_count < 0 || (d->ies_count > 0 && !d->ies)) invalid("IES profile list is inconsistent.");
+    for (int i = 0; i < d->ies_count; i++) {
+        const LuzIesDesc& q = d->ies[i];
+        if (q.vertical_count <= 0) invalid("IES vertical angle count must be a positive integer.");
+        if (q.horizontal_count <= 0) invalid("IES horizontal angle count must be a positive integer.");
+        if (!q.vertical_deg || !q.horizontal_deg || !q.candela) invalid("IES profile has incomplete angle or candela data.");
+        auto increasing = [&](const double* a, int n, const char* what) {
+            for (int k = 0; k < n; k++) {
+                if (!std::isfinite(a[k])) invalid(std::string(what) + " contain a non-finite value.");
+                if (k > 0 && a[k] <= a[k - 1]) invalid(std::string(what) + " must be strictly increasing.");
+            }
+        };
+        const int64_t nc = (int64_t)q.vertical_count * q.horizontal_count;
+        for (int64_t k = 0; k < nc; k++)
+            if (!std::isfinite(q.candela[k]) || q.candela[k] < 0.0)
+                invalid("IES profile candela values must be finite and non-negative.");
+        increasing(q.vertical_deg, q.vertical_count, "IES vertical angles");
+        increasing(q.horizontal_deg, q.horizontal_count, "IES horizontal angles");
+        const double flux = ies_flux(q.vertical_deg, q.vertical_count, q.horizontal_deg, q.horizontal_count, q.candela);
+        if (!std::isfinite(flux) || flux <= 0.0) invalid("IES profile has zero luminous flux.");
+        GIes g{q.vertical_count, q.horizontal_count, (int32_t)S.cdf.size(), 0, flux / (4.0 * kPi)};
+        S.cdf.insert(S.cdf.end(), q.vertical_deg, q.vertical_deg + q.vertical_count);
+        S.cdf.insert(S.cdf.end(), q.horizontal_deg, q.horizontal_deg + q.horizontal_count);
+        S.cdf.insert(S.cdf.end(), q.candela, q.candela + nc);
+        S.ies.push_back(g);
+    }
     auto mat_type = [&](int m) {
         if (m < 0 || m >= d->material_count) invalid("Material index out of range.");
         return d->materials[m].type;
@@ -850,6 +929,13 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
             g.f[3] = (float)r;
             g.f[4] = o.visible ? 1.f : 0.f;
             has_box = true;
+            if (o.ies != -1) {   // Sphere::setIESProfile (Sphere.cpp:188-202)
+                if (o.ies < 0 || o.ies >= d->ies_count) invalid("IES profile index out of range.");
+                const double l2 = o.ies_direction[0] * o.ies_direction[0] + o.ies_direction[1] * o.ies_direction[1]
+                                + o.ies_direction[2] * o.ies_direction[2];
+                if (!std::isfinite(l2) || l2 <= 0.0) invalid("IES profile direction must be non-zero.");
+                if (!std::isfinite(o.ies_rotation_degrees)) invalid("IES profile rotation must be finite.");
+            }
             break;
         }
         case LUZ_OBJ_CUBE: {
@@ -1076,6 +1162,7 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         const double* em = d->materials[mat].color;
         const double lum = luminance(em);
         GLight L{};
+        L.ies = -1;
         L.object = S.object_of_desc[i];
         L.material = mat;
         for (int a = 0; a < 3; a++) L.emitted[a] = (float)em[a];
@@ -1091,6 +1178,9 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         }
         case LUZ_OBJ_SPHERE: {
             L.kind = LK_SPHERE;
+            L.ies = o.ies;
+            for (int a = 0; a < 3; a++) L.ies_axis[a] = o.ies_direction[a];
+            L.ies_rotation = o.ies_rotation_degrees;
             const double area = 4.0 * kPi * o.size[0] * o.size[0];
             L.area = area;
             w = (area <= 0.0 || !std::isfinite(lum) || lum <= 0.0) ? 0.0 : area * lum;

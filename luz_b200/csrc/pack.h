@@ -55,6 +55,7 @@ struct ScenePack {
     std::vector<GTexture> textures;
     std::vector<float> texels;               // float4 per texel
     std::vector<GLight> lights;
+    std::vector<GIes> ies;
     std::vector<double> cdf;                 // all double CDF / pdf pools
     std::vector<int32_t> index_pool;         // unaccelerated object list, slot maps
     std::vector<float> env_texels;           // float4 per texel

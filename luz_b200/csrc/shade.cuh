@@ -875,7 +875,75 @@ struct LightSample {
     float pdf;
     float tmax;
     bool valid;
+    float scale;   // IES relative intensity of a sphere light sample (1 otherwise)
 };
+
+// IESProfile::candelaAt (IESProfile.cpp:231-299), FP64.
+__device__ double ies_candela(const DScene& S, const GIes& I, double vdeg, double hdeg)
+{
+    const double* va = S.cdf + I.offset;
+    const double* ha = va + I.nv;
+    const double* cd = ha + I.nh;
+    const int nv = I.nv, nh = I.nh;
+    if (!isfinite(vdeg) || vdeg < va[0] || vdeg > va[nv - 1]) return 0.0;
+    int v0 = 0;
+    while (v0 + 1 < nv && va[v0 + 1] < vdeg) v0++;
+    const int v1 = min(v0 + 1, nv - 1);
+    const double vspan = va[v1] - va[v0];
+    const double vt = vspan > 0.0 ? (vdeg - va[v0]) / vspan : 0.0;
+    int h0 = 0, h1 = 0;
+    double ht = 0.0;
+    if (nh > 1) {
+        double hz = isfinite(hdeg) ? fmod(hdeg, 360.0) : 0.0;
+        if (hz < 0.0) hz += 360.0;
+        const double first = ha[0], last = ha[nh - 1];
+        if (hz < first) hz += 360.0;
+        if (hz > last && last >= 360.0) hz = fmin(hz, last);
+        while (h0 + 1 < nh && ha[h0 + 1] < hz) h0++;
+        if (h0 + 1 < nh) {
+            h1 = h0 + 1;
+            const double hspan = ha[h1] - ha[h0];
+            ht = hspan > 0.0 ? (hz - ha[h0]) / hspan : 0.0;
+        } else {
+            h1 = 0;
+            const double hspan = (first + 360.0) - ha[h0];
+            ht = hspan > 0.0 ? (hz - ha[h0]) / hspan : 0.0;
+        }
+    }
+    const double a = cd[h0 * nv + v0] * (1.0 - vt) + cd[h0 * nv + v1] * vt;
+    const double b = cd[h1 * nv + v0] * (1.0 - vt) + cd[h1 * nv + v1] * vt;
+    return a * (1.0 - ht) + b * ht;
+}
+
+// IESProfile::relativeIntensity (IESProfile.cpp:301-323) for emission direction e (FP64).
+__device__ __noinline__ float ies_relative(const DScene& S, const GLight& L, F3 e)
+{
+    const GIes I = S.ies[L.ies];
+    if (!(I.mean_candela > 0.0) || !isfinite(I.mean_candela)) return 0.0f;
+    auto norm_or = [](double x, double y, double z, double fx, double fy, double fz, double* o) {
+        const double l2 = x * x + y * y + z * z;
+        if (!isfinite(l2) || l2 <= 0.0) {
+            o[0] = fx; o[1] = fy; o[2] = fz;
+            return;
+        }
+        const double l = sqrt(l2);
+        o[0] = x / l; o[1] = y / l; o[2] = z / l;
+    };
+    double ax[3], dr[3], tg[3];
+    norm_or(L.ies_axis[0], L.ies_axis[1], L.ies_axis[2], 0.0, -1.0, 0.0, ax);
+    norm_or((double)e.x, (double)e.y, (double)e.z, ax[0], ax[1], ax[2], dr);
+    const double ct = fmin(1.0, fmax(-1.0, dr[0] * ax[0] + dr[1] * ax[1] + dr[2] * ax[2]));
+    const double vdeg = acos(ct) * (180.0 / kPiD);
+    const double hp[3] = {fabs(ax[1]) < 0.95 ? 0.0 : 1.0, fabs(ax[1]) < 0.95 ? 1.0 : 0.0, 0.0};
+    norm_or(hp[1] * ax[2] - hp[2] * ax[1], hp[2] * ax[0] - hp[0] * ax[2], hp[0] * ax[1] - hp[1] * ax[0], 1.0, 0.0, 0.0, tg);
+    const double bt[3] = {ax[1] * tg[2] - ax[2] * tg[1], ax[2] * tg[0] - ax[0] * tg[2], ax[0] * tg[1] - ax[1] * tg[0]};
+    double hdeg = atan2(dr[0] * bt[0] + dr[1] * bt[1] + dr[2] * bt[2], dr[0] * tg[0] + dr[1] * tg[1] + dr[2] * tg[2])
+                * (180.0 / kPiD) + L.ies_rotation;
+    if (!isfinite(hdeg)) hdeg = 0.0;
+    hdeg = fmod(hdeg, 360.0);
+    if (hdeg < 0.0) hdeg += 360.0;
+    return (float)(ies_candela(S, I, vdeg, hdeg) / I.mean_candela);
+}
 __device__ __forceinline__ double clamp_sample(double v)
 {
     if (!isfinite(v) || v <= 0.0) return 0.0;
@@ -1032,6 +1100,7 @@ __device__ __noinline__ bool light_surface_sample(const DScene& S, const GLight&
         ls.dir = dir;
         ls.pdf = 1.0f / sa;
         ls.tmax = root;
+        if (L.ies >= 0) ls.scale = ies_relative(S, L, dir * -1.0f);
         return isfinite(ls.pdf) && ls.pdf > 0.0f && ls.tmax > kTMin;
     }
     case LK_MESH: {
@@ -1207,6 +1276,7 @@ __device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key&
     if (sel <= 0.0f || !isfinite(sel)) return false;
     const GLight L = S.lights[idx];
     LightSample s;
+    s.scale = 1.0f;
     if (!light_surface_sample(S, L, origin, k, s)) return false;
     ls.dir = s.dir;
     ls.pdf = s.pdf * sel;
@@ -1214,6 +1284,7 @@ __device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key&
     if (ls.pdf <= 0.0f || ls.tmax <= kTMin || !isfinite(ls.pdf) || !(ls.tmax == ls.tmax)) return false;
     if (!isfinite(ls.tmax) && L.kind != LK_DIRECTIONAL) return false;
     ls.emitted = f3(L.emitted);
+    if (L.ies >= 0) ls.emitted = ls.emitted * s.scale;
     if (maxc(ls.emitted) <= 0.0f) return false;
     ls.valid = true;
     return true;

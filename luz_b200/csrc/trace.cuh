@@ -35,6 +35,7 @@ struct DScene {
     const GTexture* textures;
     const float4* texels;
     const GLight* lights;
+    const GIes* ies;
     const double* cdf;
     const int32_t* index_pool;
     const float4* env_texels;

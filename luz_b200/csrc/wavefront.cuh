@@ -22,7 +22,6 @@ struct PathBuf {
     float4* ray_d;
     float4* thr;       // xyz throughput, w previous scatter pdf
     float4* rad;       // xyz radiance, w flags
-    float4* prev_o;
     float4* pend0;     // pending light-NEE contribution
     float4* pend1;     // pending environment-NEE contribution
     uint32_t* pixel;
@@ -316,12 +315,12 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     out.sh[0] = out.sh[1] = false;
     out.xobj = -1;
     out.xprim = -1;
-    const float4 t4 = P.thr[p], r4 = P.rad[p], po4 = P.prev_o[p];
+    const float4 t4 = P.thr[p], r4 = P.rad[p];
     F3 thr{t4.x, t4.y, t4.z};
     F3 rad{r4.x, r4.y, r4.z};
     uint32_t flags = __float_as_uint(r4.w);
     const float prev_pdf = t4.w;
-    const F3 prev_o{po4.x, po4.y, po4.z};
+
     {
         const float4 a = P.pend0[p], b = P.pend1[p];
         rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
@@ -371,7 +370,8 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         const F3 emitted = m.type == MT_EMISSIVE ? f3(m.color) : F3{0.f, 0.f, 0.f};
         Scatter sr;
         if (!scatter(S, m, h, ray.d, k, sr)) {
-            const float plp = (!prev_spec && S.k.light_count > 0) ? lights_pdf(S, prev_o, ray.d) : 0.0f;
+            // previousScatterOrigin: read only after a non-specular scatter, whose hit point is this ray's origin
+            const float plp = (!prev_spec && S.k.light_count > 0) ? lights_pdf(S, ray.o, ray.d) : 0.0f;
             const float wgt = prev_spec ? 1.0f : power_heuristic(prev_pdf, plp);
             rad = rad + clamp_ray_color((thr * emitted) * wgt);
             goto done;
@@ -472,7 +472,6 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         const bool svil = ((S.k.sky == 3) && S.k.env.lighting) || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
         flags = svil ? PF_PREV_SVIL : 0u;
         P.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
-        P.prev_o[p] = make_float4(h.p.x, h.p.y, h.p.z, 0.f);
     }
 done:
     if (bounce >= w.max_bounces) out.cont = false;

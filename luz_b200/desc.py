@@ -62,7 +62,14 @@ class ObjectDesc(C.Structure):
         ("has_axes", C.c_int32), ("visible", C.c_int32),
         ("rotation_degrees", D3), ("scale", D3), ("density", C.c_double),
         ("has_uvs", C.c_int32), ("_pad", C.c_int32), ("uv", D12),
+        ("ies", C.c_int32), ("_pad2", C.c_int32), ("ies_direction", D3), ("ies_rotation_degrees", C.c_double),
     ]
+
+
+class IesDesc(C.Structure):
+    _fields_ = [("vertical_count", C.c_int32), ("horizontal_count", C.c_int32),
+                ("vertical_deg", C.POINTER(C.c_double)), ("horizontal_deg", C.POINTER(C.c_double)),
+                ("candela", C.POINTER(C.c_double))]
 
 
 class CameraDesc(C.Structure):
@@ -90,6 +97,7 @@ class SceneDesc(C.Structure):
         ("object_count", C.c_int32), ("sky", C.c_int32), ("objects", C.POINTER(ObjectDesc)),
         ("camera", CameraDesc), ("environment", EnvironmentDesc),
         ("background", D3), ("meters_per_unit", C.c_double),
+        ("ies_count", C.c_int32), ("_pad", C.c_int32), ("ies", C.POINTER(IesDesc)),
     ]
 
 
@@ -181,6 +189,7 @@ class Scene:
     """Flat scene: materials, textures, meshes and objects in Scene::addHittable order."""
     materials: List[dict] = field(default_factory=list)
     textures: List[np.ndarray] = field(default_factory=list)
+    ies: list = field(default_factory=list)
     meshes: List[dict] = field(default_factory=list)
     objects: List[dict] = field(default_factory=list)
     camera: Camera = field(default_factory=Camera)
@@ -245,7 +254,8 @@ class Scene:
     def _obj(self, **kw) -> int:
         o = dict(kind=0, material=-1, mesh=-1, boundary_kind=0, position=(0, 0, 0), orientation=(0, 0, 1),
                  size=(1, 1, 1), width_axis=(1, 0, 0), height_axis=(0, 1, 0), has_axes=0, visible=1,
-                 rotation_degrees=(0, 0, 0), scale=(1, 1, 1), density=1.42, has_uvs=0, uv=(0,) * 12)
+                 rotation_degrees=(0, 0, 0), scale=(1, 1, 1), density=1.42, has_uvs=0, uv=(0,) * 12, ies=-1,
+                 ies_direction=(0, -1, 0), ies_rotation_degrees=0.0)
         o.update(kw)
         self.objects.append(o)
         return len(self.objects) - 1
@@ -261,9 +271,19 @@ class Scene:
         return self._obj(kind=OBJ_RECTANGLE, position=position, orientation=normal, size=(width, height, 0),
                          material=material, **kw)
 
-    def sphere(self, center, radius, material, visible=True):
+    def sphere(self, center, radius, material, visible=True, ies=-1, ies_direction=(0.0, -1.0, 0.0),
+               ies_rotation=0.0):
+        """ies: -1 or an index from ies_profile (Sphere::setIESProfile)."""
         return self._obj(kind=OBJ_SPHERE, position=center, size=(radius, 0, 0), material=material,
-                         visible=1 if visible else 0)
+                         visible=1 if visible else 0, ies=ies, ies_direction=ies_direction,
+                         ies_rotation_degrees=float(ies_rotation))
+
+    def ies_profile(self, vertical_deg, horizontal_deg, candela) -> int:
+        """candela: (len(horizontal), len(vertical)) array (IES file order, multiplier applied)."""
+        c = np.ascontiguousarray(candela, dtype=np.float64)
+        self.ies.append((np.ascontiguousarray(vertical_deg, np.float64), np.ascontiguousarray(horizontal_deg, np.float64),
+                         c.reshape(-1)))
+        return len(self.ies) - 1
 
     def cube(self, center, w, h, d, material):
         return self._obj(kind=OBJ_CUBE, position=center, size=(w, h, d), material=material)
@@ -361,6 +381,11 @@ class BuiltDesc:
             d.environment = EnvironmentDesc(env.shape[1], env.shape[0], _dptr(env), s.environment_strength,
                                             s.environment_rotation, 1 if s.environment_lighting else 0, 0)
         d.background = _d3(s.background)
+        ies = (IesDesc * max(1, len(s.ies)))()
+        for i, (va, ha, cd) in enumerate(s.ies):
+            self._keep += [va, ha, cd]
+            ies[i] = IesDesc(va.shape[0], ha.shape[0], _dptr(va), _dptr(ha), _dptr(cd))
+        d.ies_count, d.ies = len(s.ies), ies
         d.sky = s.sky
         d.meters_per_unit = s.meters_per_unit
         self._keep += [mats, texs, meshes, objs]

@@ -191,6 +191,37 @@ def spheres_linear_sky(width: int = 64, height: int = 36, spp: int = 4, max_boun
     return Workload("spheres_linear_sky", s, width, height, spp, max_bounces)
 
 
+def spot_ies_profile(power: float = 4.0, asym: float = 0.35):
+    """A synthetic type-C photometric profile: a cos^power spot around the vertical axis
+    (0..180 degrees in 10-degree steps) with a horizontal asymmetry over 0..270 degrees."""
+    v = np.arange(0.0, 181.0, 10.0)
+    h = np.array([0.0, 90.0, 180.0, 270.0])
+    cd = 1000.0 * np.maximum(0.0, np.cos(np.radians(v)))[None, :] ** power * (1.0 + asym * np.cos(np.radians(h)))[:, None]
+    return v, h, cd + 5.0
+
+
+def ies_room(width: int = 48, height: int = 36, spp: int = 4, max_bounces: int = 6) -> Workload:
+    """A room lit by two IES-profiled sphere lights (Sphere::setIESProfile) aimed at different
+    directions and rotations, plus Lambertian, metal and glass objects."""
+    s = Scene()
+    white = s.lambertian((0.75, 0.75, 0.75))
+    blue = s.lambertian((0.2, 0.3, 0.7))
+    s.rectangle((0.0, 0.0, 0.0), (0, 1, 0), 10.0, 10.0, white)
+    s.rectangle((0.0, 3.0, -4.0), (0, 0, 1), 10.0, 6.0, blue)
+    s.rectangle((-4.5, 3.0, 0.0), (1, 0, 0), 10.0, 6.0, white)
+    s.sphere((-1.0, 0.8, 0.0), 0.8, s.metal((0.9, 0.85, 0.8), roughness=0.2))
+    s.sphere((1.3, 0.6, 0.8), 0.6, s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.05))
+    s.cube((1.5, 0.5, -1.5), 1.0, 1.0, 1.0, s.lambertian((0.8, 0.4, 0.2)))
+    prof = s.ies_profile(*spot_ies_profile())
+    s.sphere((-0.5, 3.5, 0.5), 0.2, s.emissive((30.0, 28.0, 24.0)), ies=prof, ies_direction=(0.2, -1.0, -0.1),
+             ies_rotation=30.0)
+    s.sphere((2.5, 2.5, 1.5), 0.15, s.emissive((25.0, 25.0, 30.0)), ies=prof, ies_direction=(-1.0, -1.0, -0.5),
+             ies_rotation=-75.0)
+    s.camera = _pinhole((0.0, 2.2, 7.0), (0.0, 1.0, 0.0), 45.0, width / height)
+    s.background = (0.0, 0.0, 0.0)
+    return Workload("ies_room", s, width, height, spp, max_bounces)
+
+
 def checker_texture(size: int = 32, squares: int = 4, lo: float = 0.2, hi: float = 0.8) -> np.ndarray:
     """size x size x 3 checker of `squares` x `squares` cells (the target of the albedo fit)."""
     c = (np.arange(size) * squares // size)

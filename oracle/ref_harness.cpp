@@ -25,6 +25,8 @@
  * the object and primitive; traversal does not depend on material values.
  */
 #include <algorithm>
+#include <fstream>
+#include <unistd.h>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -39,6 +41,7 @@
 #include "EnvironmentMap.hpp"
 #include "Texture.hpp"
 #include "Sampler.hpp"
+#include "IESProfile.hpp"
 #include "Denoise/NFOR.hpp"
 #include "Random.hpp"
 #include "Defaults.hpp"
@@ -94,6 +97,31 @@ struct RefScene {
 };
 
 Color col(const double* c) { return Color(c[0], c[1], c[2]); }
+
+// An IESProfile can only be made by IESProfile::load: write the profile as an
+// LM-63 file (TILT=NONE, multiplier 1, type C) and load it.
+std::shared_ptr<IESProfile> ies_profile(const LuzIesDesc& q)
+{
+    char path[] = "/tmp/luzref_iesXXXXXX";
+    const int fd = mkstemp(path);
+    if (fd < 0) throw std::runtime_error("cannot create a temporary IES file");
+    close(fd);
+    {
+        std::ofstream f(path);
+        f.precision(17);
+        f << "IESNA:LM-63-2002\nTILT=NONE\n1 -1 1 " << q.vertical_count << " " << q.horizontal_count
+          << " 1 1 0 0 0\n1 1 0\n";
+        for (int i = 0; i < q.vertical_count; i++) f << q.vertical_deg[i] << " ";
+        f << "\n";
+        for (int i = 0; i < q.horizontal_count; i++) f << q.horizontal_deg[i] << " ";
+        f << "\n";
+        for (int64_t i = 0; i < (int64_t)q.vertical_count * q.horizontal_count; i++) f << q.candela[i] << " ";
+        f << "\n";
+    }
+    auto p = std::make_shared<IESProfile>(IESProfile::load(path));
+    unlink(path);
+    return p;
+}
 Vector3 vec(const double* c) { return Vector3(c[0], c[1], c[2]); }
 
 std::shared_ptr<Material> make_material(const LuzMaterialDesc& m, const std::vector<std::shared_ptr<Texture>>& textures)
@@ -240,9 +268,12 @@ RefScene* build(const LuzSceneDesc* d, int tag)
             h = r;
             break;
         }
-        case LUZ_OBJ_SPHERE:
-            h = std::make_shared<Sphere>(vec(o.position), o.size[0], mat, o.visible != 0, SphereUVProjection::LatLong);
+        case LUZ_OBJ_SPHERE: {
+            auto sp = std::make_shared<Sphere>(vec(o.position), o.size[0], mat, o.visible != 0, SphereUVProjection::LatLong);
+            if (o.ies >= 0) sp->setIESProfile(ies_profile(d->ies[o.ies]), vec(o.ies_direction), o.ies_rotation_degrees);
+            h = sp;
             break;
+        }
         case LUZ_OBJ_CUBE:
             h = std::make_shared<Cube>(Transform(vec(o.position), Vector3(0, 0, 1), Vector3(1, 1, 1)),
                                        o.size[0], o.size[1], o.size[2], mat);

@@ -32,6 +32,7 @@ CASES = {
     "glossy": lambda: scenes.mesh_glossy(96, 54, 4, 12, level=4),
     "instancing": lambda: scenes.instancing_volumes(64, 36, 4, 16, count=500),
     "linear_sky": lambda: scenes.spheres_linear_sky(64, 36, 4, 12),
+    "ies": lambda: scenes.ies_room(48, 36, 4, 6),
 }
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.

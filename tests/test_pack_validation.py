@@ -1,4 +1,5 @@
 """Scene validation mirrors the reference's std::invalid_argument messages."""
+import numpy as np
 import pytest
 
 from luz_b200 import native
@@ -26,6 +27,29 @@ def test_invalid_parameters_rejected(make, msg):
     make(s)
     with pytest.raises(native.LuzError) as e:
         packs(s)
+    assert msg in str(e.value) and e.value.code == -1
+
+
+def _ies_scene(**kw):
+    from luz_b200.scenes import spot_ies_profile
+    s = Scene()
+    v, h, c = spot_ies_profile()
+    prof = s.ies_profile(kw.pop("v", v), h, kw.pop("c", c))
+    s.sphere((0, 2, 0), 0.2, s.emissive((5, 5, 5)), ies=kw.pop("ies", prof), **kw)
+    return s
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(ies_direction=(0, 0, 0)), "IES profile direction must be non-zero."),
+    (dict(ies_rotation=float("inf")), "IES profile rotation must be finite."),
+    (dict(ies=3), "IES profile index out of range."),
+    (dict(v=[0.0, 10.0, 10.0] + list(range(20, 181, 10))), "IES vertical angles must be strictly increasing."),
+    (dict(c=-1.0 * np.ones((4, 19))), "IES profile candela values must be finite and non-negative."),
+    (dict(c=np.zeros((4, 19))), "IES profile has zero luminous flux."),
+])
+def test_ies_validation(kw, msg):
+    with pytest.raises(native.LuzError) as e:
+        packs(_ies_scene(**kw))
     assert msg in str(e.value) and e.value.code == -1
 
 
