@@ -55,6 +55,7 @@ extern "C" {
 /* Sky types: values equal enum SkyTypes (include/luz/SkyTypes.hpp). */
 #define LUZ_SKY_NONE         0
 #define LUZ_SKY_LINEAR       1   /* white-to-blue gradient, Atmospherics.cpp:44-53 */
+#define LUZ_SKY_ATMOSPHERE   2   /* single-scattering Rayleigh/Mie sky, Atmosphere.cpp */
 #define LUZ_SKY_ENVIRONMENT  3
 
 /* Scene object kinds (one per reference Hittable class on the path). */
@@ -164,6 +165,20 @@ typedef struct LuzEnvironmentDesc {
     int32_t _pad;
 } LuzEnvironmentDesc;
 
+/* Atmosphere state as Renderer::render sees it after
+ * Scene::syncAtmosphereSunDirection (src/scene/Scene.cpp:457-475): the sun
+ * direction and radiance of the first directional light, or the atmosphere's
+ * own. Read when sky = LUZ_SKY_ATMOSPHERE; meters per unit is the scene's. */
+typedef struct LuzAtmosphereDesc {
+    double  sun_direction[3];     /* towards the sun                                */
+    double  sun_radiance[3];
+    double  sun_radiance_scale;
+    double  earth_radius, atmosphere_radius;   /* metres                        */
+    double  h_r, h_m;             /* Rayleigh / Mie scale heights (metres)          */
+    int32_t samples, light_samples;
+    double  stars_brightness;
+} LuzAtmosphereDesc;
+
 typedef struct LuzSceneDesc {
     int32_t abi_version;          /* LUZ_GPU_ABI_VERSION                            */
     int32_t material_count;
@@ -173,7 +188,7 @@ typedef struct LuzSceneDesc {
     const LuzTextureDesc* textures;
     const LuzMeshDesc* meshes;
     int32_t object_count;         /* objects in Scene::addHittable order            */
-    int32_t sky;                  /* LUZ_SKY_NONE, LUZ_SKY_LINEAR or LUZ_SKY_ENVIRONMENT */
+    int32_t sky;                  /* LUZ_SKY_*                                      */
     const LuzObjectDesc* objects;
     LuzCameraDesc camera;
     LuzEnvironmentDesc environment;
@@ -182,6 +197,7 @@ typedef struct LuzSceneDesc {
     int32_t ies_count;
     int32_t _pad;
     const LuzIesDesc* ies;
+    LuzAtmosphereDesc atmosphere;
 } LuzSceneDesc;
 
 /* Render settings: the parts of Scene that Renderer::render reads for the

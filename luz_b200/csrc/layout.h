@@ -222,13 +222,23 @@ struct GEnv {
     int32_t guide_count;
 };
 
+// Atmosphere::sampleSegment inputs (FP64, metres).
+struct GAtmos {
+    double sun_dir[3];
+    double sun_rad[3];          // sun radiance * scale
+    double earth_r, atmos_r;
+    double inv_hr, inv_hm;
+    double stars;
+    int32_t samples, light_samples;
+};
+
 struct GSceneConst {
     int32_t accel_kind;       // 0 none, 1 top BVH (root node 0), 2 single object
     int32_t accel_object;
     int32_t unaccel_count;
     int32_t unaccel_offset;   // into the object-index pool
     int32_t light_count;
-    int32_t sky;              // 0 none, 3 environment
+    int32_t sky;              // 0 none, 1 linear, 2 atmosphere, 3 environment
     int32_t has_constant_background_light;
     int32_t sampled_infinite_light;
     float background[3];
@@ -239,6 +249,7 @@ struct GSceneConst {
     double meters_per_unit;
     GCamera camera;
     GEnv env;
+    GAtmos atmos;
 };
 
 }  // namespace luz

@@ -1254,9 +1254,40 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
     }
 
     // sky / environment
-    if (d->sky != LUZ_SKY_NONE && d->sky != LUZ_SKY_LINEAR && d->sky != LUZ_SKY_ENVIRONMENT)
-        unsupported("Only SKY_NONE, SKY_LINEAR and SKY_ENVIRONMENT skies are on the GPU path (not SKY_ATMOSPHERE).");
+    if (d->sky != LUZ_SKY_NONE && d->sky != LUZ_SKY_LINEAR && d->sky != LUZ_SKY_ATMOSPHERE && d->sky != LUZ_SKY_ENVIRONMENT)
+        invalid("Unknown sky type.");
     K.sky = d->sky;
+    if (d->sky == LUZ_SKY_ATMOSPHERE) {   // Atmosphere setters (Atmosphere.cpp:93-300)
+        const LuzAtmosphereDesc& a = d->atmosphere;
+        if (!std::isfinite(a.earth_radius) || a.earth_radius <= 0.0) invalid("Earth radius must be positive.");
+        if (!std::isfinite(a.atmosphere_radius) || a.atmosphere_radius <= a.earth_radius)
+            invalid("Atmosphere radius must be larger than Earth radius.");
+        if (!std::isfinite(a.h_r) || a.h_r <= 0.0) invalid("Atmosphere HR must be positive.");
+        if (!std::isfinite(a.h_m) || a.h_m <= 0.0) invalid("Atmosphere HM must be positive.");
+        if (a.samples <= 0) invalid("Atmosphere sample count must be positive.");
+        if (a.light_samples <= 0) invalid("Atmosphere light sample count must be positive.");
+        if (!std::isfinite(a.stars_brightness) || a.stars_brightness < 0.0) invalid("Stars brightness must be non-negative.");
+        const double l2 = a.sun_direction[0] * a.sun_direction[0] + a.sun_direction[1] * a.sun_direction[1]
+                        + a.sun_direction[2] * a.sun_direction[2];
+        if (!finite3(a.sun_direction) || l2 <= 0.0) invalid("Atmosphere sun direction must be finite and non-zero.");
+        if (!finite3(a.sun_radiance) || a.sun_radiance[0] < 0.0 || a.sun_radiance[1] < 0.0 || a.sun_radiance[2] < 0.0)
+            invalid("Atmosphere sun radiance must be finite and non-negative.");
+        if (!std::isfinite(a.sun_radiance_scale) || a.sun_radiance_scale < 0.0)
+            invalid("Atmosphere sun radiance scale must be finite and non-negative.");
+        GAtmos& g = K.atmos;
+        const double il = 1.0 / std::sqrt(l2);   // Utilities::normalize: (1 / length) * v
+        for (int c = 0; c < 3; c++) {
+            g.sun_dir[c] = il * a.sun_direction[c];
+            g.sun_rad[c] = a.sun_radiance[c] * a.sun_radiance_scale;
+        }
+        g.earth_r = a.earth_radius;
+        g.atmos_r = a.atmosphere_radius;
+        g.inv_hr = 1.0 / a.h_r;
+        g.inv_hm = 1.0 / a.h_m;
+        g.stars = a.stars_brightness;
+        g.samples = a.samples;
+        g.light_samples = a.light_samples;
+    }
     for (int a = 0; a < 3; a++) K.background[a] = (float)d->background[a];
     K.background_luminance = (float)luminance(d->background);
     GEnv& E = K.env;

@@ -784,6 +784,142 @@ __device__ F3 scatter_generate(const Scatter& sr, const Key& k)
     }
 }
 
+// ----------------------------------------------------------------------------- atmosphere (FP64)
+
+// planetaryHit (Atmosphere.cpp:310-341): both roots of a sphere at the origin.
+__device__ __forceinline__ bool planet_hit(double radius, const double* o, const double* d, double& t0, double& t1)
+{
+    if (!isfinite(radius) || radius <= 0.0) return false;
+    const double a = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    if (!isfinite(a) || a <= 0.0) return false;
+    const double hb = o[0] * d[0] + o[1] * d[1] + o[2] * d[2];
+    const double c = (o[0] * o[0] + o[1] * o[1] + o[2] * o[2]) - radius * radius;
+    const double disc = hb * hb - a * c;
+    if (!isfinite(disc) || disc < 0.0) return false;
+    const double sq = sqrt(fmax(0.0, disc));
+    t0 = (-hb - sq) / a;
+    t1 = (-hb + sq) / a;
+    if (t0 > t1) {
+        const double x = t0;
+        t0 = t1;
+        t1 = x;
+    }
+    return true;
+}
+__device__ __forceinline__ double atmos_density(double height, double inv_h)
+{
+    if (height < 0.0 || !isfinite(height)) return 0.0;
+    return exp(-height * inv_h);
+}
+constexpr double kDblMax = 1.7976931348623157e308;   // T_MAX (Defaults.hpp:19)
+// Atmosphere::sceneUnitsToMeters (Atmosphere.cpp:156-172)
+__device__ __forceinline__ double to_meters(double su, double mpu)
+{
+    if (!isfinite(su)) return su;
+    const double mx = kDblMax / mpu;
+    if (su >= mx) return kDblMax;
+    if (su <= -mx) return -kDblMax;
+    return su * mpu;
+}
+
+struct AtmosSample {
+    double in[3];   // in-scattering
+    double tr[3];   // view transmittance
+};
+
+// Atmosphere::sampleSegment (Atmosphere.cpp:344-471): single-scattering
+// Rayleigh + Mie along the ray up to t_max (scene units), midpoint samples on
+// the view segment and on each sample's path to the sun.
+__device__ __noinline__ AtmosSample atmos_segment(const DScene& S, const double* ro, const double* d, double t_max)
+{
+    const GAtmos& A = S.k.atmos;
+    AtmosSample out{{0.0, 0.0, 0.0}, {1.0, 1.0, 1.0}};
+    const double mpu = S.k.meters_per_unit;
+    if (!isfinite(t_max) || t_max <= 0.001) return out;
+    const double tmax_m = to_meters(t_max, mpu), tmin_m = to_meters(0.001, mpu);
+    if (!isfinite(tmax_m) || tmax_m <= tmin_m) return out;
+    const double o[3] = {ro[0] * mpu, ro[1] * mpu, ro[2] * mpu};
+    double a0, a1;
+    if (!planet_hit(A.atmos_r, o, d, a0, a1) || a1 <= tmin_m) return out;
+    double tmax = tmax_m, e0, e1;
+    if (planet_hit(A.earth_r, o, d, e0, e1) && e1 > tmin_m) tmax = fmin(tmax, fmax(0.0, e0));
+    const double tmin = fmax(tmin_m, a0);
+    tmax = fmin(tmax, a1);
+    if (!isfinite(tmin) || !isfinite(tmax) || tmax <= tmin) return out;
+    const double seg = (tmax - tmin) / A.samples;
+    if (!isfinite(seg) || seg <= 0.0) return out;
+    const double bR[3] = {3.8e-6, 13.5e-6, 33.1e-6}, bM = 21e-6;   // Atmosphere::betaR / betaM
+    const double g = 0.76;                                          // kMieG
+    double sumR[3] = {0.0, 0.0, 0.0}, sumM[3] = {0.0, 0.0, 0.0};
+    double odR = 0.0, odM = 0.0;
+    const double mu = fmin(1.0, fmax(-1.0, d[0] * A.sun_dir[0] + d[1] * A.sun_dir[1] + d[2] * A.sun_dir[2]));
+    const double mu2 = mu * mu;
+    const double phR = (3.0 / (16.0 * kPiD)) * (1.0 + mu2);
+    const double mb = fmax(1.0 + g * g - 2.0 * g * mu, 1.0e-6);
+    const double md = mb * sqrt(mb);
+    const double phM = (3.0 / (8.0 * kPiD)) * ((1.0 - g * g) * (1.0 + mu2) / ((2.0 + g * g) * md));
+    for (int i = 0; i < A.samples; i++) {
+        const double vt = tmin + ((double)i + 0.5) * seg;
+        const double p[3] = {o[0] + vt * d[0], o[1] + vt * d[1], o[2] + vt * d[2]};
+        const double h = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) - A.earth_r;
+        const double dR = atmos_density(h, A.inv_hr), dM = atmos_density(h, A.inv_hm);
+        if (dR == 0.0 && dM == 0.0) continue;
+        const double sR = dR * seg, sM = dM * seg;
+        odR += sR;
+        odM += sM;
+        double l0, l1;
+        if (!planet_hit(A.atmos_r, p, A.sun_dir, l0, l1) || l1 <= 0.0) continue;
+        const double segL = l1 / A.light_samples;
+        if (!isfinite(segL) || segL <= 0.0) continue;
+        double oLR = 0.0, oLM = 0.0;
+        bool reaches = true;
+        for (int j = 0; j < A.light_samples; j++) {
+            const double lt = ((double)j + 0.5) * segL;
+            const double q[3] = {p[0] + lt * A.sun_dir[0], p[1] + lt * A.sun_dir[1], p[2] + lt * A.sun_dir[2]};
+            const double hl = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - A.earth_r;
+            if (hl < 0.0) {
+                reaches = false;
+                break;
+            }
+            oLR += atmos_density(hl, A.inv_hr) * segL;
+            oLM += atmos_density(hl, A.inv_hm) * segL;
+        }
+        if (!reaches) continue;
+        for (int c = 0; c < 3; c++) {
+            const double tau = bR[c] * (odR + oLR) + (bM * 1.1) * (odM + oLM);   // kMieAbsorptionScale
+            const double att = exp(-tau);
+            sumR[c] += att * sR;
+            sumM[c] += att * sM;
+        }
+    }
+    for (int c = 0; c < 3; c++) {
+        out.tr[c] = exp(-(bR[c] * odR + (bM * 1.1) * odM));
+        out.in[c] = ((sumR[c] * bR[c]) * phR + (sumM[c] * bM) * phM) * A.sun_rad[c];
+    }
+    return out;
+}
+
+// primaryAtmosphereTMax (ColorHelper.cpp:624-643): a camera ray that hits the
+// scene inside the planet still sees the atmosphere up to the ground.
+__device__ __forceinline__ double primary_atmos_tmax(const DScene& S, const double* o, const double* d, double surface_t)
+{
+    if (!isfinite(surface_t) || surface_t <= 0.001) return surface_t;
+    double t0, t1;
+    if (!planet_hit(S.k.atmos.earth_r / S.k.meters_per_unit, o, d, t0, t1) || t1 <= 0.001) return surface_t;
+    const double ground = fmax(0.0, t0);
+    if (!isfinite(ground) || ground <= 0.001) return surface_t;
+    return fmax(surface_t, ground);
+}
+
+// sampleProceduralStars (ColorHelper.cpp:568-589)
+__device__ __forceinline__ float atmos_stars(const DScene& S, const Key& k, const double* in)
+{
+    if (sample1d(k, DIM_ATMOSPHERE) < 0.9996) return 0.0f;
+    double diff = (S.k.atmos.stars - 0.2 + (0.4 * sample1d(k, DIM_ATMOSPHERE + 1))) - ((in[0] + in[1] + in[2]) / 3.0);
+    diff = diff < 0.0 ? 0.0 : (diff > 1.0 ? 1.0 : diff);
+    return (float)diff;
+}
+
 // ----------------------------------------------------------------------------- environment (FP64 index math)
 
 __device__ __forceinline__ double wrap01d(double v)
@@ -926,8 +1062,8 @@ __device__ __noinline__ float ies_relative(const DScene& S, const GLight& L, F3 
             o[0] = fx; o[1] = fy; o[2] = fz;
             return;
         }
-        const double l = sqrt(l2);
-        o[0] = x / l; o[1] = y / l; o[2] = z / l;
+        const double il = 1.0 / sqrt(l2);   // Vector3 / double is (1 / d) * v
+        o[0] = il * x; o[1] = il * y; o[2] = il * z;
     };
     double ax[3], dr[3], tg[3];
     norm_or(L.ies_axis[0], L.ies_axis[1], L.ies_axis[2], 0.0, -1.0, 0.0, ax);

@@ -309,6 +309,21 @@ __device__ __noinline__ void adjoint_texture(const DScene& S, const WaveArgs& w,
     }
 }
 
+// The ray the atmosphere integrates along, in FP64: at bounce 0 the camera ray
+// is regenerated in FP64 (a planet-scale origin loses metres in FP32), later
+// rays are the FP32 ray widened.
+__device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, const TRay& ray,
+                                       double* o, double* d)
+{
+    if (bounce == 0) {
+        const uint32_t pix = P.pixel[p];
+        camera_ray(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], o, d);
+        return;
+    }
+    o[0] = ray.o.x; o[1] = ray.o.y; o[2] = ray.o.z;
+    d[0] = ray.d.x; d[1] = ray.d.y; d[2] = ray.d.z;
+}
+
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
     out.cont = false;
@@ -337,7 +352,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     if (obj < 0) {   // miss (ColorHelper.cpp:1169-1210)
         float env_mis = 1.0f;
         const bool need_pdf = bounce > 0 && !prev_spec && (flags & PF_PREV_SVIL);
-        const bool need_rad = S.k.sky == 3 && S.k.env.present;
+        const bool need_rad = (S.k.sky == 3 || S.k.sky == 2) && S.k.env.present;
         F3 env_rad{0.f, 0.f, 0.f};
         float env_p = 0.0f;
         if ((need_pdf && S.k.env.lighting) || need_rad) env_query(S, ray.d, need_rad, need_pdf && S.k.env.lighting, env_rad, env_p);
@@ -351,6 +366,19 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         if (S.k.sky == 1) {   // SKY_LINEAR: _calculateSkyInterpolation (Atmospherics.cpp:44-53), skyline 0.5
             const float tl = 0.5f * ((ray.d.y / sqrtf(len2(ray.d))) + 1.0f);
             sky = (F3{1.0f, 1.0f, 1.0f} * (1.0f - tl)) + (F3{0.5f, 0.7f, 1.0f} * tl);
+        } else if (S.k.sky == 2) {   // sampleAtmosphereSky (ColorHelper.cpp:590-605)
+            double ao[3], ad[3];
+            atmos_ray(w, P, p, bounce, ray, ao, ad);
+            const AtmosSample a = atmos_segment(S, ao, ad, kDblMax);
+            double bg[3];
+            if (need_rad) {
+                const F3 e = (env_rad * S.k.env.strength) * env_mis;
+                bg[0] = e.x; bg[1] = e.y; bg[2] = e.z;
+            } else {
+                bg[0] = bg[1] = bg[2] = atmos_stars(S, k, a.in);
+            }
+            sky = F3{(float)(a.in[0] + a.tr[0] * bg[0]), (float)(a.in[1] + a.tr[1] * bg[1]),
+                     (float)(a.in[2] + a.tr[2] * bg[2])};
         } else if (need_rad) {
             sky = (env_rad * S.k.env.strength) * env_mis;
         } else {
@@ -367,6 +395,14 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         Hit h = make_hit(S, ray, th);
         const GMaterial m = S.materials[h.material];
         if (bounce == 0 && w.nfor) store_hit_features(S, P, p, h, m);
+        if (bounce == 0 && S.k.sky == 2) {   // compositePrimaryAtmosphereSegment (ColorHelper.cpp:645-659)
+            double ao[3], ad[3];
+            atmos_ray(w, P, p, bounce, ray, ao, ad);
+            const AtmosSample a = atmos_segment(S, ao, ad, primary_atmos_tmax(S, ao, ad, (double)h.t));
+            rad = rad + clamp_ray_color(thr * F3{(float)a.in[0], (float)a.in[1], (float)a.in[2]});
+            thr = clamp_ray_color(thr * F3{(float)a.tr[0], (float)a.tr[1], (float)a.tr[2]});
+            if (terminated(thr)) goto done;
+        }
         const F3 emitted = m.type == MT_EMISSIVE ? f3(m.color) : F3{0.f, 0.f, 0.f};
         Scatter sr;
         if (!scatter(S, m, h, ray.d, k, sr)) {
@@ -469,7 +505,8 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         out.cont = true;
         out.next_o = h.p;
         out.next_d = dir;
-        const bool svil = ((S.k.sky == 3) && S.k.env.lighting) || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
+        const bool svil = ((S.k.sky == 3 || S.k.sky == 2) && S.k.env.lighting)
+                       || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
         flags = svil ? PF_PREV_SVIL : 0u;
         P.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
     }

@@ -24,7 +24,7 @@ MAT_GLOSSY, MAT_DIFFUSE_GLOSSY = 8, 9
 OBJ_RECTANGLE, OBJ_SPHERE, OBJ_CUBE, OBJ_PLANE = 1, 2, 3, 4
 OBJ_MESH, OBJ_MESH_INSTANCE, OBJ_VOLUME, OBJ_DIRECTIONAL_LIGHT = 5, 6, 7, 8
 
-SKY_NONE, SKY_LINEAR, SKY_ENVIRONMENT = 0, 1, 3
+SKY_NONE, SKY_LINEAR, SKY_ATMOSPHERE, SKY_ENVIRONMENT = 0, 1, 2, 3
 
 D3 = C.c_double * 3
 D12 = C.c_double * 12
@@ -89,6 +89,13 @@ class EnvironmentDesc(C.Structure):
     ]
 
 
+class AtmosphereDesc(C.Structure):
+    _fields_ = [("sun_direction", D3), ("sun_radiance", D3), ("sun_radiance_scale", C.c_double),
+                ("earth_radius", C.c_double), ("atmosphere_radius", C.c_double), ("h_r", C.c_double),
+                ("h_m", C.c_double), ("samples", C.c_int32), ("light_samples", C.c_int32),
+                ("stars_brightness", C.c_double)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("abi_version", C.c_int32), ("material_count", C.c_int32), ("materials", C.POINTER(MaterialDesc)),
@@ -98,6 +105,7 @@ class SceneDesc(C.Structure):
         ("camera", CameraDesc), ("environment", EnvironmentDesc),
         ("background", D3), ("meters_per_unit", C.c_double),
         ("ies_count", C.c_int32), ("_pad", C.c_int32), ("ies", C.POINTER(IesDesc)),
+        ("atmosphere", AtmosphereDesc),
     ]
 
 
@@ -190,6 +198,12 @@ class Scene:
     materials: List[dict] = field(default_factory=list)
     textures: List[np.ndarray] = field(default_factory=list)
     ies: list = field(default_factory=list)
+    # Atmosphere (sky = SKY_ATMOSPHERE): reference defaults (Defaults.hpp:21-24, Atmosphere.cpp:69-80);
+    # sun direction/radiance as Scene::syncAtmosphereSunDirection leaves them.
+    atmosphere: dict = field(default_factory=lambda: dict(
+        sun_direction=(0.0, 0.3, -0.95), sun_radiance=(1.0, 1.0, 1.0), sun_radiance_scale=1.0,
+        earth_radius=6360e3, atmosphere_radius=6420e3, h_r=7994.0, h_m=1200.0, samples=16, light_samples=8,
+        stars_brightness=0.5))
     meshes: List[dict] = field(default_factory=list)
     objects: List[dict] = field(default_factory=list)
     camera: Camera = field(default_factory=Camera)
@@ -386,6 +400,10 @@ class BuiltDesc:
             self._keep += [va, ha, cd]
             ies[i] = IesDesc(va.shape[0], ha.shape[0], _dptr(va), _dptr(ha), _dptr(cd))
         d.ies_count, d.ies = len(s.ies), ies
+        a = s.atmosphere
+        d.atmosphere = AtmosphereDesc(_d3(a["sun_direction"]), _d3(a["sun_radiance"]), a["sun_radiance_scale"],
+                                      a["earth_radius"], a["atmosphere_radius"], a["h_r"], a["h_m"], a["samples"],
+                                      a["light_samples"], a["stars_brightness"])
         d.sky = s.sky
         d.meters_per_unit = s.meters_per_unit
         self._keep += [mats, texs, meshes, objs]

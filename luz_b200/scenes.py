@@ -222,6 +222,33 @@ def ies_room(width: int = 48, height: int = 36, spp: int = 4, max_bounces: int =
     return Workload("ies_room", s, width, height, spp, max_bounces)
 
 
+def atmosphere_hills(width: int = 48, height: int = 32, spp: int = 4, max_bounces: int = 3) -> Workload:
+    """The atmosphere sky (SKY_ATMOSPHERE, metres as scene units) seen from 1.5 km above a
+    6,360-km planet at a low sun: a sky gradient, in-scattering in front of distant hills
+    (spheres near the ground), a directional-light sun that drives the atmosphere as
+    Scene::syncAtmosphereSunDirection does, and procedural stars in the sky misses."""
+    from .desc import SKY_ATMOSPHERE
+    s = Scene()
+    s.sky = SKY_ATMOSPHERE
+    R = 6360e3
+    base = np.array([0.0, R, 0.0])
+    ground = s.lambertian((0.25, 0.3, 0.18))
+    rock = s.lambertian((0.45, 0.4, 0.35))
+    s.sphere(tuple(base + np.array([0.0, -1.0e6 + 2.0, 0.0])), 1.0e6, ground)
+    for x, z, r in ((-3000.0, 9000.0, 1200.0), (1500.0, 14000.0, 2500.0), (5000.0, 7000.0, 900.0)):
+        s.sphere(tuple(base + np.array([x, 0.0, z])), r, rock)
+    sun_dir = np.array([-0.55, -0.12, -0.83])   # light travels this way: the sun is low, behind-left
+    sun = s.emissive((4.0, 3.8, 3.4))
+    s.directional_light(tuple(sun_dir), sun)
+    s.atmosphere.update(sun_direction=tuple(-sun_dir), sun_radiance=(4.0, 3.8, 3.4), stars_brightness=0.6)
+    s.camera = Camera(position=tuple(base + np.array([0.0, 1500.0, 0.0])), direction=(0.0, -0.02, 1.0),
+                      up=(0.0, 1.0, 0.0), focal_length_m=0.024, sensor_width_m=0.036, sensor_height_m=0.024,
+                      f_number=8.0, focus_distance_m=10.0, pinhole=True)
+    s.meters_per_unit = 1.0
+    s.background = (0.0, 0.0, 0.0)
+    return Workload("atmosphere_hills", s, width, height, spp, max_bounces)
+
+
 def checker_texture(size: int = 32, squares: int = 4, lo: float = 0.2, hi: float = 0.8) -> np.ndarray:
     """size x size x 3 checker of `squares` x `squares` cells (the target of the albedo fit)."""
     c = (np.arange(size) * squares // size)

@@ -315,7 +315,19 @@ RefScene* build(const LuzSceneDesc* d, int tag)
     scene.addCamera(cam);
     scene.setMetersPerUnit(d->meters_per_unit);
     scene.setBackgroundColor(col(d->background));
-    scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT : d->sky == LUZ_SKY_LINEAR ? SKY_LINEAR : SKY_NONE);
+    scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT
+                       : d->sky == LUZ_SKY_LINEAR   ? SKY_LINEAR
+                       : d->sky == LUZ_SKY_ATMOSPHERE ? SKY_ATMOSPHERE
+                                                      : SKY_NONE);
+    if (d->sky == LUZ_SKY_ATMOSPHERE) {
+        const LuzAtmosphereDesc& a = d->atmosphere;
+        Atmosphere atm(-0.4, a.earth_radius, a.atmosphere_radius, a.h_r, a.h_m, a.samples, a.light_samples,
+                       a.stars_brightness);
+        atm.setSunDirection(vec(a.sun_direction));
+        atm.setSunRadiance(col(a.sun_radiance));
+        atm.setSunRadianceScale(a.sun_radiance_scale);
+        scene.setAtmosphere(atm);   // takes the scene's meters per unit
+    }
     if (d->environment.width > 0) {
         const LuzEnvironmentDesc& e = d->environment;
         std::vector<Color> px((std::size_t)e.width * e.height);

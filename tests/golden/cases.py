@@ -33,6 +33,7 @@ CASES = {
     "instancing": lambda: scenes.instancing_volumes(64, 36, 4, 16, count=500),
     "linear_sky": lambda: scenes.spheres_linear_sky(64, 36, 4, 12),
     "ies": lambda: scenes.ies_room(48, 36, 4, 6),
+    "atmosphere": lambda: scenes.atmosphere_hills(48, 32, 4, 3),
 }
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.

@@ -53,12 +53,30 @@ def test_ies_validation(kw, msg):
     assert msg in str(e.value) and e.value.code == -1
 
 
-def test_unsupported_sky_rejected():
+def test_unknown_sky_rejected():
     s = Scene()
-    s.sky = 2   # SKY_ATMOSPHERE
+    s.sky = 7
     with pytest.raises(native.LuzError) as e:
         packs(s)
-    assert e.value.code == -3
+    assert e.value.code == -1
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(earth_radius=-1.0), "Earth radius must be positive."),
+    (dict(atmosphere_radius=6000e3), "Atmosphere radius must be larger than Earth radius."),
+    (dict(h_r=0.0), "Atmosphere HR must be positive."),
+    (dict(samples=0), "Atmosphere sample count must be positive."),
+    (dict(sun_direction=(0.0, 0.0, 0.0)), "Atmosphere sun direction must be finite and non-zero."),
+    (dict(sun_radiance=(1.0, -1.0, 1.0)), "Atmosphere sun radiance must be finite and non-negative."),
+])
+def test_atmosphere_validation(kw, msg):
+    from luz_b200.desc import SKY_ATMOSPHERE
+    s = Scene()
+    s.sky = SKY_ATMOSPHERE
+    s.atmosphere.update(kw)
+    with pytest.raises(native.LuzError) as e:
+        packs(s)
+    assert msg in str(e.value) and e.value.code == -1
 
 
 def test_camera_validation():
