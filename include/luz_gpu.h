@@ -397,6 +397,27 @@ int luz_gpu_render_ex(luz_gpu_scene* scene, const LuzRenderParams* params,
                       const LuzNforBuffers* nfor, int32_t* samples_out,
                       LuzRenderStats* stats);
 
+/* ---- NFOR denoiser ----------------------------------------------------------
+ * Denoise::applyNFOR (src/core/Denoise/NFOR.cpp:977-1102) on the GPU in FP64:
+ * firefly suppression, cross-guided feature prefilter, two-bandwidth feature
+ * regressions of each half buffer, MSE-driven bandwidth selection and a last
+ * regression. Input: the NFOR buffers of a render (luz_gpu_render_ex), host
+ * arrays; output: width*height*3 doubles (the denoised Image). settings NULL
+ * = NFORSettings defaults (include/luz/Denoise/NFOR.hpp:39-47). A zero-sized
+ * image returns LUZ_OK with nothing written. Errors: LUZ_E_INVALID with the
+ * message of luz_gpu_nfor_error (e.g. "NFOR radii must be positive."). */
+typedef struct LuzNforSettings {
+    int32_t feature_prefilter_radius;   /* 1 */
+    int32_t regression_radius;          /* 2 */
+    int32_t patch_radius;               /* 1 */
+    int32_t reserved;
+    double  min_variance;               /* 1e-5 */
+} LuzNforSettings;
+int luz_gpu_nfor_denoise(int32_t device, const LuzNforBuffers* buffers, int32_t width, int32_t height,
+                         const LuzNforSettings* settings, double* rgb_out);
+int luz_gpu_nfor_error(char* buf, size_t len);
+
+
 /* Ray batch traversal (test hook and building block): rays are
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) * count, host buffers. any_hit != 0
  * runs the shadow traversal and reports object = 0 (occluded) / -1. The

@@ -146,6 +146,12 @@ class NforBuffers(C.Structure):
                 ("features_a", C.c_void_p), ("features_b", C.c_void_p), ("feature_variance", C.c_void_p)]
 
 
+class NforSettings(C.Structure):
+    """LuzNforSettings (Denoise::NFORSettings)."""
+    _fields_ = [("feature_prefilter_radius", C.c_int32), ("regression_radius", C.c_int32),
+                ("patch_radius", C.c_int32), ("reserved", C.c_int32), ("min_variance", C.c_double)]
+
+
 class Hit(C.Structure):
     _fields_ = [("t", C.c_float), ("object", C.c_int32), ("primitive", C.c_int32), ("u", C.c_float), ("v", C.c_float)]
 

@@ -24,6 +24,7 @@ EXPORTED = [
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
     "luz_gpu_render_device_noalloc", "luz_gpu_render_ex", "luz_gpu_batch_render",
     "luz_gpu_scene_set_texture", "luz_gpu_adjoint_forward", "luz_gpu_adjoint_backward",
+    "luz_gpu_nfor_denoise", "luz_gpu_nfor_error",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -65,6 +66,8 @@ def lib():
     L.luz_gpu_render_ex.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams), vp,
                                     C.POINTER(D.NforBuffers), vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_batch_render.argtypes = [vp, vp, i32, vp, vp]
+    L.luz_gpu_nfor_denoise.argtypes = [i32, C.POINTER(D.NforBuffers), i32, i32, C.POINTER(D.NforSettings), vp]
+    L.luz_gpu_nfor_error.argtypes = [C.c_char_p, C.c_size_t]
     L.luz_gpu_scene_set_texture.argtypes = [vp, i32, vp]
     L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
@@ -236,6 +239,23 @@ class GpuScene:
         _check(lib().luz_gpu_trace_rays(self.h, rays.ctypes.data, rays.shape[0], 1 if any_hit else 0, seed,
                                         None if vk is None else vk.ctypes.data, out.ctypes.data))
         return out
+
+
+def nfor_denoise(bufs: dict, device: int = 0, prefilter_radius=1, regression_radius=2, patch_radius=1,
+                 min_variance=1e-5) -> np.ndarray:
+    """luz_gpu_nfor_denoise on NFOR buffers (dict as GpuScene.render_ex returns); H x W x 3 float64."""
+    h, w = bufs["color_variance"].shape[:2]
+    a = {k: np.ascontiguousarray(v, np.float64) for k, v in bufs.items()}
+    nb = D.NforBuffers(*[a[k].ctypes.data for k in ("color_a", "color_b", "color_variance", "features_a",
+                                                    "features_b", "feature_variance")])
+    st = D.NforSettings(int(prefilter_radius), int(regression_radius), int(patch_radius), 0, float(min_variance))
+    out = np.zeros((h, w, 3), np.float64)
+    rc = lib().luz_gpu_nfor_denoise(int(device), C.byref(nb), w, h, C.byref(st), out.ctypes.data)
+    if rc != 0:
+        buf = C.create_string_buffer(1024)
+        lib().luz_gpu_nfor_error(buf, 1024)
+        raise LuzError(rc, buf.value.decode(errors="replace"))
+    return out
 
 
 def batch_render(scenes, plist):

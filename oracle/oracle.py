@@ -62,6 +62,8 @@ class RefOracle:
         L.luzref_trace_rays.argtypes = [vp, vp, C.c_int64, C.c_int32, C.c_uint32, vp, vp, vp, vp]
         L.luzref_trace_paths.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp]
         L.luzref_render.argtypes = [vp, vp, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.luzref_nfor.argtypes = [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_int32,
+                                  C.c_double, C.c_int32, vp]
         L.luzref_trace_samples.argtypes = [vp, vp, C.c_int32, vp, vp, vp, C.c_int64, vp, vp]
         L.luzref_render_pixels.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, vp, vp,
                                            C.c_int64, vp, vp, vp]
@@ -81,6 +83,19 @@ class RefOracle:
         h = C.c_void_p()
         self._check(self.lib.luzref_scene_create(C.cast(built.ptr(), C.c_void_p), 1 if tag else 0, C.byref(h)))
         return RefScene(self, h, built)
+
+    def nfor(self, bufs: dict, prefilter_radius=1, regression_radius=2, patch_radius=1, min_variance=1e-5,
+             threads=1):
+        """Denoise::applyNFOR on NFOR buffers (dict of H x W x k arrays); returns H x W x 3."""
+        h, w = bufs["color_variance"].shape[:2]
+        a = {k: np.ascontiguousarray(v, np.float64) for k, v in bufs.items()}
+        out = np.zeros((h, w, 3), np.float64)
+        self._check(self.lib.luzref_nfor(w, h, a["color_a"].ctypes.data, a["color_b"].ctypes.data,
+                                         a["color_variance"].ctypes.data, a["features_a"].ctypes.data,
+                                         a["features_b"].ctypes.data, a["feature_variance"].ctypes.data,
+                                         prefilter_radius, regression_radius, patch_radius, min_variance, threads,
+                                         out.ctypes.data))
+        return out
 
     def sampler(self, seed, x, y, s, stream, bounce, dim, which=1):
         out = np.zeros(2, np.float64)

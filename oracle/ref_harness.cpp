@@ -608,6 +608,45 @@ int luzref_render_pixels(void* s, const LuzRenderParams* p, int32_t adaptive, in
     });
 }
 
+/* Denoise::applyNFOR (src/core/Denoise/NFOR.cpp:977-1102) on the given buffers. */
+int luzref_nfor(int32_t width, int32_t height, const double* color_a, const double* color_b,
+                const double* color_variance, const double* features_a, const double* features_b,
+                const double* feature_variance, int32_t prefilter_radius, int32_t regression_radius,
+                int32_t patch_radius, double min_variance, int32_t threads, double* rgb_out)
+{
+    return guarded([&] {
+        Denoise::NFORBuffers b;
+        b.initialize((std::size_t)width, (std::size_t)height);
+        const std::size_t n = (std::size_t)width * height;
+        for (std::size_t i = 0; i < n; i++) {
+            b.colorA[i] = Color(color_a[3 * i], color_a[3 * i + 1], color_a[3 * i + 2]);
+            b.colorB[i] = Color(color_b[3 * i], color_b[3 * i + 1], color_b[3 * i + 2]);
+            b.colorVariance[i] = color_variance[i];
+            for (std::size_t f = 0; f < Denoise::NFOR_FEATURE_COUNT; f++) {
+                b.featuresA[i][f] = features_a[Denoise::NFOR_FEATURE_COUNT * i + f];
+                b.featuresB[i][f] = features_b[Denoise::NFOR_FEATURE_COUNT * i + f];
+                b.featureVariance[i][f] = feature_variance[Denoise::NFOR_FEATURE_COUNT * i + f];
+            }
+        }
+        Denoise::NFORSettings s;
+        s.featurePrefilterRadius = (unsigned)prefilter_radius;
+        s.regressionRadius = (unsigned)regression_radius;
+        s.patchRadius = (unsigned)patch_radius;
+        s.minVariance = min_variance;
+        s.threadCount = (std::size_t)std::max(1, threads);
+        const std::unique_ptr<Image> img = Denoise::applyNFOR(b, s);
+        for (int32_t y = 0; y < height; y++)
+            for (int32_t x = 0; x < width; x++) {
+                const Color c = img->getPixel((std::size_t)x, (std::size_t)y);
+                const std::size_t k = (std::size_t)y * width + x;
+                rgb_out[3 * k] = c.getRed();
+                rgb_out[3 * k + 1] = c.getGreen();
+                rgb_out[3 * k + 2] = c.getBlue();
+            }
+        return 0;
+    });
+}
+
 int luzref_mesh_bvh(void* s, int32_t mesh, LuzMeshNode64* nodes, int64_t cap, int64_t* count, int64_t* order,
                     int64_t order_cap)
 {

@@ -56,6 +56,32 @@ def adjoint_case():
     return w, adj, picks
 
 
+def nfor_synthetic(width: int = 40, height: int = 32, seed: int = 3) -> dict:
+    """Seeded NFOR buffers with the structure of a render's: smooth colour with noise, a
+    few fireflies, an edge in the features, small variances."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:height, 0:width]
+    base = np.stack([0.3 + 0.4 * xx / width, 0.2 + 0.5 * yy / height, 0.4 + 0.1 * np.sin(xx / 5.0)], -1)
+    base[:, width // 2:] *= 0.5                        # an edge the features also show
+    def half():
+        c = base + rng.normal(0.0, 0.05, base.shape)
+        for _ in range(6):                             # fireflies
+            c[rng.integers(2, height - 2), rng.integers(2, width - 2)] = rng.uniform(3.0, 9.0, 3)
+        return np.clip(c, 0.0, None)
+    feat = np.zeros((height, width, 11))
+    feat[..., 0] = xx / (width - 1.0)
+    feat[..., 1] = yy / (height - 1.0)
+    feat[..., 2] = 1.0
+    feat[..., 3] = 0.5 + 0.1 * (xx >= width // 2)
+    feat[..., 4:7] = 0.5 + 0.3 * np.stack([np.cos(xx / 7.0), np.sin(yy / 6.0), np.full(xx.shape, 0.2)], -1)
+    feat[..., 7:10] = np.where((xx >= width // 2)[..., None], 0.3, 0.7)
+    feat[..., 10] = 1.0 / 7.0
+    fa = feat + rng.normal(0.0, 0.01, feat.shape)
+    fb = feat + rng.normal(0.0, 0.01, feat.shape)
+    return {"color_a": half(), "color_b": half(), "color_variance": rng.uniform(1e-4, 3e-3, (height, width)),
+            "features_a": fa, "features_b": fb, "feature_variance": rng.uniform(1e-6, 1e-4, (height, width, 11))}
+
+
 BVH_CASES = {
     "box": lambda: scenes.cornell().scene,
     "icosphere3": lambda: scenes.mesh_glossy(level=3).scene,

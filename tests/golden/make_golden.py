@@ -13,7 +13,8 @@ output of the unmodified reference code:
   adjoint_cornell.npz central differences of the reference's film functional
                      sum(adjoint * film) with respect to chosen texel channels
                      (the reference has no gradients; common random numbers: same seed)
-Usage: python tests/golden/make_golden.py [adaptive | adjoint | cases <name>...]   (only those files)
+  nfor.npz           Denoise::applyNFOR outputs (src/core/Denoise/NFOR.cpp:977-1102)
+Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | cases <name>...]   (only those files)
 """
 from __future__ import annotations
 
@@ -29,7 +30,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import ADAPTIVE_CASES, BVH_CASES, CASES, adjoint_case, camera_rays, path_keys  # noqa: E402
+from cases import ADAPTIVE_CASES, BVH_CASES, CASES, adjoint_case, camera_rays, nfor_synthetic, path_keys  # noqa: E402
 from luz_b200 import native  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
@@ -104,6 +105,22 @@ def case_fixtures(o, only=None):
         print("golden", name, flush=True)
 
 
+NFOR_KEYS = ("color_a", "color_b", "color_variance", "features_a", "features_b", "feature_variance")
+
+
+def nfor_fixture(o):
+    """nfor.npz: Denoise::applyNFOR outputs for the NFOR buffers of the adaptive fixtures and of
+    cases.nfor_synthetic() (default settings)."""
+    out = {}
+    for name in ("tiny_nfor", "tiny_adaptive_nfor"):
+        g = np.load(os.path.join(HERE, f"adaptive_{name}.npz"))
+        out[name] = o.nfor({k: g[k] for k in NFOR_KEYS})
+    out["synthetic"] = o.nfor(nfor_synthetic())
+    out["synthetic_r3"] = o.nfor(nfor_synthetic(), prefilter_radius=2, regression_radius=3, patch_radius=2)
+    np.savez_compressed(os.path.join(HERE, "nfor.npz"), **out)
+    print("golden nfor", flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -111,6 +128,9 @@ def main():
         return
     if sys.argv[1:] == ["adjoint"]:
         adjoint_fixture(o)
+        return
+    if sys.argv[1:] == ["nfor"]:
+        nfor_fixture(o)
         return
     if sys.argv[1:2] == ["cases"]:     # cases <name>...: only the per-case files of those cases
         case_fixtures(o, sys.argv[2:])
@@ -137,6 +157,7 @@ def main():
     case_fixtures(o)
     adaptive_fixtures(o)
     adjoint_fixture(o)
+    nfor_fixture(o)
 
 
 if __name__ == "__main__":
