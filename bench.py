@@ -386,6 +386,41 @@ def run_adjoint(args):
     tg.close()
 
 
+def run_nfor(args):
+    """--workload nfor1080: NFOR buffers of a 1920x1080, 16-spp render of the mesh + glossy
+    scene (luz_gpu_render_ex), denoised by luz_gpu_nfor_denoise (host buffers in and out, host
+    wall clock) and, once, by the reference's Denoise::applyNFOR on all host threads."""
+    from luz_b200 import native
+    w = workload("mesh_glossy", 16)
+    g = native.GpuScene(w.scene.build())
+    _, _, bufs, _ = g.render_ex(native.params(w.width, w.height, w.spp, w.max_bounces, w.seed), None, True)
+    g.close()
+    for _ in range(max(1, args.warmup)):
+        native.nfor_denoise(bufs)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        native.nfor_denoise(bufs)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    px = float(w.width * w.height)
+    out = {"metric": "Mpixels/s denoised", "value": px / t / 1e6, "unit": "Mpixels/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene render)",
+           "timing": "host wall clock around luz_gpu_nfor_denoise (host buffers in and out)",
+           "config": {"workload": "nfor1080: NFOR buffers of mesh_glossy 1920x1080 16spp, default NFORSettings"}}
+    sys.path.insert(0, REFERENCE_DIR)
+    import oracle as O
+    if O.reference_available(fast=True):
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.RefOracle(fast=True).nfor(bufs, threads=threads)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": px / tc / 1e6, "unit": "Mpixels/s", "cores": threads, "kind": "reference",
+                               "sample": f"the same buffers, Denoise::applyNFOR, {tc * 1e3:.0f} ms"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -394,6 +429,8 @@ def main():
         run_batch(args)
     elif args.workload == "adjoint_c3":
         run_adjoint(args)
+    elif args.workload == "nfor1080":
+        run_nfor(args)
     else:
         run_ours(args)
 
