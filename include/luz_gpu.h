@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LUZ_GPU_ABI_VERSION 2
+#define LUZ_GPU_ABI_VERSION 3
 
 /* status codes */
 #define LUZ_OK            0
@@ -229,6 +229,7 @@ typedef struct LuzRenderStats {
     int64_t  extend_launches, shadow_launches;
     double   ext_nodes, ext_tris, ext_top;     /* LUZ_RENDER_COUNT: mesh nodes, triangles,  */
     double   sh_nodes, sh_tris, sh_top;        /* top-level records read (ext / shadow)     */
+    double   denoise_ms;          /* luz_gpu_render_denoised: device time of NFOR    */
 } LuzRenderStats;
 
 /* One closest-hit / any-hit result (luz_gpu_trace_rays). */
@@ -416,6 +417,20 @@ typedef struct LuzNforSettings {
 int luz_gpu_nfor_denoise(int32_t device, const LuzNforBuffers* buffers, int32_t width, int32_t height,
                          const LuzNforSettings* settings, double* rgb_out);
 int luz_gpu_nfor_error(char* buf, size_t len);
+
+/* Render and denoise in one call, the NFOR buffers staying on the device: the
+ * _manageThreads tail (src/renderer/Threads.cpp:514-536) that runs
+ * Denoise::applyNFOR on the scene's denoise buffers after the sample loop.
+ * Samples use the half-buffer streams 1 and 2 as in luz_gpu_render_ex with
+ * nfor set. rgb_out (W*H*3 floats) is the film of per-pixel means, denoised_out
+ * (W*H*3 doubles) the NFOR image; settings NULL = NFORSettings defaults.
+ * stats->denoise_ms is the device time of the denoiser. Errors: those of
+ * luz_gpu_render_ex, and LUZ_E_INVALID for bad settings (radii must be
+ * positive) before any sample is rendered. */
+int luz_gpu_render_denoised(luz_gpu_scene* scene, const LuzRenderParams* params,
+                            const LuzAdaptiveParams* adaptive, const LuzNforSettings* settings,
+                            float* rgb_out, double* denoised_out, int32_t* samples_out,
+                            LuzRenderStats* stats);
 
 
 /* Ray batch traversal (test hook and building block): rays are

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "luz_gpu.h"
+#include "nfor.h"
 #include "pack.h"
 #include "wavefront.cuh"
 
@@ -873,10 +874,14 @@ std::vector<uint32_t> round_ends(const AdaptiveRule& R)
 }
 
 int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptiveParams* ad, float* rgb_out,
-                 const LuzNforBuffers* nfor, int32_t* samples_out, LuzRenderStats* stats)
+                 const LuzNforBuffers* nfor, int32_t* samples_out, LuzRenderStats* stats,
+                 const LuzNforSettings* denoise = nullptr, double* denoised_out = nullptr)
 {
     check_params(p);
     check_adaptive(ad);
+    if (denoised_out && denoise &&
+        (denoise->regression_radius <= 0 || denoise->patch_radius <= 0 || denoise->feature_prefilter_radius < 0))
+        throw Status(LUZ_E_INVALID, "NFOR radii must be positive.");
     if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported with adaptive sampling or NFOR buffers.");
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
@@ -899,7 +904,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
         R.dark_min = R.max_samples;
     }
     const std::vector<uint32_t> ends = round_ends(R);
-    const bool want_nfor = nfor != nullptr;
+    const bool want_nfor = nfor != nullptr || denoised_out != nullptr;
 
     DeviceScratch D;
     PixAcc* acc = D.get<PixAcc>(npix, st);
@@ -991,7 +996,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
     CK(cudaMemcpy(rgb_out, d_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
     if (samples_out) CK(cudaMemcpy(samples_out, d_used, sizeof(int32_t) * (std::size_t)npix, cudaMemcpyDeviceToHost));
-    if (want_nfor) {
+    if (nfor) {
         auto down = [&](double* host, const double* dev, int64_t n) {
             if (host) CK(cudaMemcpy(host, dev, sizeof(double) * (std::size_t)n, cudaMemcpyDeviceToHost));
         };
@@ -1002,9 +1007,25 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
         down(nfor->features_b, nout.features_b, LUZ_NFOR_FEATURES * npix);
         down(nfor->feature_variance, nout.feature_variance, LUZ_NFOR_FEATURES * npix);
     }
+    float denoise_ms = 0.f;
+    if (denoised_out) {
+        // Denoise::applyNFOR on the device-resident buffers (Threads.cpp:514-536)
+        double* d_den = D.get<double>(3 * npix, st);
+        std::string msg;
+        CK(cudaEventRecord(s->ev0, st));
+        const int rc = luz_nfor_on_device(nout.color_a, nout.color_b, nout.color_variance, nout.features_a,
+                                          nout.features_b, nout.feature_variance, p->width, p->height, denoise, d_den,
+                                          (void*)st, msg);
+        if (rc != LUZ_OK) throw Status(rc, msg);
+        CK(cudaEventRecord(s->ev1, st));
+        CK(cudaEventSynchronize(s->ev1));
+        CK(cudaEventElapsedTime(&denoise_ms, s->ev0, s->ev1));
+        CK(cudaMemcpy(denoised_out, d_den, sizeof(double) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    }
     if (stats) {
         *stats = LuzRenderStats{};
         stats->render_ms = ms;
+        stats->denoise_ms = denoise_ms;
         stats->samples = samples;
         stats->extension_rays = (double)tot[0];
         stats->shadow_rays = (double)tot[1];
@@ -1488,6 +1509,16 @@ int luz_gpu_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdapt
     return guard([&] {
         if (!s || !rgb_out) throw Status(LUZ_E_INVALID, "NULL argument.");
         return do_render_ex(s, p, adaptive, rgb_out, nfor, samples_out, stats);
+    });
+}
+
+int luz_gpu_render_denoised(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptiveParams* adaptive,
+                            const LuzNforSettings* settings, float* rgb_out, double* denoised_out,
+                            int32_t* samples_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !rgb_out || !denoised_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_render_ex(s, p, adaptive, rgb_out, nullptr, samples_out, stats, settings, denoised_out);
     });
 }
 

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "luz_gpu.h"
+#include "nfor.h"
 
 namespace luz_nfor {
 
@@ -170,68 +171,6 @@ __device__ __forceinline__ double weight_from_distance(double d, double bw, doub
     return exp(-d / fmax(minvar, bw * bw));
 }
 
-struct Reg {
-    double m[kR][kR];
-    double rhs[kR][3];
-};
-__device__ __forceinline__ void reg_init(Reg& R)
-{
-    for (int i = 0; i < kR; i++) {
-        for (int j = 0; j < kR; j++) R.m[i][j] = 0.0;
-        R.rhs[i][0] = R.rhs[i][1] = R.rhs[i][2] = 0.0;
-        R.m[i][i] = 1e-4;   // ridge
-    }
-}
-__device__ __forceinline__ void reg_add(Reg& R, const double* basis, double wgt, const double* c)
-{
-    for (int row = 0; row < kR; row++) {
-        const double wb = wgt * basis[row];
-        for (int col = row; col < kR; col++) R.m[row][col] += wb * basis[col];
-        R.rhs[row][0] += wb * c[0];
-        R.rhs[row][1] += wb * c[1];
-        R.rhs[row][2] += wb * c[2];
-    }
-}
-// completeRegressionMatrix + solveLinearSystemRGB (NFOR.cpp:467-517, 634-643)
-__device__ bool reg_solve(Reg& R)
-{
-    for (int row = 1; row < kR; row++)
-        for (int col = 0; col < row; col++) R.m[row][col] = R.m[col][row];
-    for (int pv = 0; pv < kR; pv++) {
-        int best = pv;
-        double bv = fabs(R.m[pv][pv]);
-        for (int row = pv + 1; row < kR; row++) {
-            const double v = fabs(R.m[row][pv]);
-            if (v > bv) {
-                bv = v;
-                best = row;
-            }
-        }
-        if (bv < 1e-10) return false;
-        if (best != pv) {
-            for (int c = 0; c < kR; c++) {
-                const double t = R.m[pv][c];
-                R.m[pv][c] = R.m[best][c];
-                R.m[best][c] = t;
-            }
-            for (int c = 0; c < 3; c++) {
-                const double t = R.rhs[pv][c];
-                R.rhs[pv][c] = R.rhs[best][c];
-                R.rhs[best][c] = t;
-            }
-        }
-        const double p = R.m[pv][pv];
-        for (int c = pv; c < kR; c++) R.m[pv][c] /= p;
-        for (int c = 0; c < 3; c++) R.rhs[pv][c] /= p;
-        for (int row = 0; row < kR; row++) {
-            if (row == pv) continue;
-            const double f = R.m[row][pv];
-            for (int c = pv; c < kR; c++) R.m[row][c] -= f * R.m[pv][c];
-            for (int c = 0; c < 3; c++) R.rhs[row][c] -= f * R.rhs[pv][c];
-        }
-    }
-    return true;
-}
 // weightedAverageFallback (NFOR.cpp:519-556)
 __device__ void fallback(Img I, const double* image, const double* var, double vscale, int x, int y, int radius,
                          double minvar, double* o)
@@ -266,41 +205,132 @@ struct RegArgs {
     double* out2;
 };
 
-// regressionPass (NFOR.cpp:674-738) / regressionPairPass (:740-831)
-__global__ void k_regression(RegArgs A)
+// regressionPass (NFOR.cpp:674-738) / regressionPairPass (:740-831) with one
+// half-warp per (pixel, bandwidth): lane c of the
+// half holds column c of the 12 x 12 normal equations (c < 12) or one colour
+// channel of the right-hand side (c = 12..14), in registers. Every entry is
+// accumulated over the neighbours in the reference's order with the
+// reference's products, the lower triangle is mirrored from the upper one
+// (completeRegressionMatrix), and Gauss-Jordan elimination with partial
+// pivoting (solveLinearSystemRGB) runs with the pivot column's lane choosing the
+// pivot row: the reference's arithmetic, spread over the lanes instead of a
+// 1.4 KB per-thread array in local memory.
+// Pair mode (bw2 >= 0): one pixel per warp, half 0 with bw1, half 1 with bw2.
+// Single mode: two pixels per warp, both with bw1.
+__global__ void __launch_bounds__(128) k_regression_warp(RegArgs A)
 {
     const Img I = A.I;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= I.w || y >= I.h) return;
-    const int center = y * I.w + x;
+    const unsigned lane = threadIdx.x & 31u, half = lane >> 4, j = lane & 15u;
+    const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
     const bool pair = A.bw2 >= 0.0;
-    Reg R1, R2;
-    reg_init(R1);
-    if (pair) reg_init(R2);
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long pix = pair ? warp : 2 * warp + half;
+    const long long npix = (long long)I.w * I.h;
+    if (pix >= npix) return;   // both halves of a warp leave together except the last odd pixel's half
+    const int x = (int)(pix % I.w), y = (int)(pix / I.w);
+    const int center = y * I.w + x;
+    const double bw = (pair && half) ? A.bw2 : A.bw1;
+    double* out = (pair && half) ? A.out2 : A.out1;
+    double M[kR];
+#pragma unroll
+    for (int r = 0; r < kR; r++) M[r] = (j < (unsigned)kR && r == (int)j) ? 1e-4 : 0.0;   // ridge on the diagonal
+    const int P = (2 * A.patch + 1) * (2 * A.patch + 1);
     for (int oy = -A.radius; oy <= A.radius; oy++)
         for (int ox = -A.radius; ox <= A.radius; ox++) {
             const int sx = clampc(x + ox, I.w), sy = clampc(y + oy, I.h);
             const int s = sy * I.w + sx;
-            const double d = patch_distance(I, A.image, A.var, A.vscale, x, y, sx, sy, A.patch, A.minvar);
+            // patchDistance: lane t of the half forms term t, the sum runs in term order
+            double d = 0.0;
+            if (!(sx == x && sy == y)) {
+                for (int t0 = 0; t0 < P; t0 += 16) {
+                    double term = 0.0;
+                    const int t = t0 + (int)j;
+                    if (t < P) {
+                        const int py = t / (2 * A.patch + 1) - A.patch, px = t % (2 * A.patch + 1) - A.patch;
+                        const int a = clampc(y + py, I.h) * I.w + clampc(x + px, I.w);
+                        const int b = clampc(sy + py, I.h) * I.w + clampc(sx + px, I.w);
+                        const double lv = (A.var[a] * A.vscale) + (A.var[b] * A.vscale) + A.minvar;
+                        term = cdist2(A.image + 3 * a, A.image + 3 * b) / lv;
+                    }
+                    const int nt = min(16, P - t0);
+                    for (int k = 0; k < nt; k++) d += __shfl_sync(hmask, term, k, 16);
+                }
+                d = d / (double)P;
+            }
+            const double wgt = weight_from_distance(d, bw, A.minvar);
             double basis[kR];
             basis[0] = 1.0;
+#pragma unroll
             for (int f = 0; f < kF; f++)
                 basis[f + 1] = A.features[(size_t)kF * s + f] - A.features[(size_t)kF * center + f];
-            reg_add(R1, basis, weight_from_distance(d, A.bw1, A.minvar), A.image + 3 * s);
-            if (pair) reg_add(R2, basis, weight_from_distance(d, A.bw2, A.minvar), A.image + 3 * s);
+            if (j < (unsigned)kR) {   // matrix column j: rows 0..j
+                double bj = 0.0;
+#pragma unroll
+                for (int k = 0; k < kR; k++)
+                    if (k == (int)j) bj = basis[k];
+#pragma unroll
+                for (int r = 0; r < kR; r++)
+                    if (r <= (int)j) M[r] += (wgt * basis[r]) * bj;
+            } else if (j < (unsigned)kR + 3) {   // right-hand side, channel j - 12
+                const double c = A.image[3 * s + (j - kR)];
+#pragma unroll
+                for (int r = 0; r < kR; r++) M[r] += (wgt * basis[r]) * c;
+            }
         }
-    double* o1 = A.out1 + 3 * center;
-    if (reg_solve(R1)) {
-        for (int k = 0; k < 3; k++) o1[k] = R1.rhs[0][k];
-    } else {
-        fallback(I, A.image, A.var, A.vscale, x, y, A.radius, A.minvar, o1);
+    // completeRegressionMatrix: m[r][i] = m[i][r] for r > i (column i takes row i of column r)
+#pragma unroll
+    for (int r = 1; r < kR; r++)
+#pragma unroll
+        for (int i = 0; i < r; i++) {
+            const double t = __shfl_sync(hmask, M[i], r, 16);
+            if ((int)j == i) M[r] = t;
+        }
+    // Gauss-Jordan with partial pivoting (solveLinearSystemRGB)
+    bool ok = true;
+#pragma unroll
+    for (int pv = 0; pv < kR; pv++) {
+        int best = pv;
+        double bv = fabs(M[pv]);
+#pragma unroll
+        for (int r = pv + 1; r < kR; r++) {
+            const double v = fabs(M[r]);
+            if (v > bv) {
+                bv = v;
+                best = r;
+            }
+        }
+        best = __shfl_sync(hmask, best, pv, 16);
+        bv = __shfl_sync(hmask, bv, pv, 16);
+        if (bv < 1e-10) {
+            ok = false;
+            break;
+        }
+        if (best != pv) {
+#pragma unroll
+            for (int r = pv + 1; r < kR; r++)
+                if (r == best) {
+                    const double t = M[r];
+                    M[r] = M[pv];
+                    M[pv] = t;
+                }
+        }
+        const double p = __shfl_sync(hmask, M[pv], pv, 16);
+        const bool mine = (int)j >= pv && j < (unsigned)kR + 3;   // columns pivot.. and the right-hand side
+        if (mine) M[pv] /= p;
+        double f[kR];
+#pragma unroll
+        for (int r = 0; r < kR; r++) f[r] = __shfl_sync(hmask, M[r], pv, 16);
+        if (mine) {
+            const double mp = M[pv];
+#pragma unroll
+            for (int r = 0; r < kR; r++)
+                if (r != pv) M[r] -= f[r] * mp;
+        }
     }
-    if (!pair) return;
-    double* o2 = A.out2 + 3 * center;
-    if (reg_solve(R2)) {
-        for (int k = 0; k < 3; k++) o2[k] = R2.rhs[0][k];
-    } else {
-        fallback(I, A.image, A.var, A.vscale, x, y, A.radius, A.minvar, o2);
+    if (ok) {
+        if (j >= (unsigned)kR && j < (unsigned)kR + 3) out[3 * center + (j - kR)] = M[0];
+    } else if (j == 0) {
+        fallback(I, A.image, A.var, A.vscale, x, y, A.radius, A.minvar, out + 3 * center);
     }
 }
 
@@ -411,16 +441,73 @@ struct Buffers {
     }
 };
 
+LuzNforSettings checked_settings(const LuzNforSettings* st)
+{
+    LuzNforSettings s{1, 2, 1, 0, 1e-5};   // NFORSettings defaults (include/luz/Denoise/NFOR.hpp:39-47)
+    if (st) s = *st;
+    if (s.regression_radius <= 0 || s.patch_radius <= 0 || s.feature_prefilter_radius < 0)
+        throw NforError{LUZ_E_INVALID, "NFOR radii must be positive."};
+    return s;
+}
+
+void run_device(const double* ca, const double* cb, const double* cv, const double* ga, const double* gb,
+                const double* gv, int32_t width, int32_t height, const LuzNforSettings& s, double* d_out,
+                cudaStream_t st)
+{
+    const size_t n = (size_t)width * height;
+    Buffers B;
+    const Img I{width, height};
+    const dim3 blk(64), grd((unsigned)((width + 63) / 64), (unsigned)height);
+    // firefly suppression of A, B and of their average (applyNFOR :989-996)
+    double* fa = B.get(3 * n);
+    double* fb = B.get(3 * n);
+    double* col = B.get(3 * n);
+    k_firefly<<<grd, blk, 0, st>>>(I, ca, nullptr, fa);
+    k_firefly<<<grd, blk, 0, st>>>(I, cb, nullptr, fb);
+    k_firefly<<<grd, blk, 0, st>>>(I, fa, fb, col);
+    // features prefiltered with the other half as the guide
+    double* pfa = B.get(kF * n);
+    double* pfb = B.get(kF * n);
+    k_prefilter<<<grd, blk, 0, st>>>(I, ga, gb, gv, s.feature_prefilter_radius, s.min_variance, pfa);
+    k_prefilter<<<grd, blk, 0, st>>>(I, gb, ga, gv, s.feature_prefilter_radius, s.min_variance, pfb);
+    // two-bandwidth regressions (variance doubled)
+    double* ra1 = B.get(3 * n);
+    double* ra2 = B.get(3 * n);
+    double* rb1 = B.get(3 * n);
+    double* rb2 = B.get(3 * n);
+    const unsigned rgrid_pair = (unsigned)((n * 32 + 127) / 128), rgrid_single = (unsigned)((((n + 1) / 2) * 32 + 127) / 128);
+    RegArgs A{I, fa, pfb, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, ra1, ra2};
+    k_regression_warp<<<rgrid_pair, 128, 0, st>>>(A);
+    RegArgs Bb{I, fb, pfa, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, rb1, rb2};
+    k_regression_warp<<<rgrid_pair, 128, 0, st>>>(Bb);
+    // MSE, filtered; selection, filtered (guide: the averaged colour, undoubled variance)
+    double* m1 = B.get(n);
+    double* m2 = B.get(n);
+    double* fm1 = B.get(n);
+    double* fm2 = B.get(n);
+    double* s1 = B.get(n);
+    double* s2 = B.get(n);
+    k_mse<<<grd, blk, 0, st>>>(I, fa, fb, ra1, rb1, ra2, rb2, cv, m1, m2);
+    k_filter_pair<<<grd, blk, 0, st>>>(I, m1, m2, 0, col, cv, 3, s.min_variance, fm1, fm2);
+    k_filter_pair<<<grd, blk, 0, st>>>(I, fm1, fm2, 1, col, cv, 3, s.min_variance, s1, s2);
+    // blend, final features and variance, last regression
+    double* comb = B.get(3 * n);
+    double* ff = B.get(kF * n);
+    double* fv = B.get(n);
+    k_combine<<<grd, blk, 0, st>>>(I, s1, s2, fm1, fm2, ra1, ra2, rb1, rb2, pfa, pfb, s.min_variance, comb, ff, fv);
+    RegArgs C{I, comb, ff, fv, 1.0, s.regression_radius, s.patch_radius, s.min_variance, 1.0, -1.0, d_out, nullptr};
+    k_regression_warp<<<rgrid_single, 128, 0, st>>>(C);
+    NCK(cudaGetLastError());
+    NCK(cudaStreamSynchronize(st));   // the scratch buffers are freed on return
+}
+
 int do_nfor(int32_t device, const LuzNforBuffers* in, int32_t width, int32_t height, const LuzNforSettings* st,
             double* rgb_out)
 {
     if (!in || !rgb_out) throw NforError{LUZ_E_INVALID, "NULL argument."};
     if (width < 0 || height < 0) throw NforError{LUZ_E_INVALID, "Image size must be non-negative."};
-    LuzNforSettings s{1, 2, 1, 0, 1e-5};   // NFORSettings defaults (include/luz/Denoise/NFOR.hpp:39-47)
-    if (st) s = *st;
+    const LuzNforSettings s = checked_settings(st);
     if (width == 0 || height == 0) return LUZ_OK;   // empty buffers: empty image
-    if (s.regression_radius <= 0 || s.patch_radius <= 0) throw NforError{LUZ_E_INVALID, "NFOR radii must be positive."};
-    if (s.feature_prefilter_radius < 0) throw NforError{LUZ_E_INVALID, "NFOR radii must be positive."};
     if (!in->color_a || !in->color_b || !in->color_variance || !in->features_a || !in->features_b || !in->feature_variance)
         throw NforError{LUZ_E_INVALID, "NFOR needs every buffer."};
     NCK(cudaSetDevice(device));
@@ -432,59 +519,34 @@ int do_nfor(int32_t device, const LuzNforBuffers* in, int32_t width, int32_t hei
     double* ga = B.get(kF * n);
     double* gb = B.get(kF * n);
     double* gv = B.get(kF * n);
+    double* out = B.get(3 * n);
     NCK(cudaMemcpy(ca, in->color_a, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
     NCK(cudaMemcpy(cb, in->color_b, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
     NCK(cudaMemcpy(cv, in->color_variance, sizeof(double) * n, cudaMemcpyHostToDevice));
     NCK(cudaMemcpy(ga, in->features_a, sizeof(double) * kF * n, cudaMemcpyHostToDevice));
     NCK(cudaMemcpy(gb, in->features_b, sizeof(double) * kF * n, cudaMemcpyHostToDevice));
     NCK(cudaMemcpy(gv, in->feature_variance, sizeof(double) * kF * n, cudaMemcpyHostToDevice));
-    const Img I{width, height};
-    const dim3 blk(64), grd((unsigned)((width + 63) / 64), (unsigned)height);
-    // firefly suppression of A, B and of their average (applyNFOR :989-996)
-    double* fa = B.get(3 * n);
-    double* fb = B.get(3 * n);
-    double* col = B.get(3 * n);
-    k_firefly<<<grd, blk>>>(I, ca, nullptr, fa);
-    k_firefly<<<grd, blk>>>(I, cb, nullptr, fb);
-    k_firefly<<<grd, blk>>>(I, fa, fb, col);
-    // features prefiltered with the other half as the guide
-    double* pfa = B.get(kF * n);
-    double* pfb = B.get(kF * n);
-    k_prefilter<<<grd, blk>>>(I, ga, gb, gv, s.feature_prefilter_radius, s.min_variance, pfa);
-    k_prefilter<<<grd, blk>>>(I, gb, ga, gv, s.feature_prefilter_radius, s.min_variance, pfb);
-    // two-bandwidth regressions (variance doubled)
-    double* ra1 = B.get(3 * n);
-    double* ra2 = B.get(3 * n);
-    double* rb1 = B.get(3 * n);
-    double* rb2 = B.get(3 * n);
-    RegArgs A{I, fa, pfb, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, ra1, ra2};
-    k_regression<<<grd, blk>>>(A);
-    RegArgs Bb{I, fb, pfa, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, rb1, rb2};
-    k_regression<<<grd, blk>>>(Bb);
-    // MSE, filtered; selection, filtered (guide: the averaged colour, undoubled variance)
-    double* m1 = B.get(n);
-    double* m2 = B.get(n);
-    double* fm1 = B.get(n);
-    double* fm2 = B.get(n);
-    double* s1 = B.get(n);
-    double* s2 = B.get(n);
-    k_mse<<<grd, blk>>>(I, fa, fb, ra1, rb1, ra2, rb2, cv, m1, m2);
-    k_filter_pair<<<grd, blk>>>(I, m1, m2, 0, col, cv, 3, s.min_variance, fm1, fm2);
-    k_filter_pair<<<grd, blk>>>(I, fm1, fm2, 1, col, cv, 3, s.min_variance, s1, s2);
-    // blend, final features and variance, last regression
-    double* comb = B.get(3 * n);
-    double* ff = B.get(kF * n);
-    double* fv = B.get(n);
-    double* out = B.get(3 * n);
-    k_combine<<<grd, blk>>>(I, s1, s2, fm1, fm2, ra1, ra2, rb1, rb2, pfa, pfb, s.min_variance, comb, ff, fv);
-    RegArgs C{I, comb, ff, fv, 1.0, s.regression_radius, s.patch_radius, s.min_variance, 1.0, -1.0, out, nullptr};
-    k_regression<<<grd, blk>>>(C);
-    NCK(cudaGetLastError());
+    run_device(ca, cb, cv, ga, gb, gv, width, height, s, out, 0);
     NCK(cudaMemcpy(rgb_out, out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
     return LUZ_OK;
 }
 
 }  // namespace
+
+int luz_nfor_on_device(const double* ca, const double* cb, const double* cv, const double* ga, const double* gb,
+                       const double* gv, int32_t width, int32_t height, const LuzNforSettings* settings,
+                       double* d_out, void* stream, std::string& msg)
+{
+    try {
+        const LuzNforSettings s = checked_settings(settings);
+        if (width > 0 && height > 0)
+            run_device(ca, cb, cv, ga, gb, gv, width, height, s, d_out, (cudaStream_t)stream);
+        return LUZ_OK;
+    } catch (const NforError& e) {
+        msg = e.msg;
+        return e.code;
+    }
+}
 
 extern "C" int luz_gpu_nfor_error(char* buf, size_t len)
 {

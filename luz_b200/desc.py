@@ -15,7 +15,7 @@ from typing import List, Optional
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE = 1, 2, 3, 4
 MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
@@ -128,6 +128,7 @@ class RenderStats(C.Structure):
         ("extend_launches", C.c_int64), ("shadow_launches", C.c_int64),
         ("ext_nodes", C.c_double), ("ext_tris", C.c_double), ("ext_top", C.c_double),
         ("sh_nodes", C.c_double), ("sh_tris", C.c_double), ("sh_top", C.c_double),
+        ("denoise_ms", C.c_double),
     ]
 
 

@@ -24,7 +24,7 @@ EXPORTED = [
     "luz_gpu_render", "luz_gpu_render_device", "luz_gpu_trace_paths", "luz_gpu_trace_rays",
     "luz_gpu_render_device_noalloc", "luz_gpu_render_ex", "luz_gpu_batch_render",
     "luz_gpu_scene_set_texture", "luz_gpu_adjoint_forward", "luz_gpu_adjoint_backward",
-    "luz_gpu_nfor_denoise", "luz_gpu_nfor_error",
+    "luz_gpu_nfor_denoise", "luz_gpu_nfor_error", "luz_gpu_render_denoised",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -68,6 +68,8 @@ def lib():
     L.luz_gpu_batch_render.argtypes = [vp, vp, i32, vp, vp]
     L.luz_gpu_nfor_denoise.argtypes = [i32, C.POINTER(D.NforBuffers), i32, i32, C.POINTER(D.NforSettings), vp]
     L.luz_gpu_nfor_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.luz_gpu_render_denoised.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams),
+                                          C.POINTER(D.NforSettings), vp, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_scene_set_texture.argtypes = [vp, i32, vp]
     L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
@@ -196,6 +198,19 @@ class GpuScene:
                                        out.ctypes.data, C.byref(nb) if nb is not None else None, used.ctypes.data,
                                        C.byref(st)))
         return out, used, bufs, st
+
+    def render_denoised(self, p: D.RenderParams, adaptive: Optional[D.AdaptiveParams] = None,
+                        settings: Optional[D.NforSettings] = None):
+        """luz_gpu_render_denoised: film, NFOR image (H x W x 3 float64), samples used per pixel and stats."""
+        h, w = p.height, p.width
+        out = np.zeros((h, w, 3), np.float32)
+        den = np.zeros((h, w, 3), np.float64)
+        used = np.zeros((h, w), np.int32)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_render_denoised(self.h, C.byref(p), C.byref(adaptive) if adaptive is not None else None,
+                                             C.byref(settings) if settings is not None else None, out.ctypes.data,
+                                             den.ctypes.data, used.ctypes.data, C.byref(st)))
+        return out, den, used, st
 
     def set_texture(self, texture: int, rgb: np.ndarray):
         rgb = np.ascontiguousarray(rgb, np.float64)

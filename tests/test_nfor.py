@@ -48,3 +48,28 @@ def test_gpu_nfor_settings_rejected():
     with pytest.raises(native.LuzError) as e:
         native.nfor_denoise(nfor_synthetic(), regression_radius=0)
     assert e.value.code == -1 and "NFOR radii must be positive." in str(e.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny_nfor", "tiny_adaptive_nfor"])
+def test_render_denoised_equals_render_then_denoise(name):
+    """luz_gpu_render_denoised (buffers stay on the device) gives the film of
+    render_ex and exactly the image of luz_gpu_nfor_denoise on its buffers."""
+    from cases import ADAPTIVE_CASES
+    from luz_b200 import desc as D
+    fn, ad, _ = ADAPTIVE_CASES[name]
+    w = fn()
+    g = native.GpuScene(w.scene.build())
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    a = native.adaptive(**ad) if ad else None
+    img, used, bufs, st = g.render_ex(p, a, True)
+    img2, den, used2, st2 = g.render_denoised(p, a)
+    assert np.array_equal(img, img2) and np.array_equal(used, used2)
+    assert np.array_equal(den, native.nfor_denoise(bufs))
+    assert st2.samples == st.samples and st2.denoise_ms > 0.0
+    s3 = D.NforSettings(2, 3, 2, 0, 1e-5)
+    _, den3, _, _ = g.render_denoised(p, a, s3)
+    assert np.array_equal(den3, native.nfor_denoise(bufs, prefilter_radius=2, regression_radius=3, patch_radius=2))
+    with pytest.raises(native.LuzError) as e:
+        g.render_denoised(p, a, D.NforSettings(1, 0, 1, 0, 1e-5))
+    assert e.value.code == -1 and "NFOR radii must be positive." in str(e.value)
