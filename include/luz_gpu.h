@@ -179,6 +179,23 @@ typedef struct LuzAtmosphereDesc {
     double  stars_brightness;
 } LuzAtmosphereDesc;
 
+/* Caustic photon map settings (Scene::setCausticsEnabled / setCausticPhotonCount
+ * / setCausticPassCount / setCausticRadiusMeters / setCausticAlpha,
+ * src/scene/Scene.cpp:302-360; defaults include/luz/Defaults.hpp:51-55: off,
+ * 100000, 8, 0.05, 0.7). Read only when enabled != 0; then photons >= 0,
+ * passes > 0, radius_meters finite > 0 and alpha in (0, 1], with the
+ * reference's messages otherwise. The map (CausticPhotonMap::build,
+ * src/renderer/CausticPhotonMap.cpp:430-551) is built on the device from the
+ * render seed and max_bounces of each render call that needs it. */
+typedef struct LuzCausticsDesc {
+    int32_t enabled;
+    int32_t photons;
+    int32_t passes;
+    int32_t reserved;
+    double  radius_meters;
+    double  alpha;
+} LuzCausticsDesc;
+
 typedef struct LuzSceneDesc {
     int32_t abi_version;          /* LUZ_GPU_ABI_VERSION                            */
     int32_t material_count;
@@ -198,6 +215,7 @@ typedef struct LuzSceneDesc {
     int32_t _pad;
     const LuzIesDesc* ies;
     LuzAtmosphereDesc atmosphere;
+    LuzCausticsDesc caustics;
 } LuzSceneDesc;
 
 /* Render settings: the parts of Scene that Renderer::render reads for the
@@ -230,6 +248,8 @@ typedef struct LuzRenderStats {
     double   ext_nodes, ext_tris, ext_top;     /* LUZ_RENDER_COUNT: mesh nodes, triangles,  */
     double   sh_nodes, sh_tris, sh_top;        /* top-level records read (ext / shadow)     */
     double   denoise_ms;          /* luz_gpu_render_denoised: device time of NFOR    */
+    double   caustic_photons;     /* photons stored in the caustic map (photonCount) */
+    double   caustic_ms;          /* device time of the caustic map build            */
 } LuzRenderStats;
 
 /* One closest-hit / any-hit result (luz_gpu_trace_rays). */

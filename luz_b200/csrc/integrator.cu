@@ -12,6 +12,7 @@
 // deferred to the shadow kernel: shade stores each candidate contribution in a
 // per-path "pending" slot and the shadow kernel clears the slot when the ray is
 // occluded, which gives the same sum as the reference's inline test.
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -466,6 +467,128 @@ __global__ void k_trace_rays(DScene S, const float* rays, int64_t n, int any, ui
 using RayKernel = void (*)(DScene, const float*, int64_t, int, uint32_t, const int32_t*, LuzHit*);
 const RayKernel kTraceRayKernels[4] = {k_trace_rays<0>, k_trace_rays<1>, k_trace_rays<2>, k_trace_rays<3>};
 
+// ----------------------------------------------------------------------------- caustic photon map
+
+// CausticPhotonMap::build photon loop (src/renderer/CausticPhotonMap.cpp:452-549),
+// one thread per photon index: photon i of pass p (passStart = target * p / passes)
+// samples with key (i, p, i - passStart, CAUSTIC_STREAM) under seed ^ CAUSTIC_SEED_SCRAMBLE.
+// A stored photon is written to slot i with its packed cell key; other slots keep
+// the empty key, so a stable sort by key gives cells in order and, inside a cell,
+// photons in index order (the reference's storePhoton order).
+template <uint32_t F>
+__global__ void __launch_bounds__(128) k_photons(DScene S, uint32_t seed, int max_bounces, float4* ph,
+                                                 unsigned long long* keys, uint32_t* order, uint32_t* stored)
+{
+    const GCaustics& G = S.k.caustics;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G.photons) return;
+    keys[i] = kEmptyCell;
+    order[i] = (uint32_t)i;
+    const int64_t target = G.photons, passes = G.passes;
+    int64_t pass = i * passes / target;
+    while (pass + 1 < passes && target * (pass + 1) / passes <= i) pass++;
+    while (pass > 0 && target * pass / passes > i) pass--;
+    const int64_t start = target * pass / passes;
+    Key k{base_key(seed ^ kCausticSeedScramble, (uint32_t)i, (uint32_t)pass, kCausticStream), (uint32_t)(i - start), 0u};
+    Emission e;
+    double sel = 0.0;
+    if (!photon_emission(S, k, e, sel)) return;
+    const double scale = e.power * G.m2_per_area, den = (double)target * sel;
+    F3 thr{(float)((double)e.emitted.x * scale / den), (float)((double)e.emitted.y * scale / den),
+           (float)((double)e.emitted.z * scale / den)};
+    if (!valid_positive(thr)) return;
+    TRay ray = make_ray(e.pos + e.dir * (2.0f * kTMin), e.dir);
+    bool caustic = false;
+    LocalStack<true> st;
+    for (int b = 0; b <= max_bounces; b++) {
+        k.bounce = (uint32_t)b;
+        VolSample vs{&k, 0.0, false};
+        const THit th = closest_hit<F>(S, ray, kTMin, kInf, vs, st);
+        if (th.obj < 0) break;
+        const Hit h = make_hit(S, ray, th);
+        const GMaterial m = S.materials[h.material];
+        if (m.type == MT_EMISSIVE) break;
+        if (caustic && receives_caustics(m)) {
+            const double r = G.radius_su;
+            unsigned long long key;
+            if (!pack_cell(floor((double)h.p.x / r), floor((double)h.p.y / r), floor((double)h.p.z / r), key)) {
+                atomicOr(S.error, ERR_CAUSTIC_GRID);
+                break;
+            }
+            ph[3 * i] = make_float4(h.p.x, h.p.y, h.p.z, thr.x);
+            ph[3 * i + 1] = make_float4(h.n.x, h.n.y, h.n.z, thr.y);
+            ph[3 * i + 2] = make_float4(ray.d.x, ray.d.y, ray.d.z, thr.z);
+            keys[i] = key;
+            atomicAdd(stored, 1u);
+            break;
+        }
+        Scatter sr;
+        if (!scatter(S, m, h, ray.d, k, sr)) break;
+        F3 att = sr.att;
+        if (!h.front && sr.absorb) {   // effectiveScatterAttenuation (:135-149)
+            const float dm = h.t * (float)S.k.meters_per_unit;
+            if (isfinite(dm) && dm > 0.0f)
+                att = att * F3{expf(-sr.absorption.x * dm), expf(-sr.absorption.y * dm), expf(-sr.absorption.z * dm)};
+        }
+        if (!valid_positive(att)) break;
+        if (!sr.specular && !(m.flags & MF_TRANSPORT)) break;
+        thr = thr * att;
+        if (!valid_positive(thr) || !photon_roulette(thr, b, k)) break;
+        ray = make_ray_x(h.p, sr.dir, h.volume ? -1 : h.obj, h.volume ? -1 : h.prim);
+        caustic = true;
+    }
+}
+
+using PhotonKernel = void (*)(DScene, uint32_t, int, float4*, unsigned long long*, uint32_t*, uint32_t*);
+const PhotonKernel kPhotonKernels[4] = {k_photons<0>, k_photons<1>, k_photons<2>, k_photons<3>};
+
+// Sorted photon j <- unsorted photon order[j].
+__global__ void k_photon_gather(const float4* raw, const uint32_t* order, uint32_t n, float4* out)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = order[j];
+    out[3 * (size_t)j] = raw[3 * (size_t)i];
+    out[3 * (size_t)j + 1] = raw[3 * (size_t)i + 1];
+    out[3 * (size_t)j + 2] = raw[3 * (size_t)i + 2];
+}
+// The first photon of each cell inserts the cell key with its begin index.
+// The table holds at least twice as many slots as photons, so a free slot exists.
+__global__ void k_cell_starts(const unsigned long long* keys, uint32_t n, unsigned long long* tkeys, uint2* ranges,
+                              uint32_t mask)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long key = keys[j];
+    if (j > 0 && keys[j - 1] == key) return;
+    uint32_t slot = cell_slot(key, mask);
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        const unsigned long long prev = atomicCAS(tkeys + slot, kEmptyCell, key);
+        if (prev == kEmptyCell || prev == key) {
+            ranges[slot].x = j;
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+}
+// The last photon of each cell writes the end of the cell's range.
+__global__ void k_cell_ends(const unsigned long long* keys, uint32_t n, const unsigned long long* tkeys, uint2* ranges,
+                            uint32_t mask)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long key = keys[j];
+    if (j + 1 < n && keys[j + 1] == key) return;
+    uint32_t slot = cell_slot(key, mask);
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        if (tkeys[slot] == key) {
+            ranges[slot].y = j + 1;
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+}
+
 }  // namespace luz
 
 // =============================================================================== host side
@@ -534,6 +657,23 @@ struct luz_gpu_scene {
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
     TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // caustic photon map: buffers grown on demand; the map is kept while the
+    // render seed and bounce limit stay the same (textures unchanged)
+    struct PhotonMap {
+        std::vector<void*> bufs, tbufs;
+        int64_t cap = 0, tcap = 0;
+        float4 *raw = nullptr, *ph = nullptr;
+        unsigned long long *kin = nullptr, *kout = nullptr, *tkeys = nullptr;
+        uint32_t *vin = nullptr, *vout = nullptr, *count = nullptr;
+        uint2* ranges = nullptr;
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0;
+        bool valid = false;
+        uint32_t seed = 0;
+        int bounces = -1;
+        uint32_t stored = 0;
+        float last_ms = 0.f;   // build time of the last call that built the map (0 when reused)
+    } cm;
 
     template <class T> T* up(const std::vector<T>& v)
     {
@@ -583,6 +723,8 @@ struct luz_gpu_scene {
     {
         cudaSetDevice(device);
         free_paths();
+        for (void* p : cm.bufs) cudaFree(p);
+        for (void* p : cm.tbufs) cudaFree(p);
         if (out_dev) cudaFree(out_dev);
         for (void* p : allocs) cudaFree(p);
         if (ctrl) cudaFree(ctrl);
@@ -672,6 +814,95 @@ WaveArgs base_args(luz_gpu_scene* s, const LuzRenderParams* p)
     return w;
 }
 
+// CausticPhotonMap::build for this render's seed and bounce limit (Renderer.cpp:40-48
+// builds it before every render): photon kernel, stable radix sort of the photon
+// slots by cell key, gather, and the cell table. Synchronous on st.
+void prepare_caustics(luz_gpu_scene* s, const LuzRenderParams* p, cudaStream_t st)
+{
+    const GCaustics& G = s->pack->consts.caustics;
+    auto& M = s->cm;
+    M.last_ms = 0.f;
+    if (!G.enabled) return;
+    if (M.valid && M.seed == p->seed && M.bounces == p->max_bounces) return;
+    M.valid = false;
+    s->ds.cm = DCaustics{};
+    const int64_t n = G.photons;
+    if (n > M.cap) {
+        for (void* q : M.bufs) cudaFree(q);
+        M.bufs.clear();
+        M.cap = 0;
+        auto get = [&](std::size_t bytes) {
+            void* q = dalloc<uint8_t>(bytes);
+            M.bufs.push_back(q);
+            return q;
+        };
+        M.raw = static_cast<float4*>(get(sizeof(float4) * 3 * (std::size_t)n));
+        M.ph = static_cast<float4*>(get(sizeof(float4) * 3 * (std::size_t)n));
+        M.kin = static_cast<unsigned long long*>(get(sizeof(unsigned long long) * (std::size_t)n));
+        M.kout = static_cast<unsigned long long*>(get(sizeof(unsigned long long) * (std::size_t)n));
+        M.vin = static_cast<uint32_t*>(get(sizeof(uint32_t) * (std::size_t)n));
+        M.vout = static_cast<uint32_t*>(get(sizeof(uint32_t) * (std::size_t)n));
+        M.count = static_cast<uint32_t*>(get(sizeof(uint32_t)));
+        M.tmp_bytes = 0;
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, M.tmp_bytes, M.kin, M.kout, M.vin, M.vout, (int)n, 0, 64, st));
+        M.tmp = get(std::max<size_t>(M.tmp_bytes, 16));
+        M.cap = n;
+    }
+    CK(cudaEventRecord(s->ev0, st));
+    CK(cudaMemsetAsync(M.count, 0, sizeof(uint32_t), st));
+    kPhotonKernels[s->ds.k.features & TF_ALL]<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+        s->ds, p->seed, p->max_bounces, M.raw, M.kin, M.vin, M.count);
+    CK(cudaGetLastError());
+    size_t tb = M.tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(M.tmp, tb, M.kin, M.kout, M.vin, M.vout, (int)n, 0, 64, st));
+    uint32_t stored = 0, err = 0;
+    CK(cudaMemcpyAsync(&stored, M.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err & ERR_CAUSTIC_GRID) {
+        CK(cudaMemset(s->ds.error, 0, sizeof(uint32_t)));
+        throw Status(LUZ_E_LIMIT, "Caustic photons lie outside the photon grid (2^21 cells per axis).");
+    }
+    int64_t T = 64;
+    while (T < 2 * (int64_t)stored) T *= 2;
+    if (T > M.tcap) {
+        for (void* q : M.tbufs) cudaFree(q);
+        M.tbufs.clear();
+        M.tcap = 0;
+        M.tkeys = dalloc<unsigned long long>((std::size_t)T);
+        M.tbufs.push_back(M.tkeys);
+        M.ranges = dalloc<uint2>((std::size_t)T);
+        M.tbufs.push_back(M.ranges);
+        M.tcap = T;
+    }
+    const uint32_t mask = (uint32_t)(T - 1);
+    CK(cudaMemsetAsync(M.tkeys, 0xff, sizeof(unsigned long long) * (std::size_t)T, st));
+    CK(cudaMemsetAsync(M.ranges, 0, sizeof(uint2) * (std::size_t)T, st));
+    if (stored > 0) {
+        const unsigned g = (stored + 127) / 128;
+        k_photon_gather<<<g, 128, 0, st>>>(M.raw, M.vout, stored, M.ph);
+        k_cell_starts<<<g, 128, 0, st>>>(M.kout, stored, M.tkeys, M.ranges, mask);
+        k_cell_ends<<<g, 128, 0, st>>>(M.kout, stored, M.tkeys, M.ranges, mask);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    CK(cudaEventElapsedTime(&M.last_ms, s->ev0, s->ev1));
+    s->ds.cm = DCaustics{M.ph, M.tkeys, M.ranges, mask, stored};
+    CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
+    M.stored = stored;
+    M.seed = p->seed;
+    M.bounces = p->max_bounces;
+    M.valid = true;
+}
+
+void caustic_stats(const luz_gpu_scene* s, LuzRenderStats* stats)
+{
+    if (!stats || !s->pack->consts.caustics.enabled) return;
+    stats->caustic_photons = (double)s->cm.stored;
+    stats->caustic_ms = s->cm.last_ms;
+}
+
 void finish_wave(luz_gpu_scene* s, cudaStream_t st, LuzRenderStats* acc, int max_b)
 {
     CK(cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
@@ -709,6 +940,7 @@ void render_prepare(RenderJob& J)
     luz_gpu_scene* s = J.s;
     check_params(p);
     CK(cudaSetDevice(s->device));
+    prepare_caustics(s, p, J.st);
     J.w = base_args(s, p);
     J.npix = (int64_t)p->width * p->height;
     J.s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
@@ -811,6 +1043,7 @@ void render_finish(RenderJob& J, LuzRenderStats* stats)
         stats->sh_nodes = (double)cnt[3];
         stats->sh_tris = (double)cnt[4];
         stats->sh_top = (double)cnt[5];
+        caustic_stats(s, stats);
     }
 }
 
@@ -887,6 +1120,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     const cudaStream_t st = s->stream;
     const int64_t npix = (int64_t)p->width * p->height;
     if (npix > (int64_t)UINT32_MAX) throw Status(LUZ_E_LIMIT, "Image has too many pixels.");
+    prepare_caustics(s, p, st);
 
     AdaptiveRule R{};
     R.max_samples = (uint32_t)p->spp;
@@ -1026,6 +1260,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
         *stats = LuzRenderStats{};
         stats->render_ms = ms;
         stats->denoise_ms = denoise_ms;
+        caustic_stats(s, stats);
         stats->samples = samples;
         stats->extension_rays = (double)tot[0];
         stats->shadow_rays = (double)tot[1];
@@ -1051,6 +1286,11 @@ void set_texture(luz_gpu_scene* s, int32_t texture, const double* rgb)
     CK(cudaSetDevice(s->device));
     CK(cudaMemcpy(const_cast<float4*>(s->ds.texels) + T.offset, tx.data(), sizeof(float4) * (std::size_t)n,
                   cudaMemcpyHostToDevice));
+    if (s->cm.valid) {   // photon throughput may depend on the texels: rebuild on the next render
+        s->cm.valid = false;
+        s->ds.cm = DCaustics{};
+        CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
+    }
 }
 
 int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t texture, const float* adj_rgb,
@@ -1058,6 +1298,8 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
 {
     check_params(p);
     if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in the adjoint pass.");
+    if (s->pack->consts.caustics.enabled)
+        throw Status(LUZ_E_UNSUPPORTED, "The adjoint pass does not differentiate caustic photon maps.");
     const ScenePack& PK = *s->pack;
     if (texture < 0 || (std::size_t)texture >= PK.textures.size()) throw Status(LUZ_E_INVALID, "Texture index out of range.");
     for (const GMaterial& m : PK.materials)
@@ -1203,6 +1445,9 @@ int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, 
 {
     check_params(p);
     if (p->flags != 0) throw Status(LUZ_E_UNSUPPORTED, "luz_gpu_render_device_noalloc takes no render flags.");
+    if (s->pack->consts.caustics.enabled && !(s->cm.valid && s->cm.seed == p->seed && s->cm.bounces == p->max_bounces))
+        throw Status(LUZ_E_UNSUPPORTED, "luz_gpu_render_device_noalloc needs the caustic photon map of this seed and "
+                                        "bounce limit built by an earlier render.");
     CK(cudaSetDevice(s->device));
     const StaticArena A = carve_static(static_scratch_address(s->device));
     const int64_t npix = (int64_t)p->width * p->height;
@@ -1534,6 +1779,7 @@ int luz_gpu_trace_paths(luz_gpu_scene* s, const LuzRenderParams* p, const int32_
                 throw Status(LUZ_E_INVALID, "Path coordinates out of range.");
         CK(cudaSetDevice(s->device));
         cudaStream_t st = s->stream;
+        prepare_caustics(s, p, st);
         const int64_t chunk = std::min<int64_t>(count, kWaveTarget);
         s->ensure_paths(chunk);
         int32_t* dx = dalloc<int32_t>(chunk);

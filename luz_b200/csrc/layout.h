@@ -139,7 +139,8 @@ enum MatType : int32_t {
     MT_PRINCIPLED = 7, MT_GLOSSY = 8, MT_DIFFUSE_GLOSSY = 9
 };
 enum MatFlags : int32_t {
-    MF_CONDUCTOR = 1, MF_THIN = 2, MF_SMOOTH_FULL_TRANSMISSION = 4, MF_CAN_TRANSMIT = 8, MF_ABSORPTION = 16
+    MF_CONDUCTOR = 1, MF_THIN = 2, MF_SMOOTH_FULL_TRANSMISSION = 4, MF_CAN_TRANSMIT = 8, MF_ABSORPTION = 16,
+    MF_TRANSPORT = 32   // materialIsTransport (CausticPhotonMap.cpp:199-223): carries caustic photons
 };
 struct alignas(16) GMaterial {
     int32_t type;
@@ -232,6 +233,22 @@ struct GAtmos {
     int32_t samples, light_samples;
 };
 
+// Caustic photon map settings resolved on the host (CausticPhotonMap::build,
+// src/renderer/CausticPhotonMap.cpp:430-450, and sampleDirectionalEmission,
+// :287-326). enabled = caustics on, photons > 0 and at least one light.
+struct GCaustics {
+    int32_t enabled;
+    int32_t photons;          // photon target
+    int32_t passes;
+    int32_t has_bounds;       // sceneBoundingBox found a box (directional-light emission)
+    double radius_m;          // progressiveRadiusMeters
+    double radius_su;         // radius_m / meters per unit (grid cell size)
+    double gather_area_m2;    // pi radius_m^2
+    double m2_per_area;       // meters per unit squared
+    double center[3];         // scene box centre
+    double disk_radius;       // |diagonal| / 2 (1 if not positive) + max(T_MIN, radius setting / meters per unit)
+};
+
 struct GSceneConst {
     int32_t accel_kind;       // 0 none, 1 top BVH (root node 0), 2 single object
     int32_t accel_object;
@@ -250,6 +267,7 @@ struct GSceneConst {
     GCamera camera;
     GEnv env;
     GAtmos atmos;
+    GCaustics caustics;
 };
 
 }  // namespace luz

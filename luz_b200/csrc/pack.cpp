@@ -208,6 +208,7 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
             }
             g.flags |= MF_CONDUCTOR;
         }
+        g.flags |= MF_TRANSPORT;
         break;
     case LUZ_MAT_DIELECTRIC:
         if (!std::isfinite(m.ior) || m.ior <= 0.0) invalid("Dielectric refractive index must be finite and positive.");
@@ -215,7 +216,7 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
             invalid("Dielectric roughness must be finite and in [0,1].");
         if (!finite3(m.absorption) || m.absorption[0] < 0 || m.absorption[1] < 0 || m.absorption[2] < 0)
             invalid("Dielectric absorption coefficient must have finite non-negative channels.");
-        g.flags |= MF_CAN_TRANSMIT;
+        g.flags |= MF_CAN_TRANSMIT | MF_TRANSPORT;
         if (absorb) g.flags |= MF_ABSORPTION;
         break;
     case LUZ_MAT_PRINCIPLED:
@@ -234,6 +235,7 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
         if (m.metallic <= 1e-6 && m.roughness <= 1e-4 && m.transmission >= 1.0 - 1e-6 && m.clearcoat <= 1e-6
             && m.sheen <= 1e-6 && m.subsurface <= 1e-6)
             g.flags |= MF_SMOOTH_FULL_TRANSMISSION;
+        if (m.metallic >= 0.5 || m.transmission > 0.05 || m.clearcoat > 0.5) g.flags |= MF_TRANSPORT;
         break;
     case LUZ_MAT_GLOSSY:
         check_unit(m.roughness, "Glossy roughness");
@@ -888,6 +890,8 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
     std::vector<int32_t> unaccel;
     S.object_of_desc.assign(d->object_count, -1);
     std::vector<Box64> obj_box;
+    bool scene_has_box = false;   // sceneBoundingBox (CausticPhotonMap.cpp:235-277): every box but directional lights'
+    Box64 scene_box{};
     for (int i = 0; i < d->object_count; i++) {
         const LuzObjectDesc& o = d->objects[i];
         GObject g{};
@@ -1076,6 +1080,17 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         S.objects.push_back(g);
         obj_box.push_back(box);
         S.object_of_desc[i] = gi;
+        if (has_box) {
+            if (!scene_has_box) {
+                scene_box = box;
+                scene_has_box = true;
+            } else {
+                for (int a = 0; a < 3; a++) {
+                    scene_box.mn[a] = std::min(scene_box.mn[a], box.mn[a]);
+                    scene_box.mx[a] = std::max(scene_box.mx[a], box.mx[a]);
+                }
+            }
+        }
         if (!hittable) continue;
         if (has_box) bounded.push_back({gi, box});
         else unaccel.push_back(gi);
@@ -1250,6 +1265,41 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         if (total > 0.0 && !cum.empty()) {
             K.light_cdf_offset = (int32_t)S.cdf.size();
             S.cdf.insert(S.cdf.end(), cum.begin(), cum.end());
+        }
+    }
+
+    // caustic photon map settings (Scene setters, Scene.cpp:317-360; CausticPhotonMap::build, :430-450)
+    if (d->caustics.enabled) {
+        const LuzCausticsDesc& c = d->caustics;
+        if (c.photons < 0) invalid("Caustic photon count must be non-negative.");
+        if (c.passes <= 0) invalid("Caustic pass count must be positive.");
+        if (!std::isfinite(c.radius_meters) || c.radius_meters <= 0.0)
+            invalid("Caustic radius must be finite and positive.");
+        if (!std::isfinite(c.alpha) || c.alpha <= 0.0 || c.alpha > 1.0)
+            invalid("Caustic alpha must be finite and in (0,1].");
+        GCaustics& g = K.caustics;
+        double radius = c.radius_meters;   // progressiveRadiusMeters (:356-368)
+        for (int pass = 1; pass < c.passes; pass++)
+            radius *= std::sqrt(((double)pass + c.alpha) / ((double)pass + 1.0));
+        g.photons = c.photons;
+        g.passes = c.passes;
+        g.radius_m = radius;
+        g.radius_su = radius / K.meters_per_unit;
+        g.gather_area_m2 = M_PI * radius * radius;
+        g.m2_per_area = K.meters_per_unit * K.meters_per_unit;
+        g.enabled = (c.photons > 0 && !S.lights.empty() && radius > 0.0 && g.radius_su > 0.0 && g.gather_area_m2 > 0.0
+                     && std::isfinite(g.radius_su)) ? 1 : 0;
+        g.has_bounds = scene_has_box ? 1 : 0;
+        if (scene_has_box) {   // sampleDirectionalEmission (:287-326)
+            double diag2 = 0.0;
+            for (int a = 0; a < 3; a++) {
+                g.center[a] = (scene_box.mn[a] + scene_box.mx[a]) * 0.5;
+                const double dd = scene_box.mx[a] - scene_box.mn[a];
+                diag2 += dd * dd;
+            }
+            double r = std::sqrt(diag2) * 0.5;
+            if (!std::isfinite(r) || r <= 0.0) r = 1.0;
+            g.disk_radius = r + std::max(kTMin64, c.radius_meters / K.meters_per_unit);
         }
     }
 

@@ -20,6 +20,17 @@
 
 namespace luz {
 
+// Caustic photon map of the current render (caustics.cuh): photons in grid-cell
+// order, three float4 each, and an open-addressing table from packed cell key
+// to the cell's [begin, end) photon range. count = 0: no map.
+struct DCaustics {
+    const float4* photons;
+    const unsigned long long* cell_keys;
+    const uint2* cell_ranges;
+    uint32_t mask;
+    uint32_t count;
+};
+
 struct DScene {
     const GRect* rects;
     const GObject* objects;
@@ -42,10 +53,11 @@ struct DScene {
     const uint8_t* obj_class;  // material type a hit on each object shades with (shade binning)
     uint32_t* error;          // device error word (bit flags)
     unsigned long long* counters;   // LUZ_RENDER_COUNT: ext nodes/tris/top, shadow nodes/tris/top
+    DCaustics cm;
     GSceneConst k;
 };
 
-enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u };
+enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u, ERR_CAUSTIC_GRID = 4u };
 
 // Scene features a traversal kernel is instantiated for (GSceneConst.features).
 // A kernel compiled without a feature never meets that object kind in its

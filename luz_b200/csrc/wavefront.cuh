@@ -1,6 +1,7 @@
 // wavefront.cuh — per-path device logic of the wavefront integrator (state
 // layout, camera rays, the shade step); kernels live in integrator.cu.
 #pragma once
+#include "caustics.cuh"
 #include "shade.cuh"
 
 namespace luz {
@@ -437,6 +438,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         rad = rad + thr * emitted;
         if (w.adjoint && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture) adjoint_texture(S, w, P, p, h, rad);
         if (terminated(thr * att)) goto done;
+        if (S.cm.count) rad = rad + clamp_ray_color(thr * caustic_estimate(S, h, sr, m, ray.d));
         if (S.k.light_count > 0) {   // estimateDirectLighting (ColorHelper.cpp:973-1033)
             const float prob = direct_prob(bounce);
             bool go = true;

@@ -96,6 +96,12 @@ class AtmosphereDesc(C.Structure):
                 ("stars_brightness", C.c_double)]
 
 
+class CausticsDesc(C.Structure):
+    """LuzCausticsDesc: Scene caustic settings (src/scene/Scene.cpp:302-360)."""
+    _fields_ = [("enabled", C.c_int32), ("photons", C.c_int32), ("passes", C.c_int32), ("reserved", C.c_int32),
+                ("radius_meters", C.c_double), ("alpha", C.c_double)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("abi_version", C.c_int32), ("material_count", C.c_int32), ("materials", C.POINTER(MaterialDesc)),
@@ -105,7 +111,7 @@ class SceneDesc(C.Structure):
         ("camera", CameraDesc), ("environment", EnvironmentDesc),
         ("background", D3), ("meters_per_unit", C.c_double),
         ("ies_count", C.c_int32), ("_pad", C.c_int32), ("ies", C.POINTER(IesDesc)),
-        ("atmosphere", AtmosphereDesc),
+        ("atmosphere", AtmosphereDesc), ("caustics", CausticsDesc),
     ]
 
 
@@ -128,7 +134,7 @@ class RenderStats(C.Structure):
         ("extend_launches", C.c_int64), ("shadow_launches", C.c_int64),
         ("ext_nodes", C.c_double), ("ext_tris", C.c_double), ("ext_top", C.c_double),
         ("sh_nodes", C.c_double), ("sh_tris", C.c_double), ("sh_top", C.c_double),
-        ("denoise_ms", C.c_double),
+        ("denoise_ms", C.c_double), ("caustic_photons", C.c_double), ("caustic_ms", C.c_double),
     ]
 
 
@@ -221,6 +227,9 @@ class Scene:
     environment_rotation: float = 0.0
     environment_lighting: bool = True
     meters_per_unit: float = 1.0
+    # Caustic photon map (Defaults.hpp:51-55); enabled by Scene.caustics(...)
+    caustics: dict = field(default_factory=lambda: dict(enabled=0, photons=100000, passes=8, radius_meters=0.05,
+                                                        alpha=0.7))
 
     # -- materials (defaults = reference constructors) --------------------------
     def _mat(self, **kw) -> int:
@@ -345,6 +354,12 @@ class Scene:
         self.environment_lighting = lighting
         self.sky = SKY_ENVIRONMENT
 
+    def set_caustics(self, photons=100000, passes=8, radius_meters=0.05, alpha=0.7, enabled=True):
+        """Scene::setCausticsEnabled / setCausticPhotonCount / setCausticPassCount /
+        setCausticRadiusMeters / setCausticAlpha."""
+        self.caustics = dict(enabled=1 if enabled else 0, photons=photons, passes=passes,
+                             radius_meters=radius_meters, alpha=alpha)
+
     # -- C description -------------------------------------------------------
     def build(self) -> "BuiltDesc":
         return BuiltDesc(self)
@@ -411,6 +426,9 @@ class BuiltDesc:
         d.atmosphere = AtmosphereDesc(_d3(a["sun_direction"]), _d3(a["sun_radiance"]), a["sun_radiance_scale"],
                                       a["earth_radius"], a["atmosphere_radius"], a["h_r"], a["h_m"], a["samples"],
                                       a["light_samples"], a["stars_brightness"])
+        c = s.caustics
+        d.caustics = CausticsDesc(int(c["enabled"]), int(c["photons"]), int(c["passes"]), 0,
+                                  float(c["radius_meters"]), float(c["alpha"]))
         d.sky = s.sky
         d.meters_per_unit = s.meters_per_unit
         self._keep += [mats, texs, meshes, objs]

@@ -390,6 +390,51 @@ def tiny_mixed(width: int = 24, height: int = 18, spp: int = 4, max_bounces: int
     return Workload("tiny_mixed", s, width, height, spp, max_bounces)
 
 
+def caustic_pool(width: int = 64, height: int = 48, spp: int = 4, max_bounces: int = 8, photons: int = 40000,
+                 passes: int = 4, radius_meters: float = 0.08, alpha: float = 0.7) -> Workload:
+    """Caustics (CausticPhotonMap): smooth and rough glass, a rough metal torus, a transmissive
+    Principled block and a rough-glass wavy sheet over Lambertian / diffuse-glossy receivers and
+    a scattering volume, lit by every emitter kind the photon pass samples (rectangle, sphere,
+    emissive mesh, emissive non-uniformly scaled instance, directional light)."""
+    s = Scene()
+    floor = s.lambertian((0.8, 0.78, 0.74))
+    wall = s.lambertian((0.35, 0.55, 0.7))
+    s.rectangle((0.0, 0.0, 0.0), (0, 1, 0), 8.0, 8.0, floor)
+    s.rectangle((0.0, 2.0, -3.0), (0, 0, 1), 8.0, 4.0, wall)
+    s.rectangle((3.0, 1.0, -1.5), (-1, 0, 0), 3.0, 2.0, s.diffuse_glossy((0.6, 0.5, 0.4), weight=0.3,
+                                                                         roughness=0.4))
+    s.sphere((0.0, 0.7, 0.0), 0.6, s.dielectric((1.0, 1.0, 1.0), ior=1.5, roughness=0.0))
+    tor, _ = s.mesh(torus_mesh(24, 12, 0.5, 0.12), s.metal((0.95, 0.85, 0.6), roughness=0.1), add_object=False)
+    s.mesh_instance(tor, (-1.6, 0.35, 0.6), (70.0, 20.0, 0.0), (1.0, 1.0, 1.0), s.metal((0.95, 0.85, 0.6),
+                                                                                     roughness=0.1))
+    s.cube((1.6, 0.4, 0.8), 0.6, 0.8, 0.6, s.principled((0.9, 0.95, 1.0), roughness=0.05, transmission=0.9,
+                                                         ior=1.45))
+    xs = np.linspace(-1.0, 1.0, 9)
+    zs = np.linspace(-0.6, 0.6, 7)
+    X, Z = np.meshgrid(xs, zs)
+    Y = 1.6 + 0.08 * np.sin(3.0 * X) * np.cos(4.0 * Z)
+    P = np.stack([X + 0.8, Y, Z - 1.4], -1)
+    quads = []
+    for i in range(len(zs) - 1):
+        for j in range(len(xs) - 1):
+            a, b, c, d = P[i, j], P[i, j + 1], P[i + 1, j + 1], P[i + 1, j]
+            quads += [[a, b, c], [a, c, d]]
+    s.mesh(np.array(quads), s.dielectric((0.85, 0.95, 1.0), ior=1.33, roughness=0.05))
+    s.volume_sphere((-0.4, 0.5, 1.5), 0.4, s.henyey_greenstein((0.8, 0.85, 0.9), 0.4), 1.2)
+    s.rectangle((0.0, 3.2, 0.0), (0, -1, 0), 0.6, 0.6, s.emissive((30.0, 29.0, 26.0)))
+    s.sphere((1.8, 2.6, 1.2), 0.15, s.emissive((40.0, 36.0, 30.0)))
+    panel = np.array([[[-0.3, 0.0, 0.0], [0.3, 0.0, 0.0], [0.3, 0.0, 0.3]],
+                      [[-0.3, 0.0, 0.0], [0.3, 0.0, 0.3], [-0.3, 0.0, 0.3]]])
+    s.mesh(panel + np.array([-1.8, 3.0, -1.0]), s.emissive((12.0, 14.0, 18.0)))
+    pm, _ = s.mesh(panel, s.emissive((10.0, 9.0, 7.0)), add_object=False)
+    s.mesh_instance(pm, (1.0, 3.1, -2.0), (180.0, 10.0, 0.0), (1.5, 1.0, 0.6), s.emissive((10.0, 9.0, 7.0)))
+    s.directional_light((-0.3, -1.0, -0.2), s.emissive((1.2, 1.15, 1.0)))
+    s.camera = _pinhole((0.0, 2.6, 4.6), (0.0, 0.4, 0.0), 50.0, width / height)
+    s.background = (0.02, 0.025, 0.03)
+    s.set_caustics(photons=photons, passes=passes, radius_meters=radius_meters, alpha=alpha)
+    return Workload("caustic_pool", s, width, height, spp, max_bounces)
+
+
 def batch_workloads(count: int = 48, seed: int = 4242) -> list:
     """Many independent scenes for luz_gpu_batch_render: triangle counts log-uniform in
     [1e3, 1e6] (displaced icospheres of the nearest level), square images with sides

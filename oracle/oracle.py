@@ -69,6 +69,7 @@ class RefOracle:
                                            C.c_int64, vp, vp, vp]
         L.luzref_mesh_bvh.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int64), vp, C.c_int64]
         L.luzref_mesh_triangle_count.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64)]
+        L.luzref_caustic_photons.argtypes = [vp, C.c_uint32, C.c_int32, C.POINTER(C.c_int64)]
         L.luzref_sampler.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32,
                                      C.c_uint32, C.c_int32, vp]
         L.luzref_last_error.argtypes = [C.c_char_p, C.c_size_t]
@@ -129,6 +130,12 @@ class RefScene:
                                                    None if vk is None else vk.ctypes.data,
                                                    t.ctypes.data, obj.ctypes.data, prim.ctypes.data))
         return t, obj, prim
+
+    def caustic_photons(self, seed: int, max_bounces: int) -> int:
+        """CausticPhotonMap::build for the render seed: photons stored."""
+        n = C.c_int64()
+        self.o._check(self.o.lib.luzref_caustic_photons(self.h, seed, max_bounces, C.byref(n)))
+        return n.value
 
     def trace_paths(self, params, x, y, s) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.int32)

@@ -68,6 +68,7 @@
 #undef private
 #include "Scene/Scene.hpp"
 #include "Renderer/Renderer.hpp"
+#include "Renderer/CausticPhotonMap.hpp"
 #include "RendererInternal.hpp"
 
 #include "luz_gpu.h"
@@ -314,6 +315,13 @@ RefScene* build(const LuzSceneDesc* d, int tag)
     if (c.pinhole) cam.setPinhole(true);
     scene.addCamera(cam);
     scene.setMetersPerUnit(d->meters_per_unit);
+    if (d->caustics.enabled) {
+        scene.setCausticsEnabled(true);
+        scene.setCausticPhotonCount(d->caustics.photons);
+        scene.setCausticPassCount(d->caustics.passes);
+        scene.setCausticRadiusMeters(d->caustics.radius_meters);
+        scene.setCausticAlpha(d->caustics.alpha);
+    }
     scene.setBackgroundColor(col(d->background));
     scene.setRenderSky(d->sky == LUZ_SKY_ENVIRONMENT ? SKY_ENVIRONMENT
                        : d->sky == LUZ_SKY_LINEAR   ? SKY_LINEAR
@@ -349,6 +357,18 @@ template <class F> int guarded(F&& f)
     } catch (const std::exception& e) {
         g_error = e.what();
         return LUZ_E_INVALID;
+    }
+}
+
+// The photon map Renderer::render builds before the sample loop (Renderer.cpp:40-52).
+void caustic_map(Scene& scene, uint32_t seed)
+{
+    if (scene.getCausticsEnabled() && scene.getCausticPhotonCount() > 0) {
+        auto m = std::make_shared<CausticPhotonMap>();
+        m->build(scene, seed);
+        scene.setCausticPhotonMap(m);
+    } else {
+        scene.setCausticPhotonMap(nullptr);
     }
 }
 
@@ -476,6 +496,7 @@ int luzref_trace_paths(void* s, const LuzRenderParams* p, const int32_t* x, cons
         configure(rs->scene, LuzSceneDesc{}, p->width, p->height);
         rs->scene.setMaxLightBounces(p->max_bounces);
         rs->scene.setSampleCount(p->spp);
+        caustic_map(rs->scene, p->seed);
         const auto cam = Renderer::internal::_prepareRenderCamera(rs->scene);
         Sampler::setRenderSeed(p->seed);
         for (int64_t i = 0; i < n; i++) {
@@ -533,6 +554,7 @@ int luzref_trace_samples(void* s, const LuzRenderParams* p, int32_t half_streams
         configure(rs->scene, LuzSceneDesc{}, p->width, p->height);
         rs->scene.setMaxLightBounces(p->max_bounces);
         rs->scene.setSampleCount(p->spp);
+        caustic_map(rs->scene, p->seed);
         const auto cam = Renderer::internal::_prepareRenderCamera(rs->scene);
         Sampler::setRenderSeed(p->seed);
         for (int64_t i = 0; i < n; i++) {
@@ -574,6 +596,7 @@ int luzref_render_pixels(void* s, const LuzRenderParams* p, int32_t adaptive, in
         }
         if (nfor) scene.initializeDenoiseBuffers((std::size_t)p->width, (std::size_t)p->height);
         else scene.clearDenoiseBuffers();
+        caustic_map(scene, p->seed);
         const auto cam = Renderer::internal::_prepareRenderCamera(scene);
         Sampler::setRenderSeed(p->seed);
         for (int64_t i = 0; i < n; i++) {
@@ -604,6 +627,20 @@ int luzref_render_pixels(void* s, const LuzRenderParams* p, int32_t adaptive, in
         }
         scene.clearDenoiseBuffers();
         scene.setAdaptiveSampling(false);
+        return 0;
+    });
+}
+
+/* CausticPhotonMap::build (src/renderer/CausticPhotonMap.cpp:430-551) for a
+ * render seed and bounce limit: the number of photons stored. */
+int luzref_caustic_photons(void* s, uint32_t seed, int32_t max_bounces, int64_t* count)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        rs->scene.setMaxLightBounces(max_bounces);
+        CausticPhotonMap m;
+        m.build(rs->scene, seed);
+        *count = (int64_t)m.photonCount();
         return 0;
     });
 }

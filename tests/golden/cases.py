@@ -34,7 +34,16 @@ CASES = {
     "linear_sky": lambda: scenes.spheres_linear_sky(64, 36, 4, 12),
     "ies": lambda: scenes.ies_room(48, 36, 4, 6),
     "atmosphere": lambda: scenes.atmosphere_hills(48, 32, 4, 3),
+    "caustics": lambda: scenes.caustic_pool(48, 36, 4, 8, photons=20000),
 }
+
+# Caustic photon map case (CausticPhotonMap): the scene with its map on, and the
+# (render seed, max bounces) pairs whose stored-photon counts are pinned.
+def caustic_case():
+    return scenes.caustic_pool(64, 48, 2, 8)
+
+
+CAUSTIC_COUNTS = [(424242424, 8), (7, 8), (424242424, 3), (99, 12)]
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.
 ADAPTIVE_CASES = {

@@ -14,7 +14,9 @@ output of the unmodified reference code:
                      sum(adjoint * film) with respect to chosen texel channels
                      (the reference has no gradients; common random numbers: same seed)
   nfor.npz           Denoise::applyNFOR outputs (src/core/Denoise/NFOR.cpp:977-1102)
-Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | cases <name>...]   (only those files)
+  caustics.npz       CausticPhotonMap::build photon counts (src/renderer/CausticPhotonMap.cpp:430-551)
+                     and per-path radiance of paths whose caustic estimate is non-zero
+Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | caustics | cases <name>...]
 """
 from __future__ import annotations
 
@@ -30,7 +32,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import ADAPTIVE_CASES, BVH_CASES, CASES, adjoint_case, camera_rays, nfor_synthetic, path_keys  # noqa: E402
+from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, adjoint_case, camera_rays,  # noqa: E402
+                   caustic_case, nfor_synthetic, path_keys)
 from luz_b200 import native  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
@@ -121,6 +124,29 @@ def nfor_fixture(o):
     print("golden nfor", flush=True)
 
 
+def caustic_fixture(o, n_paths=2000):
+    """caustics.npz: photons stored for CAUSTIC_COUNTS (seed, max_bounces) pairs, and the
+    reference radiance of up to n_paths one-sample paths whose value changes when the
+    photon map is switched off (paths that gather caustic photons)."""
+    w = caustic_case()
+    rs = o.scene(w.scene.build())
+    counts = np.array([rs.caustic_photons(sd, mb) for sd, mb in CAUSTIC_COUNTS], np.int64)
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    yy, xx = np.mgrid[0:w.height, 0:w.width]
+    x = np.repeat(xx.ravel(), w.spp).astype(np.int32)
+    y = np.repeat(yy.ravel(), w.spp).astype(np.int32)
+    s = np.tile(np.arange(w.spp), w.width * w.height).astype(np.int32)
+    on = rs.trace_paths(p, x, y, s)
+    w.scene.caustics["enabled"] = 0
+    off = o.scene(w.scene.build()).trace_paths(p, x, y, s)
+    sel = np.flatnonzero(np.abs(on - off).max(axis=1) > 0)
+    rng = np.random.default_rng(zlib.crc32(b"caustics"))
+    sel = np.sort(rng.choice(sel, min(n_paths, sel.size), replace=False))
+    np.savez_compressed(os.path.join(HERE, "caustics.npz"), counts=counts, x=x[sel], y=y[sel], s=s[sel],
+                        rgb=on[sel], rgb_off=off[sel])
+    print("golden caustics", counts, sel.size, flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -131,6 +157,9 @@ def main():
         return
     if sys.argv[1:] == ["nfor"]:
         nfor_fixture(o)
+        return
+    if sys.argv[1:] == ["caustics"]:
+        caustic_fixture(o)
         return
     if sys.argv[1:2] == ["cases"]:     # cases <name>...: only the per-case files of those cases
         case_fixtures(o, sys.argv[2:])
@@ -158,6 +187,7 @@ def main():
     adaptive_fixtures(o)
     adjoint_fixture(o)
     nfor_fixture(o)
+    caustic_fixture(o)
 
 
 if __name__ == "__main__":

@@ -18,7 +18,7 @@ from luz_b200.desc import OBJ_MESH, OBJ_MESH_INSTANCE
 pytestmark = pytest.mark.gpu
 
 # fraction of paths within 1e-4 relative of the reference, per case
-PATH_FRACTION = {"cornell": 0.995, "instancing": 0.99, "tiny": 0.98, "glossy": 0.97, "linear_sky": 0.975, "ies": 0.98, "atmosphere": 0.985}
+PATH_FRACTION = {"cornell": 0.995, "instancing": 0.99, "tiny": 0.98, "glossy": 0.97, "linear_sky": 0.975, "ies": 0.98, "atmosphere": 0.985, "caustics": 0.97}
 
 
 @pytest.fixture(scope="module")

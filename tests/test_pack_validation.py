@@ -102,3 +102,23 @@ def test_light_list_and_weights():
     s.directional_light((0, -1, 0), e)
     s.sphere((3, 0, 0), 1, s.lambertian((1, 1, 1)))
     assert packs(s).info().light_count == 3
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(photons=-1), "Caustic photon count must be non-negative."),
+    (dict(passes=0), "Caustic pass count must be positive."),
+    (dict(radius_meters=0.0), "Caustic radius must be finite and positive."),
+    (dict(radius_meters=float("inf")), "Caustic radius must be finite and positive."),
+    (dict(alpha=1.5), "Caustic alpha must be finite and in (0,1]."),
+    (dict(alpha=0.0), "Caustic alpha must be finite and in (0,1]."),
+])
+def test_caustic_settings_validation(kw, msg):
+    """Scene::setCausticPhotonCount / PassCount / RadiusMeters / Alpha (src/scene/Scene.cpp:317-360)."""
+    s = Scene()
+    s.sphere((0, 2, 0), 0.2, s.emissive((5, 5, 5)))
+    s.set_caustics(**kw)
+    with pytest.raises(native.LuzError) as e:
+        packs(s)
+    assert msg in str(e.value) and e.value.code == -1
+    s.caustics["enabled"] = 0          # settings are read only with caustics on
+    packs(s)
