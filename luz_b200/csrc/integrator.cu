@@ -172,6 +172,7 @@ using TraceKernel = void (*)(DScene, WaveArgs, PathBuf, Ctrl*, int);
 const TraceKernel kExtendKernels[4] = {k_extend<0>, k_extend<1>, k_extend<2>, k_extend<3>};
 const TraceKernel kShadowKernels[4] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>};
 
+template <bool CAUSTICS>
 __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     const DScene& S = *Sp;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DS
         uint32_t p = 0;
         if (valid) {
             p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
-            shade_path(S, w, P, p, bounce, o);
+            shade_path<CAUSTICS>(S, w, P, p, bounce, o);
         }
         __syncwarp();
         const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
@@ -205,6 +206,8 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DS
         }
     }
 }
+
+using ShadeKernel = void (*)(const DScene*, WaveArgs, PathBuf, Ctrl*, int);
 
 // Adds one wave's per-bounce queue sizes to the render totals (no host wait per wave).
 __global__ void k_tally(const Ctrl* C, int max_b, unsigned long long* totals)
@@ -656,6 +659,7 @@ struct luz_gpu_scene {
     int sms = 0;
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
     TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
+    ShadeKernel shade = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // caustic photon map: buffers grown on demand; the map is kept while the
     // render seed and bounce limit stay the same (textures unchanged)
@@ -778,7 +782,7 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
         s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
-        k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
+        s->shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
         s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
@@ -1478,7 +1482,7 @@ int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, 
             const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
             for (int b = 0; b <= w.max_bounces; b++) {
                 s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
-                k_shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, A.pb, A.ctrl, b);
+                s->shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, A.pb, A.ctrl, b);
                 s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, A.pb, A.ctrl, b);
                 launches += 3;
             }
@@ -1596,7 +1600,8 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         s->extend = kExtendKernels[feat];
         s->shadow = kShadowKernels[feat];
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, s->extend, kBlock, 0));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, k_shade, kBlock, 0));
+        s->shade = P.consts.caustics.enabled ? k_shade<true> : k_shade<false>;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, s->shade, kBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_sh, s->shadow, kBlock, 0));
         s->occ_ext = std::max(1, s->occ_ext);
         s->occ_shade = std::max(1, s->occ_shade);

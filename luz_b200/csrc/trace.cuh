@@ -173,6 +173,57 @@ __device__ __forceinline__ bool box_hit(const float* mn, const float* mx, const 
     return true;
 }
 
+__device__ __forceinline__ float fmax3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Mesh-box slab test in the form t = plane * inv + noi with noi = -(o * inv)
+// rounded once per ray: one FMA per plane instead of a subtraction and a
+// product, and three-input min/max for the running interval. Equal to
+// box_hit in real arithmetic; in FP32 each distance is off by less than
+// 2^-24 (|o| + |t d|) / |d| along its axis, below the T_MIN padding of every
+// mesh box (Triangle.cpp:114-125) while |o| < 4096 and the mesh lies within
+// 8192 units of the origin: mesh_fast_slabs checks both.
+__device__ __forceinline__ bool mesh_fast_slabs(const GMesh& M, const TRay& r)
+{
+    const float om = fmax3f(fabsf(r.o.x), fabsf(r.o.y), fabsf(r.o.z));
+    const float mm = fmaxf(fmax3f(fabsf(M.bmin[0]), fabsf(M.bmin[1]), fabsf(M.bmin[2])),
+                           fmax3f(fabsf(M.bmax[0]), fabsf(M.bmax[1]), fabsf(M.bmax[2])));
+    return !r.zero && !r.axis0 && om < 4096.0f && mm < 8192.0f;
+}
+__device__ __forceinline__ F3 neg_o_inv(const TRay& r)
+{
+    return F3{-(r.o.x * r.inv.x), -(r.o.y * r.inv.y), -(r.o.z * r.inv.z)};
+}
+__device__ __forceinline__ bool box_hit_fast(const float* mn, const float* mx, const TRay& r, const F3& noi, float tmax,
+                                             float& tnear)
+{
+    const float t0x = fmaf(mn[0], r.inv.x, noi.x), t1x = fmaf(mx[0], r.inv.x, noi.x);
+    const float t0y = fmaf(mn[1], r.inv.y, noi.y), t1y = fmaf(mx[1], r.inv.y, noi.y);
+    const float t0z = fmaf(mn[2], r.inv.z, noi.z), t1z = fmaf(mx[2], r.inv.z, noi.z);
+    const float lo = fmax3f(fmaxf(kTMin, fminf(t0x, t1x)), fminf(t0y, t1y), fminf(t0z, t1z));
+    const float hi = fmin3f(fminf(tmax, fmaxf(t0x, t1x)), fmaxf(t0y, t1y), fmaxf(t0z, t1z));
+    tnear = lo;
+    return !(hi <= lo);
+}
+// Mesh box test: the FMA form (FAST) or box_hit. noi = neg_o_inv(r) (FAST only).
+template <bool FAST>
+__device__ __forceinline__ bool mesh_box(const float* mn, const float* mx, const TRay& r, const F3& noi, float tmax,
+                                         float& tnear)
+{
+    if constexpr (FAST) return box_hit_fast(mn, mx, r, noi, tmax, tnear);
+    else return box_hit(mn, mx, r, tmax, tnear);
+}
+
 __device__ __forceinline__ bool tri_test(const GTri& T, const TRay& r, float tmin, float tmax, float& t, float& u, float& v)
 {
     const F3 e1 = f3(T.e1), e2 = f3(T.e2), v0 = f3(T.v0);
@@ -299,12 +350,13 @@ struct LocalStack {
 };
 
 // Mesh::hit — closest triangle; closest is updated in place.
-template <class Stk>
-__device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
-                                             int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs, Stk& st)
+template <bool FAST, class Stk>
+__device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& M, const TRay& r, float tmin,
+                                                  float& closest, int32_t& slot, float& bu, float& bv, int32_t skip,
+                                                  VolSample& vs, Stk& st)
 {
     float root_near;
-    if (!box_hit(M.bmin, M.bmax, r, closest, root_near)) return false;
+    if (!mesh_box<FAST>(M.bmin, M.bmax, r, neg_o_inv(r), closest, root_near)) return false;
     // Walks the collapsed BVH. The entry about to be visited stays in
     // registers (ref, near); a node visit pushes the other accepted entries in
     // reverse visit order. Pruning (near >= closest) happens when an entry is
@@ -335,14 +387,15 @@ __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, co
                 const GNode4 n = load_node4(S.nodes4, ref);
                 vs.nodes++;
                 float nl = 0.f, nr = 0.f;
-                const bool hl = box_hit(n.lmin, n.lmax, r, closest, nl);
-                const bool hr = box_hit(n.rmin, n.rmax, r, closest, nr);
+                const F3 noi = FAST ? neg_o_inv(r) : F3{0.f, 0.f, 0.f};
+                const bool hl = mesh_box<FAST>(n.lmin, n.lmax, r, noi, closest, nl);
+                const bool hr = mesh_box<FAST>(n.rmin, n.rmax, r, noi, closest, nr);
                 bool ha[4];
                 float na[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     na[k] = 0.f;
-                    ha[k] = n.ref[k] != kEmptySlot && box_hit(n.cmin[k], n.cmax[k], r, closest, na[k]);
+                    ha[k] = n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, closest, na[k]);
                 }
                 uint32_t er[4];
                 float en[4];
@@ -367,13 +420,21 @@ __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, co
     return hit;
 }
 
-// Mesh::hitAny
 template <class Stk>
-__device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
-                                         int32_t skip, VolSample& vs, Stk& st)
+__device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
+                                             int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs, Stk& st)
+{
+    if (mesh_fast_slabs(M, r)) return mesh_closest_walk<true>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
+    return mesh_closest_walk<false>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
+}
+
+// Mesh::hitAny
+template <bool FAST, class Stk>
+__device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
+                                              int32_t skip, VolSample& vs, Stk& st)
 {
     float root_near;
-    if (!box_hit(M.bmin, M.bmax, r, tmax, root_near)) return false;
+    if (!mesh_box<FAST>(M.bmin, M.bmax, r, neg_o_inv(r), tmax, root_near)) return false;
     // Same walk as mesh_closest without pruning (any accepted entry may hold an occluder).
     uint32_t ref = (uint32_t)M.root4_ref;
     int sp = 0;
@@ -397,14 +458,15 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
             const GNode4 n = load_node4(S.nodes4, ref);
             vs.nodes++;
             float nl = 0.f, nr = 0.f;
-            const bool hl = box_hit(n.lmin, n.lmax, r, tmax, nl);
-            const bool hr = box_hit(n.rmin, n.rmax, r, tmax, nr);
+            const F3 noi = FAST ? neg_o_inv(r) : F3{0.f, 0.f, 0.f};
+            const bool hl = mesh_box<FAST>(n.lmin, n.lmax, r, noi, tmax, nl);
+            const bool hr = mesh_box<FAST>(n.rmin, n.rmax, r, noi, tmax, nr);
             bool ha[4];
             float na[4];
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 na[k] = 0.f;
-                ha[k] = n.ref[k] != kEmptySlot && box_hit(n.cmin[k], n.cmax[k], r, tmax, na[k]);
+                ha[k] = n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, tmax, na[k]);
             }
             uint32_t er[4];
             float en[4];
@@ -423,6 +485,14 @@ __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const 
         ref = st.ref(--sp);
     }
     return hit;
+}
+
+template <class Stk>
+__device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
+                                         int32_t skip, VolSample& vs, Stk& st)
+{
+    if (mesh_fast_slabs(M, r)) return mesh_any_walk<true>(S, M, r, tmin, tmax, skip, vs, st);
+    return mesh_any_walk<false>(S, M, r, tmin, tmax, skip, vs, st);
 }
 
 // Rectangle::hit geometric test (Rectangle.cpp:212-249); returns t.

@@ -325,6 +325,9 @@ __device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& P, uint
     d[0] = ray.d.x; d[1] = ray.d.y; d[2] = ray.d.z;
 }
 
+// CAUSTICS: the scene has a caustic photon map (a separate instantiation, so
+// that scenes without one keep the leaner kernel).
+template <bool CAUSTICS>
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
     out.cont = false;
@@ -438,7 +441,8 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         rad = rad + thr * emitted;
         if (w.adjoint && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture) adjoint_texture(S, w, P, p, h, rad);
         if (terminated(thr * att)) goto done;
-        if (S.cm.count) rad = rad + clamp_ray_color(thr * caustic_estimate(S, h, sr, m, ray.d));
+        if constexpr (CAUSTICS)
+            if (S.cm.count) rad = rad + clamp_ray_color(thr * caustic_estimate(S, h, sr, m, ray.d));
         if (S.k.light_count > 0) {   // estimateDirectLighting (ColorHelper.cpp:973-1033)
             const float prob = direct_prob(bounce);
             bool go = true;

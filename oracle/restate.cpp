@@ -171,6 +171,41 @@ bool box(const float* mn, const float* mx, const Ray& r, float tmax, float* near
     return true;
 }
 
+/* The mesh-box slab test of the GPU traversal when the ray has no zero inverse
+ * component, |o| < 4096 and the mesh lies within 8192 units of the origin:
+ * t = fma(plane, inv, -(o * inv)); interval max(TMIN, mins) / min(tmax, maxes). */
+struct Slabs {
+    bool fast;
+    float iv[3], noi[3];
+};
+Slabs mesh_slabs(const GMesh& M, const Ray& r)
+{
+    Slabs s{};
+    float om = 0.f, mm = 0.f;
+    bool axis0 = false;
+    for (int a = 0; a < 3; a++) {
+        om = std::fmax(om, std::fabs(r.o[a]));
+        mm = std::fmax(mm, std::fmax(std::fabs(M.bmin[a]), std::fabs(M.bmax[a])));
+        axis0 = axis0 || r.iv[a] == 0.0f;
+        s.iv[a] = r.iv[a];
+        s.noi[a] = -(r.o[a] * r.iv[a]);
+    }
+    s.fast = !r.zero && !axis0 && om < 4096.0f && mm < 8192.0f;
+    return s;
+}
+bool mbox(const float* mn, const float* mx, const Ray& r, const Slabs& s, float tmax, float* near)
+{
+    if (!s.fast) return box(mn, mx, r, tmax, near);
+    float lo = TMIN, hi = tmax;
+    for (int a = 0; a < 3; a++) {
+        const float t0 = std::fma(mn[a], s.iv[a], s.noi[a]), t1 = std::fma(mx[a], s.iv[a], s.noi[a]);
+        lo = std::fmax(lo, std::fmin(t0, t1));
+        hi = std::fmin(hi, std::fmax(t0, t1));
+    }
+    *near = lo;
+    return !(hi <= lo);
+}
+
 /* Triangle::hit (Triangle.cpp:196-232) */
 bool tri(const GTri& T, const Ray& r, float tmin, float tmax, float* t, float* u, float* v)
 {
@@ -199,7 +234,8 @@ struct Hit {
 bool mesh_hit(const Scene& S, const GMesh& M, const Ray& r, float tmin, float* closest, Hit* h, int32_t oi)
 {
     float rn;
-    if (!box(M.bmin, M.bmax, r, *closest, &rn)) return false;
+    const Slabs sl = mesh_slabs(M, r);
+    if (!mbox(M.bmin, M.bmax, r, sl, *closest, &rn)) return false;
     std::vector<std::pair<uint32_t, float>> st;
     st.push_back({(uint32_t)M.root_ref, rn});
     bool any = false;
@@ -221,8 +257,8 @@ bool mesh_hit(const Scene& S, const GMesh& M, const Ray& r, float tmin, float* c
         }
         const GNode& n = S.nd[e.first];
         float ln = 0.f, rnn = 0.f;
-        const bool hl = box(n.lmin, n.lmax, r, *closest, &ln);
-        const bool hr = box(n.rmin, n.rmax, r, *closest, &rnn);
+        const bool hl = mbox(n.lmin, n.lmax, r, sl, *closest, &ln);
+        const bool hr = mbox(n.rmin, n.rmax, r, sl, *closest, &rnn);
         if (hl && hr) {
             if (ln < rnn) {
                 st.push_back({n.rref, rnn});
@@ -244,7 +280,8 @@ bool mesh_hit(const Scene& S, const GMesh& M, const Ray& r, float tmin, float* c
 bool mesh_any(const Scene& S, const GMesh& M, const Ray& r, float tmin, float tmax)
 {
     float rn;
-    if (!box(M.bmin, M.bmax, r, tmax, &rn)) return false;
+    const Slabs sl = mesh_slabs(M, r);
+    if (!mbox(M.bmin, M.bmax, r, sl, tmax, &rn)) return false;
     std::vector<uint32_t> st{(uint32_t)M.root_ref};
     while (!st.empty()) {
         const uint32_t e = st.back();
@@ -259,7 +296,7 @@ bool mesh_any(const Scene& S, const GMesh& M, const Ray& r, float tmin, float tm
         }
         const GNode& n = S.nd[e];
         float ln = 0.f, rnn = 0.f;
-        const bool hl = box(n.lmin, n.lmax, r, tmax, &ln), hr = box(n.rmin, n.rmax, r, tmax, &rnn);
+        const bool hl = mbox(n.lmin, n.lmax, r, sl, tmax, &ln), hr = mbox(n.rmin, n.rmax, r, sl, tmax, &rnn);
         if (hl && hr) {
             if (ln < rnn) {
                 st.push_back(n.rref);
