@@ -81,3 +81,25 @@ def test_caustic_scene_unsupported_in_adjoint(caustic_gpu):
     with pytest.raises(native.LuzError) as e:
         g.adjoint_backward(native.params(8, 8, 1, 4, 1), 0, np.zeros((8, 8, 3), np.float32), (2, 2, 3))
     assert e.value.code in (-1, -3)
+
+
+@pytest.mark.gpu
+def test_caustic_scene_in_batch_and_denoised_render(caustic_gpu):
+    """Every render entry point builds the map: a batch of the caustic scene and a plain scene
+    equals their one-at-a-time renders, and the render-and-denoise call films the same image."""
+    from luz_b200 import scenes
+    w, g = caustic_gpu
+    p = native.params(w.width, w.height, 2, w.max_bounces, 31)
+    t = scenes.tiny_mixed(24, 18, 2, 4)
+    gt = native.GpuScene(t.scene.build())
+    pt = native.params(t.width, t.height, t.spp, t.max_bounces, t.seed)
+    a, _ = g.render(p)
+    b, _ = gt.render(pt)
+    outs, stats = native.batch_render([g, gt], [p, pt])
+    assert np.array_equal(outs[0], a) and np.array_equal(outs[1], b)
+    assert stats[0].caustic_photons > 0 and stats[1].caustic_photons == 0
+    img, den, used, st = g.render_denoised(p)
+    assert st.caustic_photons == stats[0].caustic_photons and np.isfinite(den).all()
+    ref, _, _, _ = g.render_ex(native.params(w.width, w.height, 2, w.max_bounces, 31), None, True)
+    assert np.array_equal(img, ref)
+    gt.close()
