@@ -203,7 +203,38 @@ struct RegArgs {
     double bw1, bw2;         // bandwidths; bw2 < 0: single regression (regressionPass)
     double* out1;
     double* out2;
+    const double* dist;      // patch distances: (2 radius + 1)^2 rows of one double per pixel (k_patch_dist)
 };
+
+// patchDistance (NFOR.cpp:482-517) of every pixel to each neighbour of its
+// regression window, row k = (oy + radius) (2 radius + 1) + (ox + radius): the
+// terms summed in patch order, then divided by the patch size; 0 where the
+// clamped neighbour is the pixel itself. One thread per (neighbour, pixel).
+__global__ void k_patch_dist(RegArgs A, double* D)
+{
+    const Img I = A.I;
+    const long long npix = (long long)I.w * I.h;
+    const int side = 2 * A.radius + 1;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= npix * side * side) return;
+    const int k = (int)(idx / npix);
+    const long long pix = idx % npix;
+    const int x = (int)(pix % I.w), y = (int)(pix / I.w);
+    const int sx = clampc(x + (k % side - A.radius), I.w), sy = clampc(y + (k / side - A.radius), I.h);
+    double d = 0.0;
+    if (!(sx == x && sy == y)) {
+        const int pw = 2 * A.patch + 1, P = pw * pw;
+        for (int t = 0; t < P; t++) {
+            const int py = t / pw - A.patch, px = t % pw - A.patch;
+            const int a = clampc(y + py, I.h) * I.w + clampc(x + px, I.w);
+            const int b = clampc(sy + py, I.h) * I.w + clampc(sx + px, I.w);
+            const double lv = (A.var[a] * A.vscale) + (A.var[b] * A.vscale) + A.minvar;
+            d += cdist2(A.image + 3 * a, A.image + 3 * b) / lv;
+        }
+        d = d / (double)P;
+    }
+    D[idx] = d;
+}
 
 // regressionPass (NFOR.cpp:674-738) / regressionPairPass (:740-831) with one
 // half-warp per (pixel, bandwidth): lane c of the
@@ -215,6 +246,8 @@ struct RegArgs {
 // pivoting (solveLinearSystemRGB) runs with the pivot column's lane choosing the
 // pivot row: the reference's arithmetic, spread over the lanes instead of a
 // 1.4 KB per-thread array in local memory.
+// The neighbours' weights come from the precomputed patch distances, 16 at a
+// time with one neighbour per lane, and reach the other lanes by shuffle.
 // Pair mode (bw2 >= 0): one pixel per warp, half 0 with bw1, half 1 with bw2.
 // Single mode: two pixels per warp, both with bw1.
 __global__ void __launch_bounds__(128) k_regression_warp(RegArgs A)
@@ -234,40 +267,23 @@ __global__ void __launch_bounds__(128) k_regression_warp(RegArgs A)
     double M[kR];
 #pragma unroll
     for (int r = 0; r < kR; r++) M[r] = (j < (unsigned)kR && r == (int)j) ? 1e-4 : 0.0;   // ridge on the diagonal
-    const int P = (2 * A.patch + 1) * (2 * A.patch + 1);
-    for (int oy = -A.radius; oy <= A.radius; oy++)
-        for (int ox = -A.radius; ox <= A.radius; ox++) {
-            const int sx = clampc(x + ox, I.w), sy = clampc(y + oy, I.h);
-            const int s = sy * I.w + sx;
-            // patchDistance: lane t of the half forms term t, the sum runs in term order
-            double d = 0.0;
-            if (!(sx == x && sy == y)) {
-                for (int t0 = 0; t0 < P; t0 += 16) {
-                    double term = 0.0;
-                    const int t = t0 + (int)j;
-                    if (t < P) {
-                        const int py = t / (2 * A.patch + 1) - A.patch, px = t % (2 * A.patch + 1) - A.patch;
-                        const int a = clampc(y + py, I.h) * I.w + clampc(x + px, I.w);
-                        const int b = clampc(sy + py, I.h) * I.w + clampc(sx + px, I.w);
-                        const double lv = (A.var[a] * A.vscale) + (A.var[b] * A.vscale) + A.minvar;
-                        term = cdist2(A.image + 3 * a, A.image + 3 * b) / lv;
-                    }
-                    const int nt = min(16, P - t0);
-                    for (int k = 0; k < nt; k++) d += __shfl_sync(hmask, term, k, 16);
-                }
-                d = d / (double)P;
+    const int side = 2 * A.radius + 1, K = side * side;
+    double wreg = 0.0;
+    for (int k = 0; k < K; k++) {
+            if ((k & 15) == 0) {   // weights of neighbours k .. k + 15, one per lane
+                const int kk = k + (int)j;
+                wreg = kk < K ? weight_from_distance(A.dist[(size_t)kk * npix + pix], bw, A.minvar) : 0.0;
             }
-            const double wgt = weight_from_distance(d, bw, A.minvar);
+            const double wgt = __shfl_sync(hmask, wreg, k & 15, 16);
+            const int sx = clampc(x + (k % side - A.radius), I.w), sy = clampc(y + (k / side - A.radius), I.h);
+            const int s = sy * I.w + sx;
             double basis[kR];
             basis[0] = 1.0;
 #pragma unroll
             for (int f = 0; f < kF; f++)
                 basis[f + 1] = A.features[(size_t)kF * s + f] - A.features[(size_t)kF * center + f];
             if (j < (unsigned)kR) {   // matrix column j: rows 0..j
-                double bj = 0.0;
-#pragma unroll
-                for (int k = 0; k < kR; k++)
-                    if (k == (int)j) bj = basis[k];
+                const double bj = j == 0 ? 1.0 : A.features[(size_t)kF * s + j - 1] - A.features[(size_t)kF * center + j - 1];
 #pragma unroll
                 for (int r = 0; r < kR; r++)
                     if (r <= (int)j) M[r] += (wgt * basis[r]) * bj;
@@ -476,9 +492,14 @@ void run_device(const double* ca, const double* cb, const double* cv, const doub
     double* rb1 = B.get(3 * n);
     double* rb2 = B.get(3 * n);
     const unsigned rgrid_pair = (unsigned)((n * 32 + 127) / 128), rgrid_single = (unsigned)((((n + 1) / 2) * 32 + 127) / 128);
-    RegArgs A{I, fa, pfb, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, ra1, ra2};
+    const size_t K = (size_t)(2 * s.regression_radius + 1) * (2 * s.regression_radius + 1);
+    double* dist = B.get(K * n);
+    const unsigned dgrid = (unsigned)((K * n + 255) / 256);
+    RegArgs A{I, fa, pfb, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, ra1, ra2, dist};
+    k_patch_dist<<<dgrid, 256, 0, st>>>(A, dist);
     k_regression_warp<<<rgrid_pair, 128, 0, st>>>(A);
-    RegArgs Bb{I, fb, pfa, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, rb1, rb2};
+    RegArgs Bb{I, fb, pfa, cv, 2.0, s.regression_radius, s.patch_radius, s.min_variance, 0.5, 1.0, rb1, rb2, dist};
+    k_patch_dist<<<dgrid, 256, 0, st>>>(Bb, dist);
     k_regression_warp<<<rgrid_pair, 128, 0, st>>>(Bb);
     // MSE, filtered; selection, filtered (guide: the averaged colour, undoubled variance)
     double* m1 = B.get(n);
@@ -495,7 +516,8 @@ void run_device(const double* ca, const double* cb, const double* cv, const doub
     double* ff = B.get(kF * n);
     double* fv = B.get(n);
     k_combine<<<grd, blk, 0, st>>>(I, s1, s2, fm1, fm2, ra1, ra2, rb1, rb2, pfa, pfb, s.min_variance, comb, ff, fv);
-    RegArgs C{I, comb, ff, fv, 1.0, s.regression_radius, s.patch_radius, s.min_variance, 1.0, -1.0, d_out, nullptr};
+    RegArgs C{I, comb, ff, fv, 1.0, s.regression_radius, s.patch_radius, s.min_variance, 1.0, -1.0, d_out, nullptr, dist};
+    k_patch_dist<<<dgrid, 256, 0, st>>>(C, dist);
     k_regression_warp<<<rgrid_single, 128, 0, st>>>(C);
     NCK(cudaGetLastError());
     NCK(cudaStreamSynchronize(st));   // the scratch buffers are freed on return
