@@ -421,6 +421,57 @@ def run_nfor(args):
     print(json.dumps(out), flush=True)
 
 
+def run_cache(args):
+    """--workload cache_glossy: time to equal RMSE, learned radiance cache against the plain
+    integrator, on the mesh + glossy scene at 480x270, depth 12. The converged image is a
+    1024-spp plain render (own seed); the target RMSE is that of the plain 16-spp image (seed
+    202); each curve is device time (CUDA events of the render call; the cached call includes
+    its training steps) against RMSE at 1..64 spp, the cached renders each starting from an
+    untrained cache. value = plain time / cached time at the target, interpolated log-log."""
+    from luz_b200 import desc as D
+    from luz_b200 import native, scenes
+    w = scenes.mesh_glossy(480, 270, 1, 12)
+    g = native.GpuScene(w.scene.build())
+    W, H, MB = w.width, w.height, w.max_bounces
+    ref, _ = g.render(native.params(W, H, 1024, MB, 101))
+    ref = ref.astype(np.float64)
+
+    def rmse(img):
+        return float(np.sqrt(np.mean((img.astype(np.float64) - ref) ** 2)))
+
+    spps = [1, 2, 4, 8, 16, 32, 64]
+    for _ in range(max(1, args.warmup)):
+        g.render(native.params(W, H, 4, MB, 7))
+    plain, cached = [], []
+    for spp in spps:
+        img, st = g.render(native.params(W, H, spp, MB, 202))
+        plain.append((spp, st.render_ms, rmse(img)))
+        c = native.RadianceCache(D.cache_params(seed=3))
+        img, st = c.render(g, native.params(W, H, spp, MB, 202))
+        cached.append((spp, st.render_ms, rmse(img)))
+        c.close()
+    target = plain[spps.index(16)][2]
+
+    def time_to(curve):
+        for (s0, t0, e0), (s1, t1, e1) in zip(curve, curve[1:]):
+            if e0 >= target >= e1 and e0 > e1:
+                a = (np.log(e0) - np.log(target)) / (np.log(e0) - np.log(e1))
+                return float(np.exp(np.log(t0) + a * (np.log(t1) - np.log(t0))))
+        return curve[0][1] if curve[0][2] <= target else None
+
+    tp, tc = time_to(plain), time_to(cached)
+    out = {"metric": "time-to-equal-RMSE speedup (cached vs plain)", "value": (tp / tc) if (tp and tc) else None,
+           "unit": "x", "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": tc,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f16 (MLP)",
+           "data": "synthetic (seeded scene generator)",
+           "config": {"workload": f"cache_glossy: mesh_glossy {W}x{H} depth {MB}, converged = plain 1024 spp",
+                      "target_rmse": target, "cache": "prefix 1, one training path in 16, batch 65536, lr 1e-2"},
+           "plain": {"ms_to_target": tp, "curve": [{"spp": s, "ms": t, "rmse": e} for s, t, e in plain]},
+           "cached": {"ms_to_target": tc, "curve": [{"spp": s, "ms": t, "rmse": e} for s, t, e in cached]}}
+    print(json.dumps(out), flush=True)
+    g.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -431,6 +482,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "nfor1080":
         run_nfor(args)
+    elif args.workload == "cache_glossy":
+        run_cache(args)
     else:
         run_ours(args)
 

@@ -452,6 +452,54 @@ int luz_gpu_render_denoised(luz_gpu_scene* scene, const LuzRenderParams* params,
                             float* rgb_out, double* denoised_out, int32_t* samples_out,
                             LuzRenderStats* stats);
 
+/* ---- Learned radiance cache -------------------------------------------------
+ * No counterpart in the reference. A small MLP (inputs: position normalised to
+ * the scene box, outgoing direction, shading normal, roughness, each encoded as
+ * sin/cos(2^k pi x) for k = 0..5; four hidden layers of 64 with ReLU; RGB out)
+ * with FP16 weights and activations and FP32 accumulation on the tensor cores,
+ * trained online with Adam on the relative L2 loss sum_c (y - t)^2 / (y^2 + 0.01)
+ * (denominator held constant, per-row gradient clamped to +-100).
+ * luz_gpu_render_cached ends every path at its first surface vertex at or after
+ * bounce `prefix` that does not scatter specularly, adding throughput x the
+ * cache's prediction there (a biased estimate: the plain luz_gpu_render stays
+ * the unbiased judge of it); one path in `train_every` instead continues
+ * unbiased and supplies a training row: its inputs at that vertex and the
+ * radiance its suffix gathered divided by its throughput there. After every
+ * wave of one sample per pixel the cache takes one Adam step on up to `batch`
+ * of that wave's rows. The cache belongs to one device and one scene at a time
+ * (the position input is normalised to the box of the scene it renders). */
+typedef struct luz_gpu_cache luz_gpu_cache;
+#define LUZ_CACHE_PARAMS 21504   /* FP32 weights: W0 128x64, W1..W3 64x64, W4 64x16, row-major [in][out] */
+typedef struct LuzCacheParams {
+    uint32_t seed;                /* weight initialisation (uniform +-sqrt(6 / fan_in))    */
+    int32_t  batch;               /* training rows per step (65536); > 0                     */
+    float    learning_rate;       /* Adam step size (1e-2); beta1 0.9, beta2 0.99, eps 1e-8 */
+    int32_t  prefix;              /* first bounce whose vertex queries the cache (1); >= 0   */
+    int32_t  train_every;         /* one training path in this many (16); >= 1               */
+    int32_t  reserved;
+} LuzCacheParams;
+int luz_gpu_cache_create(int32_t device, const LuzCacheParams* params, luz_gpu_cache** out);
+int luz_gpu_cache_destroy(luz_gpu_cache* cache);
+/* Reads (get != NULL) and/or replaces (set != NULL) the LUZ_CACHE_PARAMS FP32
+ * weights; replacing resets the Adam moments and step count. */
+int luz_gpu_cache_weights(luz_gpu_cache* cache, float* get, const float* set);
+/* Predictions for n rows of 10 inputs (host arrays): rgb_out n x 3. */
+int luz_gpu_cache_predict(luz_gpu_cache* cache, const float* inputs, int64_t n, float* rgb_out);
+/* Gradient of the mean loss over n rows (targets n x 3) with respect to the
+ * weights (grad_out LUZ_CACHE_PARAMS floats, or NULL) and the mean loss; no step. */
+int luz_gpu_cache_gradient(luz_gpu_cache* cache, const float* inputs, const float* targets, int64_t n,
+                           float* grad_out, double* loss_out);
+/* `steps` Adam steps on the same n rows (n <= batch); loss_out (steps doubles,
+ * or NULL) receives the mean loss before each step. */
+int luz_gpu_cache_train(luz_gpu_cache* cache, const float* inputs, const float* targets, int64_t n, int32_t steps,
+                        double* loss_out);
+/* Renders with the cache (see above), training it as it goes: params as for
+ * luz_gpu_render (flags 0); stats->samples counts the camera samples,
+ * extension_rays / shadow_rays the rays traced. Caustic photon maps are not
+ * combined with the cache (LUZ_E_UNSUPPORTED). */
+int luz_gpu_render_cached(luz_gpu_scene* scene, luz_gpu_cache* cache, const LuzRenderParams* params,
+                          float* rgb_out, LuzRenderStats* stats);
+
 
 /* Ray batch traversal (test hook and building block): rays are
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) * count, host buffers. any_hit != 0

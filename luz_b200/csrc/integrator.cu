@@ -172,7 +172,7 @@ using TraceKernel = void (*)(DScene, WaveArgs, PathBuf, Ctrl*, int);
 const TraceKernel kExtendKernels[4] = {k_extend<0>, k_extend<1>, k_extend<2>, k_extend<3>};
 const TraceKernel kShadowKernels[4] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>};
 
-template <bool CAUSTICS>
+template <int MODE>
 __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     const DScene& S = *Sp;
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DS
         uint32_t p = 0;
         if (valid) {
             p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
-            shade_path<CAUSTICS>(S, w, P, p, bounce, o);
+            shade_path<MODE>(S, w, P, p, bounce, o);
         }
         __syncwarp();
         const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
@@ -248,6 +248,28 @@ __global__ void k_accumulate(WaveArgs w, PathBuf P, double* film)
     f[0] += sx;
     f[1] += sy;
     f[2] += sz;
+}
+
+// Training rows of a radiance-cache wave: for every path with a snapshot, the
+// cache's inputs at the vertex and the radiance its suffix gathered (final path
+// radiance, as k_accumulate adds it, minus the snapshot) over its throughput there.
+__global__ void k_cache_targets(WaveArgs w, PathBuf P, CacheRecord* rows, uint32_t* count)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w.n || !w.cache_flag[p]) return;
+    const float4 r = P.rad[p], a = P.pend0[p], b = P.pend1[p];
+    const F3 fin = clean((F3{r.x, r.y, r.z} + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z});
+    const CacheSnap& sn = w.cache_s[p];
+    CacheRecord q;
+    for (int f = 0; f < kCacheIn; f++) q.in[f] = sn.in[f];
+    const float fc[3] = {fin.x, fin.y, fin.z};
+    for (int c = 0; c < 3; c++) {
+        const float v = sn.thr[c] > 1e-20f ? (fc[c] - sn.rad[c]) / sn.thr[c] : 0.0f;
+        q.v[c] = isfinite(v) ? v : 0.0f;
+    }
+    q.path = (uint32_t)p;
+    q.pad[0] = q.pad[1] = 0.0f;
+    rows[atomicAdd(count, 1u)] = q;
 }
 
 __global__ void k_resolve(const double* film, int64_t npix, double spp, float* out)
@@ -1600,7 +1622,7 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         s->extend = kExtendKernels[feat];
         s->shadow = kShadowKernels[feat];
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, s->extend, kBlock, 0));
-        s->shade = P.consts.caustics.enabled ? k_shade<true> : k_shade<false>;
+        s->shade = P.consts.caustics.enabled ? k_shade<1> : k_shade<0>;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, s->shade, kBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_sh, s->shadow, kBlock, 0));
         s->occ_ext = std::max(1, s->occ_ext);
@@ -1864,6 +1886,342 @@ int luz_gpu_trace_rays(luz_gpu_scene* s, const float* rays, int64_t count, int32
         cudaFree(dh);
         if (dk) cudaFree(dk);
         return LUZ_OK;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- learned radiance cache
+
+struct luz_gpu_cache {
+    int device = 0;
+    LuzCacheParams prm{};
+    float *W = nullptr, *G = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
+    __half *Wf = nullptr, *Wb = nullptr;
+    int64_t step = 0;   // Adam steps taken (bias correction)
+    ~luz_gpu_cache()
+    {
+        cudaSetDevice(device);
+        for (void* p : {(void*)W, (void*)G, (void*)m, (void*)v, (void*)loss, (void*)Wf, (void*)Wb})
+            if (p) cudaFree(p);
+    }
+};
+
+namespace {
+
+constexpr int kCacheGradSmem = kCacheGradSmemHalves * 2;
+constexpr int kCacheInferSmem = kCacheHalfF * 2;
+
+void cache_pack(luz_gpu_cache* c, cudaStream_t st)
+{
+    k_cache_pack<<<(kCacheParams + 255) / 256, 256, 0, st>>>(c->W, c->Wf, c->Wb);
+    CK(cudaGetLastError());
+}
+
+// Uniform +-sqrt(6 / fan_in) weights from a splitmix64 stream.
+std::vector<float> cache_init(uint32_t seed)
+{
+    std::vector<float> w(kCacheParams);
+    for (int l = 0; l < kCacheLayers; l++) {
+        const CacheLayer L = cache_layer(l);
+        const double a = std::sqrt(6.0 / (double)L.K);
+        for (int i = 0; i < L.K * L.N; i++) {
+            const uint64_t h = splitmix64(((uint64_t)seed << 32) ^ (uint64_t)(L.w + i));
+            const double u = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+            w[(std::size_t)(L.w + i)] = (float)((2.0 * u - 1.0) * a);
+        }
+    }
+    return w;
+}
+
+void cache_set(luz_gpu_cache* c, const float* w)
+{
+    CK(cudaMemcpy(c->W, w, sizeof(float) * kCacheParams, cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->m, 0, sizeof(float) * kCacheParams));
+    CK(cudaMemset(c->v, 0, sizeof(float) * kCacheParams));
+    CK(cudaMemset(c->G, 0, sizeof(float) * kCacheParams));
+    c->step = 0;
+    cache_pack(c, 0);
+    CK(cudaDeviceSynchronize());
+}
+
+// One Adam step from the rows on the device (count: device row count, or NULL for n_max).
+void cache_step(luz_gpu_cache* c, const CacheRecord* rows, const uint32_t* count, int n_max, cudaStream_t st)
+{
+    k_cache_grad<<<(unsigned)((n_max + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem, st>>>(
+        rows, count, n_max, c->Wf, c->Wb, c->G, c->loss);
+    c->step++;
+    const float b1 = 0.9f, b2 = 0.99f;
+    k_cache_adam<<<(kCacheParams + 255) / 256, 256, 0, st>>>(c->W, c->G, c->m, c->v, c->prm.learning_rate, b1, b2, 1e-8f,
+                                                             (float)std::pow((double)b1, (double)c->step),
+                                                             (float)std::pow((double)b2, (double)c->step), count, n_max);
+    cache_pack(c, st);
+}
+
+std::vector<CacheRecord> cache_rows(const float* inputs, const float* targets, int64_t n)
+{
+    std::vector<CacheRecord> r((std::size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        CacheRecord& q = r[(std::size_t)i];
+        std::memset(&q, 0, sizeof(q));
+        for (int f = 0; f < kCacheIn; f++) q.in[f] = inputs[kCacheIn * i + f];
+        if (targets)
+            for (int k = 0; k < 3; k++) q.v[k] = targets[3 * i + k];
+    }
+    return r;
+}
+
+void cache_check_rows(const luz_gpu_cache* c, const float* inputs, int64_t n)
+{
+    if (!c || (!inputs && n > 0)) throw Status(LUZ_E_INVALID, "NULL argument.");
+    if (n < 0 || n > (int64_t)INT32_MAX / 2) throw Status(LUZ_E_INVALID, "Row count out of range.");
+}
+
+int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* p, float* rgb_out, LuzRenderStats* stats)
+{
+    check_params(p);
+    if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported with the radiance cache.");
+    if (s->pack->consts.caustics.enabled)
+        throw Status(LUZ_E_UNSUPPORTED, "The radiance cache is not combined with caustic photon maps.");
+    if (c->device != s->device) throw Status(LUZ_E_INVALID, "The cache and the scene are on different devices.");
+    CK(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    const int64_t npix = (int64_t)p->width * p->height;
+    const int64_t pix_wave = std::min<int64_t>(npix, kWaveTarget);
+    s->ensure_paths(pix_wave);
+    DeviceScratch D;
+    CacheRecord* q = D.get<CacheRecord>(pix_wave, st);
+    CacheRecord* rows = D.get<CacheRecord>(pix_wave, st);
+    CacheSnap* snaps = D.get<CacheSnap>(pix_wave, st);
+    uint8_t* tflag = D.get<uint8_t>(pix_wave, st);
+    uint32_t* counts = D.get<uint32_t>(2, st);
+    double* film = D.get<double>(3 * npix, st);
+    float* d_out = D.get<float>(3 * npix, st);
+    static const ShadeKernel shade_cached = k_shade<2>;
+    int occ = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_cached, kBlock, 0));
+    occ = std::max(1, occ);
+
+    WaveArgs w = base_args(s, p);
+    const GSceneConst& K = s->pack->consts;
+    w.cache_prefix = c->prm.prefix;
+    w.cache_train_every = (uint32_t)c->prm.train_every;
+    w.cache_q = q;
+    w.cache_s = snaps;
+    w.cache_flag = tflag;
+    w.cache_count = counts;
+    for (int a = 0; a < 3; a++) {
+        w.cache_lo[a] = K.box_lo[a];
+        w.cache_inv[a] = K.box_inv[a];
+    }
+    CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
+    CK(cudaEventRecord(s->ev0, st));
+    const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * occ;
+    const int batch = c->prm.batch;
+    int64_t launches = 0, waves = 0;
+    for (int sample = 0; sample < p->spp; sample++) {
+        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
+            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = sample;
+            w.s_count = 1;
+            w.n = pc;
+            w.list_mode = 0;
+            w.cache_wave = (uint32_t)waves;
+            CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+            CK(cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(tflag, 0, (std::size_t)pc, st));
+            CK(cudaMemsetAsync(c->loss, 0, sizeof(float), st));
+            k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
+            for (int b = 0; b <= w.max_bounces; b++) {
+                s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+                shade_cached<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
+                s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+            }
+            k_cache_infer<<<(unsigned)(2 * s->sms), 128, kCacheInferSmem, st>>>(q, counts, 0, c->Wf, nullptr, s->pb.rad);
+            k_cache_targets<<<(unsigned)((pc + 255) / 256), 256, 0, st>>>(w, s->pb, rows, counts + 1);
+            cache_step(c, rows, counts + 1, (int)std::min<int64_t>(batch, pc), st);
+            k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, film);
+            k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
+            CK(cudaGetLastError());
+            launches += 3 * (w.max_bounces + 1) + 9;
+            waves++;
+        }
+    }
+    k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(film, npix, (double)p->spp, d_out);
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    unsigned long long tot[2] = {0, 0};
+    uint32_t err = 0;
+    CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    CK(cudaMemcpy(rgb_out, d_out, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = (double)npix * p->spp;
+        stats->extension_rays = (double)tot[0];
+        stats->shadow_rays = (double)tot[1];
+        stats->kernel_launches = launches + 1;
+        stats->waves = waves;
+    }
+    return LUZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int luz_gpu_cache_create(int32_t device, const LuzCacheParams* prm, luz_gpu_cache** out)
+{
+    return guard([&] {
+        if (!prm || !out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        *out = nullptr;
+        if (prm->batch <= 0) throw Status(LUZ_E_INVALID, "Cache batch must be positive.");
+        if (!(prm->learning_rate > 0.0f) || !std::isfinite(prm->learning_rate))
+            throw Status(LUZ_E_INVALID, "Cache learning rate must be finite and positive.");
+        if (prm->prefix < 0) throw Status(LUZ_E_INVALID, "Cache prefix must be non-negative.");
+        if (prm->train_every < 1) throw Status(LUZ_E_INVALID, "Cache training interval must be at least 1.");
+        CK(cudaSetDevice(device));
+        std::unique_ptr<luz_gpu_cache> c(new luz_gpu_cache);
+        c->device = device;
+        c->prm = *prm;
+        c->W = dalloc<float>(kCacheParams);
+        c->G = dalloc<float>(kCacheParams);
+        c->m = dalloc<float>(kCacheParams);
+        c->v = dalloc<float>(kCacheParams);
+        c->loss = dalloc<float>(1);
+        c->Wf = dalloc<__half>(kCacheHalfF);
+        c->Wb = dalloc<__half>(kCacheHalfB);
+        CK(cudaMemset(c->Wf, 0, sizeof(__half) * kCacheHalfF));
+        CK(cudaMemset(c->Wb, 0, sizeof(__half) * kCacheHalfB));
+        CK(cudaFuncSetAttribute(k_cache_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, kCacheGradSmem));
+        CK(cudaFuncSetAttribute(k_cache_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kCacheInferSmem));
+        const std::vector<float> w0 = cache_init(prm->seed);
+        cache_set(c.get(), w0.data());
+        *out = c.release();
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_cache_destroy(luz_gpu_cache* c)
+{
+    delete c;
+    return LUZ_OK;
+}
+
+int luz_gpu_cache_weights(luz_gpu_cache* c, float* get, const float* set)
+{
+    return guard([&] {
+        if (!c) throw Status(LUZ_E_INVALID, "NULL argument.");
+        CK(cudaSetDevice(c->device));
+        if (get) CK(cudaMemcpy(get, c->W, sizeof(float) * kCacheParams, cudaMemcpyDeviceToHost));
+        if (set) cache_set(c, set);
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_cache_predict(luz_gpu_cache* c, const float* inputs, int64_t n, float* rgb_out)
+{
+    return guard([&] {
+        cache_check_rows(c, inputs, n);
+        if (!rgb_out && n > 0) throw Status(LUZ_E_INVALID, "NULL argument.");
+        if (n == 0) return LUZ_OK;
+        CK(cudaSetDevice(c->device));
+        const std::vector<CacheRecord> r = cache_rows(inputs, nullptr, n);
+        CacheRecord* d = dupload(r);
+        float* o = nullptr;
+        try {
+            o = dalloc<float>((std::size_t)(3 * n));
+            const int tiles = (int)((n + 15) / 16);
+            k_cache_infer<<<(unsigned)std::max(1, std::min(tiles / 4 + 1, 1184)), 128, kCacheInferSmem>>>(
+                d, nullptr, (int)n, c->Wf, o, nullptr);
+            CK(cudaGetLastError());
+            CK(cudaMemcpy(rgb_out, o, sizeof(float) * 3 * (std::size_t)n, cudaMemcpyDeviceToHost));
+        } catch (...) {
+            cudaFree(d);
+            if (o) cudaFree(o);
+            throw;
+        }
+        cudaFree(d);
+        cudaFree(o);
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_cache_gradient(luz_gpu_cache* c, const float* inputs, const float* targets, int64_t n, float* grad_out,
+                           double* loss_out)
+{
+    return guard([&] {
+        cache_check_rows(c, inputs, n);
+        if (!targets || n <= 0) throw Status(LUZ_E_INVALID, "Gradient needs rows and targets.");
+        CK(cudaSetDevice(c->device));
+        const std::vector<CacheRecord> r = cache_rows(inputs, targets, n);
+        CacheRecord* d = dupload(r);
+        try {
+            CK(cudaMemset(c->G, 0, sizeof(float) * kCacheParams));
+            CK(cudaMemset(c->loss, 0, sizeof(float)));
+            k_cache_grad<<<(unsigned)((n + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem>>>(
+                d, nullptr, (int)n, c->Wf, c->Wb, c->G, c->loss);
+            CK(cudaGetLastError());
+            std::vector<float> g(kCacheParams);
+            float l = 0.f;
+            CK(cudaMemcpy(g.data(), c->G, sizeof(float) * kCacheParams, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&l, c->loss, sizeof(float), cudaMemcpyDeviceToHost));
+            CK(cudaMemset(c->G, 0, sizeof(float) * kCacheParams));
+            if (grad_out)
+                for (int i = 0; i < kCacheParams; i++) grad_out[i] = g[(std::size_t)i] / (kCacheLossScale * (float)n);
+            if (loss_out) *loss_out = (double)l / (double)n;
+        } catch (...) {
+            cudaFree(d);
+            throw;
+        }
+        cudaFree(d);
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_cache_train(luz_gpu_cache* c, const float* inputs, const float* targets, int64_t n, int32_t steps,
+                        double* loss_out)
+{
+    return guard([&] {
+        cache_check_rows(c, inputs, n);
+        if (!targets || n <= 0) throw Status(LUZ_E_INVALID, "Training needs rows and targets.");
+        if (n > c->prm.batch) throw Status(LUZ_E_INVALID, "More rows than the cache batch.");
+        if (steps < 0) throw Status(LUZ_E_INVALID, "Step count must be non-negative.");
+        CK(cudaSetDevice(c->device));
+        const std::vector<CacheRecord> r = cache_rows(inputs, targets, n);
+        CacheRecord* d = dupload(r);
+        try {
+            for (int i = 0; i < steps; i++) {
+                CK(cudaMemset(c->loss, 0, sizeof(float)));
+                cache_step(c, d, nullptr, (int)n, 0);
+                CK(cudaGetLastError());
+                float l = 0.f;
+                CK(cudaMemcpy(&l, c->loss, sizeof(float), cudaMemcpyDeviceToHost));
+                if (loss_out) loss_out[i] = (double)l / (double)n;
+            }
+        } catch (...) {
+            cudaFree(d);
+            throw;
+        }
+        cudaFree(d);
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* p, float* rgb_out,
+                          LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !c || !rgb_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_render_cached(s, c, p, rgb_out, stats);
     });
 }
 

@@ -268,6 +268,8 @@ struct GSceneConst {
     GEnv env;
     GAtmos atmos;
     GCaustics caustics;
+    float box_lo[3];          // box of every bounded object (radiance-cache position input)
+    float box_inv[3];         // 1 / extent per axis (1 where the extent is 0 or there is no box)
 };
 
 }  // namespace luz

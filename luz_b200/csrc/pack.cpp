@@ -1268,6 +1268,12 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
         }
     }
 
+    for (int a = 0; a < 3; a++) {   // scene box for the radiance cache's position input
+        const double ext = scene_has_box ? scene_box.mx[a] - scene_box.mn[a] : 0.0;
+        K.box_lo[a] = scene_has_box ? (float)scene_box.mn[a] : 0.0f;
+        K.box_inv[a] = (std::isfinite(ext) && ext > 0.0) ? (float)(1.0 / ext) : 1.0f;
+    }
+
     // caustic photon map settings (Scene setters, Scene.cpp:317-360; CausticPhotonMap::build, :430-450)
     if (d->caustics.enabled) {
         const LuzCausticsDesc& c = d->caustics;

@@ -1,6 +1,7 @@
 // wavefront.cuh — per-path device logic of the wavefront integrator (state
 // layout, camera rays, the shade step); kernels live in integrator.cu.
 #pragma once
+#include "cache.cuh"
 #include "caustics.cuh"
 #include "shade.cuh"
 
@@ -41,6 +42,14 @@ struct PathBuf {
     uint32_t bin_stride;
 };
 
+// Training snapshot of a path at its cache vertex: inputs, throughput and the
+// radiance gathered before the vertex's own light (emission excepted).
+struct CacheSnap {
+    float in[kCacheIn];
+    float thr[3];
+    float rad[3];
+};
+
 struct WaveArgs {
     int32_t width, height;
     uint32_t seed, stream;
@@ -62,9 +71,19 @@ struct WaveArgs {
     double* grad;                 // dLoss/dTexel, texture W*H*3
     double inv_spp;
     GCamera cam;
+    // radiance-cache render (luz_gpu_render_cached)
+    int32_t cache_prefix;         // first bounce whose surface vertex queries the cache
+    uint32_t cache_train_every;   // one training path in this many
+    uint32_t cache_wave;          // wave counter: varies the training paths
+    CacheRecord* cache_q;         // queries of the paths that end at the cache
+    CacheSnap* cache_s;           // training snapshots, one slot per path
+    uint8_t* cache_flag;          // 1 where the path left a training snapshot
+    uint32_t* cache_count;        // [0] queries
+    float cache_lo[3], cache_inv[3];   // position input = (p - lo) * inv
 };
 
-enum PathFlags : uint32_t { PF_PREV_SPECULAR = 1u, PF_PREV_SVIL = 2u };
+
+enum PathFlags : uint32_t { PF_PREV_SPECULAR = 1u, PF_PREV_SVIL = 2u, PF_CACHE_DONE = 4u };
 
 __device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint32_t& x, uint32_t& y, uint32_t& s)
 {
@@ -327,7 +346,26 @@ __device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& P, uint
 
 // CAUSTICS: the scene has a caustic photon map (a separate instantiation, so
 // that scenes without one keep the leaner kernel).
-template <bool CAUSTICS>
+// Radiance-cache inputs at a surface hit: position in the scene box, outgoing
+// direction, shading normal, roughness (1 for diffuse and volume phase materials).
+__device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, const GMaterial& m, F3 ray_d, float* in)
+{
+    in[0] = (h.p.x - w.cache_lo[0]) * w.cache_inv[0];
+    in[1] = (h.p.y - w.cache_lo[1]) * w.cache_inv[1];
+    in[2] = (h.p.z - w.cache_lo[2]) * w.cache_inv[2];
+    const F3 wo = safe_normalize(ray_d * -1.0f, h.n);
+    in[3] = wo.x;
+    in[4] = wo.y;
+    in[5] = wo.z;
+    in[6] = h.n.x;
+    in[7] = h.n.y;
+    in[8] = h.n.z;
+    const bool diffuse = m.type == MT_LAMBERTIAN || m.type == MT_ISOTROPIC || m.type == MT_HG || m.type == MT_EMISSIVE;
+    in[9] = diffuse ? 1.0f : m.roughness;
+}
+
+// MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render.
+template <int MODE>
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
     out.cont = false;
@@ -439,9 +477,36 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
             goto done;
         }
         rad = rad + thr * emitted;
+        if constexpr (MODE == 2) {   // the cache answers for everything past this vertex, or it trains
+            if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE)) {
+                const uint64_t key = ((uint64_t)pix << 24) ^ (uint64_t)P.sample[p] ^ ((uint64_t)w.cache_wave << 48);
+                if (splitmix64(key) % w.cache_train_every == 0) {
+                    CacheSnap& sn = w.cache_s[p];
+                    cache_inputs(w, h, m, ray.d, sn.in);
+                    sn.thr[0] = thr.x;
+                    sn.thr[1] = thr.y;
+                    sn.thr[2] = thr.z;
+                    sn.rad[0] = rad.x;
+                    sn.rad[1] = rad.y;
+                    sn.rad[2] = rad.z;
+                    w.cache_flag[p] = 1;
+                    flags |= PF_CACHE_DONE;
+                } else {
+                    CacheRecord q;
+                    cache_inputs(w, h, m, ray.d, q.in);
+                    q.v[0] = thr.x;
+                    q.v[1] = thr.y;
+                    q.v[2] = thr.z;
+                    q.path = p;
+                    q.pad[0] = q.pad[1] = 0.0f;
+                    w.cache_q[atomicAdd(w.cache_count, 1u)] = q;
+                    goto done;
+                }
+            }
+        }
         if (w.adjoint && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture) adjoint_texture(S, w, P, p, h, rad);
         if (terminated(thr * att)) goto done;
-        if constexpr (CAUSTICS)
+        if constexpr (MODE == 1)
             if (S.cm.count) rad = rad + clamp_ray_color(thr * caustic_estimate(S, h, sr, m, ray.d));
         if (S.k.light_count > 0) {   // estimateDirectLighting (ColorHelper.cpp:973-1033)
             const float prob = direct_prob(bounce);

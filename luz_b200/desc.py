@@ -159,6 +159,19 @@ class NforSettings(C.Structure):
                 ("patch_radius", C.c_int32), ("reserved", C.c_int32), ("min_variance", C.c_double)]
 
 
+CACHE_PARAMS = 21504
+
+
+class CacheParams(C.Structure):
+    """LuzCacheParams: learned radiance cache settings."""
+    _fields_ = [("seed", C.c_uint32), ("batch", C.c_int32), ("learning_rate", C.c_float), ("prefix", C.c_int32),
+                ("train_every", C.c_int32), ("reserved", C.c_int32)]
+
+
+def cache_params(seed=1, batch=65536, learning_rate=1e-2, prefix=1, train_every=16) -> CacheParams:
+    return CacheParams(seed, batch, learning_rate, prefix, train_every, 0)
+
+
 class Hit(C.Structure):
     _fields_ = [("t", C.c_float), ("object", C.c_int32), ("primitive", C.c_int32), ("u", C.c_float), ("v", C.c_float)]
 

@@ -25,6 +25,8 @@ EXPORTED = [
     "luz_gpu_render_device_noalloc", "luz_gpu_render_ex", "luz_gpu_batch_render",
     "luz_gpu_scene_set_texture", "luz_gpu_adjoint_forward", "luz_gpu_adjoint_backward",
     "luz_gpu_nfor_denoise", "luz_gpu_nfor_error", "luz_gpu_render_denoised",
+    "luz_gpu_cache_create", "luz_gpu_cache_destroy", "luz_gpu_cache_weights", "luz_gpu_cache_predict",
+    "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -73,6 +75,13 @@ def lib():
     L.luz_gpu_scene_set_texture.argtypes = [vp, i32, vp]
     L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_cache_create.argtypes = [i32, C.POINTER(D.CacheParams), C.POINTER(vp)]
+    L.luz_gpu_cache_destroy.argtypes = [vp]
+    L.luz_gpu_cache_weights.argtypes = [vp, vp, vp]
+    L.luz_gpu_cache_predict.argtypes = [vp, vp, i64, vp]
+    L.luz_gpu_cache_gradient.argtypes = [vp, vp, vp, i64, vp, C.POINTER(C.c_double)]
+    L.luz_gpu_cache_train.argtypes = [vp, vp, vp, i64, i32, vp]
+    L.luz_gpu_render_cached.argtypes = [vp, vp, C.POINTER(D.RenderParams), vp, C.POINTER(D.RenderStats)]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int
     _lib = L
@@ -297,3 +306,61 @@ def render(scene: D.Scene, width: int, height: int, spp: int, max_bounces: int, 
         return g.render(params(width, height, spp, max_bounces, seed, stream))
     finally:
         g.close()
+
+
+class RadianceCache:
+    """luz_gpu_cache: the learned radiance cache (FP16 tensor-core MLP trained online)."""
+
+    def __init__(self, params: Optional[D.CacheParams] = None, device: int = 0):
+        self.params = params if params is not None else D.cache_params()
+        self.h = C.c_void_p()
+        _check(lib().luz_gpu_cache_create(device, C.byref(self.params), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().luz_gpu_cache_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def weights(self) -> np.ndarray:
+        w = np.zeros(D.CACHE_PARAMS, np.float32)
+        _check(lib().luz_gpu_cache_weights(self.h, w.ctypes.data, None))
+        return w
+
+    def set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        _check(lib().luz_gpu_cache_weights(self.h, None, w.ctypes.data))
+
+    def predict(self, inputs: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(inputs, np.float32)
+        out = np.zeros((x.shape[0], 3), np.float32)
+        _check(lib().luz_gpu_cache_predict(self.h, x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def gradient(self, inputs: np.ndarray, targets: np.ndarray):
+        x = np.ascontiguousarray(inputs, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        g = np.zeros(D.CACHE_PARAMS, np.float32)
+        loss = C.c_double()
+        _check(lib().luz_gpu_cache_gradient(self.h, x.ctypes.data, t.ctypes.data, x.shape[0], g.ctypes.data,
+                                            C.byref(loss)))
+        return g, loss.value
+
+    def train(self, inputs: np.ndarray, targets: np.ndarray, steps: int = 1) -> np.ndarray:
+        x = np.ascontiguousarray(inputs, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        losses = np.zeros(max(steps, 1), np.float64)
+        _check(lib().luz_gpu_cache_train(self.h, x.ctypes.data, t.ctypes.data, x.shape[0], steps, losses.ctypes.data))
+        return losses[:steps]
+
+    def render(self, scene: "GpuScene", p: D.RenderParams):
+        """luz_gpu_render_cached: film (H x W x 3) and stats; trains the cache as it renders."""
+        out = np.zeros((p.height, p.width, 3), np.float32)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_render_cached(scene.h, self.h, C.byref(p), out.ctypes.data, C.byref(st)))
+        return out, st

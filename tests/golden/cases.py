@@ -43,6 +43,12 @@ def caustic_case():
     return scenes.caustic_pool(64, 48, 2, 8)
 
 
+# Converged-oracle cases: the reference's film at 65,536 spp.
+ORACLE_64K = {
+    "cornell": lambda: scenes.cornell(24, 24, 65536, 8),
+    "tiny": lambda: scenes.tiny_mixed(24, 18, 65536, 6),
+}
+
 CAUSTIC_COUNTS = [(424242424, 8), (7, 8), (424242424, 3), (99, 12)]
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.

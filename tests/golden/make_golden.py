@@ -16,7 +16,8 @@ output of the unmodified reference code:
   nfor.npz           Denoise::applyNFOR outputs (src/core/Denoise/NFOR.cpp:977-1102)
   caustics.npz       CausticPhotonMap::build photon counts (src/renderer/CausticPhotonMap.cpp:430-551)
                      and per-path radiance of paths whose caustic estimate is non-zero
-Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | caustics | cases <name>...]
+  oracle64k_<case>.npz Renderer::render films at 65,536 spp (the converged oracle images)
+Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | caustics | oracle64k | cases <name>...]
 """
 from __future__ import annotations
 
@@ -32,8 +33,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, adjoint_case, camera_rays,  # noqa: E402
-                   caustic_case, nfor_synthetic, path_keys)
+from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, ORACLE_64K, adjoint_case,  # noqa: E402
+                   camera_rays, caustic_case, nfor_synthetic, path_keys)
 from luz_b200 import native  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
@@ -147,6 +148,16 @@ def caustic_fixture(o, n_paths=2000):
     print("golden caustics", counts, sel.size, flush=True)
 
 
+def oracle64k_fixtures(o):
+    """oracle64k_<case>.npz: the reference's own film at 65,536 spp (all host threads)."""
+    for name, fn in ORACLE_64K.items():
+        w = fn()
+        rs = o.scene(w.scene.build())
+        img, ms, _ = rs.render(native.params(w.width, w.height, w.spp, w.max_bounces, w.seed), os.cpu_count() or 1)
+        np.savez_compressed(os.path.join(HERE, f"oracle64k_{name}.npz"), rgb=img, spp=w.spp, seed=w.seed)
+        print("golden oracle64k", name, f"{ms / 1000:.1f} s", flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -160,6 +171,9 @@ def main():
         return
     if sys.argv[1:] == ["caustics"]:
         caustic_fixture(o)
+        return
+    if sys.argv[1:] == ["oracle64k"]:
+        oracle64k_fixtures(o)
         return
     if sys.argv[1:2] == ["cases"]:     # cases <name>...: only the per-case files of those cases
         case_fixtures(o, sys.argv[2:])
@@ -188,6 +202,7 @@ def main():
     adjoint_fixture(o)
     nfor_fixture(o)
     caustic_fixture(o)
+    oracle64k_fixtures(o)
 
 
 if __name__ == "__main__":

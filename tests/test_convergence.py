@@ -1,0 +1,50 @@
+"""Whole images against the converged oracle: the reference's own film at 65,536 spp
+(tests/golden/oracle64k_<case>.npz, Renderer::render, made by make_golden.py).
+
+Relative MSE = mean((image - oracle)^2) / mean(oracle^2).
+* With the oracle's seed, the GPU film at 65,536 spp is the same Monte Carlo estimate
+  (per-path parity): Cornell to a relative MSE below 1e-9 (measured 2.7e-13); on the mixed
+  scene 99% of pixels agree to 1e-3 relative, and the relative MSE is set by single paths
+  that leave a sharp specular chain differently in FP32 and FP64 (one of them carries
+  ~1.8e4 radiance into one pixel and the small emissive sphere), so it is not bounded here.
+* With an independent seed (Cornell), the error falls with the sample count, and a
+  1,048,576-spp GPU film sits within the oracle's own noise: relative MSE below 1e-6
+  (measured 3.0e-7)."""
+import numpy as np
+import pytest
+
+from cases import ORACLE_64K
+from luz_b200 import native
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img.astype(np.float64) - ref) ** 2) / np.mean(ref ** 2))
+
+
+@pytest.mark.parametrize("name", sorted(ORACLE_64K))
+def test_same_seed_matches_oracle_at_65536_spp(name, golden):
+    w = ORACLE_64K[name]()
+    ref = golden("oracle64k_" + name)
+    g = native.GpuScene(w.scene.build())
+    img, st = g.render(native.params(w.width, w.height, 65536, w.max_bounces, int(ref["seed"])))
+    g.close()
+    assert st.samples == w.width * w.height * 65536
+    rel = (np.abs(img - ref["rgb"]) / np.maximum(np.abs(ref["rgb"]), 1e-3)).max(axis=-1)
+    assert (rel <= 1e-3).mean() >= 0.99
+    if name == "cornell":
+        assert rel_mse(img, ref["rgb"]) < 1e-9
+
+
+def test_independent_seed_converges_to_oracle(golden):
+    w = ORACLE_64K["cornell"]()
+    ref = golden("oracle64k_cornell")["rgb"]
+    g = native.GpuScene(w.scene.build())
+    errs = []
+    for spp, seed in ((1024, 977), (16384, 977), (65536, 977), (1 << 20, 978)):
+        img, _ = g.render(native.params(w.width, w.height, spp, w.max_bounces, seed))
+        errs.append(rel_mse(img, ref))
+    g.close()
+    assert errs[0] > errs[1] > errs[2] > errs[3], errs
+    assert errs[3] < 1e-6, errs
