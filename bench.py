@@ -422,52 +422,70 @@ def run_nfor(args):
 
 
 def run_cache(args):
-    """--workload cache_glossy: time to equal RMSE, learned radiance cache against the plain
-    integrator, on the mesh + glossy scene at 480x270, depth 12. The converged image is a
-    1024-spp plain render (own seed); the target RMSE is that of the plain 16-spp image (seed
-    202); each curve is device time (CUDA events of the render call; the cached call includes
-    its training steps) against RMSE at 1..64 spp, the cached renders each starting from an
-    untrained cache. value = plain time / cached time at the target, interpolated log-log."""
+    """--workload cache_cornell | cache_room: time to equal error, learned radiance cache
+    against the plain integrator, on the Cornell box (300x300, depth 8) or the same box
+    closed with the camera inside (longer paths). Error = relative MSE, mean((x - ref)^2 /
+    (ref^2 + 0.01)), against a 4096-spp plain render with its own seed. Each curve is device
+    time (CUDA events around the render call; the cached call includes all its training)
+    against error at 2..256 spp (seed 202), every cached render starting from an untrained
+    cache. The speedup at a target error is plain time / cached time to reach it (log-log
+    interpolation); the targets are the plain image's errors at 16, 64 and 256 spp, and
+    value is the speedup at the 256-spp target (the quality of a finished frame)."""
     from luz_b200 import desc as D
     from luz_b200 import native, scenes
-    w = scenes.mesh_glossy(480, 270, 1, 12)
+    w = scenes.cornell(300, 300, 1, 8, closed=args.workload == "cache_room")
     g = native.GpuScene(w.scene.build())
     W, H, MB = w.width, w.height, w.max_bounces
-    ref, _ = g.render(native.params(W, H, 1024, MB, 101))
+    ref, _ = g.render(native.params(W, H, 4096, MB, 101))
     ref = ref.astype(np.float64)
 
-    def rmse(img):
-        return float(np.sqrt(np.mean((img.astype(np.float64) - ref) ** 2)))
+    def relmse(img):
+        return float(np.mean((img.astype(np.float64) - ref) ** 2 / (ref ** 2 + 0.01)))
 
-    spps = [1, 2, 4, 8, 16, 32, 64]
+    spps = [2, 4, 8, 16, 32, 64, 128, 256]
     for _ in range(max(1, args.warmup)):
         g.render(native.params(W, H, 4, MB, 7))
+        c = native.RadianceCache(D.cache_params(seed=3))
+        c.render(g, native.params(W, H, 4, MB, 7))
+        c.close()
     plain, cached = [], []
     for spp in spps:
         img, st = g.render(native.params(W, H, spp, MB, 202))
-        plain.append((spp, st.render_ms, rmse(img)))
+        plain.append((spp, st.render_ms, relmse(img)))
         c = native.RadianceCache(D.cache_params(seed=3))
         img, st = c.render(g, native.params(W, H, spp, MB, 202))
-        cached.append((spp, st.render_ms, rmse(img)))
+        cached.append((spp, st.render_ms, relmse(img)))
         c.close()
-    target = plain[spps.index(16)][2]
 
-    def time_to(curve):
+    def time_to(curve, target):
+        if curve[0][2] <= target:
+            return curve[0][1]
         for (s0, t0, e0), (s1, t1, e1) in zip(curve, curve[1:]):
             if e0 >= target >= e1 and e0 > e1:
                 a = (np.log(e0) - np.log(target)) / (np.log(e0) - np.log(e1))
                 return float(np.exp(np.log(t0) + a * (np.log(t1) - np.log(t0))))
-        return curve[0][1] if curve[0][2] <= target else None
+        return None
 
-    tp, tc = time_to(plain), time_to(cached)
-    out = {"metric": "time-to-equal-RMSE speedup (cached vs plain)", "value": (tp / tc) if (tp and tc) else None,
-           "unit": "x", "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": tc,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f16 (MLP)",
+    at = {}
+    for ts in (16, 64, 256):
+        target = plain[spps.index(ts)][2]
+        tp, tc = time_to(plain, target), time_to(cached, target)
+        at[f"plain_{ts}spp"] = {"target_error": target, "plain_ms": tp, "cached_ms": tc,
+                                "speedup": (tp / tc) if (tp and tc) else None}
+    head = at["plain_256spp"]
+    out = {"metric": "time-to-equal-error speedup (cached vs plain)", "value": head["speedup"], "unit": "x",
+           "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": head["cached_ms"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 paths, f16 MLP",
            "data": "synthetic (seeded scene generator)",
-           "config": {"workload": f"cache_glossy: mesh_glossy {W}x{H} depth {MB}, converged = plain 1024 spp",
-                      "target_rmse": target, "cache": "prefix 1, one training path in 16, batch 65536, lr 1e-2"},
-           "plain": {"ms_to_target": tp, "curve": [{"spp": s, "ms": t, "rmse": e} for s, t, e in plain]},
-           "cached": {"ms_to_target": tc, "curve": [{"spp": s, "ms": t, "rmse": e} for s, t, e in cached]}}
+           "config": {"workload": f"{args.workload}: {w.name} {W}x{H} depth {MB}, converged = plain 4096 spp",
+                      "error": "relative MSE mean((x - ref)^2 / (ref^2 + 0.01))",
+                      "target": "error of the plain 256-spp image",
+                      "cache": "prefix 1, NEE explicit at the cache vertex, one training path in 16, "
+                               "batch 16384 (up to 16 steps per wave), lr 1e-2, first sample plain with 32 "
+                               "warm-up steps"},
+           "speedup_at": at,
+           "plain": {"curve": [{"spp": s, "ms": t, "relmse": e} for s, t, e in plain]},
+           "cached": {"curve": [{"spp": s, "ms": t, "relmse": e} for s, t, e in cached]}}
     print(json.dumps(out), flush=True)
     g.close()
 
@@ -482,7 +500,7 @@ def main():
         run_adjoint(args)
     elif args.workload == "nfor1080":
         run_nfor(args)
-    elif args.workload == "cache_glossy":
+    elif args.workload in ("cache_cornell", "cache_room"):
         run_cache(args)
     else:
         run_ours(args)

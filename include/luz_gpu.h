@@ -458,21 +458,26 @@ int luz_gpu_render_denoised(luz_gpu_scene* scene, const LuzRenderParams* params,
  * sin/cos(2^k pi x) for k = 0..5; four hidden layers of 64 with ReLU; RGB out)
  * with FP16 weights and activations and FP32 accumulation on the tensor cores,
  * trained online with Adam on the relative L2 loss sum_c (y - t)^2 / (y^2 + 0.01)
- * (denominator held constant, per-row gradient clamped to +-100).
- * luz_gpu_render_cached ends every path at its first surface vertex at or after
- * bounce `prefix` that does not scatter specularly, adding throughput x the
- * cache's prediction there (a biased estimate: the plain luz_gpu_render stays
- * the unbiased judge of it); one path in `train_every` instead continues
+ * (denominator held constant, per-row gradient clamped to +-2000).
+ * luz_gpu_render_cached renders every pixel's first sample plain, every path
+ * supplying a training row, and trains the cache on them (32 Adam steps). Later
+ * samples stop at their first surface vertex at or after bounce `prefix` that
+ * does not scatter specularly: the vertex's own emission and next-event
+ * estimate stay explicit, and the cache's prediction times the path throughput
+ * stands for the continuation (a biased estimate: the plain luz_gpu_render
+ * stays the unbiased judge of it). One path in `train_every` instead continues
  * unbiased and supplies a training row: its inputs at that vertex and the
- * radiance its suffix gathered divided by its throughput there. After every
- * wave of one sample per pixel the cache takes one Adam step on up to `batch`
- * of that wave's rows. The cache belongs to one device and one scene at a time
+ * radiance its continuation gathered divided by its throughput there. Samples
+ * run in waves as in luz_gpu_render; after each wave the cache takes one Adam
+ * step per `batch` of that wave's rows (at most 16). Training rows are appended
+ * in arrival order, so cached renders are not bit-reproducible. The cache
+ * belongs to one device and one scene at a time
  * (the position input is normalised to the box of the scene it renders). */
 typedef struct luz_gpu_cache luz_gpu_cache;
 #define LUZ_CACHE_PARAMS 21504   /* FP32 weights: W0 128x64, W1..W3 64x64, W4 64x16, row-major [in][out] */
 typedef struct LuzCacheParams {
     uint32_t seed;                /* weight initialisation (uniform +-sqrt(6 / fan_in))    */
-    int32_t  batch;               /* training rows per step (65536); > 0                     */
+    int32_t  batch;               /* training rows per step (16384); > 0                     */
     float    learning_rate;       /* Adam step size (1e-2); beta1 0.9, beta2 0.99, eps 1e-8 */
     int32_t  prefix;              /* first bounce whose vertex queries the cache (1); >= 0   */
     int32_t  train_every;         /* one training path in this many (16); >= 1               */

@@ -215,9 +215,9 @@ __global__ void __launch_bounds__(128) k_cache_infer(const CacheRecord* rec, con
 }
 
 // Loss gradient of the relative L2 loss sum_c (y - t)^2 / (y^2 + 0.01) (the
-// denominator held constant), clamped to +-100, times the loss scale (|value| <= 12800, inside FP16).
-constexpr float kCacheLossScale = 128.0f;
-constexpr float kCacheGradClamp = 100.0f;
+// denominator held constant), clamped to +-2000, times the loss scale (|value| <= 16000, inside FP16).
+constexpr float kCacheLossScale = 8.0f;
+constexpr float kCacheGradClamp = 2000.0f;
 
 // Stages a 16-row tile of A fragments (KC chunks) into shared memory rows [row][ld].
 template <int KC>
@@ -257,13 +257,22 @@ __host__ __device__ constexpr int cache_x_off(int l) { return kGX0 + (l == 0 ? 0
 __host__ __device__ constexpr int cache_d_off(int l) { return cache_x_off(4) + 64 * 72 + l * 64 * 72; }
 constexpr int kCacheGradSmemHalves = cache_d_off(4) + 64 * 24;
 
-// Gradient of the summed loss over the first n = min(*count, n_max) records
-// (in: inputs, v: targets) with respect to W, times the loss scale, added into
-// G; the summed loss into *loss. Launch with ceil(n_max / 64) blocks of 128.
-__global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, const uint32_t* count, int n_max,
-                                                    const __half* Wf_g, const __half* Wb_g, float* G, float* loss)
+// Rows of one training step: records [offset, offset + n) with n = min(*count -
+// offset, n_max), at least 0 (count NULL: n_max).
+__device__ __forceinline__ int cache_step_rows(const uint32_t* count, int offset, int n_max)
 {
-    const int n = count ? min((int)*count, n_max) : n_max;
+    return count ? max(0, min((int)*count - offset, n_max)) : n_max;
+}
+
+// Gradient of the summed loss over the step's rows (in: inputs, v: targets)
+// with respect to W, times the loss scale, added into G; the summed loss into
+// *loss. Launch with ceil(n_max / 64) blocks of 128.
+__global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, const uint32_t* count, int offset,
+                                                    int n_max, const __half* Wf_g, const __half* Wb_g, float* G,
+                                                    float* loss)
+{
+    const int n = cache_step_rows(count, offset, n_max);
+    rec += offset;
     if ((int)blockIdx.x * kCacheRowsPerBlock >= n) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __half* sm = reinterpret_cast<__half*>(smem_raw);
@@ -376,13 +385,13 @@ __global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, cons
 }
 
 // Adam step (Kingma & Ba 2015) on the master weights; G holds the summed,
-// loss-scaled gradient of n = min(*count, n_max) rows. Clears G for the next step.
+// loss-scaled gradient of the step's rows. Clears G for the next step.
 __global__ void k_cache_adam(float* W, float* G, float* m, float* v, float lr, float b1, float b2, float eps,
-                             float b1t, float b2t, const uint32_t* count, int n_max)
+                             float b1t, float b2t, const uint32_t* count, int offset, int n_max)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kCacheParams) return;
-    const int n = count ? min((int)*count, n_max) : n_max;
+    const int n = cache_step_rows(count, offset, n_max);
     const float gr = G[i] / (kCacheLossScale * (float)max(n, 1));
     G[i] = 0.0f;
     if (n == 0 || !isfinite(gr)) return;

@@ -251,8 +251,9 @@ __global__ void k_accumulate(WaveArgs w, PathBuf P, double* film)
 }
 
 // Training rows of a radiance-cache wave: for every path with a snapshot, the
-// cache's inputs at the vertex and the radiance its suffix gathered (final path
-// radiance, as k_accumulate adds it, minus the snapshot) over its throughput there.
+// cache's inputs at the vertex and the radiance its continuation gathered (final
+// path radiance, as k_accumulate adds it, minus the radiance up to the vertex's
+// NEE) over its throughput there; 0 when the path ended at the vertex.
 __global__ void k_cache_targets(WaveArgs w, PathBuf P, CacheRecord* rows, uint32_t* count)
 {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -260,11 +261,12 @@ __global__ void k_cache_targets(WaveArgs w, PathBuf P, CacheRecord* rows, uint32
     const float4 r = P.rad[p], a = P.pend0[p], b = P.pend1[p];
     const F3 fin = clean((F3{r.x, r.y, r.z} + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z});
     const CacheSnap& sn = w.cache_s[p];
+    const bool ended = w.cache_flag[p] == 2;
     CacheRecord q;
     for (int f = 0; f < kCacheIn; f++) q.in[f] = sn.in[f];
     const float fc[3] = {fin.x, fin.y, fin.z};
     for (int c = 0; c < 3; c++) {
-        const float v = sn.thr[c] > 1e-20f ? (fc[c] - sn.rad[c]) / sn.thr[c] : 0.0f;
+        const float v = (!ended && sn.thr[c] > 1e-20f) ? (fc[c] - sn.rad[c]) / sn.thr[c] : 0.0f;
         q.v[c] = isfinite(v) ? v : 0.0f;
     }
     q.path = (uint32_t)p;
@@ -1945,16 +1947,19 @@ void cache_set(luz_gpu_cache* c, const float* w)
     CK(cudaDeviceSynchronize());
 }
 
-// One Adam step from the rows on the device (count: device row count, or NULL for n_max).
-void cache_step(luz_gpu_cache* c, const CacheRecord* rows, const uint32_t* count, int n_max, cudaStream_t st)
+// One Adam step on rows [offset, offset + n_max) of the device rows (count:
+// device row count, or NULL for exactly n_max rows).
+void cache_step(luz_gpu_cache* c, const CacheRecord* rows, const uint32_t* count, int offset, int n_max,
+                cudaStream_t st)
 {
     k_cache_grad<<<(unsigned)((n_max + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem, st>>>(
-        rows, count, n_max, c->Wf, c->Wb, c->G, c->loss);
+        rows, count, offset, n_max, c->Wf, c->Wb, c->G, c->loss);
     c->step++;
     const float b1 = 0.9f, b2 = 0.99f;
     k_cache_adam<<<(kCacheParams + 255) / 256, 256, 0, st>>>(c->W, c->G, c->m, c->v, c->prm.learning_rate, b1, b2, 1e-8f,
                                                              (float)std::pow((double)b1, (double)c->step),
-                                                             (float)std::pow((double)b2, (double)c->step), count, n_max);
+                                                             (float)std::pow((double)b2, (double)c->step), count, offset,
+                                                             n_max);
     cache_pack(c, st);
 }
 
@@ -1987,13 +1992,16 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
     const int64_t npix = (int64_t)p->width * p->height;
-    const int64_t pix_wave = std::min<int64_t>(npix, kWaveTarget);
-    s->ensure_paths(pix_wave);
+    // waves as the plain render makes them (samples inner), one cache update per wave
+    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, kWaveTarget / npix));
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
+    const int64_t n_wave = pix_wave * s_wave;
+    s->ensure_paths(n_wave);
     DeviceScratch D;
-    CacheRecord* q = D.get<CacheRecord>(pix_wave, st);
-    CacheRecord* rows = D.get<CacheRecord>(pix_wave, st);
-    CacheSnap* snaps = D.get<CacheSnap>(pix_wave, st);
-    uint8_t* tflag = D.get<uint8_t>(pix_wave, st);
+    CacheRecord* q = D.get<CacheRecord>(n_wave, st);
+    CacheRecord* rows = D.get<CacheRecord>(n_wave, st);
+    CacheSnap* snaps = D.get<CacheSnap>(n_wave, st);
+    uint8_t* tflag = D.get<uint8_t>(n_wave, st);
     uint32_t* counts = D.get<uint32_t>(2, st);
     double* film = D.get<double>(3 * npix, st);
     float* d_out = D.get<float>(3 * npix, st);
@@ -2020,19 +2028,25 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * occ;
     const int batch = c->prm.batch;
     int64_t launches = 0, waves = 0;
-    for (int sample = 0; sample < p->spp; sample++) {
+    // The first sample of every pixel is rendered plain, every path training the
+    // cache (kCacheWarmSteps steps over its rows); later waves use the cache.
+    constexpr int kCacheWarmSteps = 32;
+    for (int sb = 0; sb < p->spp;) {
+        const bool warm = sb == 0;
+        const int sc = warm ? 1 : std::min(s_wave, p->spp - sb);
         for (int64_t pb = 0; pb < npix; pb += pix_wave) {
             const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
             w.pix_begin = (int32_t)pb;
             w.pix_count = (int32_t)pc;
-            w.s_begin = sample;
-            w.s_count = 1;
-            w.n = pc;
+            w.s_begin = sb;
+            w.s_count = sc;
+            w.n = pc * sc;
             w.list_mode = 0;
             w.cache_wave = (uint32_t)waves;
+            w.cache_train_every = warm ? 1u : (uint32_t)c->prm.train_every;
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(tflag, 0, (std::size_t)pc, st));
+            CK(cudaMemsetAsync(tflag, 0, (std::size_t)w.n, st));
             CK(cudaMemsetAsync(c->loss, 0, sizeof(float), st));
             k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
             for (int b = 0; b <= w.max_bounces; b++) {
@@ -2041,14 +2055,21 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
                 s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
             }
             k_cache_infer<<<(unsigned)(2 * s->sms), 128, kCacheInferSmem, st>>>(q, counts, 0, c->Wf, nullptr, s->pb.rad);
-            k_cache_targets<<<(unsigned)((pc + 255) / 256), 256, 0, st>>>(w, s->pb, rows, counts + 1);
-            cache_step(c, rows, counts + 1, (int)std::min<int64_t>(batch, pc), st);
+            k_cache_targets<<<(unsigned)((w.n + 255) / 256), 256, 0, st>>>(w, s->pb, rows, counts + 1);
+            // about n / train_every rows: one step per batch of them (at most 16 per wave);
+            // the warm-up wave cycles kCacheWarmSteps steps over its rows
+            const int64_t expect = (w.n + w.cache_train_every - 1) / w.cache_train_every;
+            const int64_t chunks = std::max<int64_t>(1, (expect + batch - 1) / batch);
+            const int steps = warm ? kCacheWarmSteps : (int)std::min<int64_t>(16, chunks);
+            for (int i = 0; i < steps; i++)
+                cache_step(c, rows, counts + 1, (int)((i % chunks) * batch), (int)std::min<int64_t>(batch, w.n), st);
             k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, film);
             k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
             CK(cudaGetLastError());
-            launches += 3 * (w.max_bounces + 1) + 9;
+            launches += 3 * (w.max_bounces + 1) + 6 + 3 * steps;
             waves++;
         }
+        sb += sc;
     }
     k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(film, npix, (double)p->spp, d_out);
     CK(cudaEventRecord(s->ev1, st));
@@ -2168,7 +2189,7 @@ int luz_gpu_cache_gradient(luz_gpu_cache* c, const float* inputs, const float* t
             CK(cudaMemset(c->G, 0, sizeof(float) * kCacheParams));
             CK(cudaMemset(c->loss, 0, sizeof(float)));
             k_cache_grad<<<(unsigned)((n + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem>>>(
-                d, nullptr, (int)n, c->Wf, c->Wb, c->G, c->loss);
+                d, nullptr, 0, (int)n, c->Wf, c->Wb, c->G, c->loss);
             CK(cudaGetLastError());
             std::vector<float> g(kCacheParams);
             float l = 0.f;
@@ -2201,7 +2222,7 @@ int luz_gpu_cache_train(luz_gpu_cache* c, const float* inputs, const float* targ
         try {
             for (int i = 0; i < steps; i++) {
                 CK(cudaMemset(c->loss, 0, sizeof(float)));
-                cache_step(c, d, nullptr, (int)n, 0);
+                cache_step(c, d, nullptr, 0, (int)n, 0);
                 CK(cudaGetLastError());
                 float l = 0.f;
                 CK(cudaMemcpy(&l, c->loss, sizeof(float), cudaMemcpyDeviceToHost));

@@ -382,6 +382,15 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         const float4 a = P.pend0[p], b = P.pend1[p];
         rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
     }
+    if constexpr (MODE == 2) {   // a training snapshot taken at the previous vertex: radiance up to its NEE
+        if (w.cache_flag[p] == 2) {
+            CacheSnap& sn = w.cache_s[p];
+            sn.rad[0] = rad.x;
+            sn.rad[1] = rad.y;
+            sn.rad[2] = rad.z;
+            w.cache_flag[p] = 1;
+        }
+    }
     F3 pend0{0.f, 0.f, 0.f}, pend1{0.f, 0.f, 0.f};
     const float4 ro = P.ray_o[p], rd = P.ray_d[p];
     const TRay ray = make_ray_x(F3{ro.x, ro.y, ro.z}, F3{rd.x, rd.y, rd.z}, __float_as_int(ro.w), __float_as_int(rd.w));
@@ -472,12 +481,17 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
             out.cont = true;
             out.next_o = h.p;
             out.next_d = sr.dir;
-            flags = PF_PREV_SPECULAR;
+            flags = PF_PREV_SPECULAR | (flags & PF_CACHE_DONE);
             P.thr[p] = make_float4(thr.x, thr.y, thr.z, 0.0f);
             goto done;
         }
         rad = rad + thr * emitted;
-        if constexpr (MODE == 2) {   // the cache answers for everything past this vertex, or it trains
+        // Radiance cache: at the path's first surface vertex at or after the prefix
+        // bounce, the vertex's own light (emission here, NEE below) stays explicit and
+        // the cache answers for the continuation; one path in cache_train_every runs
+        // on and records what the continuation gathered.
+        bool cache_query = false;
+        if constexpr (MODE == 2) {
             if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE)) {
                 const uint64_t key = ((uint64_t)pix << 24) ^ (uint64_t)P.sample[p] ^ ((uint64_t)w.cache_wave << 48);
                 if (splitmix64(key) % w.cache_train_every == 0) {
@@ -486,21 +500,10 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                     sn.thr[0] = thr.x;
                     sn.thr[1] = thr.y;
                     sn.thr[2] = thr.z;
-                    sn.rad[0] = rad.x;
-                    sn.rad[1] = rad.y;
-                    sn.rad[2] = rad.z;
-                    w.cache_flag[p] = 1;
+                    w.cache_flag[p] = 2;   // radiance up to this vertex's NEE: taken at the next vertex
                     flags |= PF_CACHE_DONE;
                 } else {
-                    CacheRecord q;
-                    cache_inputs(w, h, m, ray.d, q.in);
-                    q.v[0] = thr.x;
-                    q.v[1] = thr.y;
-                    q.v[2] = thr.z;
-                    q.path = p;
-                    q.pad[0] = q.pad[1] = 0.0f;
-                    w.cache_q[atomicAdd(w.cache_count, 1u)] = q;
-                    goto done;
+                    cache_query = true;
                 }
             }
         }
@@ -565,6 +568,19 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                 }
             }
         }
+        if constexpr (MODE == 2) {
+            if (cache_query) {
+                CacheRecord q;
+                cache_inputs(w, h, m, ray.d, q.in);
+                q.v[0] = thr.x;
+                q.v[1] = thr.y;
+                q.v[2] = thr.z;
+                q.path = p;
+                q.pad[0] = q.pad[1] = 0.0f;
+                w.cache_q[atomicAdd(w.cache_count, 1u)] = q;
+                goto done;
+            }
+        }
         const F3 dir = scatter_generate(sr, k);
         if (!leaves_opaque(m, h, dir)) goto done;
         // For a BSDF record this is scatteringPDF of the sampled direction with the same
@@ -578,7 +594,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         out.next_d = dir;
         const bool svil = ((S.k.sky == 3 || S.k.sky == 2) && S.k.env.lighting)
                        || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
-        flags = svil ? PF_PREV_SVIL : 0u;
+        flags = (svil ? PF_PREV_SVIL : 0u) | (flags & PF_CACHE_DONE);
         P.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
     }
 done:

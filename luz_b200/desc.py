@@ -168,7 +168,7 @@ class CacheParams(C.Structure):
                 ("train_every", C.c_int32), ("reserved", C.c_int32)]
 
 
-def cache_params(seed=1, batch=65536, learning_rate=1e-2, prefix=1, train_every=16) -> CacheParams:
+def cache_params(seed=1, batch=16384, learning_rate=1e-2, prefix=1, train_every=16) -> CacheParams:
     return CacheParams(seed, batch, learning_rate, prefix, train_every, 0)
 
 

@@ -131,7 +131,10 @@ def _pinhole(position, look_at, vfov_deg, aspect):
                   sensor_width_m=sh * aspect, sensor_height_m=sh, f_number=8.0, focus_distance_m=10.0, pinhole=True)
 
 
-def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int = 8) -> Workload:
+def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int = 8, closed: bool = False) -> Workload:
+    """The Cornell box; closed = True closes its open side with a white wall and puts the
+    camera inside, so that paths stay in the room until Russian roulette or the depth limit
+    ends them."""
     s = Scene()
     white = s.lambertian((0.73, 0.73, 0.73))
     red = s.lambertian((0.65, 0.05, 0.05))
@@ -146,9 +149,13 @@ def cornell(width: int = 300, height: int = 300, spp: int = 50, max_bounces: int
     cube, _ = s.mesh(box_mesh(), white, add_object=False)
     s.mesh_instance(cube, (265.0, 0.0, 295.0), (0.0, 15.0, 0.0), (165.0, 330.0, 165.0), white)
     s.mesh_instance(cube, (130.0, 0.0, 65.0), (0.0, -18.0, 0.0), (165.0, 165.0, 165.0), white)
-    s.camera = _pinhole((278.0, 278.0, -800.0), (278.0, 278.0, 0.0), 40.0, width / height)
+    if closed:   # a front wall closes the box; the camera moves inside it
+        s.rectangle((277.5, 277.5, 0.0), (0, 0, 1), 555.0, 555.0, white)
+        s.camera = _pinhole((278.0, 278.0, 20.0), (278.0, 278.0, 555.0), 75.0, width / height)
+    else:
+        s.camera = _pinhole((278.0, 278.0, -800.0), (278.0, 278.0, 0.0), 40.0, width / height)
     s.background = (0.0, 0.0, 0.0)
-    return Workload("cornell", s, width, height, spp, max_bounces)
+    return Workload("cornell_closed" if closed else "cornell", s, width, height, spp, max_bounces)
 
 
 def spheres_linear_sky(width: int = 64, height: int = 36, spp: int = 4, max_bounces: int = 12,

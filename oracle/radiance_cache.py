@@ -15,7 +15,7 @@ N_IN, N_ENC, HIDDEN, N_OUT = 10, 128, 64, 16
 LAYERS = [(128, 64), (64, 64), (64, 64), (64, 64), (64, 16)]
 OFFSETS = [0, 8192, 12288, 16384, 20480]
 N_PARAMS = 21504
-LOSS_SCALE, GRAD_CLAMP, EPS_REL = 128.0, 100.0, 0.01
+LOSS_SCALE, GRAD_CLAMP, EPS_REL = 8.0, 2000.0, 0.01
 M64 = (1 << 64) - 1
 
 
