@@ -90,6 +90,9 @@ typedef struct LuzMaterialDesc {
     double  subsurface_color[3];
     double  glossy_color[3];      /* DiffuseGlossy glossy colour (color = diffuse colour) */
     double  glossy_weight;        /* DiffuseGlossy glossy weight; roughness = glossy roughness */
+    int32_t has_roughness_texture;  /* Metal only, an extension (the reference's Metal roughness */
+    int32_t roughness_texture;      /* is a scalar): roughness = red channel of this texture,   */
+                                    /* bilinear at the hit's uv, clamped to [0, 1]              */
 } LuzMaterialDesc;
 
 /* Bilinear albedo texture (src/core/Texture.cpp:142-172): width*height RGB, row 0 = top. */

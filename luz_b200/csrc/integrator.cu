@@ -274,6 +274,17 @@ __global__ void k_cache_targets(WaveArgs w, PathBuf P, CacheRecord* rows, uint32
     rows[atomicAdd(count, 1u)] = q;
 }
 
+// Roughness-gradient records still open after a replay wave (their path ended at
+// the vertex): the final light and environment samples, no continuation.
+__global__ void k_adjoint_rough_finish(DScene S, WaveArgs w, PathBuf P)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w.n || !w.adj_rough[p].active) return;
+    const float4 a = P.pend0[p], b = P.pend1[p];
+    adjoint_rough_resolve(S, w, P, (uint32_t)p, F3{a.x, a.y, a.z}, F3{b.x, b.y, b.z}, F3{0.f, 0.f, 0.f}, false,
+                          w.adj_rough[p]);
+}
+
 __global__ void k_resolve(const double* film, int64_t npix, double spp, float* out)
 {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -533,7 +544,8 @@ __global__ void __launch_bounds__(128) k_photons(DScene S, uint32_t seed, int ma
         const THit th = closest_hit<F>(S, ray, kTMin, kInf, vs, st);
         if (th.obj < 0) break;
         const Hit h = make_hit(S, ray, th);
-        const GMaterial m = S.materials[h.material];
+        GMaterial m = S.materials[h.material];
+        resolve_material(S, m, h);
         if (m.type == MT_EMISSIVE) break;
         if (caustic && receives_caustics(m)) {
             const double r = G.radius_su;
@@ -798,15 +810,18 @@ struct StageTimer {
     }
 };
 
-void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_t& launches, StageTimer& T)
+// shade: the shade instantiation to run (NULL: the scene's own).
+void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_t& launches, StageTimer& T,
+                    ShadeKernel shade = nullptr)
 {
     const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
+    if (!shade) shade = s->shade;
     for (int b = 0; b <= w.max_bounces; b++) {
         T.mark(st, 0, true);
         s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
-        s->shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
+        shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
         s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
@@ -1330,9 +1345,18 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
         throw Status(LUZ_E_UNSUPPORTED, "The adjoint pass does not differentiate caustic photon maps.");
     const ScenePack& PK = *s->pack;
     if (texture < 0 || (std::size_t)texture >= PK.textures.size()) throw Status(LUZ_E_INVALID, "Texture index out of range.");
-    for (const GMaterial& m : PK.materials)
-        if (m.texture == texture && m.type != MT_LAMBERTIAN)
-            throw Status(LUZ_E_UNSUPPORTED, "Texture gradients are defined for Lambertian albedo textures only.");
+    bool albedo = false, rough = false;
+    for (const GMaterial& m : PK.materials) {
+        if (m.texture == texture) {
+            if (m.type != MT_LAMBERTIAN)
+                throw Status(LUZ_E_UNSUPPORTED,
+                             "Texture gradients are defined for Lambertian albedo and Metal roughness textures only.");
+            albedo = true;
+        }
+        if (m.rtexture == texture) rough = true;
+    }
+    if (albedo && rough)
+        throw Status(LUZ_E_UNSUPPORTED, "A texture differentiated as both albedo and roughness is not supported.");
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
     const GTexture& T = PK.textures[(std::size_t)texture];
@@ -1343,12 +1367,14 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     CK(cudaMemcpyAsync(d_adj, adj_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyHostToDevice, st));
     WaveArgs w = base_args(s, p);
     w.grad_texture = texture;
+    w.grad_kind = rough ? 1 : 0;
     w.adj_rgb = d_adj;
     w.grad = d_grad;
     w.inv_spp = 1.0 / (double)p->spp;
     const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
     const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
     s->ensure_paths(pix_wave * s_wave);
+    w.adj_rough = rough ? D.get<AdjRough>(pix_wave * s_wave, st) : nullptr;
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(s->ev0, st));
     StageTimer T0;
@@ -1366,11 +1392,15 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
             for (int pass = 0; pass < 2; pass++) {   // 0: radiance of every path; 1: replay with gradients
                 w.adjoint = pass;
                 CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+                if (pass == 1 && rough) CK(cudaMemsetAsync(w.adj_rough, 0, sizeof(AdjRough) * (std::size_t)w.n, st));
                 k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-                launch_bounces(s, w, st, launches, T0);
+                launch_bounces(s, w, st, launches, T0, k_shade<3>);
                 launches++;
                 if (pass == 0) {
                     k_path_color<<<grid, kBlock, 0, st>>>(w, s->pb);
+                    launches++;
+                } else if (rough) {
+                    k_adjoint_rough_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
                     launches++;
                 }
             }

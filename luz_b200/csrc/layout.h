@@ -146,7 +146,7 @@ struct alignas(16) GMaterial {
     int32_t type;
     int32_t texture;
     int32_t flags;
-    int32_t pad;
+    int32_t rtexture;         // Metal: roughness texture (red channel), -1 = the scalar roughness
     float color[3];
     float roughness;
     float alpha;              // BSDF::roughnessToAlpha(roughness)

@@ -158,6 +158,13 @@ GMaterial pack_material(const LuzMaterialDesc& m, int texture_count)
     g.type = m.type;
     g.texture = m.texture;
     if (m.texture >= texture_count || m.texture < -1) invalid("Material texture index out of range.");
+    g.rtexture = -1;
+    if (m.has_roughness_texture) {   // an extension: the reference's Metal roughness is a scalar
+        if (m.type != LUZ_MAT_METAL) invalid("Roughness textures are defined for Metal materials only.");
+        if (m.roughness_texture < 0 || m.roughness_texture >= texture_count)
+            invalid("Roughness texture index out of range.");
+        g.rtexture = m.roughness_texture;
+    }
     for (int a = 0; a < 3; a++) {
         g.color[a] = (float)m.color[a];
         g.eta[a] = (float)m.eta[a];

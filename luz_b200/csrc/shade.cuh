@@ -186,6 +186,18 @@ __device__ __forceinline__ F3 color_at(const DScene& S, const GMaterial& m, cons
     return c;
 }
 
+// Metal roughness from a texture (red channel, bilinear, clamped to [0, 1]) when
+// the material has one: the per-hit copy gets roughness and alpha =
+// roughnessToAlpha(roughness) (BSDF.cpp:53-57).
+__device__ __forceinline__ void resolve_material(const DScene& S, GMaterial& m, const Hit& h)
+{
+    if (m.rtexture >= 0) {
+        const float r = texture_sample(S, m.rtexture, h.u, h.v).x;
+        m.roughness = r;
+        m.alpha = fmaxf(1e-4f, r * r);
+    }
+}
+
 // ----------------------------------------------------------------------------- BSDF helpers
 
 __device__ __forceinline__ F3 schlick(F3 f0, float cosT)

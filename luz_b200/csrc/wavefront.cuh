@@ -50,6 +50,16 @@ struct CacheSnap {
     float rad[3];
 };
 
+// Path-replay state of a Metal vertex whose roughness texture is differentiated
+// (luz_gpu_adjoint_backward on a roughness texture): d ln f / d roughness per
+// channel for the light-sample direction, the environment-sample direction and
+// the continuation, and where the texture was read.
+struct AdjRough {
+    float dn0[3], dn1[3], dc[3];
+    float u, v;
+    uint32_t active;
+};
+
 struct WaveArgs {
     int32_t width, height;
     uint32_t seed, stream;
@@ -67,6 +77,8 @@ struct WaveArgs {
     int32_t nfor;                 // store primary features in PathBuf.feat
     int32_t adjoint;              // replay pass of luz_gpu_adjoint_backward
     int32_t grad_texture;         // texture whose texel gradient is accumulated
+    int32_t grad_kind;            // 0: Lambertian albedo texture; 1: Metal roughness texture (red channel)
+    AdjRough* adj_rough;          // grad_kind 1: one record per path
     const float* adj_rgb;         // dLoss/dPixel, W*H*3
     double* grad;                 // dLoss/dTexel, texture W*H*3
     double inv_spp;
@@ -287,6 +299,62 @@ __device__ __noinline__ void store_hit_features(const DScene& S, const PathBuf& 
     P.feat[3 * p + 2] = make_float4((float)((double)m.type / (double)MT_PRINCIPLED), 0.0f, 0.0f, 0.0f);
 }
 
+// Adds g * (bilinear weight) to channel ch of the four texels a lookup at (u, v)
+// of the differentiated texture reads (texture_sample's footprint).
+__device__ __forceinline__ void scatter_texel_grad(const DScene& S, const WaveArgs& w, float u0, float v0, int ch, double g)
+{
+    if (g == 0.0 || !isfinite(g)) return;
+    const GTexture T = S.textures[w.grad_texture];
+    const float u = wrap01f(u0), v = wrap01f(v0);
+    const float x = u * (float)(T.width - 1);
+    const float y = (1.0f - v) * (float)(T.height - 1);
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    const int x1 = min(x0 + 1, T.width - 1), y1 = min(y0 + 1, T.height - 1);
+    const float tx = x - (float)x0, ty = y - (float)y0;
+    const double wt[4] = {(double)((1.0f - tx) * (1.0f - ty)), (double)(tx * (1.0f - ty)), (double)((1.0f - tx) * ty),
+                          (double)(tx * ty)};
+    const int idx[4] = {y0 * T.width + x0, y0 * T.width + x1, y1 * T.width + x0, y1 * T.width + x1};
+    for (int q = 0; q < 4; q++)
+        if (wt[q] != 0.0) atomicAdd(&w.grad[3 * (int64_t)idx[q] + ch], g * wt[q]);
+}
+
+// d ln f / d roughness of a rough Metal lobe toward dir, per channel, by a central
+// difference of the BSDF in roughness (alpha = roughness^2 >= 1e-4); 0 where f is 0.
+__device__ __noinline__ F3 dlnf_rough(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+{
+    const F3 f = bsdf_eval(S, m, h, ray_d, dir);
+    const float r = m.roughness, r1 = fminf(1.0f, r + 1e-3f), r0 = fmaxf(0.0f, r - 1e-3f);
+    GMaterial a = m, b = m;
+    a.alpha = fmaxf(1e-4f, r1 * r1);
+    b.alpha = fmaxf(1e-4f, r0 * r0);
+    const F3 fa = bsdf_eval(S, a, h, ray_d, dir), fb = bsdf_eval(S, b, h, ray_d, dir);
+    const float inv = 1.0f / (r1 - r0);
+    auto q = [&](float x, float y, float z) { return (z > 0.0f && isfinite(z)) ? ((x - y) * inv) / z : 0.0f; };
+    return F3{q(fa.x, fb.x, f.x), q(fa.y, fb.y, f.y), q(fa.z, fb.z, f.z)};
+}
+
+// Roughness gradient of the vertex recorded in ar, once its light (a) and
+// environment (b) samples are known after the shadow test: each contribution
+// times its d ln f, the continuation (final path radiance L minus the radiance
+// gathered up to this vertex's samples, rad) times d ln f of its direction
+// (sampling densities held fixed: each sample's f / pdf is differentiated in f).
+__device__ __noinline__ void adjoint_rough_resolve(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
+                                                   F3 a, F3 b, F3 rad, bool continued, AdjRough& ar)
+{
+    const float4 L = P.color[p];
+    const uint32_t pix = P.pixel[p];
+    const float la[3] = {a.x, a.y, a.z}, lb[3] = {b.x, b.y, b.z}, lr[3] = {rad.x, rad.y, rad.z};
+    const float Lc[3] = {L.x, L.y, L.z};
+    double g = 0.0;
+    for (int ch = 0; ch < 3; ch++) {
+        const double cont = continued ? (double)Lc[ch] - (double)lr[ch] : 0.0;
+        const double term = (double)la[ch] * ar.dn0[ch] + (double)lb[ch] * ar.dn1[ch] + cont * ar.dc[ch];
+        if (isfinite(term)) g += (double)w.adj_rgb[3 * (int64_t)pix + ch] * term;
+    }
+    scatter_texel_grad(S, w, ar.u, ar.v, 0, g * w.inv_spp);
+    ar.active = 0;
+}
+
 // Path replay gradient of a Lambertian albedo texture (luz_gpu_adjoint_backward).
 // Everything the path gathers from this vertex on (its NEE and every later
 // vertex) carries the vertex's albedo = colour * clamp01(bilinear(texels)) as
@@ -364,7 +432,8 @@ __device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, co
     in[9] = diffuse ? 1.0f : m.roughness;
 }
 
-// MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render.
+// MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render;
+// 3: adjoint (texture-gradient) passes.
 template <int MODE>
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
@@ -381,6 +450,8 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     {
         const float4 a = P.pend0[p], b = P.pend1[p];
         rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
+        if (MODE == 3 && w.adjoint && w.grad_kind == 1 && w.adj_rough[p].active)
+            adjoint_rough_resolve(S, w, P, p, F3{a.x, a.y, a.z}, F3{b.x, b.y, b.z}, rad, true, w.adj_rough[p]);
     }
     if constexpr (MODE == 2) {   // a training snapshot taken at the previous vertex: radiance up to its NEE
         if (w.cache_flag[p] == 2) {
@@ -444,7 +515,8 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     {
         THit th{h4.x, obj, P.hit_prim[p], h4.y, h4.z};
         Hit h = make_hit(S, ray, th);
-        const GMaterial m = S.materials[h.material];
+        GMaterial m = S.materials[h.material];
+        resolve_material(S, m, h);
         if (bounce == 0 && w.nfor) store_hit_features(S, P, p, h, m);
         if (bounce == 0 && S.k.sky == 2) {   // compositePrimaryAtmosphereSegment (ColorHelper.cpp:645-659)
             double ao[3], ad[3];
@@ -507,7 +579,17 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                 }
             }
         }
-        if (w.adjoint && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture) adjoint_texture(S, w, P, p, h, rad);
+        if (MODE == 3 && w.adjoint && w.grad_kind == 0 && m.type == MT_LAMBERTIAN && m.texture == w.grad_texture)
+            adjoint_texture(S, w, P, p, h, rad);
+        const bool rough_grad =
+            MODE == 3 && w.adjoint && w.grad_kind == 1 && m.type == MT_METAL && m.rtexture == w.grad_texture;
+        if (rough_grad) {
+            AdjRough& ar = w.adj_rough[p];
+            for (int c = 0; c < 3; c++) ar.dn0[c] = ar.dn1[c] = ar.dc[c] = 0.0f;
+            ar.u = h.u;
+            ar.v = h.v;
+            ar.active = 1;
+        }
         if (terminated(thr * att)) goto done;
         if constexpr (MODE == 1)
             if (S.cm.count) rad = rad + clamp_ray_color(thr * caustic_estimate(S, h, sr, m, ray.d));
@@ -524,6 +606,12 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                     const F3 c = (bc * ls.emitted) * (mis / (ls.pdf * prob));
                     pend0 = clamp_ray_color(thr * c);
                     out.sh[0] = true;
+                    if (rough_grad) {
+                        const F3 dl = dlnf_rough(S, m, h, ray.d, ls.dir);
+                        w.adj_rough[p].dn0[0] = dl.x;
+                        w.adj_rough[p].dn0[1] = dl.y;
+                        w.adj_rough[p].dn0[2] = dl.z;
+                    }
                     out.sh_o[0] = h.p;
                     out.sh_d[0] = ls.dir;
                     out.sh_t[0] = ls.tmax - kTMin;
@@ -562,6 +650,12 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                     if (cbg) c = clamp_bg_miss(S, c);
                     pend1 = clamp_ray_color(thr * c);
                     out.sh[1] = true;
+                    if (rough_grad) {
+                        const F3 dl = dlnf_rough(S, m, h, ray.d, ls.dir);
+                        w.adj_rough[p].dn1[0] = dl.x;
+                        w.adj_rough[p].dn1[1] = dl.y;
+                        w.adj_rough[p].dn1[2] = dl.z;
+                    }
                     out.sh_o[1] = h.p;
                     out.sh_d[1] = ls.dir;
                     out.sh_t[1] = kInf;
@@ -592,6 +686,19 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         out.cont = true;
         out.next_o = h.p;
         out.next_d = dir;
+        if (rough_grad) {
+            // A GGX sample whose half vector faces away or whose reflection falls below the
+            // surface is replaced by the mirror direction (ggx_reflection_sample, as the
+            // reference does): that direction is not drawn from the density the throughput
+            // divides by, so the sample carries no roughness derivative.
+            const F3 view = safe_normalize(ray.d * -1.0f, h.n);
+            const F3 hv = sample_ggx_half(h.n, m.alpha, sample2d(k, DIM_BSDF_DIRECTION));
+            const bool fallback = dot(view, hv) <= 0.0f || dot(reflect(ray.d, hv), h.n) <= 0.0f;
+            const F3 dl = fallback ? F3{0.f, 0.f, 0.f} : dlnf_rough(S, m, h, ray.d, dir);
+            w.adj_rough[p].dc[0] = dl.x;
+            w.adj_rough[p].dc[1] = dl.y;
+            w.adj_rough[p].dc[2] = dl.z;
+        }
         const bool svil = ((S.k.sky == 3 || S.k.sky == 2) && S.k.env.lighting)
                        || (S.k.has_constant_background_light && sr.pdf != PDF_BSDF);
         flags = (svil ? PF_PREV_SVIL : 0u) | (flags & PF_CACHE_DONE);

@@ -40,6 +40,7 @@ class MaterialDesc(C.Structure):
         ("clearcoat_roughness", C.c_double), ("sheen", C.c_double), ("subsurface", C.c_double),
         ("subsurface_radius", D3), ("subsurface_scale", C.c_double), ("subsurface_color", D3),
         ("glossy_color", D3), ("glossy_weight", C.c_double),
+        ("has_roughness_texture", C.c_int32), ("roughness_texture", C.c_int32),
     ]
 
 
@@ -259,10 +260,14 @@ class Scene:
     def lambertian(self, color, texture=-1):
         return self._mat(type=MAT_LAMBERTIAN, color=color, texture=texture)
 
-    def metal(self, color=(0.6, 0.6, 0.6), roughness=0.0, eta=None, k=None):
+    def metal(self, color=(0.6, 0.6, 0.6), roughness=0.0, eta=None, k=None, roughness_texture=None):
+        """roughness_texture: index of a texture whose red channel gives the roughness per hit
+        (an extension: the reference's Metal roughness is a scalar)."""
+        rt = {} if roughness_texture is None else dict(has_roughness_texture=1, roughness_texture=roughness_texture)
         if eta is not None:
-            return self._mat(type=MAT_METAL, color=(1.0, 1.0, 1.0), roughness=roughness, conductor=1, eta=eta, k=k)
-        return self._mat(type=MAT_METAL, color=color, roughness=roughness)
+            return self._mat(type=MAT_METAL, color=(1.0, 1.0, 1.0), roughness=roughness, conductor=1, eta=eta, k=k,
+                             **rt)
+        return self._mat(type=MAT_METAL, color=color, roughness=roughness, **rt)
 
     def glossy(self, color=(1.0, 1.0, 1.0), roughness=0.0):
         return self._mat(type=MAT_GLOSSY, color=color, roughness=roughness)

@@ -278,6 +278,23 @@ def cornell_textured(width: int = 256, height: int = 256, spp: int = 64, max_bou
     return Workload("cornell_textured", s, width, height, spp, max_bounces)
 
 
+def cornell_rough_panel(width: int = 64, height: int = 64, spp: int = 64, max_bounces: int = 8,
+                        roughness: np.ndarray = None, seed: int = 41) -> Workload:
+    """The textured Cornell box (texture 0: back-wall albedo) with a GGX Metal panel whose
+    roughness comes from a 64 x 64 map (texture 1, red channel; U[0.08, 0.25] unless given),
+    tilted to reflect the ceiling light toward the camera: the roughness-gradient workload
+    (Metal roughness textures are an extension; the reference's Metal roughness is a scalar)."""
+    w = cornell_textured(width, height, spp, max_bounces)
+    s = w.scene
+    if roughness is None:
+        roughness = np.repeat(np.random.default_rng(seed).uniform(0.08, 0.25, (64, 64, 1)), 3, axis=2)
+    t = s.texture(roughness)
+    panel = s.metal((0.95, 0.9, 0.85), roughness=0.15, roughness_texture=t)
+    n = np.array([-0.13, 0.49, -0.86])   # bisects the directions to the camera and to the light
+    s.rectangle((330.0, 300.0, 420.0), tuple(n / np.linalg.norm(n)), 220.0, 260.0, panel)
+    return Workload("cornell_rough_panel", s, width, height, spp, max_bounces)
+
+
 def sky_environment(width: int = 1024, height: int = 512, seed: int = 7, sun_peak: float = 5.0e4,
                     sun_diameter_deg: float = 0.5):
     """Equirect RGB sky: zenith-to-horizon gradient, dark ground, seeded sun lobe.

@@ -65,3 +65,81 @@ def test_gradient_support_and_errors(adjoint_run):
     with pytest.raises(native.LuzError) as e:
         g.set_texture(1, tex)
     assert e.value.code == -1
+
+
+# ---------------------------------------------------------------- Metal roughness textures
+
+def test_roughness_texture_validation():
+    from luz_b200.desc import Scene
+    s = Scene()
+    t = s.texture(np.full((4, 4, 3), 0.3))
+    s._mat(type=1, has_roughness_texture=1, roughness_texture=t)   # Lambertian
+    s.sphere((0, 0, 0), 1, 0)
+    with pytest.raises(native.LuzError) as e:
+        native.Pack(s.build())
+    assert "Roughness textures are defined for Metal materials only." in str(e.value)
+    s2 = Scene()
+    s2.sphere((0, 0, 0), 1, s2.metal(roughness_texture=3))
+    with pytest.raises(native.LuzError) as e:
+        native.Pack(s2.build())
+    assert "Roughness texture index out of range." in str(e.value)
+
+
+@pytest.mark.gpu
+def test_constant_roughness_texture_equals_scalar_roughness():
+    from luz_b200 import scenes
+    w = scenes.cornell_rough_panel(48, 48, 16, 6, roughness=np.full((64, 64, 3), 0.3))
+    g = native.GpuScene(w.scene.build())
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    a, _ = g.render(p)
+    panel = w.scene.materials[-1]
+    panel["has_roughness_texture"] = 0
+    g2 = native.GpuScene(w.scene.build())
+    b, _ = g2.render(p)
+    # the bilinear lookup of a constant map returns 0.3 to within an ulp: paths that meet the
+    # panel shift by rounding and decorrelate, the others are unchanged
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-3)
+    assert (rel.max(axis=-1) <= 1e-3).mean() >= 0.5
+    assert abs(a.mean() - b.mean()) <= 0.02 * b.mean()
+
+
+@pytest.mark.gpu
+def test_roughness_gradient_matches_finite_differences():
+    """d(sum adj * film) / d(roughness map): the red-channel texel gradients, summed over the
+    whole map and over its quadrants, against central differences of the GPU's own film
+    for a shift of those texels (common random numbers, h = 0.02), both averaged over two
+    seeds at 256 spp. The replay differentiates each sample's f in roughness with its
+    sampling density held fixed; GGX samples the reference replaces by the mirror direction
+    (half vector facing away, reflection below the surface) carry no derivative, a term the
+    narrow lobes of this panel (roughness 0.08-0.25, view 31 degrees off the normal) make
+    negligible. Measured: whole map within 1-12% per seed."""
+    from luz_b200 import scenes
+    w = scenes.cornell_rough_panel(64, 64, 256, 6)
+    g = native.GpuScene(w.scene.build())
+    rough = np.array(w.scene.textures[1])
+    adj = np.random.default_rng(5).uniform(0.5, 1.5, (w.height, w.width, 3)).astype(np.float32)
+    regions = [(slice(None), slice(None))] + [(slice(i, i + 32), slice(j, j + 32)) for i in (0, 32) for j in (0, 32)]
+    got = np.zeros(len(regions))
+    fd = np.zeros(len(regions))
+    h = 0.02
+    for seed in (1, 2):
+        p = native.params(w.width, w.height, 256, w.max_bounces, seed)
+        grad, _ = g.adjoint_backward(p, 1, adj, rough.shape)
+        assert np.all(grad[..., 1:] == 0.0) and np.isfinite(grad).all()
+
+        def loss(t):
+            img, _ = g.adjoint_forward(p, 1, t)
+            return float((adj.astype(np.float64) * img).sum())
+
+        for k, (ri, rj) in enumerate(regions):
+            tp, tm = rough.copy(), rough.copy()
+            tp[ri, rj, :] += h
+            tm[ri, rj, :] -= h
+            fd[k] += (loss(tp) - loss(tm)) / (2 * h) / 2
+            got[k] += float(grad[ri, rj, 0].sum()) / 2
+    g.set_texture(1, rough)
+    g.close()
+    assert abs(got[0] - fd[0]) <= 0.15 * abs(fd[0]), (got, fd)
+    for k in range(1, len(regions)):
+        if abs(fd[k]) > 0.1 * abs(fd[0]):
+            assert abs(got[k] - fd[k]) <= 0.3 * abs(fd[k]) + 0.02 * abs(fd[0]), (k, got, fd)
