@@ -374,9 +374,18 @@ int luz_gpu_adjoint_forward(luz_gpu_scene* scene, const LuzRenderParams* params,
  * `params` and dLoss/dpixel = adjoint_rgb (W*H*3, host), by path replay: the
  * paths are traced once for their radiance and once more to spread each
  * textured Lambertian vertex's share of it over the bilinear texel weights.
- * Russian roulette's survival probabilities are treated as constants. Only
- * Lambertian materials may use the texture (else LUZ_E_UNSUPPORTED).
- * stats->samples counts the paths replayed. */
+ * When the texture is a Metal roughness texture instead, the gradient is in the
+ * red channel (green and blue 0): at every rough vertex of such a Metal the
+ * light sample, the environment sample and the continuation each contribute
+ * their radiance times d ln f / d roughness of their direction (a central
+ * difference of the BSDF; each sample's density held fixed, so MIS weights and
+ * sampling are not differentiated), spread over the texel weights; GGX samples
+ * replaced by the mirror direction (half vector facing away or reflection below
+ * the surface) and mirror-like vertices (roughness <= 1e-4) carry none.
+ * Russian roulette's survival probabilities are treated as constants. A texture
+ * may be differentiated as the albedo of Lambertian materials or the roughness
+ * of Metal ones, not both, and no other material may use it as albedo (else
+ * LUZ_E_UNSUPPORTED). stats->samples counts the paths replayed. */
 int luz_gpu_adjoint_backward(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t texture,
                              const float* adjoint_rgb, double* grad_out, LuzRenderStats* stats);
 
