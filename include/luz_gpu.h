@@ -388,6 +388,16 @@ int luz_gpu_adjoint_forward(luz_gpu_scene* scene, const LuzRenderParams* params,
  * LUZ_E_UNSUPPORTED). stats->samples counts the paths replayed. */
 int luz_gpu_adjoint_backward(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t texture,
                              const float* adjoint_rgb, double* grad_out, LuzRenderStats* stats);
+/* dLoss/d(emitted radiance) of every light (grad_out: light_count x 3, the
+ * lights in Scene::updateLights order, LuzSceneInfo.light_count) for the film
+ * of `params` and dLoss/dpixel = adjoint_rgb, by one path replay: every emitter
+ * hit and every light sample adds adj * contribution / E per channel (both are
+ * linear in E). The light-selection distribution, which weights lights by
+ * area x luminance(E), is held fixed: with one light the result is exact up to
+ * rounding, with several it omits the change in which light is sampled. No
+ * counterpart in the reference (it has no gradients). */
+int luz_gpu_adjoint_emission(luz_gpu_scene* scene, const LuzRenderParams* params, const float* adjoint_rgb,
+                             double* grad_out, LuzRenderStats* stats);
 
 /* Adaptive sampling settings:/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
  * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),

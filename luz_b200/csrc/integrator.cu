@@ -285,6 +285,17 @@ __global__ void k_adjoint_rough_finish(DScene S, WaveArgs w, PathBuf P)
                           w.adj_rough[p]);
 }
 
+// Light samples still pending after a replay wave (their path ended at the
+// vertex): the final, shadow-tested contribution of each.
+__global__ void k_adjoint_emission_finish(DScene S, WaveArgs w, PathBuf P)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w.n || w.pend_light[p] < 0) return;
+    const float4 a = P.pend0[p];
+    adjoint_emission_add(S, w, P.pixel[p], w.pend_light[p], F3{a.x, a.y, a.z});
+    w.pend_light[p] = -1;
+}
+
 __global__ void k_resolve(const double* film, int64_t npix, double spp, float* out)
 {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1368,6 +1379,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     WaveArgs w = base_args(s, p);
     w.grad_texture = texture;
     w.grad_kind = rough ? 1 : 0;
+    w.grad_emission = 0;
     w.adj_rgb = d_adj;
     w.grad = d_grad;
     w.inv_spp = 1.0 / (double)p->spp;
@@ -1414,6 +1426,77 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
     CK(cudaMemcpy(grad_out, d_grad, sizeof(double) * 3 * (std::size_t)ntex, cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = (double)npix * p->spp;
+        stats->kernel_launches = launches;
+        stats->waves = waves;
+    }
+    return LUZ_OK;
+}
+
+// dLoss/d(emitted radiance) of every light by path replay: emitter hits and light
+// samples add adj * contribution / E (both linear in E); light selection held fixed.
+int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float* adj_rgb, double* grad_out,
+                        LuzRenderStats* stats)
+{
+    check_params(p);
+    if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in the adjoint pass.");
+    if (s->pack->consts.caustics.enabled)
+        throw Status(LUZ_E_UNSUPPORTED, "The adjoint pass does not differentiate caustic photon maps.");
+    const int64_t nl = s->pack->consts.light_count;
+    CK(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    const int64_t npix = (int64_t)p->width * p->height;
+    DeviceScratch D;
+    float* d_adj = D.get<float>(3 * npix, st);
+    double* d_grad = D.get<double>(3 * std::max<int64_t>(nl, 1), st);
+    CK(cudaMemcpyAsync(d_adj, adj_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyHostToDevice, st));
+    WaveArgs w = base_args(s, p);
+    w.grad_texture = -1;
+    w.grad_kind = 2;   // no texture hook
+    w.grad_emission = 1;
+    w.grad_light = d_grad;
+    w.adj_rgb = d_adj;
+    w.inv_spp = 1.0 / (double)p->spp;
+    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
+    s->ensure_paths(pix_wave * s_wave);
+    w.pend_light = D.get<int32_t>(pix_wave * s_wave, st);
+    CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(s->ev0, st));
+    StageTimer T0;
+    int64_t launches = 0, waves = 0;
+    for (int sb = 0; sb < p->spp; sb += s_wave) {
+        const int sc = std::min(s_wave, p->spp - sb);
+        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
+            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = sb;
+            w.s_count = sc;
+            w.n = pc * sc;
+            const unsigned grid = (unsigned)((w.n + kBlock - 1) / kBlock);
+            w.adjoint = 1;   // one replay: the contributions themselves carry the gradient
+            CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+            CK(cudaMemsetAsync(w.pend_light, 0xff, sizeof(int32_t) * (std::size_t)w.n, st));
+            k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
+            launch_bounces(s, w, st, launches, T0, k_shade<3>);
+            k_adjoint_emission_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
+            launches += 2;
+            waves++;
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    uint32_t err = 0;
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    if (nl > 0) CK(cudaMemcpy(grad_out, d_grad, sizeof(double) * 3 * (std::size_t)nl, cudaMemcpyDeviceToHost));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     if (stats) {
@@ -1804,6 +1887,16 @@ int luz_gpu_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t
     return guard([&] {
         if (!s || !adjoint_rgb || !grad_out) throw Status(LUZ_E_INVALID, "NULL argument.");
         return do_adjoint_backward(s, p, texture, adjoint_rgb, grad_out, stats);
+    });
+}
+
+int luz_gpu_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float* adjoint_rgb, double* grad_out,
+                             LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !adjoint_rgb || (!grad_out && s->pack->consts.light_count > 0))
+            throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_adjoint_emission(s, p, adjoint_rgb, grad_out, stats);
     });
 }
 

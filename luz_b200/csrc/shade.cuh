@@ -1024,6 +1024,7 @@ struct LightSample {
     float tmax;
     bool valid;
     float scale;   // IES relative intensity of a sphere light sample (1 otherwise)
+    int32_t light; // index of the sampled light (sample_light)
 };
 
 // IESProfile::candelaAt (IESProfile.cpp:231-299), FP64.
@@ -1434,6 +1435,7 @@ __device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key&
     ls.emitted = f3(L.emitted);
     if (L.ies >= 0) ls.emitted = ls.emitted * s.scale;
     if (maxc(ls.emitted) <= 0.0f) return false;
+    ls.light = idx;
     ls.valid = true;
     return true;
 }

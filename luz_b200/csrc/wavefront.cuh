@@ -79,6 +79,9 @@ struct WaveArgs {
     int32_t grad_texture;         // texture whose texel gradient is accumulated
     int32_t grad_kind;            // 0: Lambertian albedo texture; 1: Metal roughness texture (red channel)
     AdjRough* adj_rough;          // grad_kind 1: one record per path
+    int32_t grad_emission;        // replay: gradient with respect to each light's emitted radiance
+    double* grad_light;           // light_count * 3
+    int32_t* pend_light;          // per path: light of the pending light sample, -1 = none
     const float* adj_rgb;         // dLoss/dPixel, W*H*3
     double* grad;                 // dLoss/dTexel, texture W*H*3
     double inv_spp;
@@ -355,6 +358,21 @@ __device__ __noinline__ void adjoint_rough_resolve(const DScene& S, const WaveAr
     ar.active = 0;
 }
 
+// Emission gradient of light `light` for a contribution c of its emitted
+// radiance E reaching pixel pix: adj * c / E per channel (contributions are
+// linear in E; light selection weights are held fixed).
+__device__ __forceinline__ void adjoint_emission_add(const DScene& S, const WaveArgs& w, uint32_t pix, int32_t light, F3 c)
+{
+    if (light < 0 || light >= S.k.light_count) return;
+    const float* E = S.lights[light].emitted;
+    const float cc[3] = {c.x, c.y, c.z};
+    for (int ch = 0; ch < 3; ch++) {
+        if (!(E[ch] > 0.0f) || !isfinite(cc[ch]) || cc[ch] == 0.0f) continue;
+        const double g = (double)w.adj_rgb[3 * (int64_t)pix + ch] * (double)cc[ch] / (double)E[ch] * w.inv_spp;
+        atomicAdd(&w.grad_light[3 * (int64_t)light + ch], g);
+    }
+}
+
 // Path replay gradient of a Lambertian albedo texture (luz_gpu_adjoint_backward).
 // Everything the path gathers from this vertex on (its NEE and every later
 // vertex) carries the vertex's albedo = colour * clamp01(bilinear(texels)) as
@@ -452,6 +470,10 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
         if (MODE == 3 && w.adjoint && w.grad_kind == 1 && w.adj_rough[p].active)
             adjoint_rough_resolve(S, w, P, p, F3{a.x, a.y, a.z}, F3{b.x, b.y, b.z}, rad, true, w.adj_rough[p]);
+        if (MODE == 3 && w.adjoint && w.grad_emission && w.pend_light[p] >= 0) {   // the last vertex's light sample
+            adjoint_emission_add(S, w, P.pixel[p], w.pend_light[p], F3{a.x, a.y, a.z});
+            w.pend_light[p] = -1;
+        }
     }
     if constexpr (MODE == 2) {   // a training snapshot taken at the previous vertex: radiance up to its NEE
         if (w.cache_flag[p] == 2) {
@@ -533,6 +555,13 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
             const float plp = (!prev_spec && S.k.light_count > 0) ? lights_pdf(S, ray.o, ray.d) : 0.0f;
             const float wgt = prev_spec ? 1.0f : power_heuristic(prev_pdf, plp);
             rad = rad + clamp_ray_color((thr * emitted) * wgt);
+            if (MODE == 3 && w.adjoint && w.grad_emission && m.type == MT_EMISSIVE) {   // an emitter hit
+                for (int32_t li = 0; li < S.k.light_count; li++)
+                    if (S.lights[li].object == h.obj) {
+                        adjoint_emission_add(S, w, pix, li, clamp_ray_color((thr * emitted) * wgt));
+                        break;
+                    }
+            }
             goto done;
         }
         relocate_subsurface(S, m, h, sr, ray.d, k);
@@ -606,6 +635,7 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
                     const F3 c = (bc * ls.emitted) * (mis / (ls.pdf * prob));
                     pend0 = clamp_ray_color(thr * c);
                     out.sh[0] = true;
+                    if (MODE == 3 && w.adjoint && w.grad_emission) w.pend_light[p] = ls.light;
                     if (rough_grad) {
                         const F3 dl = dlnf_rough(S, m, h, ray.d, ls.dir);
                         w.adj_rough[p].dn0[0] = dl.x;

@@ -26,7 +26,7 @@ EXPORTED = [
     "luz_gpu_scene_set_texture", "luz_gpu_adjoint_forward", "luz_gpu_adjoint_backward",
     "luz_gpu_nfor_denoise", "luz_gpu_nfor_error", "luz_gpu_render_denoised",
     "luz_gpu_cache_create", "luz_gpu_cache_destroy", "luz_gpu_cache_weights", "luz_gpu_cache_predict",
-    "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached",
+    "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached", "luz_gpu_adjoint_emission",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -75,6 +75,7 @@ def lib():
     L.luz_gpu_scene_set_texture.argtypes = [vp, i32, vp]
     L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_adjoint_emission.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_cache_create.argtypes = [i32, C.POINTER(D.CacheParams), C.POINTER(vp)]
     L.luz_gpu_cache_destroy.argtypes = [vp]
     L.luz_gpu_cache_weights.argtypes = [vp, vp, vp]
@@ -241,6 +242,14 @@ class GpuScene:
         _check(lib().luz_gpu_adjoint_backward(self.h, C.byref(p), int(texture), adj.ctypes.data, grad.ctypes.data,
                                               C.byref(st)))
         return grad, st
+
+    def adjoint_emission(self, p: D.RenderParams, adjoint_rgb: np.ndarray):
+        """dLoss/d(emitted radiance) per light (light_count x 3) for dLoss/dpixel = adjoint_rgb."""
+        adj = np.ascontiguousarray(adjoint_rgb, np.float32)
+        grad = np.zeros((max(self.info().light_count, 1), 3), np.float64)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_adjoint_emission(self.h, C.byref(p), adj.ctypes.data, grad.ctypes.data, C.byref(st)))
+        return grad[:self.info().light_count], st
 
     def render_device(self, p: D.RenderParams, out_ptr: int, stream: int = 0) -> D.RenderStats:
         st = D.RenderStats()

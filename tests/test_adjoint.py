@@ -94,6 +94,7 @@ def test_constant_roughness_texture_equals_scalar_roughness():
     a, _ = g.render(p)
     panel = w.scene.materials[-1]
     panel["has_roughness_texture"] = 0
+    panel["roughness"] = 0.3
     g2 = native.GpuScene(w.scene.build())
     b, _ = g2.render(p)
     # the bilinear lookup of a constant map returns 0.3 to within an ulp: paths that meet the
@@ -143,3 +144,79 @@ def test_roughness_gradient_matches_finite_differences():
     for k in range(1, len(regions)):
         if abs(fd[k]) > 0.1 * abs(fd[0]):
             assert abs(got[k] - fd[k]) <= 0.3 * abs(fd[k]) + 0.02 * abs(fd[0]), (k, got, fd)
+
+
+# ---------------------------------------------------------------- light emission
+
+@pytest.mark.gpu
+def test_emission_gradient_single_light_is_exact():
+    """Cornell box (one area light): the film is linear in the light's emitted radiance and
+    the sampling does not depend on it, so the replay gradient equals the central
+    difference of the GPU film exactly up to rounding."""
+    from luz_b200 import scenes
+    w = scenes.cornell(48, 48, 16, 6)
+    adj = np.random.default_rng(9).uniform(0.5, 1.5, (48, 48, 3)).astype(np.float32)
+    p = native.params(48, 48, 16, 6, 3)
+    g = native.GpuScene(w.scene.build())
+    grad, st = g.adjoint_emission(p, adj)
+    assert grad.shape == (1, 3) and st.samples == 48 * 48 * 16
+    light = [m for m in w.scene.materials if m["type"] == 4][0]
+    base = np.array(light["color"], np.float64)
+    h = 0.5
+    for ch in range(3):
+        vals = []
+        for sgn in (1, -1):
+            c = base.copy()
+            c[ch] += sgn * h
+            light["color"] = tuple(c)
+            img, _ = native.GpuScene(w.scene.build()).render(p)
+            vals.append(float((adj.astype(np.float64) * img).sum()))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(grad[0, ch] - fd) <= 2e-3 * abs(fd), (ch, grad[0, ch], fd)
+    light["color"] = tuple(base)
+    g.close()
+
+
+@pytest.mark.gpu
+def test_emission_gradient_several_lights():
+    """tiny_mixed (a sphere light, a rectangle light and a directional light). Light selection
+    weighs lights by area x luminance(E); perturbations that leave every weight unchanged
+    keep the sampled paths identical, so central differences of the GPU film are exact
+    references: scaling all lights together (d loss / d scale = sum_i E_i . grad_i), and
+    changing one light's colour along a direction of zero luminance."""
+    from luz_b200 import scenes
+    w = scenes.tiny_mixed(24, 18, 64, 6)
+    adj = np.random.default_rng(9).uniform(0.5, 1.5, (18, 24, 3)).astype(np.float32)
+    p = native.params(24, 18, 64, 6, 3)
+    g = native.GpuScene(w.scene.build())
+    grad, _ = g.adjoint_emission(p, adj)
+    g.close()
+    assert grad.shape == (3, 3) and np.isfinite(grad).all() and (grad.sum(axis=1) > 0).all()
+    emitters = [m for m in w.scene.materials if m["type"] == 4]   # the lights, in addHittable order
+    base = [np.array(m["color"], np.float64) for m in emitters]
+
+    def loss():
+        img, _ = native.GpuScene(w.scene.build()).render(p)
+        return float((adj.astype(np.float64) * img).sum())
+
+    h = 0.05
+    vals = []
+    for sgn in (1, -1):
+        for m, b in zip(emitters, base):
+            m["color"] = tuple(b * (1.0 + sgn * h))
+        vals.append(loss())
+    fd = (vals[0] - vals[1]) / (2 * h)
+    got = float(sum((gr * b).sum() for gr, b in zip(grad, base)))
+    assert abs(got - fd) <= 2e-3 * abs(fd), (got, fd)
+    zero_lum = np.array([0.6740817658, -0.2722287168, 0.0])   # luminance (ACEScg) of this is 0
+    for li, m in enumerate(emitters):
+        for mm, b in zip(emitters, base):
+            mm["color"] = tuple(b)
+        vals = []
+        for sgn in (1, -1):
+            m["color"] = tuple(base[li] + sgn * h * zero_lum)
+            vals.append(loss())
+        m["color"] = tuple(base[li])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        got = float(grad[li] @ zero_lum)
+        assert abs(got - fd) <= 2e-3 * abs(fd) + 1e-4 * np.abs(grad).sum(), (li, got, fd)
