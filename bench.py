@@ -355,7 +355,9 @@ def run_batch(args):
 def run_adjoint(args):
     """--workload adjoint_c3: albedo-texture gradient of the textured Cornell box (256x256,
     64 spp, depth 8, 32x32 back-wall texture): Madjoint paths/s = W*H*spp paths replayed per
-    second of luz_gpu_adjoint_backward (both passes), device time from the call's CUDA events."""
+    second of luz_gpu_adjoint_backward (both passes), device time from the call's CUDA events;
+    beside it the same figure for the 64x64 roughness map of a Metal panel in the box and for
+    the light-emission gradient (luz_gpu_adjoint_emission)."""
     from luz_b200 import native, scenes
     w = scenes.cornell_textured(256, 256, 64, 8)
     g = native.GpuScene(w.scene.build())
@@ -375,15 +377,37 @@ def run_adjoint(args):
         bw.append(sb.render_ms)
     paths = float(w.width * w.height * w.spp)
     ms = float(np.mean(bw))
+    # the other C3 parameters on the same box with a roughness-mapped Metal panel: the 64x64
+    # roughness map (texture 1) and the light's emission, for the same kind of loss
+    wr = scenes.cornell_rough_panel(256, 256, 64, 8)
+    gr = native.GpuScene(wr.scene.build())
+    pr = native.params(wr.width, wr.height, wr.spp, wr.max_bounces, wr.seed)
+    rough = np.array(wr.scene.textures[1])
+    img, _ = gr.render(pr)
+    adj = (2.0 * (img - goal) / img.size).astype(np.float32)
+    for _ in range(max(1, args.warmup)):
+        gr.adjoint_backward(pr, 1, adj, rough.shape)
+        gr.adjoint_emission(pr, adj)
+    rw, ew = [], []
+    for _ in range(args.steps):
+        _, sr = gr.adjoint_backward(pr, 1, adj, rough.shape)
+        _, se = gr.adjoint_emission(pr, adj)
+        rw.append(sr.render_ms)
+        ew.append(se.render_ms)
     out = {"metric": "Madjoint paths/s", "value": paths / ms / 1e3, "unit": "Mpaths/s", "n_gpus": 1,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
            "config": {"workload": "adjoint_c3: textured Cornell 256x256 64spp depth8, 32x32 albedo texture",
                       "loss": "mean squared error to the 1024-spp checker render"},
-           "forward_ms": float(np.mean(fw)), "grad_norm": float(np.linalg.norm(grad))}
+           "forward_ms": float(np.mean(fw)), "grad_norm": float(np.linalg.norm(grad)),
+           "roughness_map": {"value": paths / float(np.mean(rw)) / 1e3, "unit": "Mpaths/s",
+                             "ms": float(np.mean(rw)), "what": "64x64 Metal roughness map, both passes"},
+           "emission": {"value": paths / float(np.mean(ew)) / 1e3, "unit": "Mpaths/s", "ms": float(np.mean(ew)),
+                        "what": "every light's emitted radiance, one replay"}}
     print(json.dumps(out), flush=True)
     g.close()
     tg.close()
+    gr.close()
 
 
 def run_nfor(args):

@@ -1453,7 +1453,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     const int64_t npix = (int64_t)p->width * p->height;
     DeviceScratch D;
     float* d_adj = D.get<float>(3 * npix, st);
-    double* d_grad = D.get<double>(3 * std::max<int64_t>(nl, 1), st);
+    double* d_grad = D.get<double>(kEmissionReplicas * 3 * std::max<int64_t>(nl, 1), st);
     CK(cudaMemcpyAsync(d_adj, adj_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyHostToDevice, st));
     WaveArgs w = base_args(s, p);
     w.grad_texture = -1;
@@ -1496,7 +1496,15 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     uint32_t err = 0;
     CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
-    if (nl > 0) CK(cudaMemcpy(grad_out, d_grad, sizeof(double) * 3 * (std::size_t)nl, cudaMemcpyDeviceToHost));
+    if (nl > 0) {
+        std::vector<double> rep((std::size_t)(kEmissionReplicas * 3 * nl));
+        CK(cudaMemcpy(rep.data(), d_grad, sizeof(double) * rep.size(), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < 3 * nl; i++) {
+            double acc = 0.0;
+            for (int r = 0; r < kEmissionReplicas; r++) acc += rep[(std::size_t)(r * 3 * nl + i)];
+            grad_out[i] = acc;
+        }
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     if (stats) {

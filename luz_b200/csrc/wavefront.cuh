@@ -80,7 +80,7 @@ struct WaveArgs {
     int32_t grad_kind;            // 0: Lambertian albedo texture; 1: Metal roughness texture (red channel)
     AdjRough* adj_rough;          // grad_kind 1: one record per path
     int32_t grad_emission;        // replay: gradient with respect to each light's emitted radiance
-    double* grad_light;           // light_count * 3
+    double* grad_light;           // kEmissionReplicas copies of light_count * 3 (summed on the host)
     int32_t* pend_light;          // per path: light of the pending light sample, -1 = none
     const float* adj_rgb;         // dLoss/dPixel, W*H*3
     double* grad;                 // dLoss/dTexel, texture W*H*3
@@ -361,15 +361,20 @@ __device__ __noinline__ void adjoint_rough_resolve(const DScene& S, const WaveAr
 // Emission gradient of light `light` for a contribution c of its emitted
 // radiance E reaching pixel pix: adj * c / E per channel (contributions are
 // linear in E; light selection weights are held fixed).
+// Warps add into one of kEmissionReplicas copies, so that a scene with one light
+// does not serialise every path on three addresses.
+constexpr int kEmissionReplicas = 256;
 __device__ __forceinline__ void adjoint_emission_add(const DScene& S, const WaveArgs& w, uint32_t pix, int32_t light, F3 c)
 {
     if (light < 0 || light >= S.k.light_count) return;
+    const int64_t rep = (int64_t)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) & (kEmissionReplicas - 1));
+    double* gl = w.grad_light + rep * 3 * (int64_t)S.k.light_count;
     const float* E = S.lights[light].emitted;
     const float cc[3] = {c.x, c.y, c.z};
     for (int ch = 0; ch < 3; ch++) {
         if (!(E[ch] > 0.0f) || !isfinite(cc[ch]) || cc[ch] == 0.0f) continue;
         const double g = (double)w.adj_rgb[3 * (int64_t)pix + ch] * (double)cc[ch] / (double)E[ch] * w.inv_spp;
-        atomicAdd(&w.grad_light[3 * (int64_t)light + ch], g);
+        atomicAdd(&gl[3 * (int64_t)light + ch], g);
     }
 }
 
