@@ -435,7 +435,10 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
 {
     float root_near;
     if (!mesh_box<FAST>(M.bmin, M.bmax, r, neg_o_inv(r), tmax, root_near)) return false;
-    // Same walk as mesh_closest without pruning (any accepted entry may hold an occluder).
+    // The walk of mesh_closest without pruning: any accepted entry may hold an
+    // occluder and the first one found ends the walk, so the entries of a node are
+    // taken in a fixed order (left side, then right) instead of nearest first; the
+    // answer does not depend on the order.
     uint32_t ref = (uint32_t)M.root4_ref;
     int sp = 0;
     bool hit = false;
@@ -469,8 +472,14 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
                 ha[k] = n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, tmax, na[k]);
             }
             uint32_t er[4];
-            float en[4];
-            const int ne = node4_order(n, hl, nl, hr, nr, ha, na, er, en);
+            int ne = 0;
+#pragma unroll
+            for (int side = 0; side < 2; side++) {
+                if (!(side ? hr : hl)) continue;
+                const int a = 2 * side, b = a + 1;
+                if (ha[a]) er[ne++] = n.ref[a];
+                if (n.ref[b] != kEmptySlot && ha[b]) er[ne++] = n.ref[b];
+            }
             if (sp + ne > kMeshStack4) {
                 atomicOr(S.error, ERR_MESH_STACK);
                 break;
