@@ -398,6 +398,16 @@ int luz_gpu_adjoint_backward(luz_gpu_scene* scene, const LuzRenderParams* params
  * counterpart in the reference (it has no gradients). */
 int luz_gpu_adjoint_emission(luz_gpu_scene* scene, const LuzRenderParams* params, const float* adjoint_rgb,
                              double* grad_out, LuzRenderStats* stats);
+/* dLoss/d(density) of the volume `object` (index into LuzSceneDesc.objects, a
+ * LUZ_OBJ_VOLUME) for the film of `params` and dLoss/dpixel = adjoint_rgb, as
+ * one replay with a score-function estimate: the distance a bounce's rays sample
+ * in the medium, hd = -ln(u) / density (ConstantVolume.cpp:62-121), has score
+ * 1 / density - hd, and each contribution is weighted by the scores of the
+ * bounces whose rays crossed the medium before it. Unbiased while no ray meets a
+ * second medium (media met by one ray share its u). No counterpart in the
+ * reference (it has no gradients). */
+int luz_gpu_adjoint_density(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t object,
+                            const float* adjoint_rgb, double* grad_out, LuzRenderStats* stats);
 
 /* Adaptive sampling settings:/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
  * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),

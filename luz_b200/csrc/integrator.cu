@@ -296,6 +296,15 @@ __global__ void k_adjoint_emission_finish(DScene S, WaveArgs w, PathBuf P)
     w.pend_light[p] = -1;
 }
 
+// Light samples still pending after a density-replay wave, with their scores.
+__global__ void k_adjoint_density_finish(DScene S, WaveArgs w, PathBuf P)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w.n) return;
+    const float4 a = P.pend0[p], b = P.pend1[p];
+    density_add(S, w, P.pixel[p], F3{a.x + b.x, a.y + b.y, a.z + b.z}, w.dens_score[p].y);
+}
+
 __global__ void k_resolve(const double* film, int64_t npix, double spp, float* out)
 {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1380,6 +1389,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     w.grad_texture = texture;
     w.grad_kind = rough ? 1 : 0;
     w.grad_emission = 0;
+    w.grad_volume = -1;
     w.adj_rgb = d_adj;
     w.grad = d_grad;
     w.inv_spp = 1.0 / (double)p->spp;
@@ -1459,6 +1469,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     w.grad_texture = -1;
     w.grad_kind = 2;   // no texture hook
     w.grad_emission = 1;
+    w.grad_volume = -1;
     w.grad_light = d_grad;
     w.adj_rgb = d_adj;
     w.inv_spp = 1.0 / (double)p->spp;
@@ -1505,6 +1516,85 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
             grad_out[i] = acc;
         }
     }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    if (stats) {
+        *stats = LuzRenderStats{};
+        stats->render_ms = ms;
+        stats->samples = (double)npix * p->spp;
+        stats->kernel_launches = launches;
+        stats->waves = waves;
+    }
+    return LUZ_OK;
+}
+
+// dLoss/d(density) of one volume by a score-function replay (density_score).
+int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t object, const float* adj_rgb,
+                       double* grad_out, LuzRenderStats* stats)
+{
+    check_params(p);
+    if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in the adjoint pass.");
+    if (s->pack->consts.caustics.enabled)
+        throw Status(LUZ_E_UNSUPPORTED, "The adjoint pass does not differentiate caustic photon maps.");
+    const ScenePack& PK = *s->pack;
+    if (object < 0 || (std::size_t)object >= PK.object_of_desc.size() || PK.object_of_desc[(std::size_t)object] < 0)
+        throw Status(LUZ_E_INVALID, "Object index out of range.");
+    const int32_t gi = PK.object_of_desc[(std::size_t)object];
+    if (PK.objects[(std::size_t)gi].kind != OK_VOLUME) throw Status(LUZ_E_INVALID, "The object is not a volume.");
+    CK(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    const int64_t npix = (int64_t)p->width * p->height;
+    DeviceScratch D;
+    float* d_adj = D.get<float>(3 * npix, st);
+    double* d_grad = D.get<double>(kEmissionReplicas, st);
+    CK(cudaMemcpyAsync(d_adj, adj_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyHostToDevice, st));
+    WaveArgs w = base_args(s, p);
+    w.grad_texture = -1;
+    w.grad_kind = 2;
+    w.grad_emission = 0;
+    w.grad_volume = gi;
+    w.grad_density = d_grad;
+    w.adj_rgb = d_adj;
+    w.inv_spp = 1.0 / (double)p->spp;
+    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
+    s->ensure_paths(pix_wave * s_wave);
+    w.dens_score = D.get<float2>(pix_wave * s_wave, st);
+    CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(s->ev0, st));
+    StageTimer T0;
+    int64_t launches = 0, waves = 0;
+    for (int sb = 0; sb < p->spp; sb += s_wave) {
+        const int sc = std::min(s_wave, p->spp - sb);
+        for (int64_t pb = 0; pb < npix; pb += pix_wave) {
+            const int64_t pc = std::min<int64_t>(pix_wave, npix - pb);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = sb;
+            w.s_count = sc;
+            w.n = pc * sc;
+            const unsigned grid = (unsigned)((w.n + kBlock - 1) / kBlock);
+            w.adjoint = 1;
+            CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
+            CK(cudaMemsetAsync(w.dens_score, 0, sizeof(float2) * (std::size_t)w.n, st));
+            k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
+            launch_bounces(s, w, st, launches, T0, k_shade<3>);
+            k_adjoint_density_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
+            launches += 2;
+            waves++;
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaEventSynchronize(s->ev1));
+    uint32_t err = 0;
+    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    std::vector<double> rep(kEmissionReplicas);
+    CK(cudaMemcpy(rep.data(), d_grad, sizeof(double) * rep.size(), cudaMemcpyDeviceToHost));
+    double acc = 0.0;
+    for (double v : rep) acc += v;
+    *grad_out = acc;
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     if (stats) {
@@ -1895,6 +1985,15 @@ int luz_gpu_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t
     return guard([&] {
         if (!s || !adjoint_rgb || !grad_out) throw Status(LUZ_E_INVALID, "NULL argument.");
         return do_adjoint_backward(s, p, texture, adjoint_rgb, grad_out, stats);
+    });
+}
+
+int luz_gpu_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t object, const float* adjoint_rgb,
+                            double* grad_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || !adjoint_rgb || !grad_out) throw Status(LUZ_E_INVALID, "NULL argument.");
+        return do_adjoint_density(s, p, object, adjoint_rgb, grad_out, stats);
     });
 }
 

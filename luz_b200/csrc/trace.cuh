@@ -608,6 +608,44 @@ __device__ __forceinline__ bool local_ray(const GObject& O, const TRay& r, TRay&
 
 // ConstantVolume::sampleScatteringDistance (ConstantVolume.cpp:62-121) with the
 // boundary's hitInterval(-T_MAX, T_MAX) (Cube.cpp:134-175, Sphere.cpp:304-343).
+// Length (scene units along the ray) of the part of [tmin, tmax] inside the
+// boundary of volume O: the interval volume_distance samples in.
+__device__ float volume_overlap(const GObject& O, F3 o, F3 d, float tmin, float tmax)
+{
+    float entry, exit;
+    if (O.aux == 3 /* LUZ_OBJ_CUBE */) {
+        float imin = -kInf, imax = kInf;
+        const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        for (int a = 0; a < 3; a++) {
+            if (dd[a] == 0.0f) {
+                if (oo[a] < O.f[a] || oo[a] > O.f[3 + a]) return 0.0f;
+                continue;
+            }
+            const float inv = 1.0f / dd[a];
+            const float t0 = (O.f[a] - oo[a]) * inv, t1 = (O.f[3 + a] - oo[a]) * inv;
+            imin = fmaxf(imin, fminf(t0, t1));
+            imax = fminf(imax, fmaxf(t0, t1));
+            if (imin >= imax) return 0.0f;
+        }
+        entry = imin;
+        exit = imax;
+    } else {
+        if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) return 0.0f;
+        const F3 oc = o - f3(O.f);
+        const float b = dot(oc, d);
+        const F3 f = oc - b * d;
+        const float disc = (O.f[3] * O.f[3]) - len2(f);
+        if (disc < 0.0f) return 0.0f;
+        const float sq = sqrtf(disc);
+        entry = fminf(-b - sq, -b + sq);
+        exit = fmaxf(-b - sq, -b + sq);
+    }
+    entry = fmaxf(fmaxf(entry, tmin), 0.0f);
+    exit = fminf(exit, tmax);
+    if (!(exit > entry)) return 0.0f;
+    return (exit - entry) * sqrtf(len2(d));
+}
+
 __device__ bool volume_distance(const GObject& O, const TRay& r, float tmin, float tmax, VolSample& vs, float& t)
 {
     float entry, exit;

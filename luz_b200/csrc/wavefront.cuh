@@ -82,6 +82,9 @@ struct WaveArgs {
     int32_t grad_emission;        // replay: gradient with respect to each light's emitted radiance
     double* grad_light;           // kEmissionReplicas copies of light_count * 3 (summed on the host)
     int32_t* pend_light;          // per path: light of the pending light sample, -1 = none
+    int32_t grad_volume;          // replay: GObject index of the volume whose density is differentiated, -1 = none
+    double* grad_density;         // kEmissionReplicas partial sums of dLoss/d(density)
+    float2* dens_score;           // per path: score of the path so far, score of its pending light samples
     const float* adj_rgb;         // dLoss/dPixel, W*H*3
     double* grad;                 // dLoss/dTexel, texture W*H*3
     double inv_spp;
@@ -378,6 +381,29 @@ __device__ __forceinline__ void adjoint_emission_add(const DScene& S, const Wave
     }
 }
 
+// Density gradient (luz_gpu_adjoint_density): a score-function estimate. The
+// distance a bounce's rays sample in the differentiated medium is hd = -ln(u) /
+// density (ConstantVolume.cpp:62-121), density p(hd) = density e^(-density hd),
+// score d ln p / d density = 1 / density - hd; one u per bounce serves every
+// ray of the bounce (the extension ray that reaches the vertex and the light
+// samples leaving it), so the score is counted once for them. Every
+// contribution is multiplied by the summed scores of the draws it depends on.
+__device__ __forceinline__ float density_score(const DScene& S, const WaveArgs& w, const Key& k)
+{
+    const GObject& O = S.objects[w.grad_volume];
+    const double sigma = -1.0 / (double)O.f[6];
+    const double hd = (double)O.f[6] * log(fmax(sample1d(k, DIM_VOLUME_DISTANCE), 1e-12));
+    return (float)(1.0 / sigma - hd);
+}
+__device__ __forceinline__ void density_add(const DScene& S, const WaveArgs& w, uint32_t pix, F3 c, float score)
+{
+    const double g = ((double)w.adj_rgb[3 * (int64_t)pix] * c.x + (double)w.adj_rgb[3 * (int64_t)pix + 1] * c.y
+                      + (double)w.adj_rgb[3 * (int64_t)pix + 2] * c.z) * (double)score * w.inv_spp;
+    if (g == 0.0 || !isfinite(g)) return;
+    const int64_t rep = (int64_t)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) & (kEmissionReplicas - 1));
+    atomicAdd(&w.grad_density[rep], g);
+}
+
 // Path replay gradient of a Lambertian albedo texture (luz_gpu_adjoint_backward).
 // Everything the path gathers from this vertex on (its NEE and every later
 // vertex) carries the vertex's albedo = colour * clamp01(bilinear(texels)) as
@@ -456,7 +482,7 @@ __device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, co
 }
 
 // MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render;
-// 3: adjoint (texture-gradient) passes.
+// 3: adjoint (gradient) passes.
 template <int MODE>
 __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
@@ -469,9 +495,11 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     F3 rad{r4.x, r4.y, r4.z};
     uint32_t flags = __float_as_uint(r4.w);
     const float prev_pdf = t4.w;
+    F3 pend_in{0.f, 0.f, 0.f};   // the previous vertex's light samples, as the shadow test left them
 
     {
         const float4 a = P.pend0[p], b = P.pend1[p];
+        pend_in = F3{a.x, a.y, a.z} + F3{b.x, b.y, b.z};
         rad = (rad + F3{a.x, a.y, a.z}) + F3{b.x, b.y, b.z};
         if (MODE == 3 && w.adjoint && w.grad_kind == 1 && w.adj_rough[p].active)
             adjoint_rough_resolve(S, w, P, p, F3{a.x, a.y, a.z}, F3{b.x, b.y, b.z}, rad, true, w.adj_rough[p]);
@@ -497,6 +525,20 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
     const uint32_t pix = P.pixel[p];
     const Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
     const bool prev_spec = (flags & PF_PREV_SPECULAR) != 0;
+    // density gradient: scores of the draws this vertex's contributions depend on
+    float dscore = 0.0f, dscore_b = 0.0f;
+    bool dext = false;
+    F3 rad_start = rad;
+    if constexpr (MODE == 3) {
+        if (w.adjoint && w.grad_volume >= 0) {
+            const float2 ds = w.dens_score[p];
+            density_add(S, w, pix, pend_in, ds.y);
+            const float t_hit = obj < 0 ? kInf : h4.x;
+            dscore_b = density_score(S, w, k);
+            dext = volume_overlap(S.objects[w.grad_volume], ray.o, ray.d, kTMin, t_hit) > 0.0f;
+            dscore = ds.x + (dext ? dscore_b : 0.0f);
+        }
+    }
 
     if (obj < 0) {   // miss (ColorHelper.cpp:1169-1210)
         float env_mis = 1.0f;
@@ -740,6 +782,16 @@ __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P,
         P.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
     }
 done:
+    if constexpr (MODE == 3) {
+        if (w.adjoint && w.grad_volume >= 0) {
+            density_add(S, w, pix, rad - rad_start, dscore);
+            bool sh_used = false;
+            for (int q = 0; q < 2; q++)
+                if (out.sh[q] && volume_overlap(S.objects[w.grad_volume], out.sh_o[q], out.sh_d[q], kTMin, out.sh_t[q]) > 0.0f)
+                    sh_used = true;
+            w.dens_score[p] = make_float2(dscore, (!dext && sh_used) ? dscore + dscore_b : dscore);
+        }
+    }
     if (bounce >= w.max_bounces) out.cont = false;
     P.rad[p] = make_float4(rad.x, rad.y, rad.z, __uint_as_float(flags));
     P.pend0[p] = make_float4(pend0.x, pend0.y, pend0.z, 0.f);

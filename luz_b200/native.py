@@ -27,6 +27,7 @@ EXPORTED = [
     "luz_gpu_nfor_denoise", "luz_gpu_nfor_error", "luz_gpu_render_denoised",
     "luz_gpu_cache_create", "luz_gpu_cache_destroy", "luz_gpu_cache_weights", "luz_gpu_cache_predict",
     "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached", "luz_gpu_adjoint_emission",
+    "luz_gpu_adjoint_density",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -76,6 +77,8 @@ def lib():
     L.luz_gpu_adjoint_forward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_backward.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_adjoint_emission.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_adjoint_density.argtypes = [vp, C.POINTER(D.RenderParams), i32, vp, C.POINTER(C.c_double),
+                                          C.POINTER(D.RenderStats)]
     L.luz_gpu_cache_create.argtypes = [i32, C.POINTER(D.CacheParams), C.POINTER(vp)]
     L.luz_gpu_cache_destroy.argtypes = [vp]
     L.luz_gpu_cache_weights.argtypes = [vp, vp, vp]
@@ -250,6 +253,14 @@ class GpuScene:
         st = D.RenderStats()
         _check(lib().luz_gpu_adjoint_emission(self.h, C.byref(p), adj.ctypes.data, grad.ctypes.data, C.byref(st)))
         return grad[:self.info().light_count], st
+
+    def adjoint_density(self, p: D.RenderParams, obj: int, adjoint_rgb: np.ndarray):
+        """dLoss/d(density) of volume object `obj` for dLoss/dpixel = adjoint_rgb."""
+        adj = np.ascontiguousarray(adjoint_rgb, np.float32)
+        g = C.c_double()
+        st = D.RenderStats()
+        _check(lib().luz_gpu_adjoint_density(self.h, C.byref(p), int(obj), adj.ctypes.data, C.byref(g), C.byref(st)))
+        return g.value, st
 
     def render_device(self, p: D.RenderParams, out_ptr: int, stream: int = 0) -> D.RenderStats:
         st = D.RenderStats()
