@@ -132,7 +132,8 @@ typedef struct LuzObjectDesc {
     int32_t _pad;
     double  uv[12];
     int32_t ies;                  /* sphere: -1 or index into LuzSceneDesc.ies      */
-    int32_t _pad2;
+    int32_t uv_projection;        /* sphere: 0 = lat-long, 1 = cube cross           */
+                                  /* (SphereUVProjection, Sphere.cpp:14-92)         */
     double  ies_direction[3];     /* Sphere::setIESProfile vertical axis            */
     double  ies_rotation_degrees; /* Sphere::setIESProfile horizontal rotation      */
 } LuzObjectDesc;

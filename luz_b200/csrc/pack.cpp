@@ -939,6 +939,8 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
             }
             g.f[3] = (float)r;
             g.f[4] = o.visible ? 1.f : 0.f;
+            if (o.uv_projection != 0 && o.uv_projection != 1) invalid("Unknown sphere UV projection.");
+            g.f[5] = (float)o.uv_projection;
             has_box = true;
             if (o.ies != -1) {   // Sphere::setIESProfile (Sphere.cpp:188-202)
                 if (o.ies < 0 || o.ies >= d->ies_count) invalid("IES profile index out of range.");

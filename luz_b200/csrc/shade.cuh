@@ -45,6 +45,37 @@ __device__ __forceinline__ void set_face(const F3& d, F3 outward, Hit& h)
 }
 __device__ __forceinline__ F3 face_toward(const F3& d, F3 n) { return dot(d, n) > 0.0f ? n * -1.0f : n; }
 
+// Sphere UVs in a 4x3 cube-cross atlas (setCubeCrossUV, Sphere.cpp:22-83): the
+// dominant axis of the outward normal picks the face (ties go to x, then y),
+// the face coordinates are inset by 0.02 on each side.
+__device__ __forceinline__ void sphere_cube_cross_uv(const F3& n, float& u, float& v)
+{
+    const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+    int column, row;
+    float s, t;
+    if (ax >= ay && ax >= az) {
+        column = n.x >= 0.0f ? 2 : 0;
+        row = 1;
+        s = n.x >= 0.0f ? 0.5f - (n.z / (2.0f * ax)) : 0.5f + (n.z / (2.0f * ax));
+        t = 0.5f + (n.y / (2.0f * ax));
+    } else if (ay >= ax && ay >= az) {
+        column = n.y >= 0.0f ? 2 : 0;
+        row = n.y >= 0.0f ? 2 : 0;
+        s = n.y >= 0.0f ? 0.5f - (n.z / (2.0f * ay)) : 0.5f + (n.z / (2.0f * ay));
+        t = 0.5f - (n.x / (2.0f * ay));
+    } else {
+        column = n.z >= 0.0f ? 1 : 3;
+        row = 1;
+        s = n.z >= 0.0f ? 0.5f + (n.x / (2.0f * az)) : 0.5f - (n.x / (2.0f * az));
+        t = 0.5f + (n.y / (2.0f * az));
+    }
+    const float inset = 0.02f;
+    s = inset + (fminf(fmaxf(s, 0.0f), 1.0f) * (1.0f - (2.0f * inset)));
+    t = inset + (fminf(fmaxf(t, 0.0f), 1.0f) * (1.0f - (2.0f * inset)));
+    u = ((float)column + s) / 4.0f;
+    v = ((float)row + t) / 3.0f;
+}
+
 // Triangle::hit shading (Triangle.cpp:234-269) in the frame of ray r.
 __device__ void triangle_shading(const DScene& S, const GMesh& M, int32_t slot, float bu, float bv, const F3& d,
                                  F3& n, F3& gn, bool& front, float& u, float& v)
@@ -112,10 +143,14 @@ __device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit&
     }
     case OK_SPHERE: {
         const F3 outward = vdiv(h.p - f3(O.f), O.f[3]);
-        const float phi = atan2f(outward.z, outward.x);
-        const float theta = acosf(fminf(fmaxf(outward.y, -1.0f), 1.0f));
-        h.u = 0.5f + phi / (2.0f * kPiF);
-        h.v = 1.0f - theta / kPiF;
+        if (O.f[5] != 0.0f) {
+            sphere_cube_cross_uv(outward, h.u, h.v);
+        } else {
+            const float phi = atan2f(outward.z, outward.x);
+            const float theta = acosf(fminf(fmaxf(outward.y, -1.0f), 1.0f));
+            h.u = 0.5f + phi / (2.0f * kPiF);
+            h.v = 1.0f - theta / kPiF;
+        }
         set_face(r.d, outward, h);
         break;
     }

@@ -63,7 +63,7 @@ class ObjectDesc(C.Structure):
         ("has_axes", C.c_int32), ("visible", C.c_int32),
         ("rotation_degrees", D3), ("scale", D3), ("density", C.c_double),
         ("has_uvs", C.c_int32), ("_pad", C.c_int32), ("uv", D12),
-        ("ies", C.c_int32), ("_pad2", C.c_int32), ("ies_direction", D3), ("ies_rotation_degrees", C.c_double),
+        ("ies", C.c_int32), ("uv_projection", C.c_int32), ("ies_direction", D3), ("ies_rotation_degrees", C.c_double),
     ]
 
 
@@ -320,11 +320,12 @@ class Scene:
                          material=material, **kw)
 
     def sphere(self, center, radius, material, visible=True, ies=-1, ies_direction=(0.0, -1.0, 0.0),
-               ies_rotation=0.0):
-        """ies: -1 or an index from ies_profile (Sphere::setIESProfile)."""
+               ies_rotation=0.0, uv_projection=0):
+        """ies: -1 or an index from ies_profile (Sphere::setIESProfile); uv_projection: 0 lat-long,
+        1 cube cross (SphereUVProjection)."""
         return self._obj(kind=OBJ_SPHERE, position=center, size=(radius, 0, 0), material=material,
                          visible=1 if visible else 0, ies=ies, ies_direction=ies_direction,
-                         ies_rotation_degrees=float(ies_rotation))
+                         ies_rotation_degrees=float(ies_rotation), uv_projection=int(uv_projection))
 
     def ies_profile(self, vertical_deg, horizontal_deg, candela) -> int:
         """candela: (len(horizontal), len(vertical)) array (IES file order, multiplier applied)."""

@@ -73,6 +73,8 @@ class RefOracle:
         L.luzref_sampler.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32,
                                      C.c_uint32, C.c_int32, vp]
         L.luzref_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        L.luzref_scene_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.luzref_scene_pack.argtypes = [vp, C.POINTER(vp), vp]
 
     def _check(self, rc):
         if rc != 0:
@@ -84,6 +86,14 @@ class RefOracle:
         h = C.c_void_p()
         self._check(self.lib.luzref_scene_create(C.cast(built.ptr(), C.c_void_p), 1 if tag else 0, C.byref(h)))
         return RefScene(self, h, built)
+
+    def load_luz(self, path: str) -> "RefScene":
+        """A scene read from a .luz file by the reference's own parser (SceneFile::read)."""
+        h = C.c_void_p()
+        with stdout_to_stderr():
+            rc = self.lib.luzref_scene_load(os.fsencode(path), C.byref(h))
+        self._check(rc)
+        return RefScene(self, h, None)
 
     def nfor(self, bufs: dict, prefilter_radius=1, regression_radius=2, patch_radius=1, min_variance=1e-5,
              threads=1):
@@ -102,6 +112,19 @@ class RefOracle:
         out = np.zeros(2, np.float64)
         self.lib.luzref_sampler(seed, x, y, s, stream, bounce, dim, which, out.ctypes.data)
         return out[0] if which == 1 else (out[0], out[1])
+
+
+class PackedDesc:
+    """A LuzSceneDesc owned by a reference scene (valid while that scene lives and
+    is not packed again); .ptr() is what luz_gpu_scene_create and
+    luzref_scene_create take, as for the Python-built descriptions."""
+
+    def __init__(self, owner: "RefScene", address: int, width: int, height: int, spp: int, max_bounces: int):
+        self.owner, self.address = owner, address
+        self.width, self.height, self.spp, self.max_bounces = width, height, spp, max_bounces
+
+    def ptr(self) -> int:
+        return self.address
 
 
 class RefScene:
@@ -130,6 +153,13 @@ class RefScene:
                                                    None if vk is None else vk.ctypes.data,
                                                    t.ctypes.data, obj.ctypes.data, prim.ctypes.data))
         return t, obj, prim
+
+    def pack(self) -> "PackedDesc":
+        """The scene glue (luz_b200/glue/scene_glue.cpp) applied to this scene."""
+        d = C.c_void_p()
+        st = np.zeros(4, np.int32)
+        self.o._check(self.o.lib.luzref_scene_pack(self.h, C.byref(d), st.ctypes.data))
+        return PackedDesc(self, d.value, *[int(v) for v in st])
 
     def caustic_photons(self, seed: int, max_bounces: int) -> int:
         """CausticPhotonMap::build for the render seed: photons stored."""

@@ -19,7 +19,11 @@
  *   - full render:         Renderer::render (src/renderer/Renderer.cpp:10) with
  *                          denoise/adaptive off and the Raw view transform;
  *   - mesh BVH layout:     Mesh::_packedBVHNodes / _triangleIndices, read with
- *                          private access in this translation unit only.
+ *                          private access in this translation unit only;
+ *   - .luz scenes:         SceneFile::read (src/io/SceneFile/SceneFile.cpp:256-321)
+ *                          into a reference Scene, and the reference-side scene
+ *                          glue (luz_b200/glue/scene_glue.cpp) that packs such a
+ *                          Scene into a LuzSceneDesc.
  * Hit identification: in "tag" mode every object (and every mesh triangle) gets
  * its own Lambertian-derived material so the HitRecord's material pointer names
  * the object and primitive; traversal does not depend on material values.
@@ -70,8 +74,10 @@
 #include "Renderer/Renderer.hpp"
 #include "Renderer/CausticPhotonMap.hpp"
 #include "RendererInternal.hpp"
+#include "SceneFile/SceneFile.hpp"
 
 #include "luz_gpu.h"
+#include "scene_glue.h"
 
 namespace {
 
@@ -95,6 +101,7 @@ struct RefScene {
     std::vector<int32_t> mesh_object;                         // mesh index -> first MESH object
     std::unordered_map<const Material*, std::pair<int32_t, int32_t>> tags;
     std::vector<std::shared_ptr<Material>> keep;
+    std::unique_ptr<LuzPackedScene> packed;                   // luzref_scene_pack output
 };
 
 Color col(const double* c) { return Color(c[0], c[1], c[2]); }
@@ -270,7 +277,9 @@ RefScene* build(const LuzSceneDesc* d, int tag)
             break;
         }
         case LUZ_OBJ_SPHERE: {
-            auto sp = std::make_shared<Sphere>(vec(o.position), o.size[0], mat, o.visible != 0, SphereUVProjection::LatLong);
+            auto sp = std::make_shared<Sphere>(vec(o.position), o.size[0], mat, o.visible != 0,
+                                               o.uv_projection == 1 ? SphereUVProjection::CubeCross
+                                                                    : SphereUVProjection::LatLong);
             if (o.ies >= 0) sp->setIESProfile(ies_profile(d->ies[o.ies]), vec(o.ies_direction), o.ies_rotation_degrees);
             h = sp;
             break;
@@ -428,6 +437,41 @@ int luzref_scene_destroy(void* s)
 {
     delete static_cast<RefScene*>(s);
     return 0;
+}
+
+/* A scene read from a .luz file by the reference's own parser (SceneFile::read,
+ * src/io/SceneFile/SceneFile.cpp:256-321), left as Renderer::render prepares it
+ * (Renderer.cpp:18-20). Untagged: hits are not identified per object. */
+int luzref_scene_load(const char* path, void** out)
+{
+    return guarded([&] {
+        auto rs = std::make_unique<RefScene>();
+        SceneFile::read(rs->scene, path);
+        rs->scene.syncAtmosphereSunDirection();
+        rs->scene.updateLights();
+        rs->scene.updateAccelerationStructure();
+        *out = rs.release();
+        return 0;
+    });
+}
+
+/* The scene glue (luz_b200/glue/scene_glue.cpp) applied to a reference scene:
+ * *desc stays valid until the scene is destroyed or packed again; settings
+ * receives width, height, spp and max light bounces from the scene. */
+int luzref_scene_pack(void* s, const LuzSceneDesc** desc, int32_t* settings)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        auto packed = std::make_unique<LuzPackedScene>();
+        luz_pack_scene(rs->scene, *packed);
+        rs->packed = std::move(packed);
+        *desc = &rs->packed->desc;
+        settings[0] = rs->packed->width;
+        settings[1] = rs->packed->height;
+        settings[2] = rs->packed->spp;
+        settings[3] = rs->packed->max_bounces;
+        return 0;
+    });
 }
 
 /* rays: (ox,oy,oz,tmin,dx,dy,dz,tmax) per ray, used as given (no renormalisation). */
