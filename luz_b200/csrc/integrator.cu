@@ -244,7 +244,7 @@ __global__ void k_accumulate(WaveArgs w, PathBuf P, double* film)
         sy += (double)c.y;
         sz += (double)c.z;
     }
-    double* f = film + 3 * (int64_t)(w.pix_begin + j);
+    double* f = film + 3 * (int64_t)P.pixel[b];   // the slot's pixel (path_coords)
     f[0] += sx;
     f[1] += sy;
     f[2] += sz;

@@ -270,6 +270,7 @@ struct GSceneConst {
     GCaustics caustics;
     float box_lo[3];          // box of every bounded object (radiance-cache position input)
     float box_inv[3];         // 1 / extent per axis (1 where the extent is 0 or there is no box)
+    int32_t cube_cross_spheres;   // 1 when a sphere uses the cube-cross UV projection
 };
 
 }  // namespace luz

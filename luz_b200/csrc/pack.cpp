@@ -1441,9 +1441,11 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
     }
     // Traversal kernel specialisation (TraceFeature bits: 1 instances, 2 volumes).
     K.features = 0;
+    K.cube_cross_spheres = 0;
     for (const GObject& o : S.objects) {
         if (o.kind == OK_INSTANCE) K.features |= 1;
         if (o.kind == OK_VOLUME) K.features |= 2;
+        if (o.kind == OK_SPHERE && o.f[5] != 0.f) K.cube_cross_spheres = 1;
     }
     const double bg_max = std::max(d->background[0], std::max(d->background[1], d->background[2]));
     K.has_constant_background_light = (!E.lighting && d->sky == LUZ_SKY_NONE && bg_max > 0.0) ? 1 : 0;

@@ -112,7 +112,11 @@ __device__ __forceinline__ F3 transform_normal(const GObject& O, F3 n)
 }
 
 // Builds the HitRecord the reference's hit() would fill for THit h on ray r.
-__device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit& th)
+// XUV: the scene has cube-cross spheres (a separate instantiation: the branch
+// alone enlarges this out-of-line function's frame and slowed the shade stage
+// by 3.5% on scenes without such spheres).
+template <bool XUV>
+__device__ __noinline__ Hit make_hit_t(const DScene& S, const TRay& r, const THit& th)
 {
     Hit h;
     const GObject O = S.objects[th.obj];
@@ -143,7 +147,7 @@ __device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit&
     }
     case OK_SPHERE: {
         const F3 outward = vdiv(h.p - f3(O.f), O.f[3]);
-        if (O.f[5] != 0.0f) {
+        if (XUV && O.f[5] != 0.0f) {
             sphere_cube_cross_uv(outward, h.u, h.v);
         } else {
             const float phi = atan2f(outward.z, outward.x);
@@ -185,6 +189,11 @@ __device__ __noinline__ Hit make_hit(const DScene& S, const TRay& r, const THit&
         break;
     }
     return h;
+}
+
+__device__ __forceinline__ Hit make_hit(const DScene& S, const TRay& r, const THit& th)
+{
+    return S.k.cube_cross_spheres ? make_hit_t<true>(S, r, th) : make_hit_t<false>(S, r, th);
 }
 
 // ----------------------------------------------------------------------------- textures / colour

@@ -103,6 +103,33 @@ struct WaveArgs {
 
 enum PathFlags : uint32_t { PF_PREV_SPECULAR = 1u, PF_PREV_SVIL = 2u, PF_CACHE_DONE = 4u };
 
+// Pixel of slot `i` of a width x height image walked in 8x8 tiles: tiles row
+// by row, Z-order inside a full tile, row-major inside the partial tiles of the
+// right and bottom edges. A bijection of [0, width*height); the 16 or 32
+// consecutive pixels of a warp form a 4x4 or 8x4 block, so its rays start
+// close together and traverse the same BVH nodes more often than a row strip.
+__device__ __forceinline__ void tiled_pixel(uint32_t i, uint32_t width, uint32_t height, uint32_t& x, uint32_t& y)
+{
+    const uint32_t ty = i / (8u * width);
+    const uint32_t r = i - ty * (8u * width);
+    const uint32_t th = min(8u, height - 8u * ty);
+    const uint32_t tx = r / (8u * th);
+    const uint32_t q = r - tx * (8u * th);
+    const uint32_t tw = min(8u, width - 8u * tx);
+    uint32_t lx, ly;
+    if (tw == 8u && th == 8u) {
+        lx = (q & 1u) | ((q >> 1) & 2u) | ((q >> 2) & 4u);
+        ly = ((q >> 1) & 1u) | ((q >> 2) & 2u) | ((q >> 3) & 4u);
+    } else {
+        ly = q / tw;
+        lx = q - ly * tw;
+    }
+    x = 8u * tx + lx;
+    y = 8u * ty + ly;
+}
+
+// (x, y, sample) of path p. The result of a path depends on these alone (the
+// sampler keys on them), not on which slot of a wave carries it.
 __device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint32_t& x, uint32_t& y, uint32_t& s)
 {
     if (w.list_mode) {
@@ -112,10 +139,14 @@ __device__ __forceinline__ void path_coords(const WaveArgs& w, uint32_t p, uint3
         return;
     }
     const uint32_t slot = (uint32_t)w.pix_begin + p / (uint32_t)w.s_count;
-    const uint32_t pix = w.pix_list ? w.pix_list[slot] : slot;
     s = (uint32_t)(w.s_begin + w.sample_offset) + p % (uint32_t)w.s_count;
-    x = pix % (uint32_t)w.width;
-    y = pix / (uint32_t)w.width;
+    if (w.pix_list) {
+        const uint32_t pix = w.pix_list[slot];
+        x = pix % (uint32_t)w.width;
+        y = pix / (uint32_t)w.width;
+    } else {
+        tiled_pixel(slot, (uint32_t)w.width, (uint32_t)w.height, x, y);
+    }
 }
 
 __device__ __forceinline__ Key path_key(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, uint32_t bounce)
