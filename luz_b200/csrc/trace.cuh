@@ -300,8 +300,8 @@ __device__ __forceinline__ GNode4C load_node4_entries(const GNode4* nodes, uint3
 // Visit order of a collapsed node's entries, as the binary near-first
 // traversal (Mesh::hit, Mesh.cpp:578-660) would reach them: the nearer of L
 // and R first (ties: R), and within each the nearer child first (ties: the
-// right one). ha/na: acceptance and entry distance of the four slots and of
-// L, R. Returns the number of entries written to er/en in visit order.
+// right one). mesh_closest_walk computes each accepted entry's position in
+// this order.
 //
 // Testing all boxes at N's visit instead of at L's and R's gives the same
 // visits: L is visited right after N (nothing changes `closest` in between),
@@ -311,50 +311,6 @@ __device__ __forceinline__ GNode4C load_node4_entries(const GNode4* nodes, uint3
 // are unions of their triangles' boxes, rounded outward), so a grandchild's
 // entry distance is never below its parent's and a grandchild of a rejected
 // child is itself rejected.
-__device__ __forceinline__ int node4_order(const GNode4& n, bool hl, float nl, bool hr, float nr, const bool* ha,
-                                           const float* na, uint32_t* er, float* en)
-{
-    int ne = 0;
-    auto add = [&](int k) {
-        er[ne] = n.ref[k];
-        en[ne] = na[k];
-        ne++;
-    };
-    auto side = [&](int s) {
-        const int a = 2 * s, b = 2 * s + 1;
-        if (n.ref[b] == kEmptySlot) {       // leaf child: slot a is the leaf itself
-            if (ha[a]) add(a);
-            return;
-        }
-        if (ha[a] && ha[b]) {
-            if (na[a] < na[b]) {
-                add(a);
-                add(b);
-            } else {
-                add(b);
-                add(a);
-            }
-        } else if (ha[a]) {
-            add(a);
-        } else if (ha[b]) {
-            add(b);
-        }
-    };
-    if (hl && hr) {
-        if (nl < nr) {
-            side(0);
-            side(1);
-        } else {
-            side(1);
-            side(0);
-        }
-    } else if (hl) {
-        side(0);
-    } else if (hr) {
-        side(1);
-    }
-    return ne;
-}
 
 // Mesh traversal stack in the thread's local memory: node or leaf reference
 // and near distance per entry; NEAR = false drops the distances (any-hit never
@@ -425,17 +381,42 @@ __device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& 
                     na[k] = 0.f;
                     ha[k] = n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, closest, na[k]);
                 }
-                uint32_t er[4];
-                float en[4];
-                const int ne = node4_order(n, hl, nl, hr, nr, ha, na, er, en);
+                // node4_order's visit order as a position per accepted entry
+                // (side offset + place within the side), without appending to
+                // arrays. An accepted entry implies an accepted side box (the
+                // entry box lies inside it), so hl/hr only decide which side goes
+                // first when both hold entries: the nearer (ties: R).
+                (void)hl;
+                (void)hr;
+                const int cl = (int)ha[0] + (int)ha[1], cr = (int)ha[2] + (int)ha[3];
+                const bool r_first = (cl > 0 && cr > 0) ? !(nl < nr) : (cr > 0);
+                const int ne = cl + cr;
                 if (sp + ne > kMeshStack4) {
                     atomicOr(S.error, ERR_MESH_STACK);
                     break;
                 }
                 if (ne > 0) {
-                    for (int e = ne - 1; e >= 1; e--) st.set(sp++, er[e], en[e]);
-                    ref = er[0];
-                    near = en[0];
+                    uint32_t first_ref = 0;
+                    float first_near = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int side = k >> 1;
+                        const bool a_first = na[2 * side] < na[2 * side + 1];   // ties: the right entry first
+                        const bool behind_partner = ha[k ^ 1] && ((k & 1) ? a_first : !a_first);
+                        const bool side_second = side ? !r_first : r_first;
+                        const int pos = (side_second ? (side ? cl : cr) : 0) + (behind_partner ? 1 : 0);
+                        if (ha[k]) {
+                            if (pos == 0) {
+                                first_ref = n.ref[k];
+                                first_near = na[k];
+                            } else {
+                                st.set(sp + ne - 1 - pos, n.ref[k], na[k]);
+                            }
+                        }
+                    }
+                    sp += ne - 1;
+                    ref = first_ref;
+                    near = first_near;
                     continue;
                 }
             }
