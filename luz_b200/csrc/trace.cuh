@@ -476,20 +476,32 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
             const GNode4C n = load_node4_entries(S.nodes4, ref);
             vs.nodes++;
             const F3 noi = FAST ? neg_o_inv(r) : F3{0.f, 0.f, 0.f};
-            uint32_t er[4];
-            int ne = 0;
+            bool ha[4];
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 float na;
-                if (n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, tmax, na)) er[ne++] = n.ref[k];
+                ha[k] = n.ref[k] != kEmptySlot && mesh_box<FAST>(n.cmin[k], n.cmax[k], r, noi, tmax, na);
             }
+            // Entries in slot order; an entry's place is the number of accepted
+            // entries before it (selects, no running index into an array).
+            const int ne = (int)ha[0] + (int)ha[1] + (int)ha[2] + (int)ha[3];
             if (sp + ne > kMeshStack4) {
                 atomicOr(S.error, ERR_MESH_STACK);
                 break;
             }
             if (ne > 0) {
-                for (int e = ne - 1; e >= 1; e--) st.set(sp++, er[e], 0.f);
-                ref = er[0];
+                uint32_t first_ref = 0;
+                int pos = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (ha[k]) {
+                        if (pos == 0) first_ref = n.ref[k];
+                        else st.set(sp + ne - 1 - pos, n.ref[k], 0.f);
+                        pos++;
+                    }
+                }
+                sp += ne - 1;
+                ref = first_ref;
                 continue;
             }
         }
