@@ -56,10 +56,12 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 
 // ---------------------------------------------------------------------------- extend (closest hit)
 
-// Resident blocks per SM the register allocator is asked to allow (measured on
-// B200: more resident warps beat the few spills this costs in the traversal).
+// Resident blocks per SM the register allocator is asked to allow, measured on
+// B200 (1080p glossy frame, extend / shade / shadow stage): extend 5 blocks
+// (96 registers, almost no spills) 253 ms against 266 ms at 6 and 273 ms at 7;
+// shade 4 and shadow 8 ahead of 3 / 5 and 6 / 10.
 #ifndef LUZ_EXTEND_MIN_BLOCKS
-#define LUZ_EXTEND_MIN_BLOCKS 6
+#define LUZ_EXTEND_MIN_BLOCKS 5
 #endif
 #ifndef LUZ_SHADE_MIN_BLOCKS
 #define LUZ_SHADE_MIN_BLOCKS 4
