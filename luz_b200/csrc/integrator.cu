@@ -802,7 +802,19 @@ struct luz_gpu_scene {
 
 namespace {
 
-constexpr int64_t kWaveTarget = int64_t(1) << 22;   // ~4M paths in flight per wave
+// Paths in flight per wave. A launch of the persistent trace kernels lasts at
+// least as long as its slowest warp's traversal, a tail of the order of half a
+// millisecond per bounce on incoherent rays; larger waves pay it fewer times per
+// frame (1080p glossy frame, 64 spp: 4 Mi paths 231.5, 8 Mi 305.6, 16 Mi 363.5
+// Msamples/s, the image the same bit for bit). Path state is about 270 B per
+// path (4.5 GB at 16 Mi) and stays allocated with the scene handle.
+constexpr int64_t kWaveTarget = int64_t(1) << 24;
+// A batch of scenes keeps 4 Mi paths per scene: its concurrent streams already
+// fill one another's tails, and every handle keeps its own path state.
+constexpr int64_t kBatchWaveTarget = int64_t(1) << 22;
+// The cached render updates its cache once per wave; 4 Mi paths set the
+// training cadence its error figures were measured with.
+constexpr int64_t kCacheWaveTarget = int64_t(1) << 22;
 
 // Stage timing (LUZ_RENDER_PROFILE): one event pair per stage launch, summed per wave.
 struct StageTimer {
@@ -993,6 +1005,7 @@ struct RenderJob {
     cudaStream_t st = nullptr;
     WaveArgs w{};
     int64_t npix = 0, pix_wave = 0;
+    int64_t wave_target = kWaveTarget;
     int s_wave = 0;
     StageTimer T;
     unsigned long long* counters = nullptr;
@@ -1008,8 +1021,8 @@ void render_prepare(RenderJob& J)
     prepare_caustics(s, p, J.st);
     J.w = base_args(s, p);
     J.npix = (int64_t)p->width * p->height;
-    J.s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
-    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, kWaveTarget / J.s_wave));
+    J.s_wave = (int)std::min<int64_t>(p->spp, J.wave_target);
+    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, J.wave_target / J.s_wave));
     s->ensure_paths(J.pix_wave * J.s_wave);
     if (s->film_pix < J.npix) {
         if (s->film) cudaFree(s->film);
@@ -1928,6 +1941,7 @@ int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* pa
                 J.s = scenes[i];
                 J.p = &params[i];
                 J.st = scenes[i]->stream;
+                J.wave_target = kBatchWaveTarget;
                 render_prepare(J);
                 outs[(std::size_t)i] = dalloc<float>((std::size_t)(3 * J.npix));
                 J.d_out = outs[(std::size_t)i];
@@ -2225,8 +2239,8 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     const cudaStream_t st = s->stream;
     const int64_t npix = (int64_t)p->width * p->height;
     // waves as the plain render makes them (samples inner), one cache update per wave
-    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, kWaveTarget / npix));
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
+    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, kCacheWaveTarget / npix));
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kCacheWaveTarget / s_wave));
     const int64_t n_wave = pix_wave * s_wave;
     s->ensure_paths(n_wave);
     DeviceScratch D;
