@@ -806,9 +806,10 @@ namespace {
 // least as long as its slowest warp's traversal, a tail of the order of half a
 // millisecond per bounce on incoherent rays; larger waves pay it fewer times per
 // frame (1080p glossy frame, 64 spp: 4 Mi paths 231.5, 8 Mi 305.6, 16 Mi 363.5,
-// 32 Mi 395.4 Msamples/s, the image the same bit for bit). Path state is 268 B
-// per path (9 GB at 32 Mi) and stays allocated with the scene handle.
-constexpr int64_t kWaveTarget = int64_t(1) << 25;
+// 32 Mi 395.4-400.0, 64 Mi 414.5 Msamples/s, the image the same bit for bit).
+// Path state is 268 B per path (18 GB at 64 Mi, a tenth of the B200's HBM) and
+// stays allocated with the scene handle.
+constexpr int64_t kWaveTarget = int64_t(1) << 26;
 // A batch of scenes keeps 4 Mi paths per scene: its concurrent streams already
 // fill one another's tails, and every handle keeps its own path state.
 constexpr int64_t kBatchWaveTarget = int64_t(1) << 22;
