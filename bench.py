@@ -8,12 +8,17 @@ on the GPU; `e2e` is the same metric through the C ABI call a host makes
 (luz_gpu_render with a host film, device->host copy included).
 
 Multi-GPU (torchrun, one process per GPU): every rank renders the full frame
-with its own sample range (sample_offset = rank * spp), and the films are
-summed with one NCCL all-reduce per step: weak scaling over samples.
+with its own sample range (luz_b200.shard: rank r renders samples
+[r * spp, (r + 1) * spp) of a world * spp frame), and one NCCL all-reduce per
+step sums the films, normalised to the frame's mean: weak scaling over samples.
 
 --impl reference times the Luz reference renderer (built from its own sources
 into oracle/_ref/libluzref_fast.so) on the host cores on a bounded sample of
-the same workload (the 1080p frame at 1 spp per step).
+the same workload (the frame at 4 spp per step, Renderer::render).
+
+Other workloads: --workload cornell300 (config 0: Cornell box 300x300, 50 spp,
+depth 8), --workload instancing (config 2: 1e5 instances in an HG medium,
+1280x720, 32 spp, depth 16) print the same line for those scenes.
 """
 from __future__ import annotations
 
@@ -48,9 +53,12 @@ def parse():
     return ap.parse_args()
 
 
+WORKLOAD_ALIASES = {"cornell300": "cornell", "instancing": "instancing_volumes"}
+
+
 def workload(name, spp=None):
     from luz_b200 import scenes
-    w = scenes.WORKLOADS[name]()
+    w = scenes.WORKLOADS[WORKLOAD_ALIASES.get(name, name)]()
     if spp:
         w.spp = spp
     return w
@@ -125,15 +133,26 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per extension ray of k_extend, from the committed ncu summary (profiles/)."""
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_extend_counters_mesh_glossy.md")
+
+
+def profile_counters():
+    """Per-extension-ray ncu figures of k_extend from the committed summary: DRAM bytes,
+    L2 bytes (lts__t_bytes), L2 throughput as a fraction of its peak
+    (lts__throughput.avg.pct_of_peak_sustained_elapsed / 100) and active lanes per
+    warp instruction (smsp__thread_inst_executed_per_inst_executed)."""
     import re
-    p = os.path.join(ROOT, "profiles", "launches_mesh_glossy_2spp.md")
-    if os.path.exists(p):
-        m = re.search(r"DRAM bytes per extension ray: ([0-9.]+)", open(p).read())
-        if m:
-            return float(m.group(1))
-    return None
+    out = {}
+    if os.path.exists(PROFILE_SUMMARY):
+        txt = open(PROFILE_SUMMARY).read()
+        for key, pat in (("dram", r"DRAM bytes per extension ray: ([0-9.]+)"),
+                         ("l2", r"L2 bytes per extension ray: ([0-9.]+)"),
+                         ("l2_frac", r"L2 throughput, fraction of peak: ([0-9.]+)"),
+                         ("lanes", r"active lanes per warp instruction: ([0-9.]+)")):
+            m = re.search(pat, txt)
+            if m:
+                out[key] = float(m.group(1))
+    return out
 
 
 def cpu_baseline(w, threads):
@@ -172,7 +191,8 @@ def run_reference(args):
         return
     ro = O.RefOracle(fast=True)
     rs = ro.scene(w.scene.build())
-    p = native.params(w.width, w.height, 1, w.max_bounces, w.seed)
+    spp_step = min(w.spp, 4)
+    p = native.params(w.width, w.height, spp_step, w.max_bounces, w.seed)
     for _ in range(args.warmup):
         rs.render(p, threads)
     times, samples = [], 0.0
@@ -188,7 +208,7 @@ def run_reference(args):
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)", "config": cfg,
            "impl": "reference",
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"{w.width}x{w.height} at 1 spp per step ({int(samples)} samples)"},
+                            "sample": f"{w.width}x{w.height} at {spp_step} spp per step ({int(samples)} samples)"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -215,12 +235,19 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
     p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed, 0, rank * w.spp)
+    from luz_b200.shard import render_sharded
 
     def step():
-        st = g.render_device(p, film.data_ptr(), stream.cuda_stream)
-        if dist is not None:
-            dist.all_reduce(film)
-        return st
+        if dist is None:
+            return g.render_device(p, film.data_ptr(), stream.cuda_stream)
+        out = {}
+
+        def render_mean(offset, count):   # this rank's samples of the world * spp frame
+            pr = native.params(w.width, w.height, count, w.max_bounces, w.seed, 0, offset)
+            out["st"] = g.render_device(pr, film.data_ptr(), stream.cuda_stream)
+            return film
+        render_sharded(render_mean, w.spp * world, rank, world, lambda t: dist.all_reduce(t))
+        return out["st"]
 
     for _ in range(args.warmup):
         step()
@@ -261,7 +288,7 @@ def run_ours(args):
         if dist is not None:
             ht = torch.from_numpy(host).cuda()
             dist.all_reduce(ht)
-            host = ht.cpu().numpy()
+            host = (ht / world).cpu().numpy()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2 = float(np.mean(e2e_ms))
     if dist is not None:
@@ -278,13 +305,36 @@ def run_ours(args):
     timed = g.render_device(pt, film.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     ext_rays = prof.extension_rays
-    alg_bytes = 160.0 * prof.ext_nodes + 48.0 * prof.ext_tris + 32.0 * prof.ext_top + 64.0 * ext_rays
+    # algorithmic bytes of the closest-hit walk: 32 B per child box of every binary-node
+    # visit the collapsed walk stands for (two per visit), 48 B per triangle test, 32 B
+    # per top-level record, 32 B ray read + 20 B hit write per ray
+    alg_bytes = 64.0 * prof.ext_bnodes + 48.0 * prof.ext_tris + 32.0 * prof.ext_top + 52.0 * ext_rays
     launch_ms = timed.extend_ms / max(1, timed.extend_launches)
+    rays_per_launch = ext_rays / max(1, prof.extend_launches)
     bytes_per_launch = alg_bytes / max(1, prof.extend_launches)
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9 if launch_ms > 0 else None
     peak, peak_kind = measured_peak()
-    tr = profile_traffic()
-    traffic = tr * ext_rays / max(1, prof.extend_launches) if tr else None
+    pc = profile_counters()
+    traffic = pc["dram"] * rays_per_launch if "dram" in pc else None
+    l2_gbs = pc["l2"] * rays_per_launch / (launch_ms * 1e-3) / 1e9 if ("l2" in pc and launch_ms > 0) else None
+
+    # the drop-in per frame as a host glue would run it: scene description, luz_gpu_scene_create
+    # (host BVH build + upload), one render with a host film, destroy
+    glue = None
+    if rank == 0:
+        t0 = time.perf_counter()
+        b2 = w.scene.build()
+        t1 = time.perf_counter()
+        g2 = native.GpuScene(b2, device=local)
+        t2 = time.perf_counter()
+        _, st2 = g2.render(p)
+        t3 = time.perf_counter()
+        g2.close()
+        t4 = time.perf_counter()
+        glue = {"describe_ms": (t1 - t0) * 1e3, "scene_create_ms": (t2 - t1) * 1e3,
+                "render_ms": (t3 - t2) * 1e3, "destroy_ms": (t4 - t3) * 1e3, "total_ms": (t4 - t0) * 1e3,
+                "msamples_per_s": float(npix) * w.spp / ((t4 - t0) * 1e3) / 1e3,
+                "what": "scene handle created and destroyed around one render (host wall clock)"}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -300,13 +350,20 @@ def run_ours(args):
                             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                             "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
                             "algorithmic_bytes_per_ray": alg_bytes / max(1.0, ext_rays),
-                            "rays_per_launch": ext_rays / max(1, prof.extend_launches),
+                            "bytes_formula": "64 x binary node visits + 48 x triangle tests + 32 x top-level "
+                                             "records + 52 per ray",
+                            "rays_per_launch": rays_per_launch,
                             "launch_ms": launch_ms,
-                            "traffic_source": "ncu dram bytes per extension ray (profiles/launches_mesh_glossy_2spp.md)"
-                                              " x rays per launch"},
+                            "traffic_source": "ncu dram bytes per extension ray x rays per launch "
+                                              "(profiles/k_extend_counters_mesh_glossy.md)",
+                            "l2_gbs": l2_gbs, "l2_frac": pc.get("l2_frac"),
+                            "l2_source": "ncu lts__t_bytes per extension ray x rays per launch / live launch "
+                                         "time; l2_frac = lts__throughput pct of peak (same summary)",
+                            "simt_lanes": pc.get("lanes")},
                "stages_ms": {"extend": timed.extend_ms, "shade": timed.shade_ms, "shadow": timed.shadow_ms,
                              "total": timed.render_ms},
-               "mrays_per_s": (timed.extension_rays + timed.shadow_rays) / timed.render_ms / 1e3 * world}
+               "mrays_per_s": (timed.extension_rays + timed.shadow_rays) / timed.render_ms / 1e3 * world,
+               "dropin_frame": glue}
         if world == 1 and not args.no_cpu_baseline:
             cb, why = cpu_baseline(w, os.cpu_count() or 1)
             out["cpu_baseline"] = cb if cb else {"value": None, "unavailable": why}

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LUZ_GPU_ABI_VERSION 3
+#define LUZ_GPU_ABI_VERSION 4
 
 /* status codes */
 #define LUZ_OK            0
@@ -254,6 +254,8 @@ typedef struct LuzRenderStats {
     double   denoise_ms;          /* luz_gpu_render_denoised: device time of NFOR    */
     double   caustic_photons;     /* photons stored in the caustic map (photonCount) */
     double   caustic_ms;          /* device time of the caustic map build            */
+    double   ext_bnodes, sh_bnodes;   /* LUZ_RENDER_COUNT: binary mesh-BVH node visits the */
+                                      /* collapsed walks stand for (ext / shadow)          */
 } LuzRenderStats;
 
 /* One closest-hit / any-hit result (luz_gpu_trace_rays). */
@@ -313,6 +315,24 @@ int luz_pack_array(const luz_scene_pack* pack, const char* name, const void** da
 int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene** out);
 int luz_gpu_scene_destroy(luz_gpu_scene* scene);
 int luz_gpu_scene_info(const luz_gpu_scene* scene, LuzSceneInfo* info);
+/* Caps the path state (the SoA arrays of one wave, 268 bytes per path, 316
+ * with NFOR features) the handle may hold, in bytes; -1 restores the default,
+ * a quarter of the device memory free (plus what the handle holds) when a
+ * render allocates. Renders split into more, smaller waves under a lower cap
+ * (the film does not depend on the wave size); when cudaMalloc refuses a wave
+ * the render halves it, down to 2^20 paths, before it reports LUZ_E_CUDA. A
+ * cap below what the handle holds releases the held state. No counterpart in
+ * the reference (it keeps one sample's state per thread). */
+int luz_gpu_scene_set_path_budget(luz_gpu_scene* scene, int64_t bytes);
+/* Lowers the traversal stack bounds the kernels enforce: mesh_entries entries
+ * of the collapsed mesh-BVH stack (compiled: 192) and top_entries of the
+ * top-level stack (compiled: 96); 0 restores the compiled size. A ray that
+ * needs more stops its walk, the kernel sets the scene's device error word and
+ * the call reports LUZ_E_DEVICE; the next call starts clean. The compiled sizes
+ * hold every BVH the packer accepts (Mesh.cpp's 128-entry stack bound is
+ * checked at luz_gpu_scene_create); lower bounds exercise the overflow path.
+ * The reference's counterpart is the fixed stack of Mesh::hit (Mesh.cpp:578-660). */
+int luz_gpu_scene_set_traversal_limits(luz_gpu_scene* scene, int32_t mesh_entries, int32_t top_entries);
 
 /* ---- hot path ------------------------------------------------------------- */
 /* Full render: W*H*spp paths through the wavefront integrator; rgb_out is the
@@ -335,20 +355,24 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
  * For callers that cannot call cudaMalloc while they render: a host whose
  * device memory is owned by its own allocator, or a per-frame loop that must
  * not take the implicit device synchronisation that cudaMalloc/cudaFree cause.
- * Same result as luz_gpu_render_device (same kernels, same FP64 film), but the
- * path state, queues and film live in one file-scope device array of
- * LUZ_STATIC_SCRATCH_BYTES that every GPU loading this library holds until
- * process exit; the caller passes the scene (created beforehand), the device
- * film and the stream. Limits: width*height <= LUZ_STATIC_MAX_PIXELS, otherwise
- * LUZ_E_LIMIT; flags must be 0. The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress), so make that first call before any
- * stream capture. All calls share the array and it keeps the previous call's
- * contents: calls whose GPU work overlaps (other streams, other threads) race
- * on it and must be serialised by the caller.
+ * Same result as luz_gpu_render_device (same kernels, shading binned by hit
+ * class, same FP64 film), but the path state, queues, shade bins and film live
+ * in one file-scope device array of LUZ_STATIC_SCRATCH_BYTES that every GPU
+ * loading this library holds until process exit; waves are
+ * LUZ_STATIC_WAVE_PATHS paths. The caller passes the scene (created
+ * beforehand), the device film and the stream. Limits: width*height <=
+ * LUZ_STATIC_MAX_PIXELS, otherwise LUZ_E_LIMIT; flags must be 0. The call
+ * returns once the render has finished on the stream (it waits for the
+ * stream to read the ray totals and the error word into the handle's pinned
+ * buffer). The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array and it keeps the previous call's contents: calls
+ * whose GPU work overlaps (other streams, other threads) race on it and must
+ * be serialised by the caller.
  * No counterpart in the reference: the CPU renderer has no device memory. */
 #define LUZ_STATIC_SCRATCH_BYTES (96u << 20)
 #define LUZ_STATIC_WAVE_PATHS    131072
-#define LUZ_STATIC_MAX_PIXELS    2900000
+#define LUZ_STATIC_MAX_PIXELS    2800000
 int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* params,
                                   float* d_rgb_out, void* stream, LuzRenderStats* stats);
 
@@ -410,7 +434,7 @@ int luz_gpu_adjoint_emission(luz_gpu_scene* scene, const LuzRenderParams* params
 int luz_gpu_adjoint_density(luz_gpu_scene* scene, const LuzRenderParams* params, int32_t object,
                             const float* adjoint_rgb, double* grad_out, LuzRenderStats* stats);
 
-/* Adaptive sampling settings:/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
+/* Adaptive sampling settings: Scene::setAdaptiveSampling / setAdaptiveMinSamples /
  * setAdaptiveCheckInterval / setAdaptiveThreshold (src/scene/Scene.cpp:183-222),
  * defaults include/luz/Defaults.hpp:12-15 (on, 128, 32, 0.03). */
 typedef struct LuzAdaptiveParams {

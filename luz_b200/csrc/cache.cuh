@@ -144,6 +144,9 @@ __device__ __forceinline__ void cache_forward(const __half* Wf, const uint32_t (
 
 }  // namespace luz
 
+// The cache kernels are defined in the unit that launches them (integrator.cu);
+// the shade unit (shade_kernels.cu) only needs the device-side inference above.
+#ifndef LUZ_NO_CACHE_KERNELS
 namespace luz {
 
 // FP16 copies of W: forward Wf[n][K + 8] and backward Wb[k][N + 8] per layer.
@@ -403,3 +406,4 @@ __global__ void k_cache_adam(float* W, float* G, float* m, float* v, float lr, f
 }
 
 }  // namespace luz
+#endif  // LUZ_NO_CACHE_KERNELS

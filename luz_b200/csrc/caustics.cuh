@@ -65,7 +65,7 @@ struct Emission {
 // Rectangle / Sphere / Triangle / MeshInstance / directional sampleEmission
 // (Rectangle.cpp:421-454, Sphere.cpp:467-497, Mesh.cpp:942-985,
 // Triangle.cpp:434-470, MeshInstance.cpp:549-582, CausticPhotonMap.cpp:279-326).
-__device__ __noinline__ bool light_emission(const DScene& S, const GLight& L, const Key& k, Emission& e)
+static __device__ __noinline__ bool light_emission(const DScene& S, const GLight& L, const Key& k, Emission& e)
 {
     const F3 emitted = f3(L.emitted);
     switch (L.kind) {
@@ -205,7 +205,7 @@ __device__ __forceinline__ bool photon_roulette(F3& thr, int bounce, const Key& 
 }
 
 // CausticPhotonMap::estimate (:553-618) at a diffuse hit with its scatter record.
-__device__ __noinline__ F3 caustic_estimate(const DScene& S, const Hit& h, const Scatter& sr, const GMaterial& m, F3 ray_d)
+static __device__ __noinline__ F3 caustic_estimate(const DScene& S, const Hit& h, const Scatter& sr, const GMaterial& m, F3 ray_d)
 {
     const DCaustics& C = S.cm;
     const GCaustics& G = S.k.caustics;

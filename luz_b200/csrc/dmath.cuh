@@ -1,8 +1,10 @@
 // dmath.cuh — device vector helpers and the Luz sampler stream.
 //
-// The library is compiled with -fmad=false: every float/double expression
-// below rounds exactly as written, so the double-precision sampler reproduces
-// the reference bit for bit and the FP32 traversal matches its C restatement.
+// Traversal and ray generation are compiled with -fmad=false (integrator.cu),
+// so the FP32 traversal matches its C restatement bit for bit; the shade stage
+// (shade_kernels.cu) is compiled with FMA contraction. The sampler's FP64
+// lattice arithmetic is written with explicit round-to-nearest intrinsics, so
+// it reproduces the reference bit for bit in either unit.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -111,18 +113,19 @@ __device__ __forceinline__ double hashed(const Key& k, uint32_t dk, uint32_t com
     key ^= ((uint64_t)comp + 1ull) * 0xbf58476d1ce4e5b9ull;
     return unit53(splitmix64(key));
 }
-__device__ __noinline__ double sample1d(const Key& k, uint32_t dim)
+static __device__ __noinline__ double sample1d(const Key& k, uint32_t dim)
 {
     const uint32_t dk = dim + k.bounce * 32u;
     if (!progressive(dim)) return hashed(k, dk, 0);
     const double shift = unit24(ctx_key(k, dk));
     const double step = dim_step(dk, 0);
-    return fract(0.5 + ((double)k.sample + 1.0) * step + shift);
+    // fract(0.5 + (s + 1) * step + shift), each operation rounded on its own as the reference computes it
+    return fract(__dadd_rn(__dadd_rn(0.5, __dmul_rn((double)k.sample + 1.0, step)), shift));
 }
 struct S2 {
     float x, y;
 };
-__device__ __noinline__ S2 sample2d(const Key& k, uint32_t dim)
+static __device__ __noinline__ S2 sample2d(const Key& k, uint32_t dim)
 {
     const uint32_t dk = dim + k.bounce * 32u;
     if (!progressive(dim)) return S2{(float)hashed(k, dk, 0), (float)hashed(k, dk, 1)};
@@ -130,7 +133,8 @@ __device__ __noinline__ S2 sample2d(const Key& k, uint32_t dim)
     const double sx = unit24(key);
     const double sy = unit24(key ^ 0xda942042e4dd58b5ull);
     const double s = (double)k.sample + 1.0;
-    return S2{(float)fract(0.5 + s * dim_step(dk, 0) + sx), (float)fract(0.5 + s * dim_step(dk, 1) + sy)};
+    return S2{(float)fract(__dadd_rn(__dadd_rn(0.5, __dmul_rn(s, dim_step(dk, 0))), sx)),
+              (float)fract(__dadd_rn(__dadd_rn(0.5, __dmul_rn(s, dim_step(dk, 1))), sy))};
 }
 
 constexpr float kTwoPiF = 6.28318530717958647692f;   // static_cast<float>(2.0 * D_PI)

@@ -57,14 +57,11 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 // ---------------------------------------------------------------------------- extend (closest hit)
 
 // Resident blocks per SM the register allocator is asked to allow, measured on
-// B200 (1080p glossy frame, extend / shade / shadow stage): extend 5 blocks
-// (96 registers, almost no spills) 253 ms against 266 ms at 6 and 273 ms at 7;
-// shade 4 and shadow 8 ahead of 3 / 5 and 6 / 10.
+// B200 (1080p glossy frame, extend / shadow stage): extend 5 blocks (96
+// registers, almost no spills) 253 ms against 266 ms at 6 and 273 ms at 7;
+// shadow 8 ahead of 6 / 10 (shade: shade_kernels.cu).
 #ifndef LUZ_EXTEND_MIN_BLOCKS
 #define LUZ_EXTEND_MIN_BLOCKS 5
-#endif
-#ifndef LUZ_SHADE_MIN_BLOCKS
-#define LUZ_SHADE_MIN_BLOCKS 4
 #endif
 #ifndef LUZ_SHADOW_MIN_BLOCKS
 #define LUZ_SHADOW_MIN_BLOCKS 8
@@ -84,21 +81,12 @@ __device__ __forceinline__ void bin_append(uint32_t* bin_count, const PathBuf& P
     P.bins[cls * P.bin_stride + base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = p;
 }
 
-// Path of shade slot i: slots run through the class segments in class order.
-__device__ __forceinline__ uint32_t binned_path(const PathBuf& P, const uint32_t* bin, uint32_t i)
-{
-    uint32_t k = 0, start = 0;
-    while (k < kShadeClasses - 1 && i >= start + bin[k]) {
-        start += bin[k];
-        k++;
-    }
-    return P.bins[k * P.bin_stride + (i - start)];
-}
-
 // Extend and shadow are instantiated per scene feature set (TF_* bits:
 // instances, volumes); a scene without them runs traversal code without the
 // instance transform or the volume sampler, and skips the per-ray sampler key.
-template <uint32_t F>
+// COUNT instantiations add the record counts of LUZ_RENDER_COUNT; the others
+// carry no counting code at all.
+template <uint32_t F, bool COUNT>
 __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     LocalStack<true> st;
@@ -125,17 +113,18 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
         P.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.obj));
         P.hit_prim[p] = h.prim;
         if (P.bins) bin_append(C->bin[bounce], P, vmask, h.obj < 0 ? 0u : (uint32_t)S.obj_class[h.obj], p);
-        if (S.counters) {
+        if constexpr (COUNT) {
             atomicAdd(&S.counters[0], (unsigned long long)vs.nodes);
             atomicAdd(&S.counters[1], (unsigned long long)vs.tris);
             atomicAdd(&S.counters[2], (unsigned long long)vs.top);
+            atomicAdd(&S.counters[6], (unsigned long long)vs.bnodes);
         }
     }
 }
 
 // ---------------------------------------------------------------------------- shadow (any hit)
 
-template <uint32_t F>
+template <uint32_t F, bool COUNT>
 __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     LocalStack<false> st;
@@ -162,54 +151,21 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene
             if (tag & 0x80000000u) P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
             else P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (S.counters) {
+        if constexpr (COUNT) {
             atomicAdd(&S.counters[3], (unsigned long long)vs.nodes);
             atomicAdd(&S.counters[4], (unsigned long long)vs.tris);
             atomicAdd(&S.counters[5], (unsigned long long)vs.top);
+            atomicAdd(&S.counters[7], (unsigned long long)vs.bnodes);
         }
     }
 }
 
 using TraceKernel = void (*)(DScene, WaveArgs, PathBuf, Ctrl*, int);
-const TraceKernel kExtendKernels[4] = {k_extend<0>, k_extend<1>, k_extend<2>, k_extend<3>};
-const TraceKernel kShadowKernels[4] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>};
+const TraceKernel kExtendKernels[2][4] = {{k_extend<0, false>, k_extend<1, false>, k_extend<2, false>, k_extend<3, false>},
+                                          {k_extend<0, true>, k_extend<1, true>, k_extend<2, true>, k_extend<3, true>}};
+const TraceKernel kShadowKernels[2][4] = {{k_shadow<0, false>, k_shadow<1, false>, k_shadow<2, false>, k_shadow<3, false>},
+                                          {k_shadow<0, true>, k_shadow<1, true>, k_shadow<2, true>, k_shadow<3, true>}};
 
-template <int MODE>
-__global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
-{
-    const DScene& S = *Sp;
-    const uint32_t count = C->count[bounce];
-    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
-    uint32_t* nq = (bounce & 1) ? P.queue0 : P.queue1;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    for (uint32_t base = wid * 32u; base < count; base += warps * 32u) {
-        const uint32_t i = base + lane_id();
-        const bool valid = i < count;
-        ShadeOut o;
-        o.cont = false;
-        o.sh[0] = o.sh[1] = false;
-        uint32_t p = 0;
-        if (valid) {
-            p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
-            shade_path<MODE>(S, w, P, p, bounce, o);
-        }
-        __syncwarp();
-        const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
-        if (o.cont) nq[qi] = p;
-        for (int slot = 0; slot < 2; slot++) {
-            const uint32_t si = warp_append(&C->shadow[bounce], o.sh[slot]);
-            if (o.sh[slot]) {
-                P.sh_o[si] = make_float4(o.sh_o[slot].x, o.sh_o[slot].y, o.sh_o[slot].z, o.sh_t[slot]);
-                P.sh_d[si] = make_float4(o.sh_d[slot].x, o.sh_d[slot].y, o.sh_d[slot].z,
-                                         __uint_as_float(p | ((uint32_t)slot << 31)));
-                P.sh_x[si] = make_int2(o.xobj, o.xprim);
-            }
-        }
-    }
-}
-
-using ShadeKernel = void (*)(const DScene*, WaveArgs, PathBuf, Ctrl*, int);
 
 // Adds one wave's per-bounce queue sizes to the render totals (no host wait per wave).
 __global__ void k_tally(const Ctrl* C, int max_b, unsigned long long* totals)
@@ -709,6 +665,7 @@ struct luz_gpu_scene {
     std::vector<void*> pallocs;
     Ctrl* ctrl = nullptr;
     Ctrl* ctrl_host = nullptr;
+    unsigned long long* status_host = nullptr;   // pinned: ray totals [0..1] and error word [2] of a call
     unsigned long long* totals = nullptr;   // device: extension / shadow rays of the current render
     double* film = nullptr;
     int64_t film_pix = 0;
@@ -755,11 +712,16 @@ struct luz_gpu_scene {
         pallocs.clear();
         cap = 0;
     }
-    void ensure_paths(int64_t n, bool feat = false)
+    // Bytes of path state per path: the PathBuf arrays a wave allocates (NFOR
+    // features add 3 float4).
+    static constexpr int64_t kPathBytes = 8 * 16 + 5 * 4 + 2 * (16 + 16 + 8) + kShadeClasses * 4;
+    static constexpr int64_t kFeatBytes = 3 * 16;
+    // Smallest wave a render falls back to when cudaMalloc refuses a larger one.
+    static constexpr int64_t kMinWavePaths = int64_t(1) << 20;
+    int64_t path_budget = -1;        // bytes of path state this handle may hold; -1 = a quarter of
+                                     // the device memory free (plus what the handle holds) at the time
+    void alloc_paths(int64_t n, bool feat)
     {
-        if (n <= cap && (!feat || pb.feat)) return;
-        n = std::max(n, cap);
-        free_paths();
         pb.ray_o = palloc<float4>(n);
         pb.ray_d = palloc<float4>(n);
         pb.thr = palloc<float4>(n);
@@ -781,6 +743,39 @@ struct luz_gpu_scene {
         pb.bin_stride = (uint32_t)n;
         cap = n;
     }
+    // Paths a wave of up to `want` paths may use: the buffers held when they are
+    // large enough, else new ones of min(want, budget) paths. When cudaMalloc
+    // refuses them (memory held by other work on the device) the request is
+    // halved, down to kMinWavePaths, so the render runs in more, smaller waves
+    // (the image does not depend on the wave size). Returns the paths available.
+    int64_t reserve_paths(int64_t want, bool feat = false)
+    {
+        want = std::max<int64_t>(1, want);
+        const int64_t per = kPathBytes + (feat ? kFeatBytes : 0);
+        int64_t budget = path_budget;
+        if (budget < 0) {
+            size_t free_b = 0, total_b = 0;
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            const int64_t held = cap * (kPathBytes + (pb.feat ? kFeatBytes : 0));
+            budget = ((int64_t)free_b + held) / 4;
+        }
+        int64_t n = std::min(want, std::max<int64_t>(1, budget / per));
+        if (n <= cap && (!feat || pb.feat)) return n;
+        const int64_t floor_n = std::min(n, kMinWavePaths);
+        n = std::max(n, std::min(cap, want));
+        free_paths();
+        while (true) {
+            try {
+                alloc_paths(n, feat);
+                return n;
+            } catch (const Status& e) {
+                free_paths();
+                (void)cudaGetLastError();   // clears the allocation error
+                if (e.code != LUZ_E_CUDA || n <= floor_n) throw;
+                n = std::max(floor_n, n / 2);
+            }
+        }
+    }
     ~luz_gpu_scene()
     {
         cudaSetDevice(device);
@@ -791,6 +786,7 @@ struct luz_gpu_scene {
         for (void* p : allocs) cudaFree(p);
         if (ctrl) cudaFree(ctrl);
         if (ctrl_host) cudaFreeHost(ctrl_host);
+        if (status_host) cudaFreeHost(status_host);
         if (film) cudaFree(film);
         if (dds) cudaFree(dds);
         if (totals) cudaFree(totals);
@@ -851,15 +847,18 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
 {
     const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
     if (!shade) shade = s->shade;
+    const int count = s->ds.counters ? 1 : 0;   // LUZ_RENDER_COUNT renders run the counting instantiations
+    const TraceKernel extend = kExtendKernels[count][s->ds.k.features & TF_ALL];
+    const TraceKernel shadow = kShadowKernels[count][s->ds.k.features & TF_ALL];
     for (int b = 0; b <= w.max_bounces; b++) {
         T.mark(st, 0, true);
-        s->extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
         shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
-        s->shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
         T.mark(st, 2, false);
         launches += 3;
     }
@@ -938,7 +937,8 @@ void prepare_caustics(luz_gpu_scene* s, const LuzRenderParams* p, cudaStream_t s
     CK(cudaMemcpyAsync(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (err & ERR_CAUSTIC_GRID) {
-        CK(cudaMemset(s->ds.error, 0, sizeof(uint32_t)));
+        CK(cudaMemsetAsync(s->ds.error, 0, sizeof(uint32_t), st));
+        CK(cudaStreamSynchronize(st));
         throw Status(LUZ_E_LIMIT, "Caustic photons lie outside the photon grid (2^21 cells per axis).");
     }
     int64_t T = 64;
@@ -981,6 +981,35 @@ void caustic_stats(const luz_gpu_scene* s, LuzRenderStats* stats)
     stats->caustic_ms = s->cm.last_ms;
 }
 
+// Every call clears the scene's device error word on its stream before it
+// enqueues work, and reads it back (finish_status) after the work: a flag set by
+// one call is reported by that call alone and leaves the handle usable.
+void clear_error(luz_gpu_scene* s, cudaStream_t st)
+{
+    CK(cudaMemsetAsync(s->ds.error, 0, sizeof(uint32_t), st));
+}
+
+// After a call's work on st: copies the ray totals (when `totals` is given) and
+// the error word into the handle's pinned status buffer, clears the word, waits
+// for st and throws LUZ_E_DEVICE when a kernel set a flag.
+void finish_status(luz_gpu_scene* s, cudaStream_t st, const unsigned long long* totals = nullptr,
+                   unsigned long long* tot_out = nullptr)
+{
+    unsigned long long* h = s->status_host;
+    h[0] = h[1] = h[2] = 0;
+    if (totals) CK(cudaMemcpyAsync(h, totals, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h + 2, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemsetAsync(s->ds.error, 0, sizeof(uint32_t), st));
+    CK(cudaStreamSynchronize(st));
+    if (tot_out) {
+        tot_out[0] = h[0];
+        tot_out[1] = h[1];
+    }
+    const uint32_t err = (uint32_t)h[2];
+    if (err)
+        throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+}
+
 void finish_wave(luz_gpu_scene* s, cudaStream_t st, LuzRenderStats* acc, int max_b)
 {
     CK(cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
@@ -991,9 +1020,7 @@ void finish_wave(luz_gpu_scene* s, cudaStream_t st, LuzRenderStats* acc, int max
             acc->shadow_rays += s->ctrl_host->shadow[b];
         }
     }
-    uint32_t err = 0;
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st);
 }
 
 // One render split in three phases so that a batch can allocate for every
@@ -1019,12 +1046,13 @@ void render_prepare(RenderJob& J)
     luz_gpu_scene* s = J.s;
     check_params(p);
     CK(cudaSetDevice(s->device));
+    clear_error(s, J.st);
     prepare_caustics(s, p, J.st);
     J.w = base_args(s, p);
     J.npix = (int64_t)p->width * p->height;
-    J.s_wave = (int)std::min<int64_t>(p->spp, J.wave_target);
-    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, J.wave_target / J.s_wave));
-    s->ensure_paths(J.pix_wave * J.s_wave);
+    const int64_t n = s->reserve_paths(std::min<int64_t>(J.wave_target, J.npix * (int64_t)p->spp));
+    J.s_wave = (int)std::min<int64_t>(p->spp, n);
+    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, n / J.s_wave));
     if (s->film_pix < J.npix) {
         if (s->film) cudaFree(s->film);
         s->film = nullptr;
@@ -1043,6 +1071,7 @@ void render_enqueue(RenderJob& J)
     const cudaStream_t st = J.st;
     WaveArgs& w = J.w;
     CK(cudaSetDevice(s->device));
+    clear_error(s, st);
     if (J.counters) CK(cudaMemsetAsync(J.counters, 0, 8 * sizeof(unsigned long long), st));
     s->ds.counters = J.counters;
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
@@ -1088,10 +1117,7 @@ void render_finish(RenderJob& J, LuzRenderStats* stats)
     LuzRenderStats acc{};
     {
         unsigned long long tot[2] = {0, 0};
-        uint32_t err = 0;
-        CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+        finish_status(s, J.st, s->totals, tot);
         acc.extension_rays = (double)tot[0];
         acc.shadow_rays = (double)tot[1];
     }
@@ -1122,6 +1148,8 @@ void render_finish(RenderJob& J, LuzRenderStats* stats)
         stats->sh_nodes = (double)cnt[3];
         stats->sh_tris = (double)cnt[4];
         stats->sh_top = (double)cnt[5];
+        stats->ext_bnodes = (double)cnt[6];
+        stats->sh_bnodes = (double)cnt[7];
         caustic_stats(s, stats);
     }
 }
@@ -1199,6 +1227,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     const cudaStream_t st = s->stream;
     const int64_t npix = (int64_t)p->width * p->height;
     if (npix > (int64_t)UINT32_MAX) throw Status(LUZ_E_LIMIT, "Image has too many pixels.");
+    clear_error(s, st);
     prepare_caustics(s, p, st);
 
     AdaptiveRule R{};
@@ -1250,9 +1279,9 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
         max_round = std::max(max_round, e - prev);
         prev = e;
     }
-    const int s_wave = (int)std::min<int64_t>(max_round, kWaveTarget);
-    const int64_t n_wave = std::max<int64_t>(s_wave, std::min<int64_t>(npix * s_wave, kWaveTarget));
-    s->ensure_paths(n_wave, want_nfor);
+    const int64_t n_wave =
+        s->reserve_paths(std::min<int64_t>(kWaveTarget, npix * (int64_t)std::max<uint32_t>(1u, max_round)), want_nfor);
+    const int s_wave = (int)std::min<int64_t>(max_round, n_wave);
     CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
     CK(cudaEventRecord(s->ev0, st));
 
@@ -1265,7 +1294,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
         if (n_act == 0) break;
         const int round = (int)(e - done_to);
         const int sc_max = std::min(round, s_wave);
-        const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(n_act, kWaveTarget / sc_max));
+        const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(n_act, n_wave / sc_max));
         w.pix_list = act[cur];
         for (int sb = 0; sb < round; sb += sc_max) {          // sample chunks in order: sums stay sequential
             const int sc = std::min(sc_max, round - sb);
@@ -1303,10 +1332,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     unsigned long long tot[2] = {0, 0};
-    uint32_t err = 0;
-    CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st, s->totals, tot);
     CK(cudaMemcpy(rgb_out, d_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
     if (samples_out) CK(cudaMemcpy(samples_out, d_used, sizeof(int32_t) * (std::size_t)npix, cudaMemcpyDeviceToHost));
     if (nfor) {
@@ -1395,6 +1421,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
         throw Status(LUZ_E_UNSUPPORTED, "A texture differentiated as both albedo and roughness is not supported.");
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
+    clear_error(s, st);
     const GTexture& T = PK.textures[(std::size_t)texture];
     const int64_t npix = (int64_t)p->width * p->height, ntex = (int64_t)T.width * T.height;
     DeviceScratch D;
@@ -1409,9 +1436,9 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     w.adj_rgb = d_adj;
     w.grad = d_grad;
     w.inv_spp = 1.0 / (double)p->spp;
-    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
-    s->ensure_paths(pix_wave * s_wave);
+    const int64_t n_wave = s->reserve_paths(std::min<int64_t>(kWaveTarget, npix * (int64_t)p->spp));
+    const int s_wave = (int)std::min<int64_t>(p->spp, n_wave);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, n_wave / s_wave));
     w.adj_rough = rough ? D.get<AdjRough>(pix_wave * s_wave, st) : nullptr;
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(s->ev0, st));
@@ -1432,7 +1459,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
                 CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
                 if (pass == 1 && rough) CK(cudaMemsetAsync(w.adj_rough, 0, sizeof(AdjRough) * (std::size_t)w.n, st));
                 k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-                launch_bounces(s, w, st, launches, T0, k_shade<3>);
+                launch_bounces(s, w, st, launches, T0, shade_kernel(3));
                 launches++;
                 if (pass == 0) {
                     k_path_color<<<grid, kBlock, 0, st>>>(w, s->pb);
@@ -1448,9 +1475,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
     CK(cudaGetLastError());
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaEventSynchronize(s->ev1));
-    uint32_t err = 0;
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st);
     CK(cudaMemcpy(grad_out, d_grad, sizeof(double) * 3 * (std::size_t)ntex, cudaMemcpyDeviceToHost));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
@@ -1476,6 +1501,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     const int64_t nl = s->pack->consts.light_count;
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
+    clear_error(s, st);
     const int64_t npix = (int64_t)p->width * p->height;
     DeviceScratch D;
     float* d_adj = D.get<float>(3 * npix, st);
@@ -1489,9 +1515,9 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     w.grad_light = d_grad;
     w.adj_rgb = d_adj;
     w.inv_spp = 1.0 / (double)p->spp;
-    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
-    s->ensure_paths(pix_wave * s_wave);
+    const int64_t n_wave = s->reserve_paths(std::min<int64_t>(kWaveTarget, npix * (int64_t)p->spp));
+    const int s_wave = (int)std::min<int64_t>(p->spp, n_wave);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, n_wave / s_wave));
     w.pend_light = D.get<int32_t>(pix_wave * s_wave, st);
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(s->ev0, st));
@@ -1511,7 +1537,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(w.pend_light, 0xff, sizeof(int32_t) * (std::size_t)w.n, st));
             k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, launches, T0, k_shade<3>);
+            launch_bounces(s, w, st, launches, T0, shade_kernel(3));
             k_adjoint_emission_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
             launches += 2;
             waves++;
@@ -1520,9 +1546,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
     CK(cudaGetLastError());
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaEventSynchronize(s->ev1));
-    uint32_t err = 0;
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st);
     if (nl > 0) {
         std::vector<double> rep((std::size_t)(kEmissionReplicas * 3 * nl));
         CK(cudaMemcpy(rep.data(), d_grad, sizeof(double) * rep.size(), cudaMemcpyDeviceToHost));
@@ -1559,6 +1583,7 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
     if (PK.objects[(std::size_t)gi].kind != OK_VOLUME) throw Status(LUZ_E_INVALID, "The object is not a volume.");
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
+    clear_error(s, st);
     const int64_t npix = (int64_t)p->width * p->height;
     DeviceScratch D;
     float* d_adj = D.get<float>(3 * npix, st);
@@ -1572,9 +1597,9 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
     w.grad_density = d_grad;
     w.adj_rgb = d_adj;
     w.inv_spp = 1.0 / (double)p->spp;
-    const int s_wave = (int)std::min<int64_t>(p->spp, kWaveTarget);
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kWaveTarget / s_wave));
-    s->ensure_paths(pix_wave * s_wave);
+    const int64_t n_wave = s->reserve_paths(std::min<int64_t>(kWaveTarget, npix * (int64_t)p->spp));
+    const int s_wave = (int)std::min<int64_t>(p->spp, n_wave);
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, n_wave / s_wave));
     w.dens_score = D.get<float2>(pix_wave * s_wave, st);
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(s->ev0, st));
@@ -1594,7 +1619,7 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(w.dens_score, 0, sizeof(float2) * (std::size_t)w.n, st));
             k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, launches, T0, k_shade<3>);
+            launch_bounces(s, w, st, launches, T0, shade_kernel(3));
             k_adjoint_density_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
             launches += 2;
             waves++;
@@ -1603,9 +1628,7 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
     CK(cudaGetLastError());
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaEventSynchronize(s->ev1));
-    uint32_t err = 0;
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st);
     std::vector<double> rep(kEmissionReplicas);
     CK(cudaMemcpy(rep.data(), d_grad, sizeof(double) * rep.size(), cudaMemcpyDeviceToHost));
     double acc = 0.0;
@@ -1673,6 +1696,9 @@ StaticArena carve_static(unsigned char* base)
     P.sh_d = reinterpret_cast<float4*>(take(2 * n * sizeof(float4)));
     P.sh_x = reinterpret_cast<int2*>(take(2 * n * sizeof(int2)));
     P.color = nullptr;   // used by trace_paths only
+    P.feat = nullptr;
+    P.bins = reinterpret_cast<uint32_t*>(take((std::size_t)kShadeClasses * n * sizeof(uint32_t)));
+    P.bin_stride = (uint32_t)n;
     A.ctrl = reinterpret_cast<Ctrl*>(take(sizeof(Ctrl)));
     A.totals = reinterpret_cast<unsigned long long*>(take(2 * sizeof(unsigned long long)));
     A.film = reinterpret_cast<double*>(base + off);
@@ -1709,6 +1735,7 @@ int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, 
     if (npix > LUZ_STATIC_MAX_PIXELS || npix > A.film_pixels)
         throw Status(LUZ_E_LIMIT, "Image of " + std::to_string(npix) + " pixels exceeds the static film of " +
                                       std::to_string((long long)LUZ_STATIC_MAX_PIXELS) + " pixels.");
+    clear_error(s, st);
     WaveArgs w = base_args(s, p);
     const int64_t target = LUZ_STATIC_WAVE_PATHS;
     const int s_wave = (int)std::min<int64_t>(p->spp, target);
@@ -1749,10 +1776,7 @@ int do_render_noalloc(luz_gpu_scene* s, const LuzRenderParams* p, float* d_out, 
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaEventSynchronize(s->ev1));
     unsigned long long tot[2] = {0, 0};
-    uint32_t err = 0;
-    CK(cudaMemcpy(tot, A.totals, sizeof(tot), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st, A.totals, tot);
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     if (stats) {
@@ -1838,20 +1862,23 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         s->allocs.push_back(err);
         d.error = err;
         d.counters = nullptr;
+        d.mesh_stack_limit = kMeshStack4;
+        d.top_stack_limit = kTopStack;
         d.k = P.consts;
         s->dds = dalloc<DScene>(1);
         CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
         s->ctrl = dalloc<Ctrl>(1);
         s->totals = dalloc<unsigned long long>(2);
         CK(cudaMallocHost(&s->ctrl_host, sizeof(Ctrl)));
+        CK(cudaMallocHost(&s->status_host, 4 * sizeof(unsigned long long)));
         cudaDeviceProp prop;
         CK(cudaGetDeviceProperties(&prop, device));
         s->sms = prop.multiProcessorCount;
         const int feat = P.consts.features & TF_ALL;
-        s->extend = kExtendKernels[feat];
-        s->shadow = kShadowKernels[feat];
+        s->extend = kExtendKernels[0][feat];
+        s->shadow = kShadowKernels[0][feat];
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, s->extend, kBlock, 0));
-        s->shade = P.consts.caustics.enabled ? k_shade<1> : k_shade<0>;
+        s->shade = shade_kernel(P.consts.caustics.enabled ? 1 : 0);
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, s->shade, kBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_sh, s->shadow, kBlock, 0));
         s->occ_ext = std::max(1, s->occ_ext);
@@ -1880,6 +1907,37 @@ int luz_gpu_scene_info(const luz_gpu_scene* s, LuzSceneInfo* info)
         info->device_bytes = P.device_bytes();
         info->max_mesh_depth = P.max_mesh_depth;
         info->light_count = P.consts.light_count;
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_scene_set_path_budget(luz_gpu_scene* s, int64_t bytes)
+{
+    return guard([&] {
+        if (!s) throw Status(LUZ_E_INVALID, "NULL argument.");
+        if (bytes < -1) throw Status(LUZ_E_INVALID, "Path budget must be -1 (default) or non-negative.");
+        s->path_budget = bytes;
+        const int64_t held = s->cap * (luz_gpu_scene::kPathBytes + (s->pb.feat ? luz_gpu_scene::kFeatBytes : 0));
+        if (bytes >= 0 && held > bytes) {   // release path state above the new budget
+            CK(cudaSetDevice(s->device));
+            CK(cudaStreamSynchronize(s->stream));
+            s->free_paths();
+        }
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_scene_set_traversal_limits(luz_gpu_scene* s, int32_t mesh_entries, int32_t top_entries)
+{
+    return guard([&] {
+        if (!s) throw Status(LUZ_E_INVALID, "NULL argument.");
+        if (mesh_entries < 0 || mesh_entries > kMeshStack4 || top_entries < 0 || top_entries > kTopStack)
+            throw Status(LUZ_E_INVALID, "Traversal limits must lie in [0, the compiled stack sizes].");
+        CK(cudaSetDevice(s->device));
+        CK(cudaStreamSynchronize(s->stream));
+        s->ds.mesh_stack_limit = mesh_entries ? mesh_entries : kMeshStack4;
+        s->ds.top_stack_limit = top_entries ? top_entries : kTopStack;
+        CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
         return LUZ_OK;
     });
 }
@@ -2055,9 +2113,9 @@ int luz_gpu_trace_paths(luz_gpu_scene* s, const LuzRenderParams* p, const int32_
                 throw Status(LUZ_E_INVALID, "Path coordinates out of range.");
         CK(cudaSetDevice(s->device));
         cudaStream_t st = s->stream;
+        clear_error(s, st);
         prepare_caustics(s, p, st);
-        const int64_t chunk = std::min<int64_t>(count, kWaveTarget);
-        s->ensure_paths(chunk);
+        const int64_t chunk = s->reserve_paths(std::min<int64_t>(count, kWaveTarget));
         int32_t* dx = dalloc<int32_t>(chunk);
         int32_t* dy = dalloc<int32_t>(chunk);
         int32_t* dsm = dalloc<int32_t>(chunk);
@@ -2115,16 +2173,14 @@ int luz_gpu_trace_rays(luz_gpu_scene* s, const float* rays, int64_t count, int32
         LuzHit* dh = dalloc<LuzHit>((std::size_t)count);
         int32_t* dk = volume_key ? dalloc<int32_t>((std::size_t)(4 * count)) : nullptr;
         try {
+            clear_error(s, st);
             CK(cudaMemcpyAsync(dr, rays, sizeof(float) * 8 * count, cudaMemcpyHostToDevice, st));
             if (dk) CK(cudaMemcpyAsync(dk, volume_key, sizeof(int32_t) * 4 * count, cudaMemcpyHostToDevice, st));
             kTraceRayKernels[s->ds.k.features & TF_ALL]<<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
                 s->ds, dr, count, any_hit, seed, dk, dh);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(out, dh, sizeof(LuzHit) * count, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            uint32_t err = 0;
-            CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-            if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device.");
+            finish_status(s, st);
         } catch (...) {
             cudaFree(dr);
             cudaFree(dh);
@@ -2238,12 +2294,13 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     if (c->device != s->device) throw Status(LUZ_E_INVALID, "The cache and the scene are on different devices.");
     CK(cudaSetDevice(s->device));
     const cudaStream_t st = s->stream;
+    clear_error(s, st);
     const int64_t npix = (int64_t)p->width * p->height;
     // waves as the plain render makes them (samples inner), one cache update per wave
-    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, kCacheWaveTarget / npix));
-    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, kCacheWaveTarget / s_wave));
+    const int64_t n_cap = s->reserve_paths(std::min<int64_t>(kCacheWaveTarget, npix * (int64_t)p->spp));
+    const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, n_cap / npix));
+    const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, n_cap / s_wave));
     const int64_t n_wave = pix_wave * s_wave;
-    s->ensure_paths(n_wave);
     DeviceScratch D;
     CacheRecord* q = D.get<CacheRecord>(n_wave, st);
     CacheRecord* rows = D.get<CacheRecord>(n_wave, st);
@@ -2252,7 +2309,7 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     uint32_t* counts = D.get<uint32_t>(2, st);
     double* film = D.get<double>(3 * npix, st);
     float* d_out = D.get<float>(3 * npix, st);
-    static const ShadeKernel shade_cached = k_shade<2>;
+    const ShadeKernel shade_cached = shade_kernel(2);
     int occ = 1;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_cached, kBlock, 0));
     occ = std::max(1, occ);
@@ -2325,10 +2382,7 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     unsigned long long tot[2] = {0, 0};
-    uint32_t err = 0;
-    CK(cudaMemcpy(tot, s->totals, sizeof(tot), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&err, s->ds.error, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (err) throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (flags " + std::to_string(err) + ").");
+    finish_status(s, st, s->totals, tot);
     CK(cudaMemcpy(rgb_out, d_out, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
     if (stats) {
         *stats = LuzRenderStats{};

@@ -77,7 +77,7 @@ __device__ __forceinline__ void sphere_cube_cross_uv(const F3& n, float& u, floa
 }
 
 // Triangle::hit shading (Triangle.cpp:234-269) in the frame of ray r.
-__device__ void triangle_shading(const DScene& S, const GMesh& M, int32_t slot, float bu, float bv, const F3& d,
+static __device__ void triangle_shading(const DScene& S, const GMesh& M, int32_t slot, float bu, float bv, const F3& d,
                                  F3& n, F3& gn, bool& front, float& u, float& v)
 {
     const float4 fs = __ldg(reinterpret_cast<const float4*>(S.tri_shade + slot));
@@ -116,7 +116,7 @@ __device__ __forceinline__ F3 transform_normal(const GObject& O, F3 n)
 // alone enlarges this out-of-line function's frame and slowed the shade stage
 // by 3.5% on scenes without such spheres).
 template <bool XUV>
-__device__ __noinline__ Hit make_hit_t(const DScene& S, const TRay& r, const THit& th)
+static __device__ __noinline__ Hit make_hit_t(const DScene& S, const TRay& r, const THit& th)
 {
     Hit h;
     const GObject O = S.objects[th.obj];
@@ -204,7 +204,7 @@ __device__ __forceinline__ float wrap01f(float v)
     if (v < 0.0f) v += 1.0f;
     return v;
 }
-__device__ __noinline__ F3 texture_sample(const DScene& S, int32_t ti, float u, float v)
+static __device__ __noinline__ F3 texture_sample(const DScene& S, int32_t ti, float u, float v)
 {
     const GTexture T = S.textures[ti];
     u = wrap01f(u);
@@ -251,7 +251,7 @@ __device__ __forceinline__ F3 schlick(F3 f0, float cosT)
     f0 = clamp_color01(f0);
     return F3{f0.x + (1.0f - f0.x) * factor, f0.y + (1.0f - f0.y) * factor, f0.z + (1.0f - f0.z) * factor};
 }
-__device__ float dielectric_fresnel(float c, float ei, float et)
+static __device__ float dielectric_fresnel(float c, float ei, float et)
 {
     c = clamp01f(fabsf(c));
     if (!isfinite(ei) || !isfinite(et) || ei <= 0.0f || et <= 0.0f) return 1.0f;
@@ -263,7 +263,7 @@ __device__ float dielectric_fresnel(float c, float ei, float et)
     const float rpe = ((ei * c) - (et * ct)) / ((ei * c) + (et * ct));
     return clamp01f(0.5f * (rpa * rpa + rpe * rpe));
 }
-__device__ float conductor_channel(float e, float k, float c)
+static __device__ float conductor_channel(float e, float k, float c)
 {
     if (!isfinite(e) || !isfinite(k) || e <= 0.0f || k < 0.0f) return 0.0f;
     const float c2 = c * c, e2 = e * e, k2 = k * k;
@@ -281,7 +281,7 @@ __device__ __forceinline__ F3 conductor_fresnel(F3 eta, F3 k, float c)
     c = clamp01f(c);
     return F3{conductor_channel(eta.x, k.x, c), conductor_channel(eta.y, k.y, c), conductor_channel(eta.z, k.z, c)};
 }
-__device__ F3 sample_ggx_half(F3 n, float alpha, S2 s)
+static __device__ F3 sample_ggx_half(F3 n, float alpha, S2 s)
 {
     alpha = fmaxf(1e-4f, alpha);
     const float a2 = alpha * alpha;
@@ -313,7 +313,7 @@ __device__ __forceinline__ float ggx_g1(float now, float alpha)
     return 2.0f * now / den;
 }
 __device__ __forceinline__ float ggx_g(float nov, float nol, float a) { return ggx_g1(nov, a) * ggx_g1(nol, a); }
-__device__ float ggx_reflection_pdf(F3 n, F3 view, F3 dir, float alpha)
+static __device__ float ggx_reflection_pdf(F3 n, F3 view, F3 dir, float alpha)
 {
     const float nov = dot(n, view), nol = dot(n, dir);
     if (nov <= 0.0f || nol <= 0.0f) return 0.0f;
@@ -328,7 +328,7 @@ __device__ __forceinline__ F3 color_from_scale(F3 c, float s)
     if (!isfinite(s) || s <= 0.0f) return F3{0.f, 0.f, 0.f};
     return c * s;
 }
-__device__ F3 ggx_reflection_bsdfcos(F3 fres, F3 n, F3 view, F3 dir, float alpha)
+static __device__ F3 ggx_reflection_bsdfcos(F3 fres, F3 n, F3 view, F3 dir, float alpha)
 {
     const float nov = dot(n, view), nol = dot(n, dir);
     if (nov <= 0.0f || nol <= 0.0f) return F3{0.f, 0.f, 0.f};
@@ -349,7 +349,7 @@ __device__ __forceinline__ F3 ggx_conductor_bsdfcos(F3 eta, F3 k, F3 n, F3 view,
     const float voh = fmaxf(0.0f, dot(view, h));
     return ggx_reflection_bsdfcos(conductor_fresnel(eta, k, voh), n, view, dir, alpha);
 }
-__device__ bool refract_dir(F3 inc, F3 m, float eta, F3& out)
+static __device__ bool refract_dir(F3 inc, F3 m, float eta, F3& out)
 {
     const float ct = fminf(1.0f, dot(inc * -1.0f, m));
     const F3 perp = eta * (inc + ct * m);
@@ -368,7 +368,7 @@ __device__ __forceinline__ F3 refract_smooth(F3 v, F3 n, float ratio)
     return perp + par;
 }
 __device__ __forceinline__ F3 oriented_half(F3 n, F3 h) { return dot(n, h) < 0.0f ? h * -1.0f : h; }
-__device__ float ggx_dielectric_pdf(F3 n, F3 view, F3 dir, float alpha, float ei, float et)
+static __device__ float ggx_dielectric_pdf(F3 n, F3 view, F3 dir, float alpha, float ei, float et)
 {
     const float nov = dot(n, view), nol = dot(n, dir);
     if (nov <= 0.0f || nol == 0.0f || ei <= 0.0f || et <= 0.0f) return 0.0f;
@@ -389,7 +389,7 @@ __device__ float ggx_dielectric_pdf(F3 n, F3 view, F3 dir, float alpha, float ei
     const float pdf = (1.0f - F) * ggx_d(noh, alpha) * noh * dh;
     return (isfinite(pdf) && pdf > 0.0f) ? pdf : 0.0f;
 }
-__device__ F3 ggx_dielectric_bsdfcos(F3 color, F3 n, F3 view, F3 dir, float alpha, float ei, float et)
+static __device__ F3 ggx_dielectric_bsdfcos(F3 color, F3 n, F3 view, F3 dir, float alpha, float ei, float et)
 {
     const float nov = dot(n, view), nol = dot(n, dir);
     const F3 zero{0.f, 0.f, 0.f};
@@ -429,7 +429,7 @@ __device__ __forceinline__ float principled_diffuse_scale(const GMaterial& m)
     return (1.0f - m.metallic) * (1.0f - m.transmission) * (1.0f - m.f0_diel) * (1.0f - 0.25f * m.clearcoat);
 }
 // componentWeights (Principled.cpp:159-205)
-__device__ PWeights principled_weights(const GMaterial& m, F3 base)
+static __device__ PWeights principled_weights(const GMaterial& m, F3 base)
 {
     PWeights r;
     const float bl = fmaxf(0.05f, lum_weight(base));
@@ -453,7 +453,7 @@ __device__ PWeights principled_weights(const GMaterial& m, F3 base)
     }
     return r;
 }
-__device__ __noinline__ F3 principled_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ __noinline__ F3 principled_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 base = clamp_color01(color_at(S, m, h));
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
@@ -499,7 +499,7 @@ __device__ __noinline__ F3 principled_eval(const DScene& S, const GMaterial& m, 
                                  m.clearcoat * 0.25f);
     return res;
 }
-__device__ __noinline__ float principled_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ __noinline__ float principled_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 base = clamp_color01(color_at(S, m, h));
     const PWeights W = principled_weights(m, base);
@@ -549,7 +549,7 @@ __device__ __forceinline__ F3 ray_dir_normalized(F3 d)   // Ray::_normalize (inc
 }
 
 // Material::evaluateBSDFCos / scatteringPDF for the BSDF-typed materials.
-__device__ __noinline__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ __noinline__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
     switch (m.type) {
@@ -574,7 +574,7 @@ __device__ __noinline__ F3 bsdf_eval(const DScene& S, const GMaterial& m, const 
         return F3{0.f, 0.f, 0.f};
     }
 }
-__device__ __noinline__ float bsdf_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ __noinline__ float bsdf_pdf(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 view = safe_normalize(ray_d * -1.0f, h.n);
     switch (m.type) {
@@ -629,7 +629,7 @@ __device__ __forceinline__ bool finish_bsdf(const DScene& S, const GMaterial& m,
 }
 
 // Material::scatter for every type on the path; false = no scatter (emitter or failed sample).
-__device__ __noinline__ bool scatter(const DScene& S, const GMaterial& m, const Hit& h, F3 d, const Key& k, Scatter& sr)
+static __device__ __noinline__ bool scatter(const DScene& S, const GMaterial& m, const Hit& h, F3 d, const Key& k, Scatter& sr)
 {
     sr.specular = false;
     sr.pdf = PDF_NONE;
@@ -771,7 +771,7 @@ __device__ __noinline__ bool scatter(const DScene& S, const GMaterial& m, const 
 }
 
 // scatterPDFValue (ColorHelper.cpp:38-86)
-__device__ float scatter_pdf(const DScene& S, const Scatter& sr, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ float scatter_pdf(const DScene& S, const Scatter& sr, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     switch (sr.pdf) {
     case PDF_COSINE: {
@@ -798,13 +798,13 @@ __device__ float scatter_pdf(const DScene& S, const Scatter& sr, const GMaterial
     }
 }
 // scatterBSDFCos (ColorHelper.cpp:88-106)
-__device__ F3 scatter_bsdfcos(const DScene& S, const Scatter& sr, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ F3 scatter_bsdfcos(const DScene& S, const Scatter& sr, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     if (sr.pdf == PDF_BSDF) return bsdf_eval(S, m, h, ray_d, dir);
     return sr.att * scatter_pdf(S, sr, m, h, ray_d, dir);
 }
 // henyeyGreensteinDirection (ColorHelper.cpp:108-140)
-__device__ __noinline__ F3 hg_direction(const Scatter& sr, const Key& k)
+static __device__ __noinline__ F3 hg_direction(const Scatter& sr, const Key& k)
 {
     const float pl = len2(sr.phase);
     if (pl <= 0.0f || !isfinite(pl)) return sphere_direction(k, DIM_BSDF_DIRECTION);
@@ -824,7 +824,7 @@ __device__ __noinline__ F3 hg_direction(const Scatter& sr, const Key& k)
     return onb_local(make_onb(pd), st * cosf(phi), st * sinf(phi), ct);
 }
 // scatterPDFGenerate (ColorHelper.cpp:142-158)
-__device__ F3 scatter_generate(const Scatter& sr, const Key& k)
+static __device__ F3 scatter_generate(const Scatter& sr, const Key& k)
 {
     switch (sr.pdf) {
     case PDF_COSINE:
@@ -886,7 +886,7 @@ struct AtmosSample {
 // Atmosphere::sampleSegment (Atmosphere.cpp:344-471): single-scattering
 // Rayleigh + Mie along the ray up to t_max (scene units), midpoint samples on
 // the view segment and on each sample's path to the sun.
-__device__ __noinline__ AtmosSample atmos_segment(const DScene& S, const double* ro, const double* d, double t_max)
+static __device__ __noinline__ AtmosSample atmos_segment(const DScene& S, const double* ro, const double* d, double t_max)
 {
     const GAtmos& A = S.k.atmos;
     AtmosSample out{{0.0, 0.0, 0.0}, {1.0, 1.0, 1.0}};
@@ -1001,7 +1001,7 @@ __device__ __forceinline__ void env_dir_to_uv(const GEnv& E, F3 dir, double& u, 
     u = wrap01d(0.5 + (phi / (2.0 * kPiD)) + (E.rotation / 360.0));
     v = clamp01d(0.5 + (asin(y) / kPiD));
 }
-__device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, double v)
+static __device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, double v)
 {
     const GEnv& E = S.k.env;
     u = wrap01d(u);
@@ -1028,7 +1028,7 @@ __device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, double v)
     return F3{isfinite(c.x) ? fmaxf(0.f, c.x) : 0.f, isfinite(c.y) ? fmaxf(0.f, c.y) : 0.f,
               isfinite(c.z) ? fmaxf(0.f, c.z) : 0.f};
 }
-__device__ __noinline__ F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
+static __device__ __noinline__ F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
 {
     double u, v;
     env_dir_to_uv(S.k.env, dir, u, v);
@@ -1044,14 +1044,14 @@ __device__ __forceinline__ float env_pdf_uv(const DScene& S, double u, double v)
 }
 // EnvironmentMap::sampleDirection and ::pdf of one direction: both start from the same
 // directionToUV(direction), so it is evaluated once.
-__device__ __noinline__ void env_query(const DScene& S, F3 dir, bool want_rad, bool want_pdf, F3& rad, float& pdf)
+static __device__ __noinline__ void env_query(const DScene& S, F3 dir, bool want_rad, bool want_pdf, F3& rad, float& pdf)
 {
     double u, v;
     env_dir_to_uv(S.k.env, dir, u, v);
     if (want_rad) rad = env_lookup_uv(S, u, v);
     if (want_pdf) pdf = env_pdf_uv(S, u, v);
 }
-__device__ __noinline__ float env_pdf(const DScene& S, F3 dir)
+static __device__ __noinline__ float env_pdf(const DScene& S, F3 dir)
 {
     const GEnv& E = S.k.env;
     if (E.total_weight <= 0.0 || E.pdf_offset < 0) return 1.0f / (4.0f * kPiF);
@@ -1072,7 +1072,7 @@ struct LightSample {
 };
 
 // IESProfile::candelaAt (IESProfile.cpp:231-299), FP64.
-__device__ double ies_candela(const DScene& S, const GIes& I, double vdeg, double hdeg)
+static __device__ double ies_candela(const DScene& S, const GIes& I, double vdeg, double hdeg)
 {
     const double* va = S.cdf + I.offset;
     const double* ha = va + I.nv;
@@ -1109,7 +1109,7 @@ __device__ double ies_candela(const DScene& S, const GIes& I, double vdeg, doubl
 }
 
 // IESProfile::relativeIntensity (IESProfile.cpp:301-323) for emission direction e (FP64).
-__device__ __noinline__ float ies_relative(const DScene& S, const GLight& L, F3 e)
+static __device__ __noinline__ float ies_relative(const DScene& S, const GLight& L, F3 e)
 {
     const GIes I = S.ies[L.ies];
     if (!(I.mean_candela > 0.0) || !isfinite(I.mean_candela)) return 0.0f;
@@ -1144,7 +1144,7 @@ __device__ __forceinline__ double clamp_sample(double v)
     return v;
 }
 // EnvironmentMap::sample (EnvironmentMap.cpp:468-513)
-__device__ __noinline__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
+static __device__ __noinline__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
 {
     const GEnv& E = S.k.env;
     const double sel0 = sample1d(k, DIM_ENVIRONMENT_SELECTION);
@@ -1226,7 +1226,7 @@ __device__ __forceinline__ F3 tri_point(const DScene& S, int32_t slot, const Key
     return (f3(T.v0) + (f3(T.e1) * u)) + (f3(T.e2) * v);
 }
 // Mesh area CDF pick; returns leaf slot or -1 (Mesh.cpp:844-885).
-__device__ int32_t mesh_pick(const DScene& S, const GMesh& M, const Key& k, double& selected)
+static __device__ int32_t mesh_pick(const DScene& S, const GMesh& M, const Key& k, double& selected)
 {
     if (M.tri_count <= 0 || M.total_area <= 0.0) return -1;
     const double* c = S.cdf + M.cdf_offset;
@@ -1239,7 +1239,7 @@ __device__ int32_t mesh_pick(const DScene& S, const GMesh& M, const Key& k, doub
     return S.index_pool[M.slot_offset + idx];
 }
 
-__device__ __noinline__ bool light_surface_sample(const DScene& S, const GLight& L, F3 origin, const Key& k, LightSample& ls)
+static __device__ __noinline__ bool light_surface_sample(const DScene& S, const GLight& L, F3 origin, const Key& k, LightSample& ls)
 {
     ls.valid = false;
     switch (L.kind) {
@@ -1367,7 +1367,7 @@ __device__ __noinline__ bool light_surface_sample(const DScene& S, const GLight&
 }
 
 // Hittable::pdfValue of light L toward direction vec from origin.
-__device__ __noinline__ float light_pdf_value(const DScene& S, const GLight& L, F3 origin, F3 vec)
+static __device__ __noinline__ float light_pdf_value(const DScene& S, const GLight& L, F3 origin, F3 vec)
 {
     VolSample vs{nullptr, 0.0, true};
     switch (L.kind) {
@@ -1441,7 +1441,7 @@ __device__ __forceinline__ float light_select_prob(const DScene& S, int32_t i)
     return (float)(w / S.k.light_total_weight);
 }
 // lightPDFValue (ColorHelper.cpp:233-257)
-__device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
+static __device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
 {
     const int32_t n = S.k.light_count;
     if (n <= 0) return 0.0f;
@@ -1451,7 +1451,7 @@ __device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
     return sum;
 }
 // selectLightIndex + sampleLight (ColorHelper.cpp:190-231, 925-971)
-__device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
+static __device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
 {
     ls.valid = false;
     const int32_t n = S.k.light_count;

@@ -14,7 +14,7 @@
 //   MeshInstance::hit / hitAny              src/core/Hittables/MeshInstance.cpp:251-327
 //   Rectangle / Sphere / Cube / Plane / ConstantVolume intersectors.
 // Arithmetic is FP32 with the reference's operation order (-fmad=false), so
-// oracle/restate.c reproduces every hit bit for bit on the same packed arrays.
+// oracle/restate.cpp reproduces every hit bit for bit on the same packed arrays.
 #pragma once
 #include "dmath.cuh"
 
@@ -52,7 +52,11 @@ struct DScene {
     const float4* env_texels;
     const uint8_t* obj_class;  // material type a hit on each object shades with (shade binning)
     uint32_t* error;          // device error word (bit flags)
-    unsigned long long* counters;   // LUZ_RENDER_COUNT: ext nodes/tris/top, shadow nodes/tris/top
+    unsigned long long* counters;   // LUZ_RENDER_COUNT: ext nodes/tris/top, shadow nodes/tris/top,
+                                    // ext / shadow binary-node visits (read by the counting
+                                    // instantiations of the trace kernels only)
+    int32_t mesh_stack_limit;       // traversal stack bounds enforced (<= kMeshStack4 / kTopStack;
+    int32_t top_stack_limit;        // lowered only by luz_gpu_scene_set_traversal_limits)
     DCaustics cm;
     GSceneConst k;
 };
@@ -120,6 +124,7 @@ struct VolSample {
     double u;
     bool have;
     uint32_t nodes = 0, tris = 0, top = 0;
+    uint32_t bnodes = 0;   // binary-tree node visits the collapsed walk stands for
     __device__ __forceinline__ double get()
     {
         if (!have) {
@@ -386,12 +391,13 @@ __device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& 
                 // arrays. An accepted entry implies an accepted side box (the
                 // entry box lies inside it), so hl/hr only decide which side goes
                 // first when both hold entries: the nearer (ties: R).
-                (void)hl;
-                (void)hr;
                 const int cl = (int)ha[0] + (int)ha[1], cr = (int)ha[2] + (int)ha[3];
                 const bool r_first = (cl > 0 && cr > 0) ? !(nl < nr) : (cr > 0);
                 const int ne = cl + cr;
-                if (sp + ne > kMeshStack4) {
+                // binary-node visits this node stands for: N itself, and each accepted
+                // side that is an interior node (two entries) of the binary tree
+                vs.bnodes += 1u + (uint32_t)(hl && n.ref[1] != kEmptySlot) + (uint32_t)(hr && n.ref[3] != kEmptySlot);
+                if (sp + ne > S.mesh_stack_limit) {
                     atomicOr(S.error, ERR_MESH_STACK);
                     break;
                 }
@@ -485,7 +491,10 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
             // Entries in slot order; an entry's place is the number of accepted
             // entries before it (selects, no running index into an array).
             const int ne = (int)ha[0] + (int)ha[1] + (int)ha[2] + (int)ha[3];
-            if (sp + ne > kMeshStack4) {
+            // binary-node visits: N, and each interior side with an accepted entry
+            vs.bnodes += 1u + (uint32_t)(n.ref[1] != kEmptySlot && (ha[0] || ha[1]))
+                         + (uint32_t)(n.ref[3] != kEmptySlot && (ha[2] || ha[3]));
+            if (sp + ne > S.mesh_stack_limit) {
                 atomicOr(S.error, ERR_MESH_STACK);
                 break;
             }
@@ -625,7 +634,7 @@ __device__ __forceinline__ bool local_ray(const GObject& O, const TRay& r, TRay&
 // boundary's hitInterval(-T_MAX, T_MAX) (Cube.cpp:134-175, Sphere.cpp:304-343).
 // Length (scene units along the ray) of the part of [tmin, tmax] inside the
 // boundary of volume O: the interval volume_distance samples in.
-__device__ float volume_overlap(const GObject& O, F3 o, F3 d, float tmin, float tmax)
+static __device__ float volume_overlap(const GObject& O, F3 o, F3 d, float tmin, float tmax)
 {
     float entry, exit;
     if (O.aux == 3 /* LUZ_OBJ_CUBE */) {
@@ -661,7 +670,7 @@ __device__ float volume_overlap(const GObject& O, F3 o, F3 d, float tmin, float 
     return (exit - entry) * sqrtf(len2(d));
 }
 
-__device__ bool volume_distance(const GObject& O, const TRay& r, float tmin, float tmax, VolSample& vs, float& t)
+static __device__ bool volume_distance(const GObject& O, const TRay& r, float tmin, float tmax, VolSample& vs, float& t)
 {
     float entry, exit;
     if (O.aux == 3 /* LUZ_OBJ_CUBE */) {
@@ -828,7 +837,7 @@ __device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TR
 // 1 = node (own box test), 2 = object (near check), 3 = object (no check).
 #define TOP_PUSH(ref_, kind_, near_)                       \
     do {                                                   \
-        if (sp >= kTopStack) {                             \
+        if (sp >= S.top_stack_limit) {                     \
             atomicOr(S.error, ERR_TOP_STACK);              \
             sp = 0;                                        \
             break;                                         \

@@ -172,7 +172,7 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred)
 }
 
 // _generateRay (src/renderer/RayHelper.cpp:85-106) in FP64, rounded to FP32.
-__device__ void camera_ray(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, double* o, double* d)
+static __device__ void camera_ray(const WaveArgs& w, uint32_t x, uint32_t y, uint32_t s, double* o, double* d)
 {
     const Key k = path_key(w, x, y, s, 0);
     const GCamera& c = w.cam;
@@ -252,7 +252,7 @@ __device__ __forceinline__ bool leaves_opaque(const GMaterial& m, const Hit& h, 
 __device__ __forceinline__ float direct_prob(int bounce) { return bounce < 2 ? 1.0f : 0.5f; }
 
 // relocateSubsurfaceExit (ColorHelper.cpp:428-504)
-__device__ __noinline__ void relocate_subsurface(const DScene& S, const GMaterial& m, Hit& h, Scatter& sr, F3 ray_d, const Key& k)
+static __device__ __noinline__ void relocate_subsurface(const DScene& S, const GMaterial& m, Hit& h, Scatter& sr, F3 ray_d, const Key& k)
 {
     if (!sr.subsurface || sr.thin) return;
     const float dl = maxc(sr.ss_radius_m);
@@ -310,13 +310,13 @@ __device__ __forceinline__ float nfor_channel(float v)
     if (!isfinite(v) || v <= 0.0f) return 0.0f;
     return (float)fmin(1.0, log1p((double)v) / log1p(1.0e12));   // D_MAX_RAY_COLOR_LUMINANCE
 }
-__device__ __noinline__ void store_miss_features(const PathBuf& P, uint32_t p, F3 sky)
+static __device__ __noinline__ void store_miss_features(const PathBuf& P, uint32_t p, F3 sky)
 {
     P.feat[3 * p] = make_float4(0.0f, 1.0f, 0.5f, 0.5f);
     P.feat[3 * p + 1] = make_float4(0.5f, nfor_channel(sky.x), nfor_channel(sky.y), nfor_channel(sky.z));
     P.feat[3 * p + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
-__device__ __noinline__ void store_hit_features(const DScene& S, const PathBuf& P, uint32_t p, const Hit& h,
+static __device__ __noinline__ void store_hit_features(const DScene& S, const PathBuf& P, uint32_t p, const Hit& h,
                                                 const GMaterial& m)
 {
     double nx = h.n.x, ny = h.n.y, nz = h.n.z;
@@ -357,7 +357,7 @@ __device__ __forceinline__ void scatter_texel_grad(const DScene& S, const WaveAr
 
 // d ln f / d roughness of a rough Metal lobe toward dir, per channel, by a central
 // difference of the BSDF in roughness (alpha = roughness^2 >= 1e-4); 0 where f is 0.
-__device__ __noinline__ F3 dlnf_rough(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
+static __device__ __noinline__ F3 dlnf_rough(const DScene& S, const GMaterial& m, const Hit& h, F3 ray_d, F3 dir)
 {
     const F3 f = bsdf_eval(S, m, h, ray_d, dir);
     const float r = m.roughness, r1 = fminf(1.0f, r + 1e-3f), r0 = fmaxf(0.0f, r - 1e-3f);
@@ -375,7 +375,7 @@ __device__ __noinline__ F3 dlnf_rough(const DScene& S, const GMaterial& m, const
 // times its d ln f, the continuation (final path radiance L minus the radiance
 // gathered up to this vertex's samples, rad) times d ln f of its direction
 // (sampling densities held fixed: each sample's f / pdf is differentiated in f).
-__device__ __noinline__ void adjoint_rough_resolve(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
+static __device__ __noinline__ void adjoint_rough_resolve(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
                                                    F3 a, F3 b, F3 rad, bool continued, AdjRough& ar)
 {
     const float4 L = P.color[p];
@@ -444,7 +444,7 @@ __device__ __forceinline__ void density_add(const DScene& S, const WaveArgs& w, 
 // per channel, zero where the clamp is active. The pixel's film is the mean of
 // cleanColor(L) over its samples, so each path adds adj(pixel) / spp times that.
 // Russian roulette's survival probability is held fixed (not differentiated).
-__device__ __noinline__ void adjoint_texture(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
+static __device__ __noinline__ void adjoint_texture(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p,
                                              const Hit& h, F3 before)
 {
     const float4 L = P.color[p];
@@ -480,7 +480,7 @@ __device__ __noinline__ void adjoint_texture(const DScene& S, const WaveArgs& w,
 // The ray the atmosphere integrates along, in FP64: at bounce 0 the camera ray
 // is regenerated in FP64 (a planet-scale origin loses metres in FP32), later
 // rays are the FP32 ray widened.
-__device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, const TRay& ray,
+static __device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, const TRay& ray,
                                        double* o, double* d)
 {
     if (bounce == 0) {
@@ -515,7 +515,7 @@ __device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, co
 // MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render;
 // 3: adjoint (gradient) passes.
 template <int MODE>
-__device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
+static __device__ void shade_path(const DScene& S, const WaveArgs& w, const PathBuf& P, uint32_t p, int bounce, ShadeOut& out)
 {
     out.cont = false;
     out.sh[0] = out.sh[1] = false;
@@ -839,5 +839,10 @@ __device__ __forceinline__ F3 clean(F3 c)   // cleanColor (Threads.cpp:122-137)
 {
     return F3{isfinite(c.x) ? c.x : 0.f, isfinite(c.y) ? c.y : 0.f, isfinite(c.z) ? c.z : 0.f};
 }
+
+// Shade-stage kernels k_shade<mode> (shade_kernels.cu): 0 plain, 1 with the
+// caustic estimate, 2 radiance-cache render, 3 adjoint replay.
+using ShadeKernel = void (*)(const DScene*, WaveArgs, PathBuf, Ctrl*, int);
+ShadeKernel shade_kernel(int mode);
 
 }  // namespace luz

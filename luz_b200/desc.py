@@ -1,7 +1,7 @@
 """ctypes mirror of include/luz_gpu.h and a builder for LuzSceneDesc.
 
 The builder plays the role of the C++ host-side packer a Luz maintainer adds to
-Renderer::render (see INTEGRATION.md): it turns a scene made of the reference's
+Renderer::render: it turns a scene made of the reference's
 object kinds (Rectangle, Sphere, Cube, Plane, Mesh, MeshInstance,
 ConstantVolume, DirectionalLight; src/core/Hittables/*) and materials
 (src/core/Materials/*) into the flat description both the GPU library and the
@@ -15,7 +15,7 @@ from typing import List, Optional
 
 import numpy as np
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE = 1, 2, 3, 4
 MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
@@ -136,6 +136,7 @@ class RenderStats(C.Structure):
         ("ext_nodes", C.c_double), ("ext_tris", C.c_double), ("ext_top", C.c_double),
         ("sh_nodes", C.c_double), ("sh_tris", C.c_double), ("sh_top", C.c_double),
         ("denoise_ms", C.c_double), ("caustic_photons", C.c_double), ("caustic_ms", C.c_double),
+        ("ext_bnodes", C.c_double), ("sh_bnodes", C.c_double),
     ]
 
 

@@ -27,7 +27,7 @@ EXPORTED = [
     "luz_gpu_nfor_denoise", "luz_gpu_nfor_error", "luz_gpu_render_denoised",
     "luz_gpu_cache_create", "luz_gpu_cache_destroy", "luz_gpu_cache_weights", "luz_gpu_cache_predict",
     "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached", "luz_gpu_adjoint_emission",
-    "luz_gpu_adjoint_density",
+    "luz_gpu_adjoint_density", "luz_gpu_scene_set_path_budget", "luz_gpu_scene_set_traversal_limits",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -61,6 +61,8 @@ def lib():
     L.luz_gpu_scene_create.argtypes = [vp, i32, C.POINTER(vp)]
     L.luz_gpu_scene_destroy.argtypes = [vp]
     L.luz_gpu_scene_info.argtypes = [vp, C.POINTER(D.SceneInfo)]
+    L.luz_gpu_scene_set_path_budget.argtypes = [vp, i64]
+    L.luz_gpu_scene_set_traversal_limits.argtypes = [vp, i32, i32]
     L.luz_gpu_render.argtypes = [vp, C.POINTER(D.RenderParams), vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_render_device.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_trace_paths.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, vp, i64, vp]
@@ -181,6 +183,14 @@ class GpuScene:
         i = D.SceneInfo()
         _check(lib().luz_gpu_scene_info(self.h, C.byref(i)))
         return i
+
+    def set_path_budget(self, nbytes: int):
+        """luz_gpu_scene_set_path_budget: cap on the path state held (bytes; -1 = default)."""
+        _check(lib().luz_gpu_scene_set_path_budget(self.h, int(nbytes)))
+
+    def set_traversal_limits(self, mesh_entries: int = 0, top_entries: int = 0):
+        """luz_gpu_scene_set_traversal_limits (0 = the compiled stack size)."""
+        _check(lib().luz_gpu_scene_set_traversal_limits(self.h, int(mesh_entries), int(top_entries)))
 
     def render(self, p: D.RenderParams, out: Optional[np.ndarray] = None) -> Tuple[np.ndarray, D.RenderStats]:
         """luz_gpu_render into `out` (H x W x 3 float32, C-contiguous, e.g. pinned) or a new array."""

@@ -3,7 +3,7 @@
   oracle/_ref/libluzref.so       the Luz reference itself (built by oracle/Makefile
                                  from the reference sources, -O2, no fast-math)
   oracle/_ref/libluzref_fast.so  same sources with release flags (timed CPU baseline)
-  oracle/_ref/librestate.so      oracle/restate.c, the FP32 C restatement of the
+  oracle/_ref/librestate.so      oracle/restate.cpp, the FP32 restatement of the
                                  sampler and the BVH traversal
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
@@ -75,6 +75,8 @@ class RefOracle:
         L.luzref_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.luzref_scene_load.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.luzref_scene_pack.argtypes = [vp, C.POINTER(vp), vp]
+        L.luzref_set_perturbation.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_double]
+        L.luzref_top_bvh.argtypes = [vp, vp, C.c_int64, C.POINTER(C.c_int64)]
 
     def _check(self, rc):
         if rc != 0:
@@ -107,6 +109,11 @@ class RefOracle:
                                          prefilter_radius, regression_radius, patch_radius, min_variance, threads,
                                          out.ctypes.data))
         return out
+
+    def set_perturbation(self, seed: int, delta_dir: float = 0.0, delta_dec: float = 0.0, delta_cam: float = 0.0):
+        """Moves every Sampler draw by +-delta while seed != 0 (the FP32 ambiguity probe,
+        oracle/ref_harness.cpp); seed 0 turns it off."""
+        self._check(self.lib.luzref_set_perturbation(int(seed), float(delta_dir), float(delta_dec), float(delta_cam)))
 
     def sampler(self, seed, x, y, s, stream, bounce, dim, which=1):
         out = np.zeros(2, np.float64)
@@ -153,6 +160,15 @@ class RefScene:
                                                    None if vk is None else vk.ctypes.data,
                                                    t.ctypes.data, obj.ctypes.data, prim.ctypes.data))
         return t, obj, prim
+
+    def top_bvh(self) -> np.ndarray:
+        """The reference's top-level BVHNode tree in preorder: per node its child count,
+        then per child (is_node, object, min xyz, max xyz)."""
+        n = C.c_int64(0)
+        self.o._check(self.o.lib.luzref_top_bvh(self.h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float64)
+        self.o._check(self.o.lib.luzref_top_bvh(self.h, out.ctypes.data, n.value, C.byref(n)))
+        return out
 
     def pack(self) -> "PackedDesc":
         """The scene glue (luz_b200/glue/scene_glue.cpp) applied to this scene."""
@@ -266,3 +282,146 @@ class Restate:
         self.lib.restate_trace(*ptrs, rays.ctypes.data, rays.shape[0], 1 if any_hit else 0, seed,
                                None if vk is None else vk.ctypes.data, out.ctypes.data)
         return out
+
+
+# ---------------------------------------------------------------------------- FP32 ambiguity flags
+#
+# The GPU computes in FP32 what the reference computes in FP64. Where a result
+# depends on its inputs more finely than FP32 resolves (a draw within FP32
+# rounding of a lobe, Russian-roulette or light-selection threshold, a ray
+# grazing a triangle edge, a very sharp lobe), the two may legitimately part.
+# These probes mark such rays and paths from the reference alone, before any GPU
+# result is seen: a ray or path is ambiguous when the reference's own answer
+# changes under perturbations a few times larger than FP32 rounding.
+
+# Draw perturbations (in units of the draw u in [0, 1)): 2^-21 for draws that
+# become directions or distances (FP32 directions are good to ~1e-7), 2^-16 for
+# draws compared with a threshold the GPU computes in FP32 from a long product of
+# FP32 factors (throughput for Russian roulette, Fresnel and lobe weights), and
+# for the camera and lens draws twice the FP32 rounding of the camera ray in
+# pixels or aperture widths (path_deltas). Draws compared with FP64 values both sides share bit for bit (strategy
+# probabilities, light / triangle / environment selection CDFs) are not moved.
+def path_deltas(width: int, height: int, camera) -> dict:
+    """Draw perturbations for a frame. The GPU rounds each FP64 camera ray to FP32:
+    the direction by at most 2^-25 per component, the origin by half an FP32 ulp of
+    its largest coordinate. The camera draw moves the ray by twice the former, in
+    pixels (one pixel spans ~sensor_height / focal / height rad); the lens draw moves
+    the origin by twice the latter, in units of the aperture diameter."""
+    cam = 2.0 * 2.0 ** -25 * height * camera.focal_length_m / camera.sensor_height_m
+    if not camera.pinhole and camera.f_number > 0:
+        radius = camera.focal_length_m / (2.0 * camera.f_number)
+        omax = max(1.0, max(abs(float(camera.position[i])) for i in range(3)))
+        half_ulp = float(np.spacing(np.float32(omax))) / 2.0
+        cam = max(cam, 2.0 * half_ulp / (2.0 * radius))
+    return dict(delta_dir=2.0 ** -21, delta_dec=2.0 ** -16, delta_cam=min(cam, 2.0 ** -8))
+
+
+PATH_PROBES = (1, 2, 3)
+# Ray perturbations: every origin coordinate by +-2^-20 of max(|o|, 1), every
+# direction component by +-2^-20 (renormalised).
+RAY_DELTA = 2.0 ** -20
+RAY_PROBES = (11, 12, 13)
+
+
+def path_rel(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per-path relative difference as the parity tests measure it: max over channels
+    of |a - b| / max(|b|, 1e-3); non-finite values count as different."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    r = np.abs(a - b) / np.maximum(np.abs(b), 1e-3)
+    r = np.where(np.isfinite(r), r, np.inf)
+    return r.max(axis=1)
+
+
+def ambiguous_paths(oracle: RefOracle, rs: "RefScene", params, x, y, s, base: np.ndarray, deltas: dict,
+                    tol: float = 1e-4):
+    """True per path whose reference radiance moves by more than tol under any of the
+    PATH_PROBES draw perturbations (deltas: path_deltas of the frame)."""
+    flags = np.zeros(len(x), bool)
+    try:
+        for seed in PATH_PROBES:
+            oracle.set_perturbation(seed, **deltas)
+            flags |= path_rel(rs.trace_paths(params, x, y, s), base) > tol
+    finally:
+        oracle.set_perturbation(0)
+    return flags
+
+
+def perturbed_rays(rays: np.ndarray, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    r = np.array(rays, np.float64)
+    o = r[:, 0:3]
+    r[:, 0:3] = o + rng.choice([-1.0, 1.0], o.shape) * RAY_DELTA * np.maximum(np.abs(o), 1.0)
+    d = r[:, 4:7] + rng.choice([-1.0, 1.0], (len(r), 3)) * RAY_DELTA
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    return r
+
+
+def ambiguous_rays(rs_tagged: "RefScene", rays: np.ndarray, obj: np.ndarray, prim: np.ndarray, seed: int = 0,
+                   volume_key=None):
+    """True per ray whose reference closest hit (object, primitive) changes under any of
+    the RAY_PROBES perturbations (edge grazes and near ties in t)."""
+    flags = np.zeros(len(rays), bool)
+    for k in RAY_PROBES:
+        _, o2, p2 = rs_tagged.trace_rays(perturbed_rays(rays, k), seed=seed, volume_key=volume_key)
+        flags |= (o2 != obj) | (p2 != prim)
+    return flags
+
+
+# ---------------------------------------------------------------------------- top-level BVH layout
+
+def _round_out(lo: np.ndarray, hi: np.ndarray):
+    """FP64 box bounds rounded outward to FP32 (the nearest float at or below the
+    minimum, at or above the maximum), as float64 values."""
+    f_lo = lo.astype(np.float32)
+    f_lo = np.where(f_lo.astype(np.float64) > lo, np.nextafter(f_lo, np.float32(-np.inf)), f_lo)
+    f_hi = hi.astype(np.float32)
+    f_hi = np.where(f_hi.astype(np.float64) < hi, np.nextafter(f_hi, np.float32(np.inf)), f_hi)
+    return f_lo.astype(np.float64), f_hi.astype(np.float64)
+
+
+def top_tree_from_reference(dump: np.ndarray) -> np.ndarray:
+    """RefScene.top_bvh() with every child box rounded outward to FP32: the form the
+    GPU's top-level arrays take (node preorder, children in the reference's order)."""
+    out = np.array(dump, np.float64)
+    i = 0
+    while i < len(out):
+        n = int(out[i])
+        rec = out[i + 1:i + 1 + 8 * n].reshape(n, 8)
+        rec[:, 2:5], rec[:, 5:8] = _round_out(rec[:, 2:5].copy(), rec[:, 5:8].copy())
+        out[i + 1:i + 1 + 8 * n] = rec.ravel()
+        i += 1 + 8 * n
+    return out
+
+
+TOP_NODE = np.dtype([("bmin", "<f4", 3), ("child_start", "<i4"), ("bmax", "<f4", 3), ("child_count", "<i4")])
+TOP_CHILD = np.dtype([("bmin", "<f4", 3), ("ref", "<i4"), ("bmax", "<f4", 3), ("is_node", "<i4")])
+GOBJECT = np.dtype([("kind", "<i4"), ("material", "<i4"), ("aux", "<i4"), ("id", "<i4"), ("f", "<f4", 12)])
+
+
+def top_tree_from_pack(pack) -> np.ndarray:
+    """The packed top-level arrays (luz_pack_array "top_nodes", "top_children",
+    "objects") walked in the order of top_tree_from_reference."""
+    nodes = np.frombuffer(pack.array("top_nodes").tobytes(), TOP_NODE)
+    kids = np.frombuffer(pack.array("top_children").tobytes(), TOP_CHILD)
+    objs = np.frombuffer(pack.array("objects").tobytes(), GOBJECT)
+    out = []
+    if len(nodes) == 0:
+        return np.zeros(0)
+    stack = [0]
+    order = []
+    while stack:   # preorder over nodes, children in order
+        k = stack.pop()
+        order.append(k)
+        c = kids[nodes[k]["child_start"]:nodes[k]["child_start"] + nodes[k]["child_count"]]
+        stack.extend(int(r) for r in reversed(c["ref"][c["is_node"] != 0]))
+    for k in order:
+        c = kids[nodes[k]["child_start"]:nodes[k]["child_start"] + nodes[k]["child_count"]]
+        out.append(float(len(c)))
+        rec = np.zeros((len(c), 8))
+        rec[:, 0] = c["is_node"] != 0
+        rec[:, 1] = np.where(c["is_node"] != 0, -1, objs["id"][np.where(c["is_node"] != 0, 0, c["ref"])])
+        rec[:, 2:5] = c["bmin"]
+        rec[:, 5:8] = c["bmax"]
+        out.extend(rec.ravel())
+    return np.array(out)

@@ -24,9 +24,24 @@
  *                          into a reference Scene, and the reference-side scene
  *                          glue (luz_b200/glue/scene_glue.cpp) that packs such a
  *                          Scene into a LuzSceneDesc.
+ *   - top-level BVH:       the BVHNode tree of Scene::updateAccelerationStructure
+ *                          (src/scene/Scene.cpp:655-688, BVHNode.cpp:142-185) in
+ *                          preorder, read with private access here only.
  * Hit identification: in "tag" mode every object (and every mesh triangle) gets
  * its own Lambertian-derived material so the HitRecord's material pointer names
  * the object and primitive; traversal does not depend on material values.
+ *
+ * FP32 ambiguity probe (parity build only, LUZREF_PERTURB): the Sampler's
+ * exported functions are wrapped at link time (ld --wrap, oracle/Makefile) so
+ * that, while a perturbation seed is set, every value the path loop draws is
+ * moved by +-delta (a sign hashed from the seed, the dimension and the value,
+ * so repeated draws of one dimension move together). A path whose radiance
+ * changes by more than the parity tolerance under such moves depends on its
+ * draws, and so on every quantity compared with them, finer than the FP32
+ * arithmetic of the GPU can resolve; the fixtures mark it as ambiguous. The
+ * mappings of cosineHemisphere, sphereDirection and unitDisk
+ * (src/core/Sampler.cpp:239-290) are restated below on the moved draws,
+ * because their internal calls of sample2D do not pass through the wrap.
  */
 #include <algorithm>
 #include <fstream>
@@ -67,6 +82,7 @@
 #include "Hittables/DirectionalLight.hpp"
 #include "Hittables/Triangle.hpp"
 #define private public
+#include "Hittables/BVHNode.hpp"
 #include "Hittables/Mesh.hpp"
 #include "Hittables/MeshInstance.hpp"
 #undef private
@@ -359,6 +375,31 @@ RefScene* build(const LuzSceneDesc* d, int tag)
     return rs.release();
 }
 
+// Preorder walk of the reference BVHNode tree. Per node: the child count, then
+// per child 8 doubles: is_node, desc object index (-1 for a node), box min, box max.
+void dump_bvh(const RefScene& rs, const std::unordered_map<const Hittable*, int32_t>& ids, const BVHNode& n,
+              std::vector<double>& out)
+{
+    out.push_back((double)n._childs.size());
+    for (std::size_t i = 0; i < n._childs.size(); i++) {
+        const Hittable* c = n._childs[i].get();
+        const BVHNode* cn = dynamic_cast<const BVHNode*>(c);
+        const AABB& b = n._childBoundingBoxes[i];
+        auto it = ids.find(c);
+        out.push_back(cn ? 1.0 : 0.0);
+        out.push_back(cn ? -1.0 : (it != ids.end() ? (double)it->second : -2.0));
+        out.push_back(b.getMinimum().getX());
+        out.push_back(b.getMinimum().getY());
+        out.push_back(b.getMinimum().getZ());
+        out.push_back(b.getMaximum().getX());
+        out.push_back(b.getMaximum().getY());
+        out.push_back(b.getMaximum().getZ());
+    }
+    for (const auto& c : n._childs)
+        if (const BVHNode* cn = dynamic_cast<const BVHNode*>(c.get())) dump_bvh(rs, ids, *cn, out);
+    (void)rs;
+}
+
 template <class F> int guarded(F&& f)
 {
     try {
@@ -412,9 +453,156 @@ bool occluded(Scene& scene, Ray& ray, double tmin, double tmax)
     return false;
 }
 
+// Perturbation of the Sampler's draws (see the file header). seed 0 = off.
+struct Perturb {
+    uint64_t seed = 0;
+    double dir = 0.0;    // directions and distances (surface points, BSDF and phase directions, media)
+    double dec = 0.0;    // dimensions compared with an FP32 threshold (lobe, Russian roulette)
+    double cam = 0.0;    // camera and lens (a pixel or the aperture, not a hemisphere)
+} g_perturb;
+
+uint64_t mix64(uint64_t v)
+{
+    v += 0x9e3779b97f4a7c15ull;
+    v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ull;
+    v = (v ^ (v >> 27)) * 0x94d049bb133111ebull;
+    return v ^ (v >> 31);
+}
+
+// Draws the GPU compares with the same FP64 values as the reference (constant
+// strategy probabilities, FP64 selection CDFs built bit-identically on the host)
+// are exact on both sides and are not moved.
+double perturb_delta(uint32_t dimension)
+{
+    switch (dimension % 32u) {
+    case Sampler::DIM_LIGHT_STRATEGY:
+    case Sampler::DIM_LIGHT_SELECTION:
+    case Sampler::DIM_LIGHT_SURFACE_SELECTION:
+    case Sampler::DIM_ENVIRONMENT_SELECTION:
+    case Sampler::DIM_ENVIRONMENT_STRATEGY:
+    case Sampler::DIM_LIGHT_EMISSION_SIDE: return 0.0;
+    case Sampler::DIM_CAMERA:
+    case Sampler::DIM_LENS: return g_perturb.cam;
+    case Sampler::DIM_LIGHT_SURFACE_POINT:
+    case Sampler::DIM_BSDF_DIRECTION:
+    case Sampler::DIM_MATERIAL_FUZZ:
+    case Sampler::DIM_ATMOSPHERE:
+    case Sampler::DIM_ENVIRONMENT_POINT:
+    case Sampler::DIM_LIGHT_EMISSION_DIRECTION:
+    case Sampler::DIM_SUBSURFACE_SPATIAL:
+    case Sampler::DIM_VOLUME_DISTANCE: return g_perturb.dir;
+    default: return g_perturb.dec;
+    }
+}
+
+double moved(double u, uint32_t dimension, uint32_t component, double top)
+{
+    uint64_t bits;
+    std::memcpy(&bits, &u, sizeof bits);
+    const uint64_t h = mix64(g_perturb.seed ^ mix64(((uint64_t)dimension << 8 | component) ^ mix64(bits)));
+    const double v = u + ((h >> 63) ? 1.0 : -1.0) * perturb_delta(dimension);
+    return v < 0.0 ? 0.0 : (v > top ? top : v);
+}
+
 }  // namespace
 
+#ifdef LUZREF_PERTURB
+// ld --wrap targets (mangled names of the Sampler namespace functions).
+extern "C" double __real__ZN7Sampler8sample1DEj(std::uint32_t dimension);
+extern "C" Sampler::Sample2D __real__ZN7Sampler8sample2DEj(std::uint32_t dimension);
+
+extern "C" double __wrap__ZN7Sampler8sample1DEj(std::uint32_t dimension)
+{
+    const double u = __real__ZN7Sampler8sample1DEj(dimension);
+    if (!g_perturb.seed || !Sampler::isActive()) return u;
+    return moved(u, dimension, 0, 0x1.fffffffffffffp-1);
+}
+
+extern "C" Sampler::Sample2D __wrap__ZN7Sampler8sample2DEj(std::uint32_t dimension)
+{
+    Sampler::Sample2D s = __real__ZN7Sampler8sample2DEj(dimension);
+    if (!g_perturb.seed || !Sampler::isActive()) return s;
+    s.x = (float)moved((double)s.x, dimension, 0, 0x1.fffffep-1);
+    s.y = (float)moved((double)s.y, dimension, 1, 0x1.fffffep-1);
+    return s;
+}
+
+extern "C" Vector3 __wrap__ZN7Sampler16cosineHemisphereEj(std::uint32_t dimension)
+{
+    const Sampler::Sample2D u = __wrap__ZN7Sampler8sample2DEj(dimension);
+    const float phi = static_cast<float>(2.0 * D_PI) * u.x;
+    const float r = std::sqrt(u.y);
+    const float z = std::sqrt(std::max(0.0f, 1.0f - u.y));
+    return Vector3(r * std::cos(phi), r * std::sin(phi), z);
+}
+
+extern "C" Vector3 __wrap__ZN7Sampler15sphereDirectionEj(std::uint32_t dimension)
+{
+    const Sampler::Sample2D u = __wrap__ZN7Sampler8sample2DEj(dimension);
+    const float z = 1.0f - (2.0f * u.y);
+    const float r = std::sqrt(std::max(0.0f, 1.0f - z * z));
+    const float phi = static_cast<float>(2.0 * D_PI) * u.x;
+    return Vector3(r * std::cos(phi), r * std::sin(phi), z);
+}
+
+extern "C" Vector3 __wrap__ZN7Sampler8unitDiskEj(std::uint32_t dimension)
+{
+    const Sampler::Sample2D u = __wrap__ZN7Sampler8sample2DEj(dimension);
+    const float sx = (2.0f * u.x) - 1.0f;
+    const float sy = (2.0f * u.y) - 1.0f;
+    if (sx == 0.0f && sy == 0.0f) return Vector3(0.0, 0.0, 0.0);
+    float radius, theta;
+    if (std::fabs(sx) > std::fabs(sy)) {
+        radius = sx;
+        theta = (static_cast<float>(D_PI) / 4.0f) * (sy / sx);
+    } else {
+        radius = sy;
+        theta = (static_cast<float>(D_PI) / 2.0f) - ((static_cast<float>(D_PI) / 4.0f) * (sx / sy));
+    }
+    return Vector3(radius * std::cos(theta), radius * std::sin(theta), 0.0);
+}
+#endif
+
 extern "C" {
+
+/* Sets the draw perturbation of the ambiguity probe (seed 0 = off); the
+ * parity library only (LUZ_E_UNSUPPORTED elsewhere). */
+int luzref_set_perturbation(uint64_t seed, double delta_dir, double delta_dec, double delta_cam)
+{
+#ifdef LUZREF_PERTURB
+    g_perturb.seed = seed;
+    g_perturb.dir = delta_dir;
+    g_perturb.dec = delta_dec;
+    g_perturb.cam = delta_cam;
+    return 0;
+#else
+    (void)seed;
+    (void)delta_dir;
+    (void)delta_dec;
+    (void)delta_cam;
+    g_error = "draw perturbation is built into the parity library only";
+    return LUZ_E_UNSUPPORTED;
+#endif
+}
+
+/* The top-level BVHNode tree in preorder (dump_bvh): up to cap doubles into out,
+ * the full length into *count. *count = 0 when the acceleration structure is
+ * not a BVHNode (no object or one bounded object). */
+int luzref_top_bvh(void* s, double* out, int64_t cap, int64_t* count)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        std::unordered_map<const Hittable*, int32_t> ids;
+        for (std::size_t i = 0; i < rs->objects.size(); i++)
+            if (rs->objects[i]) ids[rs->objects[i].get()] = (int32_t)i;
+        std::vector<double> v;
+        const auto& accel = rs->scene.getAccelerationStructure();
+        if (const BVHNode* n = dynamic_cast<const BVHNode*>(accel.get())) dump_bvh(*rs, ids, *n, v);
+        *count = (int64_t)v.size();
+        if (out) std::memcpy(out, v.data(), sizeof(double) * (std::size_t)std::min<int64_t>(cap, *count));
+        return 0;
+    });
+}
 
 int luzref_last_error(char* buf, size_t len)
 {

@@ -37,6 +37,15 @@ CASES = {
     "caustics": lambda: scenes.caustic_pool(48, 36, 4, 8, photons=20000),
 }
 
+# The benchmarked frames at full size (1920x1080 over the 1,310,722-triangle mesh;
+# 1280x720 over 1e5 instances in an HG medium): the mesh BVH and top-level BVHNode
+# layouts (hashes of the full arrays), 2,000 ray hits and 4,096 paths, with the
+# reference's FP32-ambiguity flags (oracle.ambiguous_rays / ambiguous_paths).
+FULL_CASES = {
+    "glossy_full": lambda: scenes.mesh_glossy(),
+    "instancing_full": lambda: scenes.instancing_volumes(),
+}
+
 # Caustic photon map case (CausticPhotonMap): the scene with its map on, and the
 # (render seed, max bounces) pairs whose stored-photon counts are pinned.
 def caustic_case():
@@ -47,6 +56,12 @@ def caustic_case():
 ORACLE_64K = {
     "cornell": lambda: scenes.cornell(24, 24, 65536, 8),
     "tiny": lambda: scenes.tiny_mixed(24, 18, 65536, 6),
+}
+
+# The config-0 frame itself (Cornell box, 300x300, depth 8) at 65,536 spp: the whole
+# converged image, against which GPU films at increasing spp are measured.
+ORACLE_64K_FULL = {
+    "cornell300": lambda: scenes.cornell(300, 300, 65536, 8),
 }
 
 CAUSTIC_COUNTS = [(424242424, 8), (7, 8), (424242424, 3), (99, 12)]

@@ -17,6 +17,10 @@ output of the unmodified reference code:
   caustics.npz       CausticPhotonMap::build photon counts (src/renderer/CausticPhotonMap.cpp:430-551)
                      and per-path radiance of paths whose caustic estimate is non-zero
   oracle64k_<case>.npz Renderer::render films at 65,536 spp (the converged oracle images)
+  full_<case>.npz    the benchmarked frames at full size: sha256 of the reference's mesh
+                     BVH arrays and of its top-level BVHNode tree (BVHNode.cpp:142-185),
+                     ray hits and per-path radiance with FP32-ambiguity flags
+  The hits_ and paths_ files carry the same ambiguity flags (oracle/oracle.py).
 Usage: python tests/golden/make_golden.py [adaptive | adjoint | nfor | caustics | oracle64k | cases <name>...]
 """
 from __future__ import annotations
@@ -33,9 +37,11 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, ORACLE_64K, adjoint_case,  # noqa: E402
+from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, FULL_CASES, ORACLE_64K,  # noqa: E402
+                   ORACLE_64K_FULL, adjoint_case,
                    camera_rays, caustic_case, nfor_synthetic, path_keys)
 from luz_b200 import native  # noqa: E402
+import oracle as O  # noqa: E402
 from oracle import RefOracle  # noqa: E402
 
 
@@ -82,6 +88,77 @@ def adjoint_fixture(o, h=0.05):
     print("golden adjoint_cornell", flush=True)
 
 
+def sha256(*arrays) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def ray_fixture(rt, w, name, rng, n=2000):
+    """Rays, volume keys, the reference's closest / any hits and ambiguity flags."""
+    rays = camera_rays(w, n, seed=len(name))
+    vkey = np.stack([rng.integers(0, w.width, n), rng.integers(0, w.height, n),
+                     rng.integers(0, w.spp, n), rng.integers(0, 4, n)], 1).astype(np.int32)
+    r64 = rays.astype(np.float64)
+    t, ob, pr = rt.trace_rays(r64, seed=w.seed, volume_key=vkey)
+    _, occ, _ = rt.trace_rays(r64, any_hit=True, seed=w.seed, volume_key=vkey)
+    amb = O.ambiguous_rays(rt, r64, ob, pr, seed=w.seed, volume_key=vkey)
+    amb_any = np.zeros(n, bool)
+    for k in O.RAY_PROBES:
+        _, o2, _ = rt.trace_rays(O.perturbed_rays(r64, k), any_hit=True, seed=w.seed, volume_key=vkey)
+        amb_any |= o2 != occ
+    return dict(rays=rays, vkey=vkey, t=t, obj=ob, prim=pr, occluded=occ >= 0, ambiguous=amb,
+                ambiguous_any=amb_any)
+
+
+def path_fixture(o, rs, w, x, y, s):
+    p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+    rgb = rs.trace_paths(p, x, y, s)
+    amb = O.ambiguous_paths(o, rs, p, x, y, s, rgb, O.path_deltas(w.width, w.height, w.scene.camera))
+    return dict(x=x, y=y, s=s, rgb=rgb, ambiguous=amb)
+
+
+def full_fixtures(o, only=None):
+    """full_<case>.npz for FULL_CASES."""
+    for name, fn in FULL_CASES.items():
+        if only and name not in only:
+            continue
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        w = fn()
+        b = w.scene.build()
+        rs = o.scene(b)
+        out = {}
+        for mi in range(len(w.scene.meshes)):
+            nodes, order = rs.mesh_bvh(mi)
+            out[f"mesh{mi}_sha256"] = sha256(nodes, order)
+            out[f"mesh{mi}_nodes"] = len(nodes)
+            out[f"mesh{mi}_head"] = nodes[:64]
+        top = O.top_tree_from_reference(rs.top_bvh())
+        out["top_sha256"] = sha256(top)
+        out["top_len"] = len(top)
+        out["top_head"] = top[:4096]
+        rt = o.scene(b, tag=True)
+        for k, v in ray_fixture(rt, w, name, rng).items():
+            out["hit_" + k] = v
+        rt.close()
+        x, y, s = path_keys(w, 4096, seed=7 + len(name))
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        lit = rs.trace_paths(p, x, y, s).max(axis=1) > 0
+        if lit.mean() < 0.25:
+            # a mostly dark frame (the 1e5-instance box is opaque a few units into it):
+            # add the lit paths among 2^21 seeded candidates, up to 1,024 of them
+            cx, cy, cs = path_keys(w, 1 << 21, seed=8 + len(name))
+            nz = np.flatnonzero(rs.trace_paths(p, cx, cy, cs).max(axis=1) > 0)[:1024]
+            x, y, s = np.concatenate([x, cx[nz]]), np.concatenate([y, cy[nz]]), np.concatenate([s, cs[nz]])
+        for k, v in path_fixture(o, rs, w, x, y, s).items():
+            out["path_" + k] = v
+        np.savez_compressed(os.path.join(HERE, f"full_{name}.npz"), **out)
+        print("golden", name, "ambiguous rays %.4f paths %.4f" % (out["hit_ambiguous"].mean(),
+                                                                  out["path_ambiguous"].mean()), flush=True)
+
+
 def case_fixtures(o, only=None):
     """hits_/paths_/image_<case>.npz; each case draws from its own seeded generator."""
     for name, fn in CASES.items():
@@ -92,17 +169,12 @@ def case_fixtures(o, only=None):
         b = w.scene.build()
         rs = o.scene(b)
         rt = o.scene(b, tag=True)
-        rays = camera_rays(w, 2000, seed=len(name))
-        vkey = np.stack([rng.integers(0, w.width, 2000), rng.integers(0, w.height, 2000),
-                         rng.integers(0, w.spp, 2000), rng.integers(0, 4, 2000)], 1).astype(np.int32)
-        t, ob, pr = rt.trace_rays(rays.astype(np.float64), seed=w.seed, volume_key=vkey)
-        _, occ, _ = rt.trace_rays(rays.astype(np.float64), any_hit=True, seed=w.seed, volume_key=vkey)
-        np.savez_compressed(os.path.join(HERE, f"hits_{name}.npz"), rays=rays, vkey=vkey, t=t, obj=ob, prim=pr,
-                            occluded=occ >= 0)
-        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        hits = ray_fixture(rt, w, name, rng)
+        hits["top"] = O.top_tree_from_reference(rs.top_bvh())
+        np.savez_compressed(os.path.join(HERE, f"hits_{name}.npz"), **hits)
         x, y, s = path_keys(w, 1500, seed=7 + len(name))
-        rgb = rs.trace_paths(p, x, y, s)
-        np.savez_compressed(os.path.join(HERE, f"paths_{name}.npz"), x=x, y=y, s=s, rgb=rgb)
+        np.savez_compressed(os.path.join(HERE, f"paths_{name}.npz"), **path_fixture(o, rs, w, x, y, s))
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
         if name in ("cornell", "tiny"):
             img, _, _ = rs.render(p, os.cpu_count() or 1)
             np.savez_compressed(os.path.join(HERE, f"image_{name}.npz"), rgb=img, spp=w.spp)
@@ -158,6 +230,19 @@ def oracle64k_fixtures(o):
         print("golden oracle64k", name, f"{ms / 1000:.1f} s", flush=True)
 
 
+def oracle64k_full_fixtures(o, threads=None):
+    """oracle64k_<case>.npz for the full-size frames of ORACLE_64K_FULL (FP32 film: the
+    oracle's own Monte Carlo noise at 65,536 spp is far above FP32 rounding)."""
+    threads = threads or os.cpu_count() or 1
+    for name, fn in ORACLE_64K_FULL.items():
+        w = fn()
+        rs = o.scene(w.scene.build())
+        img, ms, _ = rs.render(native.params(w.width, w.height, w.spp, w.max_bounces, w.seed), threads)
+        np.savez_compressed(os.path.join(HERE, f"oracle64k_{name}.npz"), rgb=img.astype(np.float32), spp=w.spp,
+                            seed=w.seed, render_ms=ms, threads=threads)
+        print("golden oracle64k", name, f"{ms / 1000:.1f} s", flush=True)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -175,8 +260,14 @@ def main():
     if sys.argv[1:] == ["oracle64k"]:
         oracle64k_fixtures(o)
         return
+    if sys.argv[1:2] == ["full"]:      # full [name...]: the full-size frames
+        full_fixtures(o, sys.argv[2:])
+        return
+    if sys.argv[1:2] == ["oracle64k_full"]:
+        oracle64k_full_fixtures(o, int(sys.argv[2]) if len(sys.argv) > 2 else None)
+        return
     if sys.argv[1:2] == ["cases"]:     # cases <name>...: only the per-case files of those cases
-        case_fixtures(o, sys.argv[2:])
+        case_fixtures(o, sys.argv[2:] or None)
         return
     rng = np.random.default_rng(20261203)
     n = 600

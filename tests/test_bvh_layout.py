@@ -1,11 +1,30 @@
-"""Host BVH builders reproduce the reference node layout bit for bit
-(Mesh::_buildPackedBVH, src/core/Hittables/Mesh.cpp:383-521): node boxes in
-double, child/leaf indices and the triangle order (_triangleIndices)."""
+"""Host BVH builders reproduce the reference node layouts bit for bit.
+
+* Mesh BVH (Mesh::_buildPackedBVH, src/core/Hittables/Mesh.cpp:383-521): node
+  boxes in double, child/leaf indices and the triangle order (_triangleIndices),
+  on small meshes and on the benchmarked 1,310,722-triangle mesh (sha256 of the
+  reference's full arrays).
+* Top-level tree (BVHNode::BVHNode, src/core/Hittables/BVHNode.cpp:142-185, built
+  by Scene::updateAccelerationStructure, src/scene/Scene.cpp:655-688): node order,
+  child order, child kinds and object ids exactly, child boxes as the reference's
+  double boxes rounded outward to FP32; on every parity case and on the 1e5-instance
+  benchmark frame.
+"""
+import hashlib
+
 import numpy as np
 import pytest
 
-from cases import BVH_CASES
+import oracle as O
+from cases import BVH_CASES, CASES, FULL_CASES
 from luz_b200 import native
+
+
+def sha256(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
 
 
 @pytest.mark.parametrize("name", sorted(BVH_CASES))
@@ -42,3 +61,27 @@ def test_empty_scene_packs():
     from luz_b200.desc import Scene
     pk = native.Pack(Scene().build())
     assert pk.info().top_leaf_objects == 0
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_top_level_tree_matches_reference(name, golden):
+    ref = golden("hits_" + name)["top"]
+    ours = O.top_tree_from_pack(native.Pack(CASES[name]().scene.build()))
+    assert len(ours) == len(ref) and np.array_equal(ours, ref)
+
+
+@pytest.mark.parametrize("name", sorted(FULL_CASES))
+def test_full_size_layouts_match_reference(name, golden):
+    """The benchmarked frames: every mesh BVH (the 1,310,722-triangle mesh has 448,391
+    nodes) and the top-level tree (1e5 instances) equal the reference's arrays."""
+    g = golden("full_" + name)
+    w = FULL_CASES[name]()
+    pk = native.Pack(w.scene.build())
+    for mi in range(len(w.scene.meshes)):
+        nodes, order = pk.mesh_bvh(mi)
+        assert len(nodes) == int(g[f"mesh{mi}_nodes"])
+        assert nodes[:64].tobytes() == g[f"mesh{mi}_head"].tobytes()
+        assert sha256(nodes, order) == str(g[f"mesh{mi}_sha256"])
+    top = O.top_tree_from_pack(pk)
+    assert len(top) == int(g["top_len"]) and np.array_equal(top[:4096], g["top_head"])
+    assert sha256(top) == str(g["top_sha256"])

@@ -1,24 +1,49 @@
 """GPU parity against the oracle (the reference's own outputs and the FP32 restatement).
 
 - ray batches: GPU traversal == FP32 restatement bit for bit (t, object,
-  primitive, u, v), and agrees with the reference's hits;
+  primitive, u, v); against the reference, object and primitive ids are equal
+  on every ray the oracle does not mark as FP32-ambiguous;
 - per-path radiance under the reference Sampler stream: within 1e-4 relative
-  for almost every path (the rest are grazing / very sharp-lobe paths where
-  FP32 and FP64 diverge; see the thresholds);
+  (absolute below 1e-3) on every path the oracle does not mark as ambiguous
+  (oracle.ambiguous_paths: the reference's own radiance moves by more than the
+  tolerance when its draws move by a few FP32 ulps of what they become: a draw
+  within rounding of a lobe or Russian-roulette threshold, a very sharp lobe, a
+  grazing vertex); the excluded fraction is bounded and printed per case;
+- the same at the benchmarked sizes: the 1920x1080 frame over the
+  1,310,722-triangle mesh and the 1280x720 frame over 1e5 instances;
 - whole images against the reference film;
 - full-size properties: determinism, sample additivity, finiteness.
 """
 import numpy as np
 import pytest
 
-from cases import CASES, camera_rays
+from cases import CASES, FULL_CASES, camera_rays
 from luz_b200 import native, scenes
 from luz_b200.desc import OBJ_MESH, OBJ_MESH_INSTANCE
 
 pytestmark = pytest.mark.gpu
 
-# fraction of paths within 1e-4 relative of the reference, per case
-PATH_FRACTION = {"cornell": 0.995, "instancing": 0.99, "tiny": 0.98, "glossy": 0.97, "linear_sky": 0.975, "ies": 0.98, "atmosphere": 0.985, "caustics": 0.97}
+# upper bound on the fraction of paths the oracle may exclude as ambiguous, per case
+# (measured: linear_sky 0.078 (f/16 thin lens, mirror spheres), glossy 0.010, ies 0.005,
+# cornell 0.003, tiny 0.003, caustics 0.001, instancing 0.001, atmosphere 0)
+AMBIGUOUS_MAX = {"linear_sky": 0.10}
+REL_TOL = 1e-4
+
+
+def path_rel(rgb, ref):
+    """max over channels of |gpu - ref| / max(|ref|, 1e-3)"""
+    return (np.abs(rgb - ref) / np.maximum(np.abs(ref), 1e-3)).max(axis=1)
+
+
+def check_paths(label, rgb, ref, amb, amb_max=0.02):
+    rel = path_rel(rgb.astype(np.float64), ref)
+    print(f"{label}: {amb.mean():.4f} of {len(amb)} paths ambiguous; "
+          f"{(rel <= REL_TOL).mean():.4f} of all paths within {REL_TOL}")
+    assert amb.mean() <= amb_max, amb.mean()
+    bad = np.flatnonzero((rel > REL_TOL) & ~amb)
+    assert bad.size == 0, (bad[:10], rel[bad[:10]])
+    ok = ~amb
+    assert abs(rgb[ok].mean() - ref[ok].mean()) <= 1e-4 * max(ref[ok].mean(), 1e-6) + 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +78,11 @@ def test_hits_agree_with_reference(name, gpu_scenes, golden):
     kinds = np.array([w.scene.objects[o]["kind"] if o >= 0 else 0 for o in gd["obj"]])
     meshy = np.isin(kinds, [OBJ_MESH, OBJ_MESH_INSTANCE])
     agree = (h["object"] == gd["obj"]) & (~meshy | (h["primitive"] == gd["prim"]))
-    assert agree.mean() >= 0.995
+    amb = gd["ambiguous"]
+    assert amb.mean() <= 0.01 and agree[~amb].all(), np.flatnonzero(~agree & ~amb)[:10]
+    a = g.trace_rays(gd["rays"], any_hit=True, seed=w.seed, volume_key=gd["vkey"])
+    same = (a["object"] >= 0) == gd["occluded"]
+    assert same[~gd["ambiguous_any"]].all()
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -61,12 +90,38 @@ def test_per_path_radiance_matches_reference(name, gpu_scenes, golden):
     w, b, g = gpu_scenes[name]
     gd = golden("paths_" + name)
     p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
-    rgb = g.trace_paths(p, gd["x"], gd["y"], gd["s"]).astype(np.float64)
-    ref = gd["rgb"]
-    rel = np.abs(rgb - ref) / np.maximum(np.abs(ref), 1e-3)   # 1e-4 relative (absolute below 1e-3)
-    frac = (rel.max(axis=1) <= 1e-4).mean()
-    assert frac >= PATH_FRACTION[name], frac
-    assert abs(rgb.mean() - ref.mean()) <= 1e-3 * max(ref.mean(), 1e-6) + 1e-6
+    rgb = g.trace_paths(p, gd["x"], gd["y"], gd["s"])
+    check_paths(name, rgb, gd["rgb"], gd["ambiguous"], AMBIGUOUS_MAX.get(name, 0.02))
+
+
+@pytest.mark.parametrize("name", sorted(FULL_CASES))
+def test_full_size_frame_parity(name, golden, restate):
+    """The benchmarked frames at full size: 2,000 rays (bit for bit with the FP32
+    restatement; ids equal to the reference's on unambiguous rays) and 4,096 paths
+    (plus the lit paths of the mostly dark 1e5-instance frame) within 1e-4 of the
+    reference on unambiguous paths."""
+    w = FULL_CASES[name]()
+    b = w.scene.build()
+    gd = golden("full_" + name)
+    g = native.GpuScene(b)
+    try:
+        rays, vkey = gd["hit_rays"], gd["hit_vkey"]
+        h = g.trace_rays(rays, seed=w.seed, volume_key=vkey)
+        hr = restate.trace(native.Pack(b), rays, seed=w.seed, volume_key=vkey)
+        assert h.tobytes() == hr.tobytes()
+        kinds = np.array([w.scene.objects[o]["kind"] if o >= 0 else 0 for o in gd["hit_obj"]])
+        meshy = np.isin(kinds, [OBJ_MESH, OBJ_MESH_INSTANCE])
+        agree = (h["object"] == gd["hit_obj"]) & (~meshy | (h["primitive"] == gd["hit_prim"]))
+        amb = gd["hit_ambiguous"]
+        assert amb.mean() <= 0.01 and agree[~amb].all(), np.flatnonzero(~agree & ~amb)[:10]
+        a = g.trace_rays(rays, any_hit=True, seed=w.seed, volume_key=vkey)
+        assert ((a["object"] >= 0) == gd["hit_occluded"])[~gd["hit_ambiguous_any"]].all()
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        rgb = g.trace_paths(p, gd["path_x"], gd["path_y"], gd["path_s"])
+        check_paths(name, rgb, gd["path_rgb"], gd["path_ambiguous"])
+        assert (gd["path_rgb"].max(axis=1) > 0).sum() >= 50   # lit paths are part of the check
+    finally:
+        g.close()
 
 
 @pytest.mark.parametrize("name", ["cornell", "tiny"])

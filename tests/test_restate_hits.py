@@ -1,9 +1,13 @@
 """The FP32 restatement of the traversal against the reference's own hits
-(closest hit: object and mesh primitive ids; any hit: occlusion)."""
+(closest hit: object and mesh primitive ids; any hit: occlusion).
+
+Rays the oracle marks as FP32-ambiguous (their reference hit changes under
+perturbations of a few FP32 ulps: edge grazes, near ties in t;
+oracle.ambiguous_rays) are excluded; on every other ray the ids are equal."""
 import numpy as np
 import pytest
 
-from cases import CASES
+from cases import CASES, FULL_CASES
 from luz_b200 import native
 from luz_b200.desc import OBJ_MESH, OBJ_MESH_INSTANCE
 
@@ -25,7 +29,9 @@ def test_restated_closest_hits_match_reference(name, golden, restate):
     meshy = np.isin(kinds, [OBJ_MESH, OBJ_MESH_INSTANCE])
     same_prim = ~meshy | (h["primitive"] == g["prim"])
     agree = same_obj & same_prim
-    assert agree.mean() >= 0.995, agree.mean()
+    amb = g["ambiguous"]
+    assert amb.mean() <= 0.01, amb.mean()
+    assert agree[~amb].all(), np.flatnonzero(~agree & ~amb)[:10]
     hit = agree & (g["obj"] >= 0)
     rel = np.abs(h["t"][hit] - g["t"][hit]) / np.maximum(g["t"][hit], 1e-6)
     assert np.all(rel < T_TOLERANCE.get(name, 1e-4)), rel.max()
@@ -37,4 +43,23 @@ def test_restated_any_hits_match_reference(name, golden, restate):
     w = CASES[name]()
     pk = native.Pack(w.scene.build())
     h = restate.trace(pk, g["rays"], any_hit=True, seed=w.seed, volume_key=g["vkey"])
-    assert ((h["object"] >= 0) == g["occluded"]).mean() >= 0.995
+    same = (h["object"] >= 0) == g["occluded"]
+    amb = g["ambiguous_any"]
+    assert amb.mean() <= 0.01 and same[~amb].all(), np.flatnonzero(~same & ~amb)[:10]
+
+
+@pytest.mark.parametrize("name", sorted(FULL_CASES))
+def test_restated_hits_match_reference_full_size(name, golden, restate):
+    """2,000 rays into the benchmarked frames (the 1,310,722-triangle mesh; 1e5 instances)."""
+    g = golden("full_" + name)
+    w = FULL_CASES[name]()
+    pk = native.Pack(w.scene.build())
+    h = restate.trace(pk, g["hit_rays"], seed=w.seed, volume_key=g["hit_vkey"])
+    kinds = np.array([w.scene.objects[o]["kind"] if o >= 0 else 0 for o in g["hit_obj"]])
+    meshy = np.isin(kinds, [OBJ_MESH, OBJ_MESH_INSTANCE])
+    agree = (h["object"] == g["hit_obj"]) & (~meshy | (h["primitive"] == g["hit_prim"]))
+    amb = g["hit_ambiguous"]
+    assert amb.mean() <= 0.01 and agree[~amb].all(), np.flatnonzero(~agree & ~amb)[:10]
+    a = restate.trace(pk, g["hit_rays"], any_hit=True, seed=w.seed, volume_key=g["hit_vkey"])
+    same = (a["object"] >= 0) == g["hit_occluded"]
+    assert same[~g["hit_ambiguous_any"]].all()

@@ -25,13 +25,19 @@ from luz_b200 import native
 
 SCENE_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scenes")
 SCENES = sorted(os.path.basename(p) for p in glob.glob(os.path.join(SCENE_DIR, "*.luz")))
-# Where the reference's own example scenes live when its sources are present
-# (same default as oracle/Makefile's REF_ROOT).
-REF_ROOT = os.environ.get("LUZ_REF_ROOT", "/root/reference")
-# fraction of paths within 1e-4 relative on the GPU (FP32 traversal and shading
-# against the reference's FP64; the glossy and atmosphere cases of the parity
-# suite sit at 0.97-0.985)
-GPU_PATH_FRACTION = 0.95
+
+
+def _reference_tree():
+    """The reference tree the oracle libraries were built from (oracle/Makefile records
+    it in oracle/_ref/ref_root.txt), or LUZ_REFERENCE; None where neither is present."""
+    root = os.environ.get("LUZ_REFERENCE")
+    rec = os.path.join(os.path.dirname(SCENE_DIR), "..", "..", "oracle", "_ref", "ref_root.txt")
+    if not root and os.path.exists(rec):
+        root = open(rec).read().strip() or None
+    return root
+# bound on the fraction of paths the oracle's FP32-ambiguity probe may exclude
+# (oracle.ambiguous_paths); every other path is within 1e-4 of the reference
+GPU_AMBIGUOUS_MAX = 0.05
 
 
 def _oracle():
@@ -106,7 +112,8 @@ def test_packed_settings_and_objects():
 def test_reference_example_scenes_pack():
     """Every example scene the reference ships packs, and its packed description
     traces as the parsed scene (runs only where the reference sources are)."""
-    examples = sorted(glob.glob(os.path.join(REF_ROOT, "examples", "scenes", "*.luz")))
+    root = _reference_tree()
+    examples = sorted(glob.glob(os.path.join(root, "examples", "scenes", "*.luz"))) if root else []
     if not examples:
         pytest.skip("the reference's example scenes are not on this machine")
     o = _oracle()
@@ -132,10 +139,16 @@ def test_gpu_renders_parsed_scene_as_reference(name):
     x, y, s = _paths(pk, n=1500, seed=11)
     p = native.params(pk.width, pk.height, pk.spp, pk.max_bounces, 31337)
     ref = parsed.trace_paths(p, x, y, s)
+    import ctypes as C
+    import oracle as O
+    from luz_b200 import desc as D
+    cam = C.cast(C.c_void_p(pk.ptr()), C.POINTER(D.SceneDesc)).contents.camera
+    amb = O.ambiguous_paths(o, parsed, p, x, y, s, ref, O.path_deltas(pk.width, pk.height, cam))
     rgb = g.trace_paths(p, x, y, s).astype(np.float64)
-    rel = np.abs(rgb - ref) / np.maximum(np.abs(ref), 1e-3)
-    frac = (rel.max(axis=1) <= 1e-4).mean()
-    assert frac >= GPU_PATH_FRACTION, frac
+    rel = (np.abs(rgb - ref) / np.maximum(np.abs(ref), 1e-3)).max(axis=1)
+    print(f"{name}: {amb.mean():.4f} of paths ambiguous; {(rel <= 1e-4).mean():.4f} within 1e-4")
+    assert amb.mean() <= GPU_AMBIGUOUS_MAX, amb.mean()
+    assert (rel[~amb] <= 1e-4).all(), np.flatnonzero((rel > 1e-4) & ~amb)[:10]
     assert abs(rgb.mean() - ref.mean()) <= 0.02 * max(ref.mean(), 1e-6) + 1e-6
     img, _ = g.render(native.params(pk.width, pk.height, pk.spp, pk.max_bounces, 31337))
     assert np.isfinite(img).all() and img.mean() > 0

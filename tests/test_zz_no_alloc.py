@@ -3,10 +3,12 @@
 Some hosts cannot call cudaMalloc while they render: an engine whose device
 memory belongs to its own allocator, or a per-frame loop that cannot afford the
 device-wide synchronisation cudaMalloc/cudaFree imply. This entry point keeps
-its path state and film in a fixed file-scope device array instead. The test
-calls it through the C ABI twice in a row and compares both films with the
-allocating entry point (luz_gpu_render_device) on the same scene; it also checks
-that an image larger than the static film is refused. It runs last so that a
+its path state and film in a fixed file-scope device array instead. The tests
+call it through the C ABI twice in a row and compare both films with the
+allocating entry point (luz_gpu_render_device) on the same scene, once on an
+image that fits one static wave and once on one that takes several waves
+(pixel chunks of the 131,072-path arena); they also check that an image larger
+than the static film is refused. The file runs last so that a
 stop-at-first-failure run has executed every other test already.
 """
 import ctypes as C
@@ -53,13 +55,38 @@ def test_noalloc_matches_allocating_render_twice():
         g.close()
 
 
+def test_noalloc_multi_wave_equals_allocating_render():
+    """512x288 pixels x 4 samples = 589,824 paths: five waves of the static arena
+    against one wave of the allocating render. Each wave holds all four samples of
+    its pixels in both, so every pixel's FP64 sum is the same sequence: equal bit
+    for bit, on two calls in a row."""
+    import torch
+    lib = native.lib()
+    w = CASES["instancing"]()
+    g = native.GpuScene(w.scene.build())
+    try:
+        p = native.params(512, 288, 4, w.max_bounces, w.seed)
+        n = 512 * 288 * 3
+        stream = torch.cuda.current_stream().cuda_stream
+        ref = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _render(lib.luz_gpu_render_device, g, p, ref, stream)
+        for _ in range(2):
+            out = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
+            st = _render(lib.luz_gpu_render_device_noalloc, g, p, out, stream)
+            torch.cuda.synchronize()
+            assert st.waves == 5
+            assert np.array_equal(out.cpu().numpy(), ref.cpu().numpy())
+    finally:
+        g.close()
+
+
 def test_noalloc_rejects_image_beyond_static_film():
     import torch
     lib = native.lib()
     w = CASES["tiny"]()
     g = native.GpuScene(w.scene.build())
     try:
-        p = native.params(2000, 1500, 1, 2, 1)   # 3,000,000 pixels > 2,900,000
+        p = native.params(2000, 1500, 1, 2, 1)   # 3,000,000 pixels > 2,800,000
         out = torch.zeros(3, dtype=torch.float32, device="cuda")
         with pytest.raises(native.LuzError) as e:
             _render(lib.luz_gpu_render_device_noalloc, g, p, out, torch.cuda.current_stream().cuda_stream)
