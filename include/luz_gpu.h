@@ -334,6 +334,39 @@ int luz_gpu_scene_set_path_budget(luz_gpu_scene* scene, int64_t bytes);
  * The reference's counterpart is the fixed stack of Mesh::hit (Mesh.cpp:578-660). */
 int luz_gpu_scene_set_traversal_limits(luz_gpu_scene* scene, int32_t mesh_entries, int32_t top_entries);
 
+/* Launch tuning of a scene handle (zeros = defaults). None of it changes a film: the
+ * image does not depend on the wave size, the grid or where nodes are read from.
+ *   wave_paths:           paths per wave (default 64 Mi, capped by the path budget);
+ *   staged_top_nodes:     1 = the trace kernels copy the breadth-first top of the scene's
+ *                         largest collapsed mesh BVH (21 nodes) into shared memory per
+ *                         block and read those nodes there;
+ *   *_blocks_per_sm:      blocks per SM of the persistent closest-hit / any-hit grids and
+ *                         of the shade grid (default: full occupancy; larger values are
+ *                         capped at it).
+ * No counterpart in the reference (its worker count is Scene::setRenderingThreads). */
+typedef struct LuzTuneParams {
+    int64_t wave_paths;
+    int32_t staged_top_nodes;
+    int32_t extend_blocks_per_sm;
+    int32_t shadow_blocks_per_sm;
+    int32_t shade_blocks_per_sm;
+} LuzTuneParams;
+typedef struct LuzTuneTrial {
+    LuzTuneParams params;
+    double render_ms;             /* device time of the trial render */
+} LuzTuneTrial;
+int luz_gpu_scene_set_tuning(luz_gpu_scene* scene, const LuzTuneParams* tune);
+int luz_gpu_scene_get_tuning(const luz_gpu_scene* scene, LuzTuneParams* tune);
+/* Autotuner: times renders of `params` on the device (CUDA events; each trial rendered
+ * twice, the second timed) while it changes one knob at a time from the handle's
+ * current tuning (staged nodes on/off; waves of 4 Mi, 16 Mi and 64 Mi paths; the
+ * closest-hit grid at full occupancy or one block fewer; the any-hit grid at full or
+ * half occupancy), keeps every change that lowers the time, and leaves the best
+ * tuning on the handle (also copied to `chosen` when not NULL). The trials (up to
+ * trial_capacity) and their count go to trials / trial_count when not NULL. */
+int luz_gpu_autotune(luz_gpu_scene* scene, const LuzRenderParams* params, LuzTuneParams* chosen,
+                     LuzTuneTrial* trials, int32_t trial_capacity, int32_t* trial_count);
+
 /* ---- hot path ------------------------------------------------------------- */
 /* Full render: W*H*spp paths through the wavefront integrator; rgb_out is the
  * host film (W*H*3, row-major, y = 0 first) holding per-pixel means, exactly
@@ -474,6 +507,15 @@ int luz_gpu_render_ex(luz_gpu_scene* scene, const LuzRenderParams* params,
                       const LuzAdaptiveParams* adaptive, float* rgb_out,
                       const LuzNforBuffers* nfor, int32_t* samples_out,
                       LuzRenderStats* stats);
+
+/* Renders listed pixels only: the _threadRender loop (src/renderer/Threads.cpp:551-641,
+ * adaptive sampling off) for each pixel index (y * width + x; distinct, inside the
+ * image, else LUZ_E_INVALID), as the reference's block scheduler hands pixels to its
+ * workers (Threads.cpp:410-451). rgb_out (count * 3 floats, host) receives each
+ * listed pixel's mean over params->spp samples, the value luz_gpu_render writes for
+ * it. stats->samples = count * spp. */
+int luz_gpu_render_pixels(luz_gpu_scene* scene, const LuzRenderParams* params, const int32_t* pixels, int64_t count,
+                          float* rgb_out, LuzRenderStats* stats);
 
 /* ---- NFOR denoiser ----------------------------------------------------------
  * Denoise::applyNFOR (src/core/Denoise/NFOR.cpp:977-1102) on the GPU in FP64:

@@ -85,10 +85,11 @@ __device__ __forceinline__ void bin_append(uint32_t* bin_count, const PathBuf& P
 // instances, volumes); a scene without them runs traversal code without the
 // instance transform or the volume sampler, and skips the per-ray sampler key.
 // COUNT instantiations add the record counts of LUZ_RENDER_COUNT; the others
-// carry no counting code at all.
+// carry no counting code (the shadow kernel counts under a runtime branch).
 template <uint32_t F, bool COUNT>
 __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
+    if constexpr ((F & TF_STAGED) != 0) stage_top_nodes(S);
     LocalStack<true> st;
     const uint32_t count = C->count[bounce];
     const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
@@ -124,9 +125,13 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
 
 // ---------------------------------------------------------------------------- shadow (any hit)
 
-template <uint32_t F, bool COUNT>
+// (The record counts stay a runtime branch here: an instantiation without them
+// measured 2.6x slower on B200, at 2.3 instead of 7.0 active threads per warp
+// instruction for the same rays, a reconvergence effect of the smaller loop body.)
+template <uint32_t F>
 __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
+    if constexpr ((F & TF_STAGED) != 0) stage_top_nodes(S);
     LocalStack<false> st;
     const uint32_t count = C->shadow[bounce];
     while (true) {
@@ -151,7 +156,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene
             if (tag & 0x80000000u) P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
             else P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if constexpr (COUNT) {
+        if (S.counters) {
             atomicAdd(&S.counters[3], (unsigned long long)vs.nodes);
             atomicAdd(&S.counters[4], (unsigned long long)vs.tris);
             atomicAdd(&S.counters[5], (unsigned long long)vs.top);
@@ -161,10 +166,16 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow(DScene
 }
 
 using TraceKernel = void (*)(DScene, WaveArgs, PathBuf, Ctrl*, int);
-const TraceKernel kExtendKernels[2][4] = {{k_extend<0, false>, k_extend<1, false>, k_extend<2, false>, k_extend<3, false>},
-                                          {k_extend<0, true>, k_extend<1, true>, k_extend<2, true>, k_extend<3, true>}};
-const TraceKernel kShadowKernels[2][4] = {{k_shadow<0, false>, k_shadow<1, false>, k_shadow<2, false>, k_shadow<3, false>},
-                                          {k_shadow<0, true>, k_shadow<1, true>, k_shadow<2, true>, k_shadow<3, true>}};
+// Indexed [count][features | staged]: TF_STAGED variants read the scene's top
+// collapsed nodes from shared memory (a tuning choice, off by default: on the
+// 1080p glossy frame they measured 2.5% slower, the nodes being L1-resident).
+const TraceKernel kExtendKernels[2][8] = {
+    {k_extend<0, false>, k_extend<1, false>, k_extend<2, false>, k_extend<3, false>,
+     k_extend<4, false>, k_extend<5, false>, k_extend<6, false>, k_extend<7, false>},
+    {k_extend<0, true>, k_extend<1, true>, k_extend<2, true>, k_extend<3, true>,
+     k_extend<4, true>, k_extend<5, true>, k_extend<6, true>, k_extend<7, true>}};
+const TraceKernel kShadowKernels[8] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>,
+                                       k_shadow<4>, k_shadow<5>, k_shadow<6>, k_shadow<7>};
 
 
 // Adds one wave's per-bounce queue sizes to the render totals (no host wait per wave).
@@ -673,6 +684,7 @@ struct luz_gpu_scene {
     int64_t out_cap = 0;
     int sms = 0;
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
+    LuzTuneParams tune{};            // luz_gpu_scene_set_tuning / luz_gpu_autotune; zeros = defaults
     TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
     ShadeKernel shade = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -845,11 +857,15 @@ struct StageTimer {
 void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_t& launches, StageTimer& T,
                     ShadeKernel shade = nullptr)
 {
-    const int g_ext = s->sms * s->occ_ext, g_sh = s->sms * s->occ_sh, g_shade = s->sms * s->occ_shade;
+    auto blocks = [](int tuned, int occ) { return tuned > 0 ? std::min(tuned, occ) : occ; };
+    const int g_ext = s->sms * blocks(s->tune.extend_blocks_per_sm, s->occ_ext);
+    const int g_sh = s->sms * blocks(s->tune.shadow_blocks_per_sm, s->occ_sh);
+    const int g_shade = s->sms * blocks(s->tune.shade_blocks_per_sm, s->occ_shade);
     if (!shade) shade = s->shade;
     const int count = s->ds.counters ? 1 : 0;   // LUZ_RENDER_COUNT renders run the counting instantiations
-    const TraceKernel extend = kExtendKernels[count][s->ds.k.features & TF_ALL];
-    const TraceKernel shadow = kShadowKernels[count][s->ds.k.features & TF_ALL];
+    const uint32_t kv = (s->ds.k.features & TF_ALL) | (s->tune.staged_top_nodes && s->ds.top4_count ? TF_STAGED : 0u);
+    const TraceKernel extend = kExtendKernels[count][kv];
+    const TraceKernel shadow = kShadowKernels[kv];
     for (int b = 0; b <= w.max_bounces; b++) {
         T.mark(st, 0, true);
         extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
@@ -1050,7 +1066,8 @@ void render_prepare(RenderJob& J)
     prepare_caustics(s, p, J.st);
     J.w = base_args(s, p);
     J.npix = (int64_t)p->width * p->height;
-    const int64_t n = s->reserve_paths(std::min<int64_t>(J.wave_target, J.npix * (int64_t)p->spp));
+    const int64_t target = s->tune.wave_paths > 0 ? std::min<int64_t>(s->tune.wave_paths, J.wave_target) : J.wave_target;
+    const int64_t n = s->reserve_paths(std::min<int64_t>(target, J.npix * (int64_t)p->spp));
     J.s_wave = (int)std::min<int64_t>(p->spp, n);
     J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, n / J.s_wave));
     if (s->film_pix < J.npix) {
@@ -1213,9 +1230,12 @@ std::vector<uint32_t> round_ends(const AdaptiveRule& R)
     return e;
 }
 
+// pixels / pixel_count: render only these pixels (y * width + x, distinct); rgb_out then
+// holds pixel_count means in list order.
 int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptiveParams* ad, float* rgb_out,
                  const LuzNforBuffers* nfor, int32_t* samples_out, LuzRenderStats* stats,
-                 const LuzNforSettings* denoise = nullptr, double* denoised_out = nullptr)
+                 const LuzNforSettings* denoise = nullptr, double* denoised_out = nullptr,
+                 const int32_t* pixels = nullptr, int64_t pixel_count = 0)
 {
     check_params(p);
     check_adaptive(ad);
@@ -1264,10 +1284,23 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     uint32_t* act_count = D.get<uint32_t>(2, st);
     float* d_rgb = D.get<float>(3 * npix, st);
     int32_t* d_used = D.get<int32_t>(npix, st);
+    const int64_t n_start = pixels ? pixel_count : npix;
     {
-        std::vector<uint32_t> all((std::size_t)npix);
-        for (int64_t i = 0; i < npix; i++) all[(std::size_t)i] = (uint32_t)i;
-        CK(cudaMemcpyAsync(act[0], all.data(), sizeof(uint32_t) * (std::size_t)npix, cudaMemcpyHostToDevice, st));
+        std::vector<uint32_t> all((std::size_t)n_start);
+        if (pixels) {
+            std::vector<char> seen((std::size_t)npix, 0);
+            for (int64_t i = 0; i < pixel_count; i++) {
+                if (pixels[i] < 0 || pixels[i] >= npix || seen[(std::size_t)pixels[i]])
+                    throw Status(LUZ_E_INVALID, "Pixel list entries must be distinct and inside the image.");
+                seen[(std::size_t)pixels[i]] = 1;
+                all[(std::size_t)i] = (uint32_t)pixels[i];
+            }
+        } else {
+            for (int64_t i = 0; i < npix; i++) all[(std::size_t)i] = (uint32_t)i;
+        }
+        if (n_start > 0)
+            CK(cudaMemcpyAsync(act[0], all.data(), sizeof(uint32_t) * (std::size_t)n_start, cudaMemcpyHostToDevice,
+                               st));
         CK(cudaStreamSynchronize(st));
     }
 
@@ -1288,7 +1321,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     StageTimer T;
     int64_t launches = 0, waves = 0;
     double samples = 0.0;
-    uint32_t n_act = (uint32_t)npix, done_to = 0;
+    uint32_t n_act = (uint32_t)n_start, done_to = 0;
     int cur = 0;
     for (uint32_t e : ends) {
         if (n_act == 0) break;
@@ -1333,7 +1366,14 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     unsigned long long tot[2] = {0, 0};
     finish_status(s, st, s->totals, tot);
-    CK(cudaMemcpy(rgb_out, d_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    if (pixels) {
+        std::vector<float> full((std::size_t)(3 * npix));
+        CK(cudaMemcpy(full.data(), d_rgb, sizeof(float) * full.size(), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < pixel_count; i++)
+            for (int k = 0; k < 3; k++) rgb_out[3 * i + k] = full[(std::size_t)(3 * (int64_t)pixels[i] + k)];
+    } else {
+        CK(cudaMemcpy(rgb_out, d_rgb, sizeof(float) * 3 * (std::size_t)npix, cudaMemcpyDeviceToHost));
+    }
     if (samples_out) CK(cudaMemcpy(samples_out, d_used, sizeof(int32_t) * (std::size_t)npix, cudaMemcpyDeviceToHost));
     if (nfor) {
         auto down = [&](double* host, const double* dev, int64_t n) {
@@ -1864,6 +1904,20 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         d.counters = nullptr;
         d.mesh_stack_limit = kMeshStack4;
         d.top_stack_limit = kTopStack;
+        // the breadth-first top of the largest mesh's collapsed BVH, staged by the trace kernels
+        d.top4_base = 0;
+        d.top4_count = 0;
+        int64_t best = -1;
+        for (std::size_t m = 0; m < P.meshes.size(); m++) {
+            const GMesh& M = P.meshes[m];
+            if (M.node4_offset < 0 || (int64_t)M.tri_count <= best) continue;
+            int64_t end = (int64_t)P.nodes4.size();
+            for (const GMesh& o : P.meshes)
+                if (o.node4_offset > M.node4_offset) end = std::min<int64_t>(end, o.node4_offset);
+            best = M.tri_count;
+            d.top4_base = (uint32_t)M.node4_offset;
+            d.top4_count = (uint32_t)std::min<int64_t>(kTopNodes4, end - M.node4_offset);
+        }
         d.k = P.consts;
         s->dds = dalloc<DScene>(1);
         CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
@@ -1876,7 +1930,7 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         s->sms = prop.multiProcessorCount;
         const int feat = P.consts.features & TF_ALL;
         s->extend = kExtendKernels[0][feat];
-        s->shadow = kShadowKernels[0][feat];
+        s->shadow = kShadowKernels[feat];
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_ext, s->extend, kBlock, 0));
         s->shade = shade_kernel(P.consts.caustics.enabled ? 1 : 0);
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_shade, s->shade, kBlock, 0));
@@ -1923,6 +1977,104 @@ int luz_gpu_scene_set_path_budget(luz_gpu_scene* s, int64_t bytes)
             CK(cudaStreamSynchronize(s->stream));
             s->free_paths();
         }
+        return LUZ_OK;
+    });
+}
+
+static void check_tune(const LuzTuneParams& t)
+{
+    if (t.wave_paths < 0 || t.staged_top_nodes < 0 || t.staged_top_nodes > 1 || t.extend_blocks_per_sm < 0
+        || t.shadow_blocks_per_sm < 0 || t.shade_blocks_per_sm < 0)
+        throw Status(LUZ_E_INVALID, "Tuning parameters out of range.");
+}
+
+int luz_gpu_scene_set_tuning(luz_gpu_scene* s, const LuzTuneParams* tune)
+{
+    return guard([&] {
+        if (!s) throw Status(LUZ_E_INVALID, "NULL argument.");
+        LuzTuneParams t{};
+        if (tune) t = *tune;
+        check_tune(t);
+        s->tune = t;
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_scene_get_tuning(const luz_gpu_scene* s, LuzTuneParams* tune)
+{
+    return guard([&] {
+        if (!s || !tune) throw Status(LUZ_E_INVALID, "NULL argument.");
+        *tune = s->tune;
+        return LUZ_OK;
+    });
+}
+
+int luz_gpu_autotune(luz_gpu_scene* s, const LuzRenderParams* p, LuzTuneParams* chosen, LuzTuneTrial* trials,
+                     int32_t trial_capacity, int32_t* trial_count)
+{
+    return guard([&] {
+        if (!s) throw Status(LUZ_E_INVALID, "NULL argument.");
+        check_params(p);
+        if (p->flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported by the autotuner.");
+        CK(cudaSetDevice(s->device));
+        const int64_t npix = (int64_t)p->width * p->height;
+        float* d_out = dalloc<float>((std::size_t)(3 * npix));
+        std::vector<LuzTuneTrial> log;
+        try {
+            // coordinate descent over the knobs, each trial one timed render of the frame
+            LuzTuneParams best = s->tune;
+            auto time_of = [&](const LuzTuneParams& t) {
+                s->tune = t;
+                LuzRenderStats st{};
+                do_render(s, p, d_out, s->stream, &st);   // warm: the first render of a shape allocates
+                do_render(s, p, d_out, s->stream, &st);
+                LuzTuneTrial r{};
+                r.params = t;
+                r.render_ms = st.render_ms;
+                log.push_back(r);
+                return st.render_ms;
+            };
+            double best_ms = time_of(best);
+            auto consider = [&](LuzTuneParams t) {
+                const double ms = time_of(t);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            };
+            {
+                LuzTuneParams t = best;
+                t.staged_top_nodes = best.staged_top_nodes ? 0 : 1;
+                consider(t);
+            }
+            for (int64_t wave : {int64_t(1) << 22, int64_t(1) << 24, int64_t(0)}) {
+                if (wave == best.wave_paths) continue;
+                LuzTuneParams t = best;
+                t.wave_paths = wave;
+                consider(t);
+            }
+            for (int b : {s->occ_ext - 1, s->occ_ext}) {
+                if (b < 1 || b == (best.extend_blocks_per_sm ? best.extend_blocks_per_sm : s->occ_ext)) continue;
+                LuzTuneParams t = best;
+                t.extend_blocks_per_sm = b == s->occ_ext ? 0 : b;
+                consider(t);
+            }
+            for (int b : {s->occ_sh / 2, s->occ_sh}) {
+                if (b < 1 || b == (best.shadow_blocks_per_sm ? best.shadow_blocks_per_sm : s->occ_sh)) continue;
+                LuzTuneParams t = best;
+                t.shadow_blocks_per_sm = b == s->occ_sh ? 0 : b;
+                consider(t);
+            }
+            s->tune = best;
+            if (chosen) *chosen = best;
+        } catch (...) {
+            cudaFree(d_out);
+            throw;
+        }
+        cudaFree(d_out);
+        if (trial_count) *trial_count = (int32_t)log.size();
+        if (trials)
+            for (int32_t i = 0; i < std::min<int32_t>(trial_capacity, (int32_t)log.size()); i++) trials[i] = log[(std::size_t)i];
         return LUZ_OK;
     });
 }
@@ -2088,6 +2240,17 @@ int luz_gpu_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdapt
     return guard([&] {
         if (!s || !rgb_out) throw Status(LUZ_E_INVALID, "NULL argument.");
         return do_render_ex(s, p, adaptive, rgb_out, nfor, samples_out, stats);
+    });
+}
+
+int luz_gpu_render_pixels(luz_gpu_scene* s, const LuzRenderParams* p, const int32_t* pixels, int64_t count,
+                          float* rgb_out, LuzRenderStats* stats)
+{
+    return guard([&] {
+        if (!s || (count > 0 && (!pixels || !rgb_out))) throw Status(LUZ_E_INVALID, "NULL argument.");
+        if (count < 0) throw Status(LUZ_E_INVALID, "Pixel count must be non-negative.");
+        if (count == 0) return LUZ_OK;
+        return do_render_ex(s, p, nullptr, rgb_out, nullptr, nullptr, stats, nullptr, nullptr, pixels, count);
     });
 }
 

@@ -90,6 +90,10 @@ struct alignas(16) GNode {
 // entries the binary near-first traversal would visit after N, L and R, in the
 // same order (see trace.cuh). ref: node4 index, leaf ref, or kEmptySlot.
 constexpr uint32_t kEmptySlot = 0xffffffffu;
+// Collapsed nodes at the front of each mesh's node range in breadth-first order
+// (the root and the next two collapsed levels: the nodes every ray of the mesh
+// visits first); the trace kernels stage them in shared memory.
+constexpr int kTopNodes4 = 21;
 struct alignas(16) GNode4 {
     float lmin[3], lmax[3];
     float rmin[3], rmax[3];

@@ -848,6 +848,30 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
                     return qi;
                 };
                 g.root4_ref = (int32_t)collapse((uint32_t)g.root_ref);
+                // Relayout: the first kTopNodes4 nodes in breadth-first order, the rest in
+                // the collapse's preorder. Only node indices move; every walk is unchanged.
+                const uint32_t b = (uint32_t)g.node4_offset, e = (uint32_t)S.nodes4.size();
+                std::vector<uint32_t> order{(uint32_t)g.root4_ref};
+                for (std::size_t i = 0; i < order.size() && order.size() < (std::size_t)kTopNodes4; i++)
+                    for (int k = 0; k < 4 && order.size() < (std::size_t)kTopNodes4; k++) {
+                        const uint32_t r = S.nodes4[order[i]].ref[k];
+                        if (!(r & kLeafBit)) order.push_back(r);
+                    }
+                std::vector<char> front(e - b, 0);
+                for (uint32_t n : order) front[n - b] = 1;
+                for (uint32_t n = b; n < e; n++)
+                    if (!front[n - b]) order.push_back(n);
+                std::vector<uint32_t> at(e - b);
+                for (std::size_t i = 0; i < order.size(); i++) at[order[i] - b] = b + (uint32_t)i;
+                std::vector<GNode4> re(e - b);
+                for (std::size_t i = 0; i < order.size(); i++) {
+                    GNode4 q = S.nodes4[order[i]];
+                    for (int k = 0; k < 4; k++)
+                        if (!(q.ref[k] & kLeafBit)) q.ref[k] = at[q.ref[k] - b];
+                    re[i] = q;
+                }
+                std::copy(re.begin(), re.end(), S.nodes4.begin() + b);
+                g.root4_ref = (int32_t)at[(uint32_t)g.root4_ref - b];
             }
             // triangles in leaf order
             const bool vn = !mb.vn.empty();

@@ -287,18 +287,25 @@ static __device__ F3 sample_ggx_half(F3 n, float alpha, S2 s)
     const float a2 = alpha * alpha;
     const float phi = kTwoPiF * clamp01f(s.x);
     const float u = fminf(1.0f - 1e-7f, clamp01f(s.y));
-    // (1-u) / (1 + (a2-1) u) and 1 - ct^2 in cancellation-free form (same values in exact arithmetic).
+    // cos^2 = (1-u) / (1 + (a2-1) u) and sin^2 = 1 - cos^2 = a2 u / ((1-u) + a2 u), each from its
+    // own quotient: the same values in exact arithmetic, and sin stays accurate where cos is
+    // within FP32 rounding of 1 (narrow lobes: 1 - ct would carry ~1e-3 relative error there).
     const float omu = 1.0f - u;
-    const float ct = sqrtf(omu / (omu + a2 * u));
-    const float st = sqrtf(fmaxf(0.0f, (1.0f - ct) * (1.0f + ct)));
+    const float q = omu + a2 * u;
+    const float ct = sqrtf(omu / q);
+    const float st = sqrtf((a2 * u) / q);
     return onb_local(make_onb(n), st * cosf(phi), st * sinf(phi), ct);
 }
-__device__ __forceinline__ float ggx_d(float noh, float alpha)
+// GGX D of the half vector h about the normal n (both unit): noh^2 (a2 - 1) + 1 is
+// written as sin^2 + a2 cos^2 with sin^2 = |n x h|^2, which keeps its relative
+// accuracy where noh is within FP32 rounding of 1 (narrow lobes), unlike (1 - noh)(1 + noh).
+__device__ __forceinline__ float ggx_d(F3 n, F3 h, float alpha)
 {
-    noh = clamp01f(noh);
+    const float noh = clamp01f(dot(n, h));
     alpha = fmaxf(1e-4f, alpha);
     const float a2 = alpha * alpha;
-    const float den = ((1.0f - noh) * (1.0f + noh)) + a2 * (noh * noh);   // noh^2 (a2 - 1) + 1
+    const float s2 = noh > 0.0f ? fminf(len2(cross(n, h)), 1.0f) : 1.0f;
+    const float den = s2 + a2 * (noh * noh);
     const float val = a2 / (kPiF * den * den);
     return isfinite(val) ? val : 0.0f;
 }
@@ -320,7 +327,7 @@ static __device__ float ggx_reflection_pdf(F3 n, F3 view, F3 dir, float alpha)
     const F3 h = safe_normalize(view + dir, n);
     const float voh = dot(view, h), noh = dot(n, h);
     if (voh <= 1e-10f || noh <= 0.0f) return 0.0f;
-    const float pdf = ggx_d(noh, alpha) * noh / (4.0f * voh);
+    const float pdf = ggx_d(n, h, alpha) * noh / (4.0f * voh);
     return (isfinite(pdf) && pdf > 0.0f) ? pdf : 0.0f;
 }
 __device__ __forceinline__ F3 color_from_scale(F3 c, float s)
@@ -333,8 +340,7 @@ static __device__ F3 ggx_reflection_bsdfcos(F3 fres, F3 n, F3 view, F3 dir, floa
     const float nov = dot(n, view), nol = dot(n, dir);
     if (nov <= 0.0f || nol <= 0.0f) return F3{0.f, 0.f, 0.f};
     const F3 h = safe_normalize(view + dir, n);
-    const float noh = dot(n, h);
-    const float scale = ggx_d(noh, alpha) * ggx_g(nov, nol, alpha) / (4.0f * nov);
+    const float scale = ggx_d(n, h, alpha) * ggx_g(nov, nol, alpha) / (4.0f * nov);
     return color_from_scale(clamp_color01(fres), scale);
 }
 __device__ __forceinline__ F3 ggx_schlick_bsdfcos(F3 f0, F3 n, F3 view, F3 dir, float alpha)
@@ -386,7 +392,7 @@ static __device__ float ggx_dielectric_pdf(F3 n, F3 view, F3 dir, float alpha, f
     if (fabsf(den) <= 1e-10f) return 0.0f;
     const float F = dielectric_fresnel(voh, ei, et);
     const float dh = fabsf((eta * eta * loh) / (den * den));
-    const float pdf = (1.0f - F) * ggx_d(noh, alpha) * noh * dh;
+    const float pdf = (1.0f - F) * ggx_d(n, h, alpha) * noh * dh;
     return (isfinite(pdf) && pdf > 0.0f) ? pdf : 0.0f;
 }
 static __device__ F3 ggx_dielectric_bsdfcos(F3 color, F3 n, F3 view, F3 dir, float alpha, float ei, float et)
@@ -408,7 +414,7 @@ static __device__ F3 ggx_dielectric_bsdfcos(F3 color, F3 n, F3 view, F3 dir, flo
     const float den = voh + eta * loh;
     if (fabsf(den) <= 1e-10f) return zero;
     const float F = dielectric_fresnel(voh, ei, et);
-    const float scale = (1.0f - F) * ggx_d(noh, alpha) * ggx_g(nov, fabsf(nol), alpha) * eta * eta * fabsf(voh * loh)
+    const float scale = (1.0f - F) * ggx_d(n, h, alpha) * ggx_g(nov, fabsf(nol), alpha) * eta * eta * fabsf(voh * loh)
                         / (nov * den * den);
     return color_from_scale(color, scale);
 }
@@ -1398,7 +1404,7 @@ static __device__ __noinline__ float light_pdf_value(const DScene& S, const GLig
         float closest = kInf, u, v;
         int32_t slot;
         LocalStack<true> st;
-        if (!mesh_closest(S, M, r, kTMin, closest, slot, u, v, -1, vs, st)) return 0.0f;
+        if (!mesh_closest<0u>(S, M, r, kTMin, closest, slot, u, v, -1, vs, st)) return 0.0f;
         F3 n, gn;
         bool front;
         float tu, tv;

@@ -57,6 +57,8 @@ struct DScene {
                                     // instantiations of the trace kernels only)
     int32_t mesh_stack_limit;       // traversal stack bounds enforced (<= kMeshStack4 / kTopStack;
     int32_t top_stack_limit;        // lowered only by luz_gpu_scene_set_traversal_limits)
+    uint32_t top4_base;             // staged nodes: [top4_base, top4_base + top4_count) of nodes4, the
+    uint32_t top4_count;            // breadth-first top of the scene's largest mesh (0: none)
     DCaustics cm;
     GSceneConst k;
 };
@@ -68,7 +70,21 @@ enum ErrBits : uint32_t { ERR_TOP_STACK = 1u, ERR_MESH_STACK = 2u, ERR_CAUSTIC_G
 // scene. (Analytic primitives are always compiled in: an instantiation with
 // meshes as its only kind measured 2.3x slower in the any-hit kernel, at 2.4
 // instead of 6.1 active threads per warp instruction.)
-enum TraceFeature : uint32_t { TF_INSTANCE = 1u, TF_VOLUME = 2u, TF_ALL = 3u };
+// TF_STAGED: the kernel has staged the scene's top collapsed nodes in shared
+// memory (stage_top_nodes) and the mesh walks read them there.
+enum TraceFeature : uint32_t { TF_INSTANCE = 1u, TF_VOLUME = 2u, TF_ALL = 3u, TF_STAGED = 4u };
+
+// The staged nodes (kTopNodes4 x 160 B) of a trace kernel's block.
+static __shared__ float4 s_top4[kTopNodes4 * 10];
+
+// Copies the staged node range into shared memory; every thread of the block calls it
+// once, before its first traversal.
+__device__ __forceinline__ void stage_top_nodes(const DScene& S)
+{
+    const float4* src = reinterpret_cast<const float4*>(S.nodes4 + S.top4_base);
+    for (uint32_t i = threadIdx.x; i < S.top4_count * 10u; i += blockDim.x) s_top4[i] = __ldg(src + i);
+    __syncthreads();
+}
 
 // xobj / xprim name the primitive a secondary ray leaves from. A ray that
 // starts on a planar primitive cannot meet it again at t > 0 in exact
@@ -338,8 +354,41 @@ struct LocalStack {
     }
 };
 
+// A collapsed node from the staged copy when it lies in the staged range, else from
+// global memory (the same bytes either way).
+template <uint32_t F>
+__device__ __forceinline__ GNode4 fetch_node4(const DScene& S, uint32_t ref)
+{
+    if constexpr ((F & TF_STAGED) != 0) {
+        const uint32_t j = ref - S.top4_base;
+        if (j < S.top4_count) {
+            GNode4 n;
+            float4* d = reinterpret_cast<float4*>(&n);
+#pragma unroll
+            for (int k = 0; k < 10; k++) d[k] = s_top4[10 * j + k];
+            return n;
+        }
+    }
+    return load_node4(S.nodes4, ref);
+}
+template <uint32_t F>
+__device__ __forceinline__ GNode4C fetch_node4_entries(const DScene& S, uint32_t ref)
+{
+    if constexpr ((F & TF_STAGED) != 0) {
+        const uint32_t j = ref - S.top4_base;
+        if (j < S.top4_count) {
+            GNode4C n;
+            float4* d = reinterpret_cast<float4*>(&n);
+#pragma unroll
+            for (int k = 0; k < 7; k++) d[k] = s_top4[10 * j + 3 + k];
+            return n;
+        }
+    }
+    return load_node4_entries(S.nodes4, ref);
+}
+
 // Mesh::hit — closest triangle; closest is updated in place.
-template <bool FAST, class Stk>
+template <bool FAST, uint32_t F, class Stk>
 __device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& M, const TRay& r, float tmin,
                                                   float& closest, int32_t& slot, float& bu, float& bv, int32_t skip,
                                                   VolSample& vs, Stk& st)
@@ -373,7 +422,7 @@ __device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& 
                     }
                 }
             } else {
-                const GNode4 n = load_node4(S.nodes4, ref);
+                const GNode4 n = fetch_node4<F>(S, ref);
                 vs.nodes++;
                 float nl = 0.f, nr = 0.f;
                 const F3 noi = FAST ? neg_o_inv(r) : F3{0.f, 0.f, 0.f};
@@ -435,16 +484,16 @@ __device__ __forceinline__ bool mesh_closest_walk(const DScene& S, const GMesh& 
     return hit;
 }
 
-template <class Stk>
+template <uint32_t F, class Stk>
 __device__ __forceinline__ bool mesh_closest(const DScene& S, const GMesh& M, const TRay& r, float tmin, float& closest,
                                              int32_t& slot, float& bu, float& bv, int32_t skip, VolSample& vs, Stk& st)
 {
-    if (mesh_fast_slabs(M, r)) return mesh_closest_walk<true>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
-    return mesh_closest_walk<false>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
+    if (mesh_fast_slabs(M, r)) return mesh_closest_walk<true, F>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
+    return mesh_closest_walk<false, F>(S, M, r, tmin, closest, slot, bu, bv, skip, vs, st);
 }
 
 // Mesh::hitAny
-template <bool FAST, class Stk>
+template <bool FAST, uint32_t F, class Stk>
 __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
                                               int32_t skip, VolSample& vs, Stk& st)
 {
@@ -479,7 +528,7 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
             // monotone in the plane coordinate, so a ray that misses a side box
             // misses the entry boxes inside it. The triangles tested, and so the
             // answer, are the same as with the side tests.
-            const GNode4C n = load_node4_entries(S.nodes4, ref);
+            const GNode4C n = fetch_node4_entries<F>(S, ref);
             vs.nodes++;
             const F3 noi = FAST ? neg_o_inv(r) : F3{0.f, 0.f, 0.f};
             bool ha[4];
@@ -520,12 +569,12 @@ __device__ __forceinline__ bool mesh_any_walk(const DScene& S, const GMesh& M, c
     return hit;
 }
 
-template <class Stk>
+template <uint32_t F, class Stk>
 __device__ __forceinline__ bool mesh_any(const DScene& S, const GMesh& M, const TRay& r, float tmin, float tmax,
                                          int32_t skip, VolSample& vs, Stk& st)
 {
-    if (mesh_fast_slabs(M, r)) return mesh_any_walk<true>(S, M, r, tmin, tmax, skip, vs, st);
-    return mesh_any_walk<false>(S, M, r, tmin, tmax, skip, vs, st);
+    if (mesh_fast_slabs(M, r)) return mesh_any_walk<true, F>(S, M, r, tmin, tmax, skip, vs, st);
+    return mesh_any_walk<false, F>(S, M, r, tmin, tmax, skip, vs, st);
 }
 
 // Rectangle::hit geometric test (Rectangle.cpp:212-249); returns t.
@@ -766,7 +815,7 @@ __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, cons
     case OK_MESH: {
         int32_t slot;
         float u, v;
-        if (mesh_closest(S, S.meshes[O.aux], r, tmin, closest, slot, u, v, src ? r.xprim : -1, vs, st))
+        if (mesh_closest<F>(S, S.meshes[O.aux], r, tmin, closest, slot, u, v, src ? r.xprim : -1, vs, st))
             h = THit{closest, oi, slot, u, v};
         break;
     }
@@ -778,7 +827,7 @@ __device__ __forceinline__ void object_closest(const DScene& S, int32_t oi, cons
         float lc = closest * s;
         int32_t slot;
         float u, v;
-        if (!mesh_closest(S, S.meshes[O.aux], lr, tmin * s, lc, slot, u, v, src ? r.xprim : -1, vs, st)) break;
+        if (!mesh_closest<F>(S, S.meshes[O.aux], lr, tmin * s, lc, slot, u, v, src ? r.xprim : -1, vs, st)) break;
         const float wt = lc / s;
         if (!isfinite(wt) || wt < tmin || wt > closest) break;
         closest = wt;
@@ -817,13 +866,13 @@ __device__ __forceinline__ bool object_any(const DScene& S, int32_t oi, const TR
     case OK_PLANE:
         return !src && plane_test(O, r, tmin, tmax, t);
     case OK_MESH:
-        return mesh_any(S, S.meshes[O.aux], r, tmin, tmax, src ? r.xprim : -1, vs, st);
+        return mesh_any<F>(S, S.meshes[O.aux], r, tmin, tmax, src ? r.xprim : -1, vs, st);
     case OK_INSTANCE: {
         if constexpr (!(F & TF_INSTANCE)) return false;
         TRay lr;
         float s;
         if (!local_ray(O, r, lr, s)) return false;
-        return mesh_any(S, S.meshes[O.aux], lr, tmin * s, tmax * s, src ? r.xprim : -1, vs, st);
+        return mesh_any<F>(S, S.meshes[O.aux], lr, tmin * s, tmax * s, src ? r.xprim : -1, vs, st);
     }
     case OK_VOLUME:
         if constexpr (!(F & TF_VOLUME)) return false;

@@ -140,6 +140,16 @@ class RenderStats(C.Structure):
     ]
 
 
+class TuneParams(C.Structure):
+    """LuzTuneParams: launch tuning of a scene handle (zeros = defaults)."""
+    _fields_ = [("wave_paths", C.c_int64), ("staged_top_nodes", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
+                ("shadow_blocks_per_sm", C.c_int32), ("shade_blocks_per_sm", C.c_int32)]
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("params", TuneParams), ("render_ms", C.c_double)]
+
+
 class AdaptiveParams(C.Structure):
     """LuzAdaptiveParams: Scene adaptive settings (src/scene/Scene.cpp:183-222)."""
     _fields_ = [("enabled", C.c_int32), ("min_samples", C.c_int32), ("check_interval", C.c_int32),

@@ -28,6 +28,7 @@ EXPORTED = [
     "luz_gpu_cache_create", "luz_gpu_cache_destroy", "luz_gpu_cache_weights", "luz_gpu_cache_predict",
     "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached", "luz_gpu_adjoint_emission",
     "luz_gpu_adjoint_density", "luz_gpu_scene_set_path_budget", "luz_gpu_scene_set_traversal_limits",
+    "luz_gpu_render_pixels", "luz_gpu_scene_set_tuning", "luz_gpu_scene_get_tuning", "luz_gpu_autotune",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -62,6 +63,10 @@ def lib():
     L.luz_gpu_scene_destroy.argtypes = [vp]
     L.luz_gpu_scene_info.argtypes = [vp, C.POINTER(D.SceneInfo)]
     L.luz_gpu_scene_set_path_budget.argtypes = [vp, i64]
+    L.luz_gpu_render_pixels.argtypes = [vp, C.POINTER(D.RenderParams), vp, i64, vp, C.POINTER(D.RenderStats)]
+    L.luz_gpu_scene_set_tuning.argtypes = [vp, C.POINTER(D.TuneParams)]
+    L.luz_gpu_scene_get_tuning.argtypes = [vp, C.POINTER(D.TuneParams)]
+    L.luz_gpu_autotune.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.TuneParams), vp, i32, C.POINTER(i32)]
     L.luz_gpu_scene_set_traversal_limits.argtypes = [vp, i32, i32]
     L.luz_gpu_render.argtypes = [vp, C.POINTER(D.RenderParams), vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_render_device.argtypes = [vp, C.POINTER(D.RenderParams), vp, vp, C.POINTER(D.RenderStats)]
@@ -183,6 +188,34 @@ class GpuScene:
         i = D.SceneInfo()
         _check(lib().luz_gpu_scene_info(self.h, C.byref(i)))
         return i
+
+    def render_pixels(self, p: D.RenderParams, x, y) -> Tuple[np.ndarray, D.RenderStats]:
+        """luz_gpu_render_pixels: means of the listed pixels (n x 3)."""
+        idx = np.ascontiguousarray(np.asarray(y, np.int64) * p.width + np.asarray(x, np.int64), np.int32)
+        out = np.zeros((len(idx), 3), np.float32)
+        st = D.RenderStats()
+        _check(lib().luz_gpu_render_pixels(self.h, C.byref(p), idx.ctypes.data, len(idx), out.ctypes.data,
+                                           C.byref(st)))
+        return out, st
+
+    def set_tuning(self, **kw):
+        """luz_gpu_scene_set_tuning: fields of LuzTuneParams (unset = 0 = default)."""
+        t = D.TuneParams(**kw)
+        _check(lib().luz_gpu_scene_set_tuning(self.h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = D.TuneParams()
+        _check(lib().luz_gpu_scene_get_tuning(self.h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in D.TuneParams._fields_}
+
+    def autotune(self, p: D.RenderParams):
+        """luz_gpu_autotune: (chosen tuning as a dict, [(tuning dict, render_ms) per trial])."""
+        chosen = D.TuneParams()
+        trials = (D.TuneTrial * 32)()
+        n = C.c_int32(0)
+        _check(lib().luz_gpu_autotune(self.h, C.byref(p), C.byref(chosen), trials, 32, C.byref(n)))
+        as_dict = lambda t: {f: getattr(t, f) for f, _ in D.TuneParams._fields_}
+        return as_dict(chosen), [(as_dict(trials[i].params), trials[i].render_ms) for i in range(n.value)]
 
     def set_path_budget(self, nbytes: int):
         """luz_gpu_scene_set_path_budget: cap on the path state held (bytes; -1 = default)."""

@@ -75,8 +75,9 @@ class RefOracle:
         L.luzref_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.luzref_scene_load.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.luzref_scene_pack.argtypes = [vp, C.POINTER(vp), vp]
-        L.luzref_set_perturbation.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_double]
+        L.luzref_set_perturbation.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double]
         L.luzref_top_bvh.argtypes = [vp, vp, C.c_int64, C.POINTER(C.c_int64)]
+        L.luzref_render_pixels_mt.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_int32, vp]
 
     def _check(self, rc):
         if rc != 0:
@@ -110,10 +111,12 @@ class RefOracle:
                                          out.ctypes.data))
         return out
 
-    def set_perturbation(self, seed: int, delta_dir: float = 0.0, delta_dec: float = 0.0, delta_cam: float = 0.0):
+    def set_perturbation(self, seed: int, delta_dir: float = 0.0, delta_dec: float = 0.0, delta_cam: float = 0.0,
+                         delta_bsdf: float = 0.0):
         """Moves every Sampler draw by +-delta while seed != 0 (the FP32 ambiguity probe,
         oracle/ref_harness.cpp); seed 0 turns it off."""
-        self._check(self.lib.luzref_set_perturbation(int(seed), float(delta_dir), float(delta_dec), float(delta_cam)))
+        self._check(self.lib.luzref_set_perturbation(int(seed), float(delta_dir), float(delta_dec), float(delta_cam),
+                                                     float(delta_bsdf)))
 
     def sampler(self, seed, x, y, s, stream, bounce, dim, which=1):
         out = np.zeros(2, np.float64)
@@ -160,6 +163,15 @@ class RefScene:
                                                    None if vk is None else vk.ctypes.data,
                                                    t.ctypes.data, obj.ctypes.data, prim.ctypes.data))
         return t, obj, prim
+
+    def render_pixels_mt(self, params, x, y, threads: int) -> np.ndarray:
+        """_threadRender for listed pixels on `threads` host threads: n x 3 pixel means."""
+        x = np.ascontiguousarray(x, np.int32)
+        y = np.ascontiguousarray(y, np.int32)
+        out = np.zeros((len(x), 3), np.float64)
+        self.o._check(self.o.lib.luzref_render_pixels_mt(self.h, C.byref(params), x.ctypes.data, y.ctypes.data,
+                                                         len(x), int(threads), out.ctypes.data))
+        return out
 
     def top_bvh(self) -> np.ndarray:
         """The reference's top-level BVHNode tree in preorder: per node its child count,
@@ -292,7 +304,8 @@ class Restate:
 # grazing a triangle edge, a very sharp lobe), the two may legitimately part.
 # These probes mark such rays and paths from the reference alone, before any GPU
 # result is seen: a ray or path is ambiguous when the reference's own answer
-# changes under perturbations a few times larger than FP32 rounding.
+# changes under perturbations of the size of FP32 rounding: of the draws (a few
+# FP32 ulps of what they become) and of the geometry (its FP32 storage).
 
 # Draw perturbations (in units of the draw u in [0, 1)): 2^-21 for draws that
 # become directions or distances (FP32 directions are good to ~1e-7), 2^-16 for
@@ -313,7 +326,7 @@ def path_deltas(width: int, height: int, camera) -> dict:
         omax = max(1.0, max(abs(float(camera.position[i])) for i in range(3)))
         half_ulp = float(np.spacing(np.float32(omax))) / 2.0
         cam = max(cam, 2.0 * half_ulp / (2.0 * radius))
-    return dict(delta_dir=2.0 ** -21, delta_dec=2.0 ** -16, delta_cam=min(cam, 2.0 ** -8))
+    return dict(delta_dir=2.0 ** -21, delta_dec=2.0 ** -16, delta_cam=min(cam, 2.0 ** -8), delta_bsdf=2.0 ** -21)
 
 
 PATH_PROBES = (1, 2, 3)
@@ -333,10 +346,46 @@ def path_rel(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return r.max(axis=1)
 
 
+def perturbed_geometry(scene, seed: int):
+    """A copy of a luz_b200.desc.Scene whose geometry carries the GPU's FP32 storage error:
+    every triangle translated rigidly by the FP32 rounding of its first vertex (the GPU keeps
+    v0 in FP32 and the edges, formed in FP64, in FP32: a triangle moves as a whole), vertex
+    normals and object parameters (centres, sizes, orientations) rounded to FP32; seeds other
+    than 0 add a further +-1 FP32 ulp (relative 2^-24) of random sign. The camera is left
+    alone: the GPU forms camera rays in FP64 (the camera draws carry that rounding)."""
+    import copy
+    sc = copy.deepcopy(scene)
+    rng = np.random.default_rng(seed)
+
+    def jitter(v):
+        v = np.asarray(v, np.float64)
+        return 0.0 if seed == 0 else rng.choice([-1.0, 1.0], v.shape) * 2.0 ** -24 * np.abs(v)
+
+    def rounded(v):
+        v = np.asarray(v, np.float64)
+        return v.astype(np.float32).astype(np.float64) + jitter(v)
+
+    for m in sc.meshes:
+        tri = np.asarray(m["positions"], np.float64).reshape(-1, 3, 3)
+        v0 = tri[:, 0, :]
+        shift = v0.astype(np.float32).astype(np.float64) - v0 + jitter(v0)
+        m["positions"] = np.ascontiguousarray((tri + shift[:, None, :]).reshape(-1, 9))
+        if m["normals"] is not None:
+            m["normals"] = np.ascontiguousarray(rounded(m["normals"]))
+    for ob in sc.objects:
+        for k in ("position", "size", "orientation", "width_axis", "height_axis"):
+            ob[k] = tuple(rounded(ob[k]))
+    return sc
+
+
+GEOMETRY_PROBES = (0, 1, 2)
+
+
 def ambiguous_paths(oracle: RefOracle, rs: "RefScene", params, x, y, s, base: np.ndarray, deltas: dict,
-                    tol: float = 1e-4):
+                    tol: float = 1e-4, scene=None):
     """True per path whose reference radiance moves by more than tol under any of the
-    PATH_PROBES draw perturbations (deltas: path_deltas of the frame)."""
+    PATH_PROBES draw perturbations (deltas: path_deltas of the frame) or, when the
+    luz_b200.desc.Scene is given, under any of the GEOMETRY_PROBES (perturbed_geometry)."""
     flags = np.zeros(len(x), bool)
     try:
         for seed in PATH_PROBES:
@@ -344,6 +393,11 @@ def ambiguous_paths(oracle: RefOracle, rs: "RefScene", params, x, y, s, base: np
             flags |= path_rel(rs.trace_paths(params, x, y, s), base) > tol
     finally:
         oracle.set_perturbation(0)
+    if scene is not None:
+        for seed in GEOMETRY_PROBES:
+            rg = oracle.scene(perturbed_geometry(scene, seed).build())
+            flags |= path_rel(rg.trace_paths(params, x, y, s), base) > tol
+            rg.close()
     return flags
 
 

@@ -52,6 +52,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -459,6 +460,7 @@ struct Perturb {
     double dir = 0.0;    // directions and distances (surface points, BSDF and phase directions, media)
     double dec = 0.0;    // dimensions compared with an FP32 threshold (lobe, Russian roulette)
     double cam = 0.0;    // camera and lens (a pixel or the aperture, not a hemisphere)
+    double bsdf = 0.0;   // BSDF and fuzz directions (a narrow lobe maps the draw onto a small angle)
 } g_perturb;
 
 uint64_t mix64(uint64_t v)
@@ -483,9 +485,9 @@ double perturb_delta(uint32_t dimension)
     case Sampler::DIM_LIGHT_EMISSION_SIDE: return 0.0;
     case Sampler::DIM_CAMERA:
     case Sampler::DIM_LENS: return g_perturb.cam;
-    case Sampler::DIM_LIGHT_SURFACE_POINT:
     case Sampler::DIM_BSDF_DIRECTION:
-    case Sampler::DIM_MATERIAL_FUZZ:
+    case Sampler::DIM_MATERIAL_FUZZ: return g_perturb.bsdf;
+    case Sampler::DIM_LIGHT_SURFACE_POINT:
     case Sampler::DIM_ATMOSPHERE:
     case Sampler::DIM_ENVIRONMENT_POINT:
     case Sampler::DIM_LIGHT_EMISSION_DIRECTION:
@@ -567,19 +569,21 @@ extern "C" {
 
 /* Sets the draw perturbation of the ambiguity probe (seed 0 = off); the
  * parity library only (LUZ_E_UNSUPPORTED elsewhere). */
-int luzref_set_perturbation(uint64_t seed, double delta_dir, double delta_dec, double delta_cam)
+int luzref_set_perturbation(uint64_t seed, double delta_dir, double delta_dec, double delta_cam, double delta_bsdf)
 {
 #ifdef LUZREF_PERTURB
     g_perturb.seed = seed;
     g_perturb.dir = delta_dir;
     g_perturb.dec = delta_dec;
     g_perturb.cam = delta_cam;
+    g_perturb.bsdf = delta_bsdf;
     return 0;
 #else
     (void)seed;
     (void)delta_dir;
     (void)delta_dec;
     (void)delta_cam;
+    (void)delta_bsdf;
     g_error = "draw perturbation is built into the parity library only";
     return LUZ_E_UNSUPPORTED;
 #endif
@@ -859,6 +863,41 @@ int luzref_render_pixels(void* s, const LuzRenderParams* p, int32_t adaptive, in
         }
         scene.clearDenoiseBuffers();
         scene.setAdaptiveSampling(false);
+        return 0;
+    });
+}
+
+/* _threadRender (src/renderer/Threads.cpp:551-641) for listed pixels, adaptive
+ * sampling and denoise buffers off, on `threads` host threads (pixels dealt round
+ * robin): the stored pixel (mean of params->spp cleaned samples) per pixel. */
+int luzref_render_pixels_mt(void* s, const LuzRenderParams* p, const int32_t* x, const int32_t* y, int64_t n,
+                            int32_t threads, double* rgb_out)
+{
+    return guarded([&] {
+        RefScene* rs = static_cast<RefScene*>(s);
+        Scene& scene = rs->scene;
+        configure(scene, LuzSceneDesc{}, p->width, p->height);
+        scene.setMaxLightBounces(p->max_bounces);
+        scene.setSampleCount(p->spp);
+        scene.setAdaptiveSampling(false);
+        scene.clearDenoiseBuffers();
+        caustic_map(scene, p->seed);
+        const auto cam = Renderer::internal::_prepareRenderCamera(scene);
+        Sampler::setRenderSeed(p->seed);
+        const int nt = std::max(1, threads);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; t++)
+            pool.emplace_back([&, t] {
+                for (int64_t i = t; i < n; i += nt) {
+                    const std::size_t px = (std::size_t)x[i], py = (std::size_t)y[i];
+                    Renderer::internal::_threadRender(scene, cam, px, py);
+                    const Color c = scene.getImage()->getPixel(px, py);
+                    rgb_out[3 * i] = c.getRed();
+                    rgb_out[3 * i + 1] = c.getGreen();
+                    rgb_out[3 * i + 2] = c.getBlue();
+                }
+            });
+        for (auto& th : pool) th.join();
         return 0;
     });
 }

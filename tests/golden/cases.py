@@ -64,6 +64,21 @@ ORACLE_64K_FULL = {
     "cornell300": lambda: scenes.cornell(300, 300, 65536, 8),
 }
 
+# Seeded 4,096-pixel subsets of the full-size benchmarked frames, rendered by the reference
+# at 65,536 spp (the converged oracle where a full 1080p or 720p frame at that count is out
+# of reach on host cores).
+ORACLE_64K_SUBSET = {
+    "glossy_full": lambda: scenes.mesh_glossy(spp=65536),
+    "instancing_full": lambda: scenes.instancing_volumes(spp=65536),
+}
+
+
+def oracle_subset_pixels(w, n=4096, seed=4242):
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(w.width * w.height, n, replace=False))
+    return (idx % w.width).astype(np.int32), (idx // w.width).astype(np.int32)
+
+
 CAUSTIC_COUNTS = [(424242424, 8), (7, 8), (424242424, 3), (99, 12)]
 
 # Adaptive sampling / NFOR buffer cases: workload, adaptive settings (None = off), NFOR on.
@@ -84,6 +99,29 @@ def adjoint_case():
     adj = rng.normal(0.0, 1.0, (w.height, w.width, 3)).astype(np.float32)
     picks = np.stack([rng.integers(0, 32, 8), rng.integers(0, 32, 8), rng.integers(0, 3, 8)], 1)
     return w, adj, picks
+
+
+# Differentiation at the C3 configuration: the 256 x 256 textured Cornell box at depth 8
+# (Russian roulette from bounce 3), a seeded dLoss/dpixel image, and central differences of
+# the reference's own film at 65,536 spp (common random numbers) along three directions:
+# every back-wall texel scaled together (albedo), the light's emission scaled (emission), and
+# the density of a fog cube in the same box (density). The GPU's replay gradients, projected
+# on the same directions, must agree within 2%.
+C3_H = 1e-3
+C3_SPP_FD = 65536
+
+
+def c3_case(spp=64):
+    w = scenes.cornell_textured(256, 256, spp, 8)
+    adj = np.random.default_rng(78).uniform(0.5, 1.5, (256, 256, 3)).astype(np.float32)
+    return w, adj
+
+
+def c3_fog_case(spp=64, density=0.0035):
+    w = scenes.cornell_textured(256, 256, spp, 8)
+    fog = w.scene.henyey_greenstein((0.8, 0.8, 0.8), 0.3)
+    obj = w.scene.volume_cube((278.0, 250.0, 280.0), 300.0, 300.0, 300.0, fog, density)
+    return w, obj
 
 
 def nfor_synthetic(width: int = 40, height: int = 32, seed: int = 3) -> dict:

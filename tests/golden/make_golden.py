@@ -37,8 +37,9 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
-from cases import (ADAPTIVE_CASES, BVH_CASES, CASES, CAUSTIC_COUNTS, FULL_CASES, ORACLE_64K,  # noqa: E402
-                   ORACLE_64K_FULL, adjoint_case,
+from cases import (ADAPTIVE_CASES, BVH_CASES, C3_H, C3_SPP_FD, CASES, CAUSTIC_COUNTS, FULL_CASES,  # noqa: E402
+                   ORACLE_64K, ORACLE_64K_FULL, ORACLE_64K_SUBSET, adjoint_case, c3_case, c3_fog_case,
+                   oracle_subset_pixels,
                    camera_rays, caustic_case, nfor_synthetic, path_keys)
 from luz_b200 import native  # noqa: E402
 import oracle as O  # noqa: E402
@@ -114,10 +115,21 @@ def ray_fixture(rt, w, name, rng, n=2000):
 
 
 def path_fixture(o, rs, w, x, y, s):
+    """Per-path radiance with its ambiguity flags; for a scene with a caustic photon map
+    also `photon`: paths whose radiance changes when the map is switched off (they
+    gather photons, whose FP32 tracing test_caustics compares on its own)."""
     p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
     rgb = rs.trace_paths(p, x, y, s)
-    amb = O.ambiguous_paths(o, rs, p, x, y, s, rgb, O.path_deltas(w.width, w.height, w.scene.camera))
-    return dict(x=x, y=y, s=s, rgb=rgb, ambiguous=amb)
+    amb = O.ambiguous_paths(o, rs, p, x, y, s, rgb, O.path_deltas(w.width, w.height, w.scene.camera),
+                            scene=w.scene)
+    out = dict(x=x, y=y, s=s, rgb=rgb, ambiguous=amb)
+    if w.scene.caustics.get("enabled"):
+        import copy
+        sc = copy.deepcopy(w.scene)
+        sc.caustics["enabled"] = 0
+        off = o.scene(sc.build()).trace_paths(p, x, y, s)
+        out["photon"] = np.abs(off - rgb).max(axis=1) > 0
+    return out
 
 
 def full_fixtures(o, only=None):
@@ -243,6 +255,73 @@ def oracle64k_full_fixtures(o, threads=None):
         print("golden oracle64k", name, f"{ms / 1000:.1f} s", flush=True)
 
 
+def oracle64k_subset_fixtures(o, threads=None, only=None):
+    """oracle64k_<case>.npz for ORACLE_64K_SUBSET: the reference's pixel means at 65,536 spp
+    on a seeded 4,096-pixel subset of the frame (_threadRender per pixel, host threads)."""
+    import time
+    threads = threads or os.cpu_count() or 1
+    for name, fn in ORACLE_64K_SUBSET.items():
+        if only and name not in only:
+            continue
+        w = fn()
+        x, y = oracle_subset_pixels(w)
+        rs = o.scene(w.scene.build())
+        t0 = time.time()
+        rgb = rs.render_pixels_mt(native.params(w.width, w.height, w.spp, w.max_bounces, w.seed), x, y, threads)
+        np.savez_compressed(os.path.join(HERE, f"oracle64k_{name}.npz"), x=x, y=y, rgb=rgb.astype(np.float32),
+                            spp=w.spp, seed=w.seed, seconds=time.time() - t0, threads=threads)
+        print("golden oracle64k subset", name, f"{time.time() - t0:.0f} s", flush=True)
+
+
+def adjoint_c3_fixture(o, threads=None, only=None):
+    """adjoint_c3.npz: central differences of the reference's film functional
+    L = sum(adj * film) at the C3 configuration (cases.c3_case), Renderer::render with
+    common random numbers (one seed for both sides): 65,536 spp for the albedo (all
+    back-wall texels scaled by 1 +- h) and for the density of the fog cube (c3_fog_case,
+    density scaled by 1 +- h); 1,024 spp for the emission (the film is linear in it, and
+    light selection does not depend on it with one light)."""
+    threads = threads or os.cpu_count() or 1
+    path = os.path.join(HERE, "adjoint_c3.npz")
+    out = dict(np.load(path)) if os.path.exists(path) else {}
+    w, adj = c3_case()
+    out["adj"] = adj
+    out["h"] = C3_H
+    seed = 20261204
+    out["seed"] = seed
+    a64 = adj.astype(np.float64)
+
+    def loss(workload, spp):
+        rs = o.scene(workload.scene.build())
+        img, ms, _ = rs.render(native.params(workload.width, workload.height, spp, workload.max_bounces, seed),
+                               threads)
+        rs.close()
+        return float((a64 * img).sum()), ms
+
+    jobs = [("albedo", C3_SPP_FD), ("emission", 1024), ("density", C3_SPP_FD)]
+    for name, spp in jobs:
+        if only and name not in only:
+            continue
+        vals = []
+        for sgn in (1.0, -1.0):
+            if name == "density":
+                wk, obj = c3_fog_case(spp)
+                wk.scene.objects[obj]["density"] *= 1.0 + sgn * C3_H
+            else:
+                wk, _ = c3_case()
+                wk.spp = spp
+                if name == "albedo":
+                    wk.scene.textures[0] = wk.scene.textures[0] * (1.0 + sgn * C3_H)
+                else:
+                    light = [m for m in wk.scene.materials if m["type"] == 4][0]
+                    light["color"] = tuple(np.array(light["color"]) * (1.0 + sgn * C3_H))
+            v, ms = loss(wk, spp)
+            vals.append(v)
+            print("adjoint_c3", name, sgn, v, f"{ms / 1000:.0f} s", flush=True)
+        out[f"fd_{name}"] = (vals[0] - vals[1]) / (2.0 * C3_H)
+        out[f"spp_{name}"] = spp
+        np.savez_compressed(path, **out)
+
+
 def main():
     o = RefOracle()
     if sys.argv[1:] == ["adaptive"]:
@@ -259,6 +338,12 @@ def main():
         return
     if sys.argv[1:] == ["oracle64k"]:
         oracle64k_fixtures(o)
+        return
+    if sys.argv[1:2] == ["oracle64k_subset"]:
+        oracle64k_subset_fixtures(o, only=sys.argv[2:] or None)
+        return
+    if sys.argv[1:2] == ["adjoint_c3"]:    # adjoint_c3 [albedo|emission|density ...]
+        adjoint_c3_fixture(o, only=sys.argv[2:] or None)
         return
     if sys.argv[1:2] == ["full"]:      # full [name...]: the full-size frames
         full_fixtures(o, sys.argv[2:])

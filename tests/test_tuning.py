@@ -1,0 +1,48 @@
+"""Launch tuning and the autotuner (luz_gpu_scene_set_tuning, luz_gpu_autotune): no
+tuning choice changes a film. Staged top BVH nodes (shared memory), wave sizes and
+persistent grid sizes give the same image bit for bit; the autotuner leaves its choice
+on the handle and reports its timed trials."""
+import numpy as np
+import pytest
+
+from cases import CASES
+from luz_b200 import native
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["glossy", "instancing"])
+def test_tuning_choices_leave_the_film_unchanged(name):
+    w = CASES[name]()
+    g = native.GpuScene(w.scene.build())
+    try:
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        ref, _ = g.render(p)
+        for kw in (dict(staged_top_nodes=1), dict(wave_paths=4096), dict(extend_blocks_per_sm=2, shadow_blocks_per_sm=3,
+                                                                         shade_blocks_per_sm=1),
+                   dict(staged_top_nodes=1, wave_paths=5000, extend_blocks_per_sm=1)):
+            g.set_tuning(**kw)
+            img, _ = g.render(p)
+            assert np.array_equal(img, ref), kw
+            assert all(g.tuning()[k] == v for k, v in kw.items())
+        g.set_tuning()
+        with pytest.raises(native.LuzError):
+            g.set_tuning(staged_top_nodes=2)
+    finally:
+        g.close()
+
+
+def test_autotune_keeps_the_best_trial():
+    w = CASES["glossy"]()
+    g = native.GpuScene(w.scene.build())
+    try:
+        p = native.params(w.width, w.height, 16, w.max_bounces, w.seed)
+        ref, _ = g.render(p)
+        chosen, trials = g.autotune(p)
+        assert len(trials) >= 4 and chosen == g.tuning()
+        best = min(ms for _, ms in trials)
+        assert any(t == chosen and ms == best for t, ms in trials)
+        img, _ = g.render(p)
+        assert np.array_equal(img, ref)
+    finally:
+        g.close()
