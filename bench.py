@@ -375,35 +375,49 @@ def run_ours(args):
 
 
 def run_batch(args):
-    """--workload batch48: 48 independent scenes (scenes.batch_workloads) rendered one
-    luz_gpu_render after another, then as one luz_gpu_batch_render call. Host wall clock
-    around the calls (host films, device->host copies included): an end-to-end figure."""
+    """--workload batch48: 48 independent scenes (scenes.batch_workloads: 1e3-1e6 triangles,
+    128^2-1024^2, 4-256 spp, depth 4-16) rendered one luz_gpu_render after another, then as
+    one luz_gpu_batch_render call (multi-scene waves over one geometry arena, each wave a
+    replayed CUDA graph, wave size autotuned on the first call). --workload batch48_small:
+    the same mix at 64^2-256^2 and 1-16 spp, where a single render's fixed costs (launches,
+    per-bounce tails) dominate. Host wall clock around the calls (host films, device->host
+    copies included): an end-to-end figure."""
     from luz_b200 import native, scenes
-    ws = scenes.batch_workloads(48)
+    small = args.workload == "batch48_small"
+    ws = scenes.batch_workloads(48, side_range=(64, 256), spp_range=(1, 16)) if small else scenes.batch_workloads(48)
     gs = [native.GpuScene(w.scene.build()) for w in ws]
     ps = [native.params(w.width, w.height, w.spp, w.max_bounces, w.seed) for w in ws]
     samples = float(sum(w.width * w.height * w.spp for w in ws))
+    _, _, first = native.batch_render(gs, ps, report=True)      # autotunes the wave size
     for _ in range(max(1, args.warmup)):
         native.batch_render(gs, ps)
-    t_seq, t_bat = [], []
+        for g, p in zip(gs, ps):
+            g.render(p)
+    t_seq, t_bat, dev_ms = [], [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         for g, p in zip(gs, ps):
             g.render(p)
         t_seq.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
-        native.batch_render(gs, ps)
+        _, _, rep = native.batch_render(gs, ps, report=True)
         t_bat.append(time.perf_counter() - t0)
+        dev_ms.append(rep["render_ms"])
     tb, ts = statistics.median(t_bat), statistics.median(t_seq)
     out = {"metric": METRIC, "value": samples / tb / 1e6, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": tb * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
            "timing": "host wall clock around the C ABI calls (e2e, host films)",
-           "config": {"workload": "batch48: 48 scenes, 1e3-1e6 triangles, 128^2-1024^2, 4-256 spp, depth 4-16",
+           "config": {"workload": ("batch48_small: 48 scenes, 1e3-1e6 triangles, 64^2-256^2, 1-16 spp, depth 4-16"
+                                   if small else
+                                   "batch48: 48 scenes, 1e3-1e6 triangles, 128^2-1024^2, 4-256 spp, depth 4-16"),
                       "samples_per_step": samples,
                       "triangles": int(sum(g.info().mesh_triangles for g in gs))},
            "sequential": {"value": samples / ts / 1e6, "unit": UNIT, "ms_per_step": ts * 1e3},
-           "batch_speedup": ts / tb}
+           "batch_speedup": ts / tb,
+           "batch_device_ms": float(np.median(dev_ms)),
+           "autotuner": {"chosen_wave_paths": first["wave_paths"], "trials": first["trials"]},
+           "waves": rep["waves"], "kernel_launches": rep["kernel_launches"]}
     print(json.dumps(out), flush=True)
     for g in gs:
         g.close()
@@ -575,7 +589,7 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "batch48":
+    elif args.workload in ("batch48", "batch48_small"):
         run_batch(args)
     elif args.workload == "adjoint_c3":
         run_adjoint(args)

@@ -342,7 +342,8 @@ int luz_gpu_scene_set_traversal_limits(luz_gpu_scene* scene, int32_t mesh_entrie
  *                         block and read those nodes there;
  *   *_blocks_per_sm:      blocks per SM of the persistent closest-hit / any-hit grids and
  *                         of the shade grid (default: full occupancy; larger values are
- *                         capped at it).
+ *                         capped at it);
+ *   sort_rays:            see the field.
  * No counterpart in the reference (its worker count is Scene::setRenderingThreads). */
 typedef struct LuzTuneParams {
     int64_t wave_paths;
@@ -350,7 +351,9 @@ typedef struct LuzTuneParams {
     int32_t extend_blocks_per_sm;
     int32_t shadow_blocks_per_sm;
     int32_t shade_blocks_per_sm;
-} LuzTuneParams;
+    int32_t sort_rays;            /* 1: extension rays of bounces >= 1 are traced in coherence  */
+    int32_t reserved;             /* order (direction octant, then the Morton cell of the ray */
+} LuzTuneParams;                  /* origin in a 16^3 grid over the scene box)                */
 typedef struct LuzTuneTrial {
     LuzTuneParams params;
     double render_ms;             /* device time of the trial render */
@@ -359,7 +362,7 @@ int luz_gpu_scene_set_tuning(luz_gpu_scene* scene, const LuzTuneParams* tune);
 int luz_gpu_scene_get_tuning(const luz_gpu_scene* scene, LuzTuneParams* tune);
 /* Autotuner: times renders of `params` on the device (CUDA events; each trial rendered
  * twice, the second timed) while it changes one knob at a time from the handle's
- * current tuning (staged nodes on/off; waves of 4 Mi, 16 Mi and 64 Mi paths; the
+ * current tuning (staged nodes on/off; ray sorting on/off; waves of 4 Mi, 16 Mi and 64 Mi paths; the
  * closest-hit grid at full occupancy or one block fewer; the any-hit grid at full or
  * half occupancy), keeps every change that lowers the time, and leaves the best
  * tuning on the handle (also copied to `chosen` when not NULL). The trials (up to
@@ -409,15 +412,42 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
 int luz_gpu_render_device_noalloc(luz_gpu_scene* scene, const LuzRenderParams* params,
                                   float* d_rgb_out, void* stream, LuzRenderStats* stats);
 
-/* Many independent renders in one call (a batch of scenes, one result each).
- * Every scene renders on its own stream: all device memory is taken first,
- * then the waves of every scene are queued, so small scenes overlap on the GPU
- * instead of each waiting for the previous one. Each result equals
- * luz_gpu_render(scenes[i], &params[i], rgb_out[i], &stats[i]) bit for bit.
- * A handle may appear once per batch; params[i].flags must be 0; stats may be
- * NULL. No counterpart in the reference (it renders one scene per process). */
+/* Many independent renders in one call (a batch of scenes and views of uneven size,
+ * one result each). The scenes' arrays are copied into one geometry arena (kept for
+ * later calls with the same scene contents) and their paths share the wavefront:
+ * a wave packs runs of pixels of any scenes (every sample of a pixel in the same
+ * wave), and each bounce runs one persistent closest-hit, one shade and one any-hit
+ * launch over the rays of all scenes, every ray traversing its own scene. A wave's
+ * launches are recorded once per call as a CUDA graph and replayed for every wave.
+ * The wave size is autotuned per scene set: the first call times one wave at 4 Mi,
+ * 16 Mi and 64 Mi paths and keeps the fastest rate for later calls. Each result
+ * equals luz_gpu_render(scenes[i], &params[i], rgb_out[i], &stats[i]) bit for bit;
+ * stats[i] counts scene i's samples and rays, with the batch's device time. All
+ * handles on one device, each at most once; params[i].flags must be 0; stats may
+ * be NULL. Calls on one device are serialised. The reference renders one scene
+ * per process; its workers share an atomic block counter (Threads.cpp:410-451),
+ * which the shared ray queues generalise to many scenes. */
 int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
                          float* const* rgb_out, LuzRenderStats* stats);
+/* The same, with what the batch did: the wave size used (tuned or cached), the waves
+ * and launches, the device time, and the autotuner's trials of this call (none when
+ * the scene set's wave size was already tuned). */
+typedef struct LuzBatchTrial {
+    int64_t wave_paths;
+    double  paths;                /* paths of the trial wave */
+    double  ms;                   /* its device time */
+} LuzBatchTrial;
+typedef struct LuzBatchReport {
+    int64_t wave_paths;
+    int64_t waves;
+    int64_t kernel_launches;
+    double  render_ms;
+    int32_t trial_count;
+    int32_t reserved;
+    LuzBatchTrial trials[8];
+} LuzBatchReport;
+int luz_gpu_batch_render_ex(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
+                            float* const* rgb_out, LuzRenderStats* stats, LuzBatchReport* report);
 
 /* ---- differentiation (albedo textures) ------------------------------------
  * No counterpart in the reference (it has no gradients); the oracle is central

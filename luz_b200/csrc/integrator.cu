@@ -16,7 +16,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene
     if constexpr ((F & TF_STAGED) != 0) stage_top_nodes(S);
     LocalStack<true> st;
     const uint32_t count = C->count[bounce];
-    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
+    const uint32_t* q = (w.sorted_queue && bounce >= 1) ? w.sorted_queue : ((bounce & 1) ? P.queue1 : P.queue0);
     while (true) {
         uint32_t base = 0;
         if (lane_id() == 0) base = atomicAdd(&C->fetch_ext[bounce], 32u);
@@ -177,6 +179,236 @@ const TraceKernel kExtendKernels[2][8] = {
 const TraceKernel kShadowKernels[8] = {k_shadow<0>, k_shadow<1>, k_shadow<2>, k_shadow<3>,
                                        k_shadow<4>, k_shadow<5>, k_shadow<6>, k_shadow<7>};
 
+
+// ---------------------------------------------------------------------------- coherence sort
+//
+// A counting sort of an extension queue by (direction octant, cell of the ray
+// origin in a 16^3 grid over the scene box, Morton order): rays of a warp then start
+// close together and head the same way. Keys and counts stay on the device (the
+// queue length is C->count[bounce]); the order inside a key is arbitrary, and the
+// image does not depend on the order rays are traced in.
+constexpr int kSortCellBits = 4;
+constexpr int kSortBins = 8 << (3 * kSortCellBits);
+
+__device__ __forceinline__ uint32_t spread3_4(uint32_t v)   // 4 bits -> bits 0, 3, 6, 9
+{
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+}
+
+__global__ void k_sort_keys(const Ctrl* C, int bounce, const uint32_t* q, PathBuf P, GSceneConst K)
+{
+    const uint32_t count = C->count[bounce];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t p = q[i];
+        const float4 o = P.ray_o[p], d = P.ray_d[p];
+        const float fo[3] = {o.x, o.y, o.z};
+        uint32_t cell = 0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float c = (fo[a] - K.box_lo[a]) * K.box_inv[a] * (float)(1 << kSortCellBits);
+            const uint32_t ci = (uint32_t)fminf(fmaxf(c, 0.0f), (float)((1 << kSortCellBits) - 1));
+            cell |= spread3_4(ci) << a;
+        }
+        const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+        const uint32_t key = (oct << (3 * kSortCellBits)) | cell;
+        P.sort_keys[i] = key;
+        const unsigned m = __activemask();
+        const unsigned peers = __match_any_sync(m, key);
+        if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&P.sort_hist[key], (uint32_t)__popc(peers));
+    }
+}
+
+// Exclusive scan of the kSortBins counts in place (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist)
+{
+    constexpr int per = kSortBins / 1024;
+    __shared__ uint32_t part[1024];
+    uint32_t v[per], sum = 0;
+#pragma unroll
+    for (int k = 0; k < per; k++) {
+        v[k] = hist[threadIdx.x * per + k];
+        sum += v[k];
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const uint32_t add = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - sum;
+#pragma unroll
+    for (int k = 0; k < per; k++) {
+        hist[threadIdx.x * per + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void k_sort_scatter(const Ctrl* C, int bounce, const uint32_t* q, PathBuf P)
+{
+    const uint32_t count = C->count[bounce];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t key = P.sort_keys[i];
+        const unsigned m = __activemask();
+        const unsigned peers = __match_any_sync(m, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if ((int)lane_id() == leader) base = atomicAdd(&P.sort_hist[key], (uint32_t)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        P.qsort[base + (uint32_t)__popc(peers & ((1u << lane_id()) - 1u))] = q[i];
+    }
+}
+
+// ---------------------------------------------------------------------------- multi-scene waves
+//
+// luz_gpu_batch_render packs the paths of many scenes into one wave: the wave is a
+// list of segments (WaveArgs with batch_scene / batch_offset), each covering every
+// sample of a run of pixels of one scene, and every path records its segment in
+// P.seg. One launch per stage and bounce then serves all scenes: the persistent
+// trace kernels fetch rays of any scene from the shared queues, look up the ray's
+// scene in the table of DScene records (all of them pointing into one geometry
+// arena) and traverse it; the shade kernel does the same. Rays traced per scene
+// are counted for the per-scene statistics.
+
+// Segment of wave slot p: the last segment starting at or before p.
+__device__ __forceinline__ uint32_t find_segment(const WaveArgs* segs, uint32_t nseg, int64_t p)
+{
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (segs[mid].batch_offset <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The size of a multi-scene wave, read by the kernels of the wave's replayed graph.
+struct BatchWaveHeader {
+    int64_t n;
+    uint32_t nseg;
+    uint32_t pad;
+};
+
+__global__ void __launch_bounds__(kBlock) k_raygen_batch(const WaveArgs* segs, const BatchWaveHeader* hdr, PathBuf P,
+                                                         Ctrl* C)
+{
+    const int64_t n = hdr->n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) C->count[0] = (uint32_t)n;
+    if (p >= n) return;
+    const uint32_t sg = find_segment(segs, hdr->nseg, p);
+    const WaveArgs& w = segs[sg];
+    uint32_t x, y, s;
+    path_coords(w, (uint32_t)(p - w.batch_offset), x, y, s);
+    double o[3], d[3];
+    camera_ray(w, x, y, s, o, d);
+    P.ray_o[p] = make_float4((float)o[0], (float)o[1], (float)o[2], __int_as_float(-1));
+    P.ray_d[p] = make_float4((float)d[0], (float)d[1], (float)d[2], __int_as_float(-1));
+    P.thr[p] = make_float4(1.f, 1.f, 1.f, 0.f);
+    P.rad[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(PF_PREV_SPECULAR));
+    P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    P.pixel[p] = y * (uint32_t)w.width + x;
+    P.sample[p] = s;
+    P.seg[p] = sg;
+    P.queue0[p] = (uint32_t)p;
+}
+
+// One per-scene counter add per group of lanes with the same scene.
+__device__ __forceinline__ void count_by_scene(unsigned mask, uint32_t sid, unsigned long long* counts)
+{
+    const unsigned peers = __match_any_sync(mask, sid);
+    if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&counts[sid], (unsigned long long)__popc(peers));
+}
+
+__global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend_batch(const DScene* __restrict__ scenes,
+                                                                               const WaveArgs* __restrict__ segs,
+                                                                               PathBuf P, Ctrl* C, int bounce,
+                                                                               unsigned long long* ext_rays)
+{
+    LocalStack<true> st;
+    const uint32_t count = C->count[bounce];
+    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(&C->fetch_ext[bounce], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        const unsigned vmask = __ballot_sync(0xffffffffu, i < count);
+        if (i >= count) continue;
+        const uint32_t p = q[i];
+        const WaveArgs& w = segs[P.seg[p]];
+        const DScene& S = scenes[w.batch_scene];
+        const float4 o = P.ray_o[p], d = P.ray_d[p];
+        const TRay r = make_ray_x(F3{o.x, o.y, o.z}, F3{d.x, d.y, d.z}, __float_as_int(o.w), __float_as_int(d.w));
+        const uint32_t pix = P.pixel[p];
+        Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        VolSample vs{&k, 0.0, false};
+        const THit h = closest_hit<TF_ALL>(S, r, kTMin, kInf, vs, st);
+        P.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.obj));
+        P.hit_prim[p] = h.prim;
+        bin_append(C->bin[bounce], P, vmask, h.obj < 0 ? 0u : (uint32_t)S.obj_class[h.obj], p);
+        count_by_scene(vmask, (uint32_t)w.batch_scene, ext_rays);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, LUZ_SHADOW_MIN_BLOCKS) k_shadow_batch(const DScene* __restrict__ scenes,
+                                                                               const WaveArgs* __restrict__ segs,
+                                                                               PathBuf P, Ctrl* C, int bounce,
+                                                                               unsigned long long* sh_rays)
+{
+    LocalStack<false> st;
+    const uint32_t count = C->shadow[bounce];
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(&C->fetch_sh[bounce], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        const unsigned vmask = __ballot_sync(0xffffffffu, i < count);
+        if (i >= count) continue;
+        const float4 o = P.sh_o[i], d = P.sh_d[i];
+        const uint32_t tag = __float_as_uint(d.w);
+        const uint32_t p = tag & 0x7fffffffu;
+        const WaveArgs& w = segs[P.seg[p]];
+        const DScene& S = scenes[w.batch_scene];
+        const int2 x = P.sh_x[i];
+        const TRay r = make_ray_x(F3{o.x, o.y, o.z}, F3{d.x, d.y, d.z}, x.x, x.y);
+        const uint32_t pix = P.pixel[p];
+        Key k = path_key(w, pix % (uint32_t)w.width, pix / (uint32_t)w.width, P.sample[p], (uint32_t)bounce);
+        VolSample vs{&k, 0.0, false};
+        if (any_hit<TF_ALL>(S, r, kTMin, o.w, vs, st)) {
+            if (tag & 0x80000000u) P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            else P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        count_by_scene(vmask, (uint32_t)w.batch_scene, sh_rays);
+    }
+}
+
+// k_accumulate over the segments of a multi-scene wave (blockIdx.y = segment): each
+// pixel's samples, in sample order, into its scene's FP64 film.
+__global__ void k_accumulate_batch(const WaveArgs* segs, const BatchWaveHeader* hdr, PathBuf P, double* const* films)
+{
+    if (blockIdx.y >= hdr->nseg) return;
+    const WaveArgs& w = segs[blockIdx.y];
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= w.pix_count) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    const int64_t b = w.batch_offset + j * w.s_count;
+    for (int s = 0; s < w.s_count; s++) {
+        const float4 r = P.rad[b + s], a = P.pend0[b + s], c2 = P.pend1[b + s];
+        const F3 c = clean((F3{r.x, r.y, r.z} + F3{a.x, a.y, a.z}) + F3{c2.x, c2.y, c2.z});
+        sx += (double)c.x;
+        sy += (double)c.y;
+        sz += (double)c.z;
+    }
+    double* f = films[w.batch_scene] + 3 * (int64_t)P.pixel[b];
+    f[0] += sx;
+    f[1] += sy;
+    f[2] += sz;
+}
 
 // Adds one wave's per-bounce queue sizes to the render totals (no host wait per wave).
 __global__ void k_tally(const Ctrl* C, int max_b, unsigned long long* totals)
@@ -647,6 +879,12 @@ template <class T> T* dupload(const std::vector<T>& v)
     return p;
 }
 
+uint64_t next_scene_uid()
+{
+    static std::atomic<uint64_t> n{0};
+    return ++n;
+}
+
 int guard(const std::function<int()>& f)
 {
     try {
@@ -685,6 +923,11 @@ struct luz_gpu_scene {
     int sms = 0;
     int occ_ext = 1, occ_shade = 1, occ_sh = 1;
     LuzTuneParams tune{};            // luz_gpu_scene_set_tuning / luz_gpu_autotune; zeros = defaults
+    // multi-scene batches copy the scene arrays into their geometry arena: byte offset of
+    // each array pointer inside DScene and the array's size; uid / version name the
+    // content (version changes with texels or the caustic map)
+    std::vector<std::pair<std::size_t, std::size_t>> arena_fields;
+    uint64_t uid = 0, version = 0;
     TraceKernel extend = nullptr, shadow = nullptr;   // instantiations for this scene's features
     ShadeKernel shade = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -726,7 +969,7 @@ struct luz_gpu_scene {
     }
     // Bytes of path state per path: the PathBuf arrays a wave allocates (NFOR
     // features add 3 float4).
-    static constexpr int64_t kPathBytes = 8 * 16 + 5 * 4 + 2 * (16 + 16 + 8) + kShadeClasses * 4;
+    static constexpr int64_t kPathBytes = 8 * 16 + 5 * 4 + 2 * (16 + 16 + 8) + kShadeClasses * 4 + 2 * 4;
     static constexpr int64_t kFeatBytes = 3 * 16;
     // Smallest wave a render falls back to when cudaMalloc refuses a larger one.
     static constexpr int64_t kMinWavePaths = int64_t(1) << 20;
@@ -753,6 +996,9 @@ struct luz_gpu_scene {
         pb.feat = feat ? palloc<float4>(3 * n) : nullptr;
         pb.bins = palloc<uint32_t>(kShadeClasses * n);
         pb.bin_stride = (uint32_t)n;
+        pb.sort_keys = palloc<uint32_t>(n);
+        pb.qsort = palloc<uint32_t>(n);
+        pb.sort_hist = palloc<uint32_t>(kSortBins);
         cap = n;
     }
     // Paths a wave of up to `want` paths may use: the buffers held when they are
@@ -866,9 +1112,20 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
     const uint32_t kv = (s->ds.k.features & TF_ALL) | (s->tune.staged_top_nodes && s->ds.top4_count ? TF_STAGED : 0u);
     const TraceKernel extend = kExtendKernels[count][kv];
     const TraceKernel shadow = kShadowKernels[kv];
+    WaveArgs ws = w;
+    const bool sort = s->tune.sort_rays != 0 && s->pb.qsort;
+    if (sort) ws.sorted_queue = s->pb.qsort;
     for (int b = 0; b <= w.max_bounces; b++) {
+        if (sort && b >= 1) {
+            const uint32_t* q = (b & 1) ? s->pb.queue1 : s->pb.queue0;
+            CK(cudaMemsetAsync(s->pb.sort_hist, 0, sizeof(uint32_t) * kSortBins, st));
+            k_sort_keys<<<s->sms * 8, 256, 0, st>>>(s->ctrl, b, q, s->pb, s->ds.k);
+            k_sort_scan<<<1, 1024, 0, st>>>(s->pb.sort_hist);
+            k_sort_scatter<<<s->sms * 8, 256, 0, st>>>(s->ctrl, b, q, s->pb);
+            launches += 3;
+        }
         T.mark(st, 0, true);
-        extend<<<g_ext, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        extend<<<g_ext, kBlock, 0, st>>>(s->ds, ws, s->pb, s->ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
         shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
@@ -983,6 +1240,7 @@ void prepare_caustics(luz_gpu_scene* s, const LuzRenderParams* p, cudaStream_t s
     CK(cudaEventSynchronize(s->ev1));
     CK(cudaEventElapsedTime(&M.last_ms, s->ev0, s->ev1));
     s->ds.cm = DCaustics{M.ph, M.tkeys, M.ranges, mask, stored};
+    s->version++;
     CK(cudaMemcpy(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice));
     M.stored = stored;
     M.seed = p->seed;
@@ -1431,6 +1689,7 @@ void set_texture(luz_gpu_scene* s, int32_t texture, const double* rgb)
     CK(cudaSetDevice(s->device));
     CK(cudaMemcpy(const_cast<float4*>(s->ds.texels) + T.offset, tx.data(), sizeof(float4) * (std::size_t)n,
                   cudaMemcpyHostToDevice));
+    s->version++;
     if (s->cm.valid) {   // photon throughput may depend on the texels: rebuild on the next render
         s->cm.valid = false;
         s->ds.cm = DCaustics{};
@@ -1686,6 +1945,432 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
     return LUZ_OK;
 }
 
+// ---------------------------------------------------------------------------- multi-scene batches
+//
+// One batch context per device holds the geometry arena (a copy of every scene's
+// arrays in one allocation, reused while the same scene contents come back), the
+// table of DScene records pointing into it, the shared path state, the segment
+// tables and the CUDA graph of one wave. A wave is recorded once per batch call
+// (raygen, every bounce's extend / shade / shadow, accumulate) and replayed for
+// every wave with that wave's segment table copied to a fixed device address.
+
+constexpr int64_t kBatchWaveDefault = int64_t(1) << 24;
+constexpr int kBatchMaxSegments = 4096;   // segments per wave (scenes split across waves)
+
+struct BatchContext {
+    std::mutex mu;
+    int device = -1;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    unsigned char* arena = nullptr;
+    std::size_t arena_bytes = 0;
+    std::vector<uint64_t> arena_key;         // (uid, version) of the scenes in the arena, in order
+    DScene* d_scenes = nullptr;
+    std::vector<DScene> h_scenes;
+    int64_t cap = 0;
+    PathBuf pb{};
+    std::vector<void*> pallocs;
+    Ctrl* ctrl = nullptr;
+    WaveArgs* d_segs = nullptr;              // kBatchMaxSegments entries
+    WaveArgs* h_segs = nullptr;              // pinned, one region per wave of the call
+    int64_t h_seg_cap = 0;
+    std::map<std::vector<uint64_t>, int64_t> tuned_wave;   // autotuned wave size per scene set
+    LuzBatchReport last_report{};
+    ~BatchContext()
+    {
+        if (device < 0) return;
+        cudaSetDevice(device);
+        for (void* p : pallocs) cudaFree(p);
+        if (arena) cudaFree(arena);
+        if (d_scenes) cudaFree(d_scenes);
+        if (ctrl) cudaFree(ctrl);
+        if (d_segs) cudaFree(d_segs);
+        if (h_segs) cudaFreeHost(h_segs);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+    void ensure_paths(int64_t n)
+    {
+        if (n <= cap) return;
+        for (void* p : pallocs) cudaFree(p);
+        pallocs.clear();
+        cap = 0;
+        auto get = [&](std::size_t bytes) {
+            void* p = dalloc<uint8_t>(bytes);
+            pallocs.push_back(p);
+            return p;
+        };
+        pb = PathBuf{};
+        pb.ray_o = static_cast<float4*>(get(16 * n));
+        pb.ray_d = static_cast<float4*>(get(16 * n));
+        pb.thr = static_cast<float4*>(get(16 * n));
+        pb.rad = static_cast<float4*>(get(16 * n));
+        pb.pend0 = static_cast<float4*>(get(16 * n));
+        pb.pend1 = static_cast<float4*>(get(16 * n));
+        pb.pixel = static_cast<uint32_t*>(get(4 * n));
+        pb.sample = static_cast<uint32_t*>(get(4 * n));
+        pb.hit = static_cast<float4*>(get(16 * n));
+        pb.hit_prim = static_cast<int32_t*>(get(4 * n));
+        pb.queue0 = static_cast<uint32_t*>(get(4 * n));
+        pb.queue1 = static_cast<uint32_t*>(get(4 * n));
+        pb.sh_o = static_cast<float4*>(get(32 * n));
+        pb.sh_d = static_cast<float4*>(get(32 * n));
+        pb.sh_x = static_cast<int2*>(get(16 * n));
+        pb.bins = static_cast<uint32_t*>(get(4 * kShadeClasses * n));
+        pb.bin_stride = (uint32_t)n;
+        pb.seg = static_cast<uint32_t*>(get(4 * n));
+        cap = n;
+    }
+};
+
+BatchContext& batch_context(int device)
+{
+    static std::mutex mu;
+    static std::vector<std::unique_ptr<BatchContext>> ctx;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)ctx.size() <= device) ctx.resize(device + 1);
+    if (!ctx[device]) {
+        ctx[device] = std::make_unique<BatchContext>();
+        BatchContext& c = *ctx[device];
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&c.ev0));
+        CK(cudaEventCreate(&c.ev1));
+        c.ctrl = dalloc<Ctrl>(1);
+        c.d_segs = dalloc<WaveArgs>(kBatchMaxSegments);
+        c.device = device;
+    }
+    return *ctx[device];
+}
+
+// The geometry arena for these scenes (rebuilt when the set or a scene's content changed).
+void batch_arena(BatchContext& C, luz_gpu_scene* const* scenes, int32_t count)
+{
+    std::vector<uint64_t> key;
+    for (int32_t i = 0; i < count; i++) {
+        key.push_back(scenes[i]->uid);
+        key.push_back(scenes[i]->version);
+    }
+    if (key == C.arena_key && C.arena) return;
+    struct Copy {
+        const void* src;
+        std::size_t off, bytes;
+    };
+    std::vector<Copy> copies;
+    std::vector<DScene> hs((std::size_t)count);
+    std::size_t total = 0;
+    auto place = [&](const void* src, std::size_t bytes) {
+        const std::size_t off = total;
+        total += (std::max<std::size_t>(bytes, 16) + 255) & ~std::size_t(255);
+        if (src && bytes) copies.push_back(Copy{src, off, bytes});
+        return off;
+    };
+    std::vector<std::vector<std::pair<std::size_t, std::size_t>>> offs((std::size_t)count);   // (field, arena offset)
+    std::vector<std::size_t> err_off((std::size_t)count), cm_off((std::size_t)count * 3);
+    for (int32_t i = 0; i < count; i++) {
+        const luz_gpu_scene* sc = scenes[i];
+        for (const auto& f : sc->arena_fields) {
+            const void* src = *reinterpret_cast<const void* const*>((const char*)&sc->ds + f.first);
+            offs[(std::size_t)i].push_back({f.first, place(src, f.second)});
+        }
+        err_off[(std::size_t)i] = place(nullptr, sizeof(uint32_t));
+        const DCaustics& cm = sc->ds.cm;
+        cm_off[3 * i] = place(cm.photons, cm.count ? sizeof(float4) * 3 * (std::size_t)cm.count : 0);
+        cm_off[3 * i + 1] = place(cm.cell_keys, cm.count ? sizeof(unsigned long long) * ((std::size_t)cm.mask + 1) : 0);
+        cm_off[3 * i + 2] = place(cm.cell_ranges, cm.count ? sizeof(uint2) * ((std::size_t)cm.mask + 1) : 0);
+    }
+    if (C.arena) cudaFree(C.arena);
+    C.arena = nullptr;
+    C.arena_key.clear();
+    C.arena = dalloc<unsigned char>(total);
+    C.arena_bytes = total;
+    CK(cudaMemsetAsync(C.arena, 0, total, C.st));
+    for (const Copy& c : copies) CK(cudaMemcpyAsync(C.arena + c.off, c.src, c.bytes, cudaMemcpyDeviceToDevice, C.st));
+    for (int32_t i = 0; i < count; i++) {
+        DScene d = scenes[i]->ds;
+        for (const auto& f : offs[(std::size_t)i])
+            *reinterpret_cast<const void**>((char*)&d + f.first) = C.arena + f.second;
+        d.error = reinterpret_cast<uint32_t*>(C.arena + err_off[(std::size_t)i]);
+        d.counters = nullptr;
+        if (d.cm.count) {
+            d.cm.photons = reinterpret_cast<const float4*>(C.arena + cm_off[3 * i]);
+            d.cm.cell_keys = reinterpret_cast<const unsigned long long*>(C.arena + cm_off[3 * i + 1]);
+            d.cm.cell_ranges = reinterpret_cast<const uint2*>(C.arena + cm_off[3 * i + 2]);
+        }
+        hs[(std::size_t)i] = d;
+    }
+    if ((int)C.h_scenes.size() < count || !C.d_scenes) {
+        if (C.d_scenes) cudaFree(C.d_scenes);
+        C.d_scenes = nullptr;
+        C.d_scenes = dalloc<DScene>((std::size_t)count);
+    }
+    C.h_scenes = hs;
+    CK(cudaMemcpyAsync(C.d_scenes, hs.data(), sizeof(DScene) * (std::size_t)count, cudaMemcpyHostToDevice, C.st));
+    CK(cudaStreamSynchronize(C.st));
+    C.arena_key = key;
+}
+
+// Pixel runs of every scene packed into waves of at most `cap` paths; a run always takes
+// every sample of its pixels, so each pixel's FP64 sum is the same sequence as in a
+// single render (films equal bit for bit).
+std::vector<std::vector<WaveArgs>> batch_waves(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
+                                               int64_t cap)
+{
+    std::vector<std::vector<WaveArgs>> waves(1);
+    int64_t used = 0;
+    for (int32_t i = 0; i < count; i++) {
+        const LuzRenderParams& p = params[i];
+        const int64_t npix = (int64_t)p.width * p.height;
+        const int64_t spp = p.spp;
+        if (spp > cap) throw Status(LUZ_E_LIMIT, "A batched scene's sample count exceeds the wave size.");
+        for (int64_t pb = 0; pb < npix;) {
+            int64_t fit = (cap - used) / spp;
+            if (fit <= 0 || (int64_t)waves.back().size() >= kBatchMaxSegments) {
+                waves.emplace_back();
+                used = 0;
+                continue;
+            }
+            const int64_t pc = std::min(fit, npix - pb);
+            WaveArgs w = base_args(scenes[i], &p);
+            w.pix_begin = (int32_t)pb;
+            w.pix_count = (int32_t)pc;
+            w.s_begin = 0;
+            w.s_count = (int32_t)spp;
+            w.n = pc * spp;
+            w.list_mode = 0;
+            w.batch_scene = i;
+            w.batch_offset = used;
+            waves.back().push_back(w);
+            used += pc * spp;
+            pb += pc;
+        }
+    }
+    if (waves.back().empty()) waves.pop_back();
+    return waves;
+}
+
+// Records the launches of one wave (the segment table at C.d_segs, its header at hdr)
+// into a graph: every kernel reads the wave's size from device memory.
+cudaGraphExec_t batch_graph(BatchContext& C, const BatchWaveHeader* hdr, int max_b, int64_t cap_paths,
+                            int64_t max_pix, int64_t max_segs, double* const* d_films, unsigned long long* d_rays,
+                            int32_t count, bool caustics, int sms, int occ_ext, int occ_sh, int occ_shade,
+                            int64_t& launches)
+{
+    (void)hdr;
+    (void)count;
+    const BatchShadeKernel shade = batch_shade_kernel(caustics ? 1 : 0);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(C.st, cudaStreamCaptureModeThreadLocal));
+    try {
+        CK(cudaMemsetAsync(C.ctrl, 0, sizeof(Ctrl), C.st));
+        k_raygen_batch<<<(unsigned)((cap_paths + kBlock - 1) / kBlock), kBlock, 0, C.st>>>(C.d_segs, hdr, C.pb, C.ctrl);
+        launches++;
+        for (int b = 0; b <= max_b; b++) {
+            k_extend_batch<<<sms * occ_ext, kBlock, 0, C.st>>>(C.d_scenes, C.d_segs, C.pb, C.ctrl, b, d_rays);
+            shade<<<sms * occ_shade, kBlock, 0, C.st>>>(C.d_scenes, C.d_segs, C.pb, C.ctrl, b);
+            k_shadow_batch<<<sms * occ_sh, kBlock, 0, C.st>>>(C.d_scenes, C.d_segs, C.pb, C.ctrl, b, d_rays + count);
+            launches += 3;
+        }
+        dim3 ag((unsigned)((max_pix + 127) / 128), (unsigned)max_segs);
+        k_accumulate_batch<<<ag, 128, 0, C.st>>>(C.d_segs, hdr, C.pb, d_films);
+        launches++;
+        CK(cudaGetLastError());
+    } catch (...) {
+        cudaStreamEndCapture(C.st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    CK(cudaStreamEndCapture(C.st, &g));
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    return ex;
+}
+
+int batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count, float* const* rgb_out,
+                 LuzRenderStats* stats, LuzBatchReport* report)
+{
+    const int device = scenes[0]->device;
+    BatchContext& C = batch_context(device);
+    std::lock_guard<std::mutex> lock(C.mu);
+    CK(cudaSetDevice(device));
+    bool caustics = false;
+    int max_b = 0;
+    int64_t max_pix = 0, max_spp = 0;
+    for (int32_t i = 0; i < count; i++) {   // photon maps are built per scene before the arena copy
+        clear_error(scenes[i], scenes[i]->stream);
+        prepare_caustics(scenes[i], &params[i], scenes[i]->stream);
+        CK(cudaStreamSynchronize(scenes[i]->stream));
+        caustics |= scenes[i]->pack->consts.caustics.enabled != 0;
+        max_b = std::max(max_b, params[i].max_bounces);
+        max_pix = std::max<int64_t>(max_pix, (int64_t)params[i].width * params[i].height);
+        max_spp = std::max<int64_t>(max_spp, params[i].spp);
+    }
+    batch_arena(C, scenes, count);
+    const cudaStream_t st = C.st;
+    // wave size: the autotuned choice for this scene set, else the default
+    std::vector<uint64_t> key;
+    for (int32_t i = 0; i < count; i++) {
+        key.push_back(scenes[i]->uid);
+        key.push_back((uint64_t)params[i].width << 40 ^ (uint64_t)params[i].height << 20 ^ (uint64_t)params[i].spp);
+    }
+    const auto it = C.tuned_wave.find(key);
+    int64_t cap = it != C.tuned_wave.end() ? it->second : kBatchWaveDefault;
+    cap = std::max<int64_t>(cap, max_spp);
+    // per-scene FP64 films and device output films, ray counters, the wave header
+    std::vector<int64_t> film_off((std::size_t)count), out_off((std::size_t)count);
+    int64_t film_doubles = 0, out_floats = 0;
+    for (int32_t i = 0; i < count; i++) {
+        const int64_t npix = (int64_t)params[i].width * params[i].height;
+        film_off[(std::size_t)i] = film_doubles;
+        out_off[(std::size_t)i] = out_floats;
+        film_doubles += 3 * npix;
+        out_floats += 3 * npix;
+    }
+    DeviceScratch D;
+    double* films = D.get<double>(film_doubles, st);
+    float* outs = D.get<float>(out_floats, st);
+    double** d_films = D.get<double*>(count, st);
+    unsigned long long* d_rays = D.get<unsigned long long>(2 * (int64_t)count, st);
+    BatchWaveHeader* hdr = D.get<BatchWaveHeader>(1, st);
+    {
+        std::vector<double*> hf((std::size_t)count);
+        for (int32_t i = 0; i < count; i++) hf[(std::size_t)i] = films + film_off[(std::size_t)i];
+        CK(cudaMemcpyAsync(d_films, hf.data(), sizeof(double*) * (std::size_t)count, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    int occ_ext = 1, occ_sh = 1, occ_shade = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_batch, kBlock, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_batch, kBlock, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_shade, batch_shade_kernel(caustics ? 1 : 0), kBlock, 0));
+    occ_ext = std::max(1, occ_ext);
+    occ_sh = std::max(1, occ_sh);
+    occ_shade = std::max(1, occ_shade);
+    const int sms = scenes[0]->sms;
+
+    // autotuner: on the first call for a scene set, time one wave at each candidate size
+    // (the first wave's pixels, every candidate processing the same work) and keep the
+    // fastest paths per millisecond; the trial waves' films are discarded
+    std::vector<LuzBatchTrial> trials;
+    auto run = [&](int64_t wave_cap, bool first_only, int64_t& launches, int64_t& nwaves, float& ms) {
+        const auto waves = batch_waves(scenes, params, count, wave_cap);
+        int64_t total_segs = 0;
+        for (const auto& wv : waves) total_segs += (int64_t)wv.size();
+        if (total_segs > C.h_seg_cap) {
+            if (C.h_segs) cudaFreeHost(C.h_segs);
+            C.h_segs = nullptr;
+            C.h_seg_cap = 0;
+            CK(cudaMallocHost(&C.h_segs, sizeof(WaveArgs) * (std::size_t)total_segs));
+            C.h_seg_cap = total_segs;
+        }
+        int64_t wave_max = 0;
+        for (const auto& wv : waves) {
+            int64_t n = 0;
+            for (const WaveArgs& w : wv) n += w.n;
+            wave_max = std::max(wave_max, n);
+        }
+        C.ensure_paths(wave_max);
+        int64_t pix_max = 0, segs_max = 0;
+        for (const auto& wv : waves) {
+            segs_max = std::max<int64_t>(segs_max, (int64_t)wv.size());
+            for (const WaveArgs& w : wv) pix_max = std::max<int64_t>(pix_max, w.pix_count);
+        }
+        cudaGraphExec_t ex = batch_graph(C, hdr, max_b, wave_max, pix_max, segs_max, d_films, d_rays, count, caustics,
+                                         sms, occ_ext, occ_sh, occ_shade, launches);
+        CK(cudaMemsetAsync(films, 0, sizeof(double) * (std::size_t)film_doubles, st));
+        CK(cudaMemsetAsync(d_rays, 0, sizeof(unsigned long long) * 2 * (std::size_t)count, st));
+        CK(cudaEventRecord(C.ev0, st));
+        int64_t seg_at = 0;
+        std::vector<BatchWaveHeader> hh(waves.size());
+        for (std::size_t k = 0; k < waves.size(); k++) {
+            const auto& wv = waves[k];
+            std::memcpy(C.h_segs + seg_at, wv.data(), sizeof(WaveArgs) * wv.size());
+            int64_t n = 0;
+            for (const WaveArgs& w : wv) n += w.n;
+            hh[k] = BatchWaveHeader{n, (uint32_t)wv.size(), 0u};
+            CK(cudaMemcpyAsync(C.d_segs, C.h_segs + seg_at, sizeof(WaveArgs) * wv.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(hdr, &hh[k], sizeof(BatchWaveHeader), cudaMemcpyHostToDevice, st));
+            CK(cudaGraphLaunch(ex, st));
+            seg_at += (int64_t)wv.size();
+            nwaves++;
+            if (first_only) break;
+        }
+        CK(cudaEventRecord(C.ev1, st));
+        CK(cudaEventSynchronize(C.ev1));
+        cudaGraphExecDestroy(ex);
+        CK(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
+        return first_only ? hh[0].n : (int64_t)0;
+    };
+    if (it == C.tuned_wave.end()) {
+        double best = -1.0;
+        int64_t best_cap = cap;
+        for (int64_t c : {int64_t(1) << 22, int64_t(1) << 24, int64_t(1) << 26}) {
+            if (c < max_spp) continue;
+            int64_t l = 0, nw = 0;
+            float ms = 0.f;
+            const int64_t n = run(c, true, l, nw, ms);
+            const double rate = (double)n / std::max(1e-3, (double)ms);
+            trials.push_back(LuzBatchTrial{c, (double)n, (double)ms});
+            if (rate > best) {
+                best = rate;
+                best_cap = c;
+            }
+        }
+        cap = best_cap;
+        C.tuned_wave[key] = cap;
+    }
+    int64_t launches = 0, nwaves = 0;
+    float ms = 0.f;
+    run(cap, false, launches, nwaves, ms);
+    // films: means per scene, each scene's error word, ray counts
+    for (int32_t i = 0; i < count; i++) {
+        const int64_t npix = (int64_t)params[i].width * params[i].height;
+        k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(films + film_off[(std::size_t)i], npix,
+                                                                 (double)params[i].spp, outs + out_off[(std::size_t)i]);
+        launches++;
+    }
+    CK(cudaGetLastError());
+    for (int32_t i = 0; i < count; i++)
+        CK(cudaMemcpyAsync(rgb_out[i], outs + out_off[(std::size_t)i],
+                           sizeof(float) * 3 * (std::size_t)params[i].width * params[i].height, cudaMemcpyDeviceToHost,
+                           st));
+    std::vector<unsigned long long> rays(2 * (std::size_t)count);
+    std::vector<uint32_t> errs((std::size_t)count);
+    CK(cudaMemcpyAsync(rays.data(), d_rays, sizeof(unsigned long long) * rays.size(), cudaMemcpyDeviceToHost, st));
+    for (int32_t i = 0; i < count; i++)
+        CK(cudaMemcpyAsync(&errs[(std::size_t)i], C.h_scenes[(std::size_t)i].error, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           st));
+    CK(cudaStreamSynchronize(st));
+    for (int32_t i = 0; i < count; i++)
+        if (errs[(std::size_t)i])
+            throw Status(LUZ_E_DEVICE, "Traversal stack overflow reported by the device (scene " + std::to_string(i) +
+                                           ", flags " + std::to_string(errs[(std::size_t)i]) + ").");
+    if (stats)
+        for (int32_t i = 0; i < count; i++) {
+            LuzRenderStats& o = stats[i];
+            o = LuzRenderStats{};
+            o.render_ms = ms;
+            o.samples = (double)params[i].width * params[i].height * params[i].spp;
+            o.extension_rays = (double)rays[(std::size_t)i];
+            o.shadow_rays = (double)rays[(std::size_t)(count + i)];
+            o.kernel_launches = launches;
+            o.waves = nwaves;
+            caustic_stats(scenes[i], &o);
+        }
+    LuzBatchReport r{};
+    r.wave_paths = cap;
+    r.waves = nwaves;
+    r.render_ms = ms;
+    r.kernel_launches = launches;
+    r.trial_count = (int32_t)trials.size();
+    for (std::size_t k = 0; k < trials.size() && k < 8; k++) r.trials[k] = trials[k];
+    C.last_report = r;
+    if (report) *report = r;
+    return LUZ_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------- no-allocation render
@@ -1878,25 +2563,32 @@ int luz_gpu_scene_create(const LuzSceneDesc* desc, int32_t device, luz_gpu_scene
         CK(cudaEventCreate(&s->ev1));
         const ScenePack& P = *s->pack;
         DScene& d = s->ds;
-        d.rects = s->up(P.rects);
-        d.objects = s->up(P.objects);
-        d.top_nodes = s->up(P.top_nodes);
-        d.top_children = s->up(P.top_children);
-        d.nodes4 = s->up(P.nodes4);
-        d.tris = s->up(P.tris);
-        d.tri_shade = s->up(P.tri_shade);
-        d.vnormals = s->up(P.vnormals);
-        d.vuvs = s->up(P.vuvs);
-        d.meshes = s->up(P.meshes);
-        d.materials = s->up(P.materials);
-        d.textures = s->up(P.textures);
-        d.texels = reinterpret_cast<const float4*>(s->up(P.texels));
-        d.lights = s->up(P.lights);
-        d.ies = s->up(P.ies);
-        d.cdf = s->up(P.cdf);
-        d.index_pool = s->up(P.index_pool);
-        d.env_texels = reinterpret_cast<const float4*>(s->up(P.env_texels));
-        d.obj_class = s->up(P.obj_class);
+        luz_gpu_scene* sp = s.get();
+        auto field = [&](auto& dst, const auto& v) {
+            using T = typename std::decay_t<decltype(v)>::value_type;
+            dst = reinterpret_cast<std::decay_t<decltype(dst)>>(sp->up(v));
+            sp->arena_fields.push_back({(std::size_t)((const char*)&dst - (const char*)&sp->ds), v.size() * sizeof(T)});
+        };
+        field(d.rects, P.rects);
+        field(d.objects, P.objects);
+        field(d.top_nodes, P.top_nodes);
+        field(d.top_children, P.top_children);
+        field(d.nodes4, P.nodes4);
+        field(d.tris, P.tris);
+        field(d.tri_shade, P.tri_shade);
+        field(d.vnormals, P.vnormals);
+        field(d.vuvs, P.vuvs);
+        field(d.meshes, P.meshes);
+        field(d.materials, P.materials);
+        field(d.textures, P.textures);
+        field(d.texels, P.texels);
+        field(d.lights, P.lights);
+        field(d.ies, P.ies);
+        field(d.cdf, P.cdf);
+        field(d.index_pool, P.index_pool);
+        field(d.env_texels, P.env_texels);
+        field(d.obj_class, P.obj_class);
+        s->uid = next_scene_uid();
         uint32_t* err = dalloc<uint32_t>(1);
         CK(cudaMemset(err, 0, sizeof(uint32_t)));
         s->allocs.push_back(err);
@@ -1983,7 +2675,8 @@ int luz_gpu_scene_set_path_budget(luz_gpu_scene* s, int64_t bytes)
 
 static void check_tune(const LuzTuneParams& t)
 {
-    if (t.wave_paths < 0 || t.staged_top_nodes < 0 || t.staged_top_nodes > 1 || t.extend_blocks_per_sm < 0
+    if (t.wave_paths < 0 || t.staged_top_nodes < 0 || t.staged_top_nodes > 1 || t.sort_rays < 0 || t.sort_rays > 1
+        || t.extend_blocks_per_sm < 0
         || t.shadow_blocks_per_sm < 0 || t.shade_blocks_per_sm < 0)
         throw Status(LUZ_E_INVALID, "Tuning parameters out of range.");
 }
@@ -2045,6 +2738,11 @@ int luz_gpu_autotune(luz_gpu_scene* s, const LuzRenderParams* p, LuzTuneParams* 
             {
                 LuzTuneParams t = best;
                 t.staged_top_nodes = best.staged_top_nodes ? 0 : 1;
+                consider(t);
+            }
+            {
+                LuzTuneParams t = best;
+                t.sort_rays = best.sort_rays ? 0 : 1;
                 consider(t);
             }
             for (int64_t wave : {int64_t(1) << 22, int64_t(1) << 24, int64_t(0)}) {
@@ -2133,54 +2831,27 @@ int luz_gpu_batch_render(luz_gpu_scene* const* scenes, const LuzRenderParams* pa
         for (int32_t i = 0; i < count; i++) {
             if (!scenes[i] || !rgb_out[i]) throw Status(LUZ_E_INVALID, "NULL argument.");
             if (params[i].flags) throw Status(LUZ_E_UNSUPPORTED, "Render flags are not supported in a batch.");
+            check_params(&params[i]);
+            if (scenes[i]->device != scenes[0]->device)
+                throw Status(LUZ_E_INVALID, "The scenes of a batch must be on one device.");
             for (int32_t j = 0; j < i; j++)
                 if (scenes[j] == scenes[i])
                     throw Status(LUZ_E_INVALID, "A scene handle appears twice in one batch.");
         }
-        std::vector<RenderJob> jobs((std::size_t)count);
-        std::vector<float*> outs((std::size_t)count, nullptr);
-        auto release = [&] {
-            for (int32_t i = 0; i < count; i++)
-                if (outs[(std::size_t)i]) {
-                    cudaSetDevice(scenes[i]->device);
-                    cudaFree(outs[(std::size_t)i]);
-                }
-        };
-        try {
-            for (int32_t i = 0; i < count; i++) {   // every allocation before any work is queued
-                RenderJob& J = jobs[(std::size_t)i];
-                J.s = scenes[i];
-                J.p = &params[i];
-                J.st = scenes[i]->stream;
-                J.wave_target = kBatchWaveTarget;
-                render_prepare(J);
-                outs[(std::size_t)i] = dalloc<float>((std::size_t)(3 * J.npix));
-                J.d_out = outs[(std::size_t)i];
-            }
-            for (RenderJob& J : jobs) render_enqueue(J);
-            for (int32_t i = 0; i < count; i++) {
-                RenderJob& J = jobs[(std::size_t)i];
-                CK(cudaSetDevice(J.s->device));
-                CK(cudaMemcpyAsync(rgb_out[i], J.d_out, sizeof(float) * 3 * (std::size_t)J.npix, cudaMemcpyDeviceToHost,
-                                   J.st));
-            }
-            for (int32_t i = 0; i < count; i++) {
-                RenderJob& J = jobs[(std::size_t)i];
-                CK(cudaSetDevice(J.s->device));
-                CK(cudaStreamSynchronize(J.st));
-                render_finish(J, stats ? &stats[i] : nullptr);
-            }
-        } catch (...) {
-            for (RenderJob& J : jobs) {
-                if (J.s) {
-                    cudaSetDevice(J.s->device);
-                    cudaStreamSynchronize(J.st);
-                }
-            }
-            release();
-            throw;
-        }
-        release();
+        return batch_render(scenes, params, count, rgb_out, stats, nullptr);
+    });
+}
+
+int luz_gpu_batch_render_ex(luz_gpu_scene* const* scenes, const LuzRenderParams* params, int32_t count,
+                            float* const* rgb_out, LuzRenderStats* stats, LuzBatchReport* report)
+{
+    if (report) *report = LuzBatchReport{};
+    const int rc = luz_gpu_batch_render(scenes, params, count, rgb_out, stats);
+    if (rc != LUZ_OK || !report || count == 0) return rc;
+    return guard([&] {
+        BatchContext& C = batch_context(scenes[0]->device);
+        std::lock_guard<std::mutex> lock(C.mu);
+        *report = C.last_report;
         return LUZ_OK;
     });
 }

@@ -66,6 +66,49 @@ __global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DS
 }
 
 
+// k_shade over a multi-scene wave: the scene and wave arguments are the path's segment's.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade_batch(const DScene* __restrict__ scenes,
+                                                                             const WaveArgs* __restrict__ segs,
+                                                                             PathBuf P, Ctrl* C, int bounce)
+{
+    const uint32_t count = C->count[bounce];
+    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
+    uint32_t* nq = (bounce & 1) ? P.queue0 : P.queue1;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (uint32_t base = wid * 32u; base < count; base += warps * 32u) {
+        const uint32_t i = base + lane_id();
+        const bool valid = i < count;
+        ShadeOut o;
+        o.cont = false;
+        o.sh[0] = o.sh[1] = false;
+        uint32_t p = 0;
+        if (valid) {
+            p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
+            const WaveArgs& w = segs[P.seg[p]];
+            shade_path<MODE>(scenes[w.batch_scene], w, P, p, bounce, o);
+        }
+        __syncwarp();
+        const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
+        if (o.cont) nq[qi] = p;
+        for (int slot = 0; slot < 2; slot++) {
+            const uint32_t si = warp_append(&C->shadow[bounce], o.sh[slot]);
+            if (o.sh[slot]) {
+                P.sh_o[si] = make_float4(o.sh_o[slot].x, o.sh_o[slot].y, o.sh_o[slot].z, o.sh_t[slot]);
+                P.sh_d[si] = make_float4(o.sh_d[slot].x, o.sh_d[slot].y, o.sh_d[slot].z,
+                                         __uint_as_float(p | ((uint32_t)slot << 31)));
+                P.sh_x[si] = make_int2(o.xobj, o.xprim);
+            }
+        }
+    }
+}
+
+BatchShadeKernel batch_shade_kernel(int mode)
+{
+    return mode == 1 ? k_shade_batch<1> : k_shade_batch<0>;
+}
+
 ShadeKernel shade_kernel(int mode)
 {
     switch (mode) {

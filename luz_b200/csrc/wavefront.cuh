@@ -40,6 +40,10 @@ struct PathBuf {
     uint32_t* bins;    // kShadeClasses segments of bin_stride paths, filled by extend in hit-class order
                        // (NULL: shade reads the extension queue as it is)
     uint32_t bin_stride;
+    uint32_t* seg;     // multi-scene waves: the wave segment (scene) of each path; NULL otherwise
+    uint32_t* sort_keys;   // coherence sort of the extension queue (tuning): key per queue entry,
+    uint32_t* qsort;       // the sorted queue,
+    uint32_t* sort_hist;   // and the per-key counts / offsets (kSortBins)
 };
 
 // Training snapshot of a path at its cache vertex: inputs, throughput and the
@@ -98,6 +102,12 @@ struct WaveArgs {
     uint8_t* cache_flag;          // 1 where the path left a training snapshot
     uint32_t* cache_count;        // [0] queries
     float cache_lo[3], cache_inv[3];   // position input = (p - lo) * inv
+    const uint32_t* sorted_queue;   // extension queue in coherence order for bounces >= 1 (NULL: as shaded)
+    // multi-scene waves (luz_gpu_batch_render): one WaveArgs per segment of a wave, the
+    // segment's scene and the first wave slot it covers
+    int32_t batch_scene;
+    int32_t batch_pad;
+    int64_t batch_offset;
 };
 
 
@@ -844,5 +854,10 @@ __device__ __forceinline__ F3 clean(F3 c)   // cleanColor (Threads.cpp:122-137)
 // caustic estimate, 2 radiance-cache render, 3 adjoint replay.
 using ShadeKernel = void (*)(const DScene*, WaveArgs, PathBuf, Ctrl*, int);
 ShadeKernel shade_kernel(int mode);
+
+// Multi-scene waves: every path finds its segment in P.seg, the segment's WaveArgs
+// in segs and its scene in scenes[segs[seg].batch_scene]. Modes 0 and 1 as above.
+using BatchShadeKernel = void (*)(const DScene*, const WaveArgs*, PathBuf, Ctrl*, int);
+BatchShadeKernel batch_shade_kernel(int mode);
 
 }  // namespace luz

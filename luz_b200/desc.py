@@ -143,11 +143,23 @@ class RenderStats(C.Structure):
 class TuneParams(C.Structure):
     """LuzTuneParams: launch tuning of a scene handle (zeros = defaults)."""
     _fields_ = [("wave_paths", C.c_int64), ("staged_top_nodes", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
-                ("shadow_blocks_per_sm", C.c_int32), ("shade_blocks_per_sm", C.c_int32)]
+                ("shadow_blocks_per_sm", C.c_int32), ("shade_blocks_per_sm", C.c_int32), ("sort_rays", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class TuneTrial(C.Structure):
     _fields_ = [("params", TuneParams), ("render_ms", C.c_double)]
+
+
+class BatchTrial(C.Structure):
+    _fields_ = [("wave_paths", C.c_int64), ("paths", C.c_double), ("ms", C.c_double)]
+
+
+class BatchReport(C.Structure):
+    """LuzBatchReport: what luz_gpu_batch_render_ex did."""
+    _fields_ = [("wave_paths", C.c_int64), ("waves", C.c_int64), ("kernel_launches", C.c_int64),
+                ("render_ms", C.c_double), ("trial_count", C.c_int32), ("reserved", C.c_int32),
+                ("trials", BatchTrial * 8)]
 
 
 class AdaptiveParams(C.Structure):

@@ -29,6 +29,7 @@ EXPORTED = [
     "luz_gpu_cache_gradient", "luz_gpu_cache_train", "luz_gpu_render_cached", "luz_gpu_adjoint_emission",
     "luz_gpu_adjoint_density", "luz_gpu_scene_set_path_budget", "luz_gpu_scene_set_traversal_limits",
     "luz_gpu_render_pixels", "luz_gpu_scene_set_tuning", "luz_gpu_scene_get_tuning", "luz_gpu_autotune",
+    "luz_gpu_batch_render_ex",
 ]
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "unsupported", -4: "limit exceeded",
@@ -76,6 +77,7 @@ def lib():
     L.luz_gpu_render_ex.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams), vp,
                                     C.POINTER(D.NforBuffers), vp, C.POINTER(D.RenderStats)]
     L.luz_gpu_batch_render.argtypes = [vp, vp, i32, vp, vp]
+    L.luz_gpu_batch_render_ex.argtypes = [vp, vp, i32, vp, vp, C.POINTER(D.BatchReport)]
     L.luz_gpu_nfor_denoise.argtypes = [i32, C.POINTER(D.NforBuffers), i32, i32, C.POINTER(D.NforSettings), vp]
     L.luz_gpu_nfor_error.argtypes = [C.c_char_p, C.c_size_t]
     L.luz_gpu_render_denoised.argtypes = [vp, C.POINTER(D.RenderParams), C.POINTER(D.AdaptiveParams),
@@ -345,19 +347,27 @@ def nfor_denoise(bufs: dict, device: int = 0, prefilter_radius=1, regression_rad
     return out
 
 
-def batch_render(scenes, plist):
-    """luz_gpu_batch_render: renders every (scene, params) pair concurrently; returns the
-    films (H x W x 3 each) and the per-scene stats."""
+def batch_render(scenes, plist, report: bool = False):
+    """luz_gpu_batch_render(_ex): renders every (scene, params) pair in shared multi-scene
+    waves; returns the films (H x W x 3 each) and the per-scene stats (and the batch report
+    as a dict when report=True)."""
     n = len(scenes)
     if len(plist) != n:
         raise ValueError("one RenderParams per scene")
-    handles = (C.c_void_p * n)(*[g.h.value for g in scenes])
-    ps = (D.RenderParams * n)(*plist)
+    handles = (C.c_void_p * max(n, 1))(*[g.h.value for g in scenes])
+    ps = (D.RenderParams * max(n, 1))(*plist)
     outs = [np.zeros((p.height, p.width, 3), np.float32) for p in plist]
-    optrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
-    stats = (D.RenderStats * n)()
-    _check(lib().luz_gpu_batch_render(handles, ps, n, optrs, stats))
-    return outs, list(stats)
+    optrs = (C.c_void_p * max(n, 1))(*[o.ctypes.data for o in outs])
+    stats = (D.RenderStats * max(n, 1))()
+    rep = D.BatchReport()
+    _check(lib().luz_gpu_batch_render_ex(handles, ps, n, optrs, stats, C.byref(rep)))
+    if not report:
+        return outs, list(stats)[:n]
+    r = {"wave_paths": rep.wave_paths, "waves": rep.waves, "kernel_launches": rep.kernel_launches,
+         "render_ms": rep.render_ms,
+         "trials": [{"wave_paths": rep.trials[i].wave_paths, "paths": rep.trials[i].paths, "ms": rep.trials[i].ms}
+                    for i in range(rep.trial_count)]}
+    return outs, list(stats)[:n], r
 
 
 def render(scene: D.Scene, width: int, height: int, spp: int, max_bounces: int, seed: int, device: int = 0,

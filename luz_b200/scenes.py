@@ -459,17 +459,17 @@ def caustic_pool(width: int = 64, height: int = 48, spp: int = 4, max_bounces: i
     return Workload("caustic_pool", s, width, height, spp, max_bounces)
 
 
-def batch_workloads(count: int = 48, seed: int = 4242) -> list:
+def batch_workloads(count: int = 48, seed: int = 4242, side_range=(128, 1024), spp_range=(4, 256)) -> list:
     """Many independent scenes for luz_gpu_batch_render: triangle counts log-uniform in
     [1e3, 1e6] (displaced icospheres of the nearest level), square images with sides
-    log-uniform in [128, 1024], spp log-uniform in [4, 256], max depth uniform in [4, 16]."""
+    log-uniform in side_range, spp log-uniform in spp_range, max depth uniform in [4, 16]."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         tris = float(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
         level = int(np.clip(np.round(np.log(tris / 20.0) / np.log(4.0)), 3, 8))
-        side = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
-        spp = int(np.exp(rng.uniform(np.log(4), np.log(256))))
+        side = int(np.exp(rng.uniform(np.log(side_range[0]), np.log(side_range[1]))))
+        spp = int(np.exp(rng.uniform(np.log(spp_range[0]), np.log(spp_range[1]))))
         depth = int(rng.integers(4, 17))
         w = mesh_glossy(side, side, spp, depth, level=level, seed=seed + i)
         w.name = f"batch{i}"

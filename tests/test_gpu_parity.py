@@ -232,3 +232,32 @@ def test_batch_render_equals_individual_renders():
         native.batch_render([gs[0], gs[0]], [ps[0], ps[0]])
     assert e.value.code == -1
     assert native.batch_render([], []) == ([], [])
+    for g in gs:
+        g.close()
+
+
+@pytest.mark.gpu
+def test_batch_of_many_waves_with_caustics_equals_individual_renders():
+    """A batch larger than the largest autotuned wave (75.5 M paths of one Cornell view, so
+    at least two multi-scene waves replay the wave graph), with a caustic-map scene (the
+    shade instantiation with the photon estimate) and a second view of the same geometry:
+    every film equals its single render bit for bit, the autotuner reports its trials on
+    the first call and its choice is reused on the second."""
+    from cases import caustic_case
+    ws = [scenes.cornell(1024, 1024, 72, 8), caustic_case(), scenes.cornell(200, 120, 9, 5),
+          scenes.mesh_glossy(96, 64, 3, 12, level=5)]
+    gs = [native.GpuScene(w.scene.build()) for w in ws]
+    ps = [native.params(w.width, w.height, w.spp, w.max_bounces, w.seed) for w in ws]
+    imgs, stats, rep = native.batch_render(gs, ps, report=True)
+    assert rep["waves"] >= 2 and len(rep["trials"]) >= 2
+    assert rep["wave_paths"] in [t["wave_paths"] for t in rep["trials"]]
+    for g, p, img, st in zip(gs, ps, imgs, stats):
+        ref, rst = g.render(p)
+        assert np.array_equal(img, ref)
+        assert st.extension_rays == rst.extension_rays and st.shadow_rays == rst.shadow_rays
+        assert st.samples == p.width * p.height * p.spp
+    imgs2, _, rep2 = native.batch_render(gs, ps, report=True)
+    assert rep2["trials"] == [] and rep2["wave_paths"] == rep["wave_paths"]
+    assert all(np.array_equal(a, b) for a, b in zip(imgs, imgs2))
+    for g in gs:
+        g.close()

@@ -1,7 +1,7 @@
 """Launch tuning and the autotuner (luz_gpu_scene_set_tuning, luz_gpu_autotune): no
-tuning choice changes a film. Staged top BVH nodes (shared memory), wave sizes and
-persistent grid sizes give the same image bit for bit; the autotuner leaves its choice
-on the handle and reports its timed trials."""
+tuning choice changes a film. Staged top BVH nodes (shared memory), the coherence sort
+of the extension queue, wave sizes and persistent grid sizes give the same image bit
+for bit; the autotuner leaves its choice on the handle and reports its timed trials."""
 import numpy as np
 import pytest
 
@@ -18,9 +18,9 @@ def test_tuning_choices_leave_the_film_unchanged(name):
     try:
         p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
         ref, _ = g.render(p)
-        for kw in (dict(staged_top_nodes=1), dict(wave_paths=4096), dict(extend_blocks_per_sm=2, shadow_blocks_per_sm=3,
-                                                                         shade_blocks_per_sm=1),
-                   dict(staged_top_nodes=1, wave_paths=5000, extend_blocks_per_sm=1)):
+        for kw in (dict(staged_top_nodes=1), dict(sort_rays=1), dict(wave_paths=4096),
+                   dict(extend_blocks_per_sm=2, shadow_blocks_per_sm=3, shade_blocks_per_sm=1),
+                   dict(staged_top_nodes=1, sort_rays=1, wave_paths=5000, extend_blocks_per_sm=1)):
             g.set_tuning(**kw)
             img, _ = g.render(p)
             assert np.array_equal(img, ref), kw
