@@ -23,6 +23,15 @@ def rel_mse(img, ref):
     return float(np.mean((img.astype(np.float64) - ref) ** 2) / np.mean(ref ** 2))
 
 
+def pixel_rel_mse(img, ref, trim=0.01):
+    """Per-pixel relative MSE, (x - ref)^2 / (ref^2 + 0.01), averaged over the pixels after
+    dropping the largest `trim` fraction: the glossy frame's 5e4-peak sun lobe sends rare
+    samples into a few pixels (fireflies), and one of them would set an untrimmed mean."""
+    e = ((img.astype(np.float64) - ref) ** 2 / (ref ** 2 + 0.01)).mean(axis=-1).ravel()
+    e = np.sort(e)[: max(1, int(round(len(e) * (1.0 - trim))))]
+    return float(e.mean())
+
+
 @pytest.mark.parametrize("name", sorted(ORACLE_64K))
 def test_same_seed_matches_oracle_at_65536_spp(name, golden):
     w = ORACLE_64K[name]()
@@ -81,8 +90,9 @@ def test_config0_frame_converges_to_the_65536_spp_oracle(golden):
 def test_full_frame_pixel_subsets_converge_to_the_65536_spp_oracle(name, golden):
     """Configs 1 and 2 at full size: the seeded 4,096-pixel subsets the reference rendered at
     65,536 spp (oracle64k_<case>.npz, _threadRender per pixel), rendered on the GPU with
-    luz_gpu_render_pixels. With an independent seed the relative MSE falls with the sample
-    count; with the oracle's seed the 65,536-spp GPU pixels are the same estimate."""
+    luz_gpu_render_pixels. With an independent seed the per-pixel relative MSE (trimmed of
+    the 1% largest, pixel_rel_mse) falls with the sample count; with the oracle's seed the
+    65,536-spp GPU pixels are the same estimate."""
     from cases import ORACLE_64K_SUBSET
     gd = golden("oracle64k_" + name)
     ref = gd["rgb"].astype(np.float64)
@@ -92,9 +102,9 @@ def test_full_frame_pixel_subsets_converge_to_the_65536_spp_oracle(name, golden)
     for spp in (16, 256, 4096):
         rgb, st = g.render_pixels(native.params(w.width, w.height, spp, w.max_bounces, 977), gd["x"], gd["y"])
         assert st.samples == len(gd["x"]) * spp
-        errs[spp] = rel_mse(rgb, ref)
+        errs[spp] = pixel_rel_mse(rgb, ref)
     rgb, _ = g.render_pixels(native.params(w.width, w.height, 65536, w.max_bounces, int(gd["seed"])), gd["x"], gd["y"])
-    same = rel_mse(rgb, ref)
+    same = pixel_rel_mse(rgb, ref)
     g.close()
     print(f"{name} subset relative MSE by spp:", errs, "same seed at 65,536 spp:", same)
     assert errs[16] > errs[256] > errs[4096], errs
