@@ -610,7 +610,10 @@ typedef struct LuzCacheParams {
     float    learning_rate;       /* Adam step size (1e-2); beta1 0.9, beta2 0.99, eps 1e-8 */
     int32_t  prefix;              /* first bounce whose vertex queries the cache (1); >= 0   */
     int32_t  train_every;         /* one training path in this many (16); >= 1               */
-    int32_t  reserved;
+    float    min_roughness;       /* in [0, 1]: a surface vertex whose roughness is below this
+                                     continues the path and a later vertex queries the cache
+                                     (0: the first vertex at or after `prefix` always does);
+                                     diffuse and phase-function materials count as 1          */
 } LuzCacheParams;
 int luz_gpu_cache_create(int32_t device, const LuzCacheParams* params, luz_gpu_cache** out);
 int luz_gpu_cache_destroy(luz_gpu_cache* cache);

@@ -3152,6 +3152,7 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     const GSceneConst& K = s->pack->consts;
     w.cache_prefix = c->prm.prefix;
     w.cache_train_every = (uint32_t)c->prm.train_every;
+    w.cache_min_rough = c->prm.min_roughness;
     w.cache_q = q;
     w.cache_s = snaps;
     w.cache_flag = tflag;
@@ -3244,6 +3245,8 @@ int luz_gpu_cache_create(int32_t device, const LuzCacheParams* prm, luz_gpu_cach
             throw Status(LUZ_E_INVALID, "Cache learning rate must be finite and positive.");
         if (prm->prefix < 0) throw Status(LUZ_E_INVALID, "Cache prefix must be non-negative.");
         if (prm->train_every < 1) throw Status(LUZ_E_INVALID, "Cache training interval must be at least 1.");
+        if (!(prm->min_roughness >= 0.0f && prm->min_roughness <= 1.0f))
+            throw Status(LUZ_E_INVALID, "Cache minimum roughness must lie in [0, 1].");
         CK(cudaSetDevice(device));
         std::unique_ptr<luz_gpu_cache> c(new luz_gpu_cache);
         c->device = device;

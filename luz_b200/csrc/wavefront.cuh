@@ -102,6 +102,7 @@ struct WaveArgs {
     uint8_t* cache_flag;          // 1 where the path left a training snapshot
     uint32_t* cache_count;        // [0] queries
     float cache_lo[3], cache_inv[3];   // position input = (p - lo) * inv
+    float cache_min_rough;        // vertices rougher than this (cache_roughness) query the cache
     const uint32_t* sorted_queue;   // extension queue in coherence order for bounces >= 1 (NULL: as shaded)
     // multi-scene waves (luz_gpu_batch_render): one WaveArgs per segment of a wave, the
     // segment's scene and the first wave slot it covers
@@ -504,6 +505,13 @@ static __device__ __noinline__ void atmos_ray(const WaveArgs& w, const PathBuf& 
 
 // CAUSTICS: the scene has a caustic photon map (a separate instantiation, so
 // that scenes without one keep the leaner kernel).
+// Roughness the radiance cache sees: 1 for diffuse and volume phase materials.
+__device__ __forceinline__ float cache_roughness(const GMaterial& m)
+{
+    const bool diffuse = m.type == MT_LAMBERTIAN || m.type == MT_ISOTROPIC || m.type == MT_HG || m.type == MT_EMISSIVE;
+    return diffuse ? 1.0f : m.roughness;
+}
+
 // Radiance-cache inputs at a surface hit: position in the scene box, outgoing
 // direction, shading normal, roughness (1 for diffuse and volume phase materials).
 __device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, const GMaterial& m, F3 ray_d, float* in)
@@ -518,8 +526,7 @@ __device__ __forceinline__ void cache_inputs(const WaveArgs& w, const Hit& h, co
     in[6] = h.n.x;
     in[7] = h.n.y;
     in[8] = h.n.z;
-    const bool diffuse = m.type == MT_LAMBERTIAN || m.type == MT_ISOTROPIC || m.type == MT_HG || m.type == MT_EMISSIVE;
-    in[9] = diffuse ? 1.0f : m.roughness;
+    in[9] = cache_roughness(m);
 }
 
 // MODE 0: plain; 1: with the caustic photon map; 2: radiance-cache render;
@@ -681,7 +688,8 @@ static __device__ void shade_path(const DScene& S, const WaveArgs& w, const Path
         // on and records what the continuation gathered.
         bool cache_query = false;
         if constexpr (MODE == 2) {
-            if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE)) {
+            if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE) &&
+                cache_roughness(m) >= w.cache_min_rough) {
                 const uint64_t key = ((uint64_t)pix << 24) ^ (uint64_t)P.sample[p] ^ ((uint64_t)w.cache_wave << 48);
                 if (splitmix64(key) % w.cache_train_every == 0) {
                     CacheSnap& sn = w.cache_s[p];

@@ -86,13 +86,17 @@ def test_config0_frame_converges_to_the_65536_spp_oracle(golden):
     assert same < 1e-8 and st.samples == w.width * w.height * 65536
 
 
-@pytest.mark.parametrize("name", ["glossy_full", "instancing_full"])
-def test_full_frame_pixel_subsets_converge_to_the_65536_spp_oracle(name, golden):
+@pytest.mark.parametrize("name,trim", [("glossy_full", 0.01), ("instancing_full", 0.0)])
+def test_full_frame_pixel_subsets_converge_to_the_65536_spp_oracle(name, trim, golden):
     """Configs 1 and 2 at full size: the seeded 4,096-pixel subsets the reference rendered at
     65,536 spp (oracle64k_<case>.npz, _threadRender per pixel), rendered on the GPU with
     luz_gpu_render_pixels. With an independent seed the per-pixel relative MSE (trimmed of
     the 1% largest, pixel_rel_mse) falls with the sample count; with the oracle's seed the
-    65,536-spp GPU pixels are the same estimate."""
+    65,536-spp GPU pixels are the same estimate. The dark 1e5-instance frame is measured
+    untrimmed: its light arrives on rare lit paths, so its per-pixel errors are heavy-tailed
+    by nature and the trimmed mean (or the median) of independent renders rises with spp
+    there, for the reference's own renders too (measured: trimmed 1.2e-8, 1.7e-8, 1.9e-8 at
+    16, 256, 4,096 spp; untrimmed 0.64, 0.0031, 0.00069)."""
     from cases import ORACLE_64K_SUBSET
     gd = golden("oracle64k_" + name)
     ref = gd["rgb"].astype(np.float64)
@@ -102,9 +106,9 @@ def test_full_frame_pixel_subsets_converge_to_the_65536_spp_oracle(name, golden)
     for spp in (16, 256, 4096):
         rgb, st = g.render_pixels(native.params(w.width, w.height, spp, w.max_bounces, 977), gd["x"], gd["y"])
         assert st.samples == len(gd["x"]) * spp
-        errs[spp] = pixel_rel_mse(rgb, ref)
+        errs[spp] = pixel_rel_mse(rgb, ref, trim)
     rgb, _ = g.render_pixels(native.params(w.width, w.height, 65536, w.max_bounces, int(gd["seed"])), gd["x"], gd["y"])
-    same = pixel_rel_mse(rgb, ref)
+    same = pixel_rel_mse(rgb, ref, trim)
     g.close()
     print(f"{name} subset relative MSE by spp:", errs, "same seed at 65,536 spp:", same)
     assert errs[16] > errs[256] > errs[4096], errs

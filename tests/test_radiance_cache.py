@@ -135,6 +135,9 @@ def test_training_fits_a_smooth_field(cache):
 def test_invalid_arguments(cache):
     with pytest.raises(native.LuzError):
         native.RadianceCache(D.cache_params(batch=0))
+    for bad in (-0.1, 1.5, float("nan")):
+        with pytest.raises(native.LuzError):
+            native.RadianceCache(D.cache_params(min_roughness=bad))
     with pytest.raises(native.LuzError):
         cache.train(rows(5000), smooth_target(rows(5000)), steps=1)   # more rows than the batch
 
@@ -167,3 +170,27 @@ def test_cached_render_against_plain():
     assert sc.extension_rays < 0.8 * sp.extension_rays, facts
     assert abs(cached.mean() - ref.mean()) < 0.05 * ref.mean(), facts
     assert rmse(cached, ref) < rmse(plain, ref), facts
+
+
+@pytest.mark.gpu
+def test_min_roughness_gate():
+    """Glass (roughness 0.1) sphere over a metal (0.3) floor under an environment map: with
+    min_roughness 0.5 no vertex is rough enough to query the cache, so the cached render
+    traces every path to its end like the plain render (same rays, same image up to
+    contraction differences between the two shading instantiations); with the gate at 0 the
+    cache ends the paths that reach a second vertex there."""
+    from luz_b200 import scenes
+    w = scenes.mesh_glossy(64, 36, 1, 8, level=3)
+    g = native.GpuScene(w.scene.build())
+    p = native.params(64, 36, 16, 8, 5)
+    plain, sp = g.render(p)
+    c = native.RadianceCache(D.cache_params(seed=3, batch=4096, min_roughness=0.5))
+    gated, sg = c.render(g, p)
+    c.close()
+    c = native.RadianceCache(D.cache_params(seed=3, batch=4096, min_roughness=0.0))
+    _, so = c.render(g, p)
+    c.close()
+    g.close()
+    assert sg.extension_rays == sp.extension_rays and sg.shadow_rays == sp.shadow_rays
+    assert np.allclose(gated, plain, rtol=1e-4, atol=1e-5)
+    assert so.extension_rays < 0.9 * sp.extension_rays   # most paths leave for the environment first
