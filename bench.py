@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cache-min-rough", type=float, default=None,
                     help="cache workloads: LuzCacheParams.min_roughness (default per workload)")
+    ap.add_argument("--cache-batch", type=int, default=16384, help="cache workloads: training rows per step")
+    ap.add_argument("--cache-train-every", type=int, default=16, help="cache workloads: one training path in this many")
+    ap.add_argument("--cache-wave", type=int, default=0,
+                    help="cache workloads: paths per wave of the cached render (0: its default, 4 Mi)")
     return ap.parse_args()
 
 
@@ -552,6 +556,7 @@ def run_cache(args):
         targets = (16, 64, 256)
     g = native.GpuScene(w.scene.build())
     W, H, MB = w.width, w.height, w.max_bounces
+    tuned = {"wave_paths": args.cache_wave} if args.cache_wave else {}
     if args.workload == "cache_cornell":
         ref = np.load(os.path.join(golden, "oracle64k_cornell300.npz"))["rgb"].astype(np.float64)
         ref_kind = "reference film at 65,536 spp (Renderer::render)"
@@ -569,20 +574,28 @@ def run_cache(args):
         e = np.sort(np.mean((x - ref) ** 2 / (ref ** 2 + 0.01), axis=1))
         return float(np.mean(e[:len(e) - len(e) // 100]))
 
+    def cached_render(c, p):   # the handle's wave size applies to the cached render only
+        g.set_tuning(**tuned)
+        try:
+            return c.render(g, p)
+        finally:
+            g.set_tuning()
+
     def new_cache():
-        return native.RadianceCache(D.cache_params(seed=3, min_roughness=min_rough))
+        return native.RadianceCache(D.cache_params(seed=3, batch=args.cache_batch, train_every=args.cache_train_every,
+                                                   min_roughness=min_rough))
 
     for _ in range(max(1, args.warmup)):
         g.render(native.params(W, H, 2, MB, 7))
         c = new_cache()
-        c.render(g, native.params(W, H, 2, MB, 7))
+        cached_render(c, native.params(W, H, 2, MB, 7))
         c.close()
     plain, cached = [], []
     for spp in spps:
         img, st = g.render(native.params(W, H, spp, MB, 202))
         plain.append((spp, st.render_ms, relmse(img)))
         c = new_cache()
-        img, st = c.render(g, native.params(W, H, spp, MB, 202))
+        img, st = cached_render(c, native.params(W, H, spp, MB, 202))
         cached.append((spp, st.render_ms, relmse(img)))
         c.close()
 
@@ -610,9 +623,10 @@ def run_cache(args):
                       "error": "relative MSE mean((x - ref)^2 / (ref^2 + 0.01))"
                                + (", 1% largest pixels dropped" if sub is not None else ""), "reference": ref_kind,
                       "target": f"error of the plain {targets[-1]}-spp image",
-                      "cache": "prefix 1, NEE explicit at the cache vertex, one training path in 16, "
-                               "batch 16384 (up to 16 steps per wave), lr 1e-2, first sample plain with 32 "
-                               f"warm-up steps, min roughness {min_rough:g}"},
+                      "cache": f"prefix 1, NEE explicit at the cache vertex, one training path in {args.cache_train_every}, "
+                               f"batch {args.cache_batch} (up to 16 steps per wave), lr 1e-2, first sample plain with 32 "
+                               f"warm-up steps, min roughness {min_rough:g}, "
+                               f"waves of {args.cache_wave or 4194304} paths"},
            "speedup_at": at,
            "plain": {"curve": [{"spp": s, "ms": t, "relmse": e} for s, t, e in plain]},
            "cached": {"curve": [{"spp": s, "ms": t, "relmse": e} for s, t, e in cached]}}

@@ -336,14 +336,15 @@ int luz_gpu_scene_set_traversal_limits(luz_gpu_scene* scene, int32_t mesh_entrie
 
 /* Launch tuning of a scene handle (zeros = defaults). None of it changes a film: the
  * image does not depend on the wave size, the grid or where nodes are read from.
- *   wave_paths:           paths per wave (default 64 Mi, capped by the path budget);
+ *   wave_paths:           paths per wave (default 64 Mi; 4 Mi for luz_gpu_render_cached, which
+ *                         trains its cache between waves), capped by the path budget;
  *   staged_top_nodes:     1 = the trace kernels copy the breadth-first top of the scene's
  *                         largest collapsed mesh BVH (21 nodes) into shared memory per
  *                         block and read those nodes there;
  *   *_blocks_per_sm:      blocks per SM of the persistent closest-hit / any-hit grids and
  *                         of the shade grid (default: full occupancy; larger values are
  *                         capped at it);
- *   sort_rays:            see the field.
+ *   sort_rays, lanes:     see the fields.
  * No counterpart in the reference (its worker count is Scene::setRenderingThreads). */
 typedef struct LuzTuneParams {
     int64_t wave_paths;
@@ -351,9 +352,15 @@ typedef struct LuzTuneParams {
     int32_t extend_blocks_per_sm;
     int32_t shadow_blocks_per_sm;
     int32_t shade_blocks_per_sm;
-    int32_t sort_rays;            /* 1: extension rays of bounces >= 1 are traced in coherence  */
-    int32_t reserved;             /* order (direction octant, then the Morton cell of the ray */
-} LuzTuneParams;                  /* origin in a 16^3 grid over the scene box)                */
+    int32_t sort_rays;            /* 1: extension rays of bounces >= 1 are traced in coherence
+                                     order (direction octant, then the Morton cell of the ray
+                                     origin in a 16^3 grid over the scene box)                 */
+    int32_t lanes;                /* 0: a frame that takes more than one wave splits the path
+                                     state in two halves and runs consecutive waves on two
+                                     streams, the last bounces of one overlapping the first of
+                                     the next (film accumulation stays in wave order);
+                                     1: one wave at a time                                     */
+} LuzTuneParams;
 typedef struct LuzTuneTrial {
     LuzTuneParams params;
     double render_ms;             /* device time of the trial render */
@@ -362,7 +369,7 @@ int luz_gpu_scene_set_tuning(luz_gpu_scene* scene, const LuzTuneParams* tune);
 int luz_gpu_scene_get_tuning(const luz_gpu_scene* scene, LuzTuneParams* tune);
 /* Autotuner: times renders of `params` on the device (CUDA events; each trial rendered
  * twice, the second timed) while it changes one knob at a time from the handle's
- * current tuning (staged nodes on/off; ray sorting on/off; waves of 4 Mi, 16 Mi and 64 Mi paths; the
+ * current tuning (staged nodes on/off; ray sorting on/off; one or two wave lanes; waves of 4 Mi, 16 Mi and 64 Mi paths; the
  * closest-hit grid at full occupancy or one block fewer; the any-hit grid at full or
  * half occupancy), keeps every change that lowers the time, and leaves the best
  * tuning on the handle (also copied to `chosen` when not NULL). The trials (up to

@@ -6,6 +6,10 @@
 // lattice arithmetic is written with explicit round-to-nearest intrinsics, so
 // it reproduces the reference bit for bit in either unit.
 #pragma once
+// Out of line by default; the shade kernels' translation unit inlines the sampler.
+#ifndef LUZ_SAMPLER_ATTR
+#define LUZ_SAMPLER_ATTR __noinline__
+#endif
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -113,7 +117,7 @@ __device__ __forceinline__ double hashed(const Key& k, uint32_t dk, uint32_t com
     key ^= ((uint64_t)comp + 1ull) * 0xbf58476d1ce4e5b9ull;
     return unit53(splitmix64(key));
 }
-static __device__ __noinline__ double sample1d(const Key& k, uint32_t dim)
+static __device__ LUZ_SAMPLER_ATTR double sample1d(const Key& k, uint32_t dim)
 {
     const uint32_t dk = dim + k.bounce * 32u;
     if (!progressive(dim)) return hashed(k, dk, 0);
@@ -125,7 +129,7 @@ static __device__ __noinline__ double sample1d(const Key& k, uint32_t dim)
 struct S2 {
     float x, y;
 };
-static __device__ __noinline__ S2 sample2d(const Key& k, uint32_t dim)
+static __device__ LUZ_SAMPLER_ATTR S2 sample2d(const Key& k, uint32_t dim)
 {
     const uint32_t dk = dim + k.bounce * 32u;
     if (!progressive(dim)) return S2{(float)hashed(k, dk, 0), (float)hashed(k, dk, 1)};

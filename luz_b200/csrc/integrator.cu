@@ -914,6 +914,12 @@ struct luz_gpu_scene {
     std::vector<void*> pallocs;
     Ctrl* ctrl = nullptr;
     Ctrl* ctrl_host = nullptr;
+    // second wave lane (render_enqueue): its counters, stream and the events that order
+    // the lanes (setup before lane 1; each wave's film accumulation after the previous
+    // wave's; lane 1 done before the resolve); created by the first two-lane render
+    Ctrl* ctrl2 = nullptr;
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t lane_setup = nullptr, lane_done = nullptr, lane_acc[2] = {nullptr, nullptr};
     unsigned long long* status_host = nullptr;   // pinned: ray totals [0..1] and error word [2] of a call
     unsigned long long* totals = nullptr;   // device: extension / shadow rays of the current render
     double* film = nullptr;
@@ -998,7 +1004,7 @@ struct luz_gpu_scene {
         pb.bin_stride = (uint32_t)n;
         pb.sort_keys = palloc<uint32_t>(n);
         pb.qsort = palloc<uint32_t>(n);
-        pb.sort_hist = palloc<uint32_t>(kSortBins);
+        pb.sort_hist = palloc<uint32_t>(2 * kSortBins);   // one histogram per wave lane
         cap = n;
     }
     // Paths a wave of up to `want` paths may use: the buffers held when they are
@@ -1051,10 +1057,62 @@ struct luz_gpu_scene {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
+        if (ctrl2) cudaFree(ctrl2);
+        for (cudaEvent_t e : {lane_setup, lane_done, lane_acc[0], lane_acc[1]})
+            if (e) cudaEventDestroy(e);
+        if (stream2) cudaStreamDestroy(stream2);
+    }
+    void ensure_lanes()
+    {
+        if (stream2) return;
+        ctrl2 = dalloc<Ctrl>(1);
+        CK(cudaEventCreateWithFlags(&lane_setup, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&lane_done, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&lane_acc[0], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&lane_acc[1], cudaEventDisableTiming));
+        CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
     }
 };
 
 namespace {
+
+// Lane 1's view of a path buffer: the upper half of every per-path array, from
+// path `off` on (shadow records 2 per path, features 3; the class segments keep
+// their stride, so lane 1 uses the upper half of each), and the second sort histogram.
+PathBuf lane_view(const PathBuf& b, int64_t off)
+{
+    PathBuf v = b;
+    v.ray_o += off;
+    v.ray_d += off;
+    v.thr += off;
+    v.rad += off;
+    v.pend0 += off;
+    v.pend1 += off;
+    v.pixel += off;
+    v.sample += off;
+    v.hit += off;
+    v.hit_prim += off;
+    v.queue0 += off;
+    v.queue1 += off;
+    v.sh_o += 2 * off;
+    v.sh_d += 2 * off;
+    v.sh_x += 2 * off;
+    v.color += off;
+    if (v.feat) v.feat += 3 * off;
+    v.bins += off;
+    if (v.seg) v.seg += off;
+    v.sort_keys += off;
+    v.qsort += off;
+    v.sort_hist += kSortBins;
+    return v;
+}
+
+}  // namespace
+
+namespace {
+
+// Smallest lane of a two-lane render (render_prepare).
+constexpr int64_t kMinLanePaths = int64_t(1) << 22;
 
 // Paths in flight per wave. A launch of the persistent trace kernels lasts at
 // least as long as its slowest warp's traversal, a tail of the order of half a
@@ -1064,11 +1122,8 @@ namespace {
 // Path state is 268 B per path (18 GB at 64 Mi, a tenth of the B200's HBM) and
 // stays allocated with the scene handle.
 constexpr int64_t kWaveTarget = int64_t(1) << 26;
-// A batch of scenes keeps 4 Mi paths per scene: its concurrent streams already
-// fill one another's tails, and every handle keeps its own path state.
-constexpr int64_t kBatchWaveTarget = int64_t(1) << 22;
-// The cached render updates its cache once per wave; 4 Mi paths set the
-// training cadence its error figures were measured with.
+// The cached render updates its cache once per wave; its default wave is 4 Mi
+// paths (a handle's tuned wave_paths replaces it).
 constexpr int64_t kCacheWaveTarget = int64_t(1) << 22;
 
 // Stage timing (LUZ_RENDER_PROFILE): one event pair per stage launch, summed per wave.
@@ -1101,7 +1156,7 @@ struct StageTimer {
 
 // shade: the shade instantiation to run (NULL: the scene's own).
 void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_t& launches, StageTimer& T,
-                    ShadeKernel shade = nullptr)
+                    ShadeKernel shade, const PathBuf& pb, Ctrl* ctrl)
 {
     auto blocks = [](int tuned, int occ) { return tuned > 0 ? std::min(tuned, occ) : occ; };
     const int g_ext = s->sms * blocks(s->tune.extend_blocks_per_sm, s->occ_ext);
@@ -1113,25 +1168,25 @@ void launch_bounces(luz_gpu_scene* s, const WaveArgs& w, cudaStream_t st, int64_
     const TraceKernel extend = kExtendKernels[count][kv];
     const TraceKernel shadow = kShadowKernels[kv];
     WaveArgs ws = w;
-    const bool sort = s->tune.sort_rays != 0 && s->pb.qsort;
-    if (sort) ws.sorted_queue = s->pb.qsort;
+    const bool sort = s->tune.sort_rays != 0 && pb.qsort;
+    if (sort) ws.sorted_queue = pb.qsort;
     for (int b = 0; b <= w.max_bounces; b++) {
         if (sort && b >= 1) {
-            const uint32_t* q = (b & 1) ? s->pb.queue1 : s->pb.queue0;
-            CK(cudaMemsetAsync(s->pb.sort_hist, 0, sizeof(uint32_t) * kSortBins, st));
-            k_sort_keys<<<s->sms * 8, 256, 0, st>>>(s->ctrl, b, q, s->pb, s->ds.k);
-            k_sort_scan<<<1, 1024, 0, st>>>(s->pb.sort_hist);
-            k_sort_scatter<<<s->sms * 8, 256, 0, st>>>(s->ctrl, b, q, s->pb);
+            const uint32_t* q = (b & 1) ? pb.queue1 : pb.queue0;
+            CK(cudaMemsetAsync(pb.sort_hist, 0, sizeof(uint32_t) * kSortBins, st));
+            k_sort_keys<<<s->sms * 8, 256, 0, st>>>(ctrl, b, q, pb, s->ds.k);
+            k_sort_scan<<<1, 1024, 0, st>>>(pb.sort_hist);
+            k_sort_scatter<<<s->sms * 8, 256, 0, st>>>(ctrl, b, q, pb);
             launches += 3;
         }
         T.mark(st, 0, true);
-        extend<<<g_ext, kBlock, 0, st>>>(s->ds, ws, s->pb, s->ctrl, b);
+        extend<<<g_ext, kBlock, 0, st>>>(s->ds, ws, pb, ctrl, b);
         T.mark(st, 0, false);
         T.mark(st, 1, true);
-        shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, s->pb, s->ctrl, b);
+        shade<<<g_shade, kBlock, 0, st>>>(s->dds, w, pb, ctrl, b);
         T.mark(st, 1, false);
         T.mark(st, 2, true);
-        shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, s->pb, s->ctrl, b);
+        shadow<<<g_sh, kBlock, 0, st>>>(s->ds, w, pb, ctrl, b);
         T.mark(st, 2, false);
         launches += 3;
     }
@@ -1309,6 +1364,8 @@ struct RenderJob {
     int64_t npix = 0, pix_wave = 0;
     int64_t wave_target = kWaveTarget;
     int s_wave = 0;
+    int lanes = 1;                 // 2: waves alternate between two halves of the path state
+    int64_t lane_paths = 0;        // paths per lane
     StageTimer T;
     unsigned long long* counters = nullptr;
     int64_t launches = 0, waves = 0;
@@ -1324,10 +1381,18 @@ void render_prepare(RenderJob& J)
     prepare_caustics(s, p, J.st);
     J.w = base_args(s, p);
     J.npix = (int64_t)p->width * p->height;
-    const int64_t target = s->tune.wave_paths > 0 ? std::min<int64_t>(s->tune.wave_paths, J.wave_target) : J.wave_target;
+    const int64_t target = s->tune.wave_paths > 0 ? s->tune.wave_paths : J.wave_target;   // the budget caps both
     const int64_t n = s->reserve_paths(std::min<int64_t>(target, J.npix * (int64_t)p->spp));
-    J.s_wave = (int)std::min<int64_t>(p->spp, n);
-    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, n / J.s_wave));
+    // Two lanes when the frame takes more than one wave: the path state is split in
+    // halves and consecutive waves run on two streams, so that the last bounces of
+    // one wave (few rays, each launch as long as its slowest warp) overlap the first
+    // bounces of the next. Stage-timed renders keep one lane.
+    J.T.on = (p->flags & LUZ_RENDER_PROFILE) != 0;
+    J.lanes = (!J.T.on && s->tune.lanes != 1 && J.npix * (int64_t)p->spp > n && n >= 2 * kMinLanePaths) ? 2 : 1;
+    J.lane_paths = n / J.lanes;
+    if (J.lanes == 2) s->ensure_lanes();
+    J.s_wave = (int)std::min<int64_t>(p->spp, J.lane_paths);
+    J.pix_wave = std::max<int64_t>(1, std::min<int64_t>(J.npix, J.lane_paths / J.s_wave));
     if (s->film_pix < J.npix) {
         if (s->film) cudaFree(s->film);
         s->film = nullptr;
@@ -1335,7 +1400,6 @@ void render_prepare(RenderJob& J)
         s->film = dalloc<double>((std::size_t)(3 * J.npix));
         s->film_pix = J.npix;
     }
-    J.T.on = (p->flags & LUZ_RENDER_PROFILE) != 0;
     if (p->flags & LUZ_RENDER_COUNT) J.counters = dalloc<unsigned long long>(8);
 }
 
@@ -1353,28 +1417,47 @@ void render_enqueue(RenderJob& J)
     CK(cudaMemsetAsync(s->film, 0, sizeof(double) * 3 * J.npix, st));
     CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
     CK(cudaEventRecord(s->ev0, st));
+    const bool two = J.lanes == 2;
+    const cudaStream_t lane_st[2] = {st, two ? s->stream2 : st};
+    Ctrl* const lane_ctrl[2] = {s->ctrl, two ? s->ctrl2 : s->ctrl};
+    const PathBuf lane_pb[2] = {s->pb, two ? lane_view(s->pb, J.lane_paths) : s->pb};
+    if (two) {   // lane 1 starts after the film, totals and scene copy are set
+        CK(cudaEventRecord(s->lane_setup, st));
+        CK(cudaStreamWaitEvent(s->stream2, s->lane_setup, 0));
+    }
+    int64_t k = 0;
     for (int sb = 0; sb < p->spp; sb += J.s_wave) {
         const int sc = std::min(J.s_wave, p->spp - sb);
         for (int64_t pb = 0; pb < J.npix; pb += J.pix_wave) {
             const int64_t pc = std::min<int64_t>(J.pix_wave, J.npix - pb);
+            const int L = two ? (int)(k & 1) : 0;
+            const cudaStream_t ls = lane_st[L];
             w.pix_begin = (int32_t)pb;
             w.pix_count = (int32_t)pc;
             w.s_begin = sb;
             w.s_count = sc;
             w.n = pc * sc;
             w.list_mode = 0;
-            CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
-            k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, J.launches, J.T);
-            k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, s->film);
-            k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
+            CK(cudaMemsetAsync(lane_ctrl[L], 0, sizeof(Ctrl), ls));
+            k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, ls>>>(w, lane_pb[L], lane_ctrl[L]);
+            launch_bounces(s, w, ls, J.launches, J.T, nullptr, lane_pb[L], lane_ctrl[L]);
+            // the film adds waves in order (samples of a pixel in sample order), the totals one at a time
+            if (two && k > 0) CK(cudaStreamWaitEvent(ls, s->lane_acc[1 - L], 0));
+            k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, ls>>>(w, lane_pb[L], s->film);
+            k_tally<<<1, 1, 0, ls>>>(lane_ctrl[L], w.max_bounces, s->totals);
+            if (two) CK(cudaEventRecord(s->lane_acc[L], ls));
             J.launches += 3;
             J.waves++;
+            k++;
             if (J.T.on) {
                 CK(cudaStreamSynchronize(st));
                 J.T.collect();
             }
         }
+    }
+    if (two) {
+        CK(cudaEventRecord(s->lane_done, s->stream2));
+        CK(cudaStreamWaitEvent(st, s->lane_done, 0));
     }
     k_resolve<<<(unsigned)((J.npix + 255) / 256), 256, 0, st>>>(s->film, J.npix, (double)p->spp, J.d_out);
     J.launches++;
@@ -1599,7 +1682,7 @@ int do_render_ex(luz_gpu_scene* s, const LuzRenderParams* p, const LuzAdaptivePa
                 w.list_mode = 0;
                 CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
                 k_raygen<<<(unsigned)((w.n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
-                launch_bounces(s, w, st, launches, T);
+                launch_bounces(s, w, st, launches, T, nullptr, s->pb, s->ctrl);
                 k_accumulate_px<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, acc, nf);
                 k_tally<<<1, 1, 0, st>>>(s->ctrl, w.max_bounces, s->totals);
                 launches += 3;
@@ -1758,7 +1841,7 @@ int do_adjoint_backward(luz_gpu_scene* s, const LuzRenderParams* p, int32_t text
                 CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
                 if (pass == 1 && rough) CK(cudaMemsetAsync(w.adj_rough, 0, sizeof(AdjRough) * (std::size_t)w.n, st));
                 k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-                launch_bounces(s, w, st, launches, T0, shade_kernel(3));
+                launch_bounces(s, w, st, launches, T0, shade_kernel(3), s->pb, s->ctrl);
                 launches++;
                 if (pass == 0) {
                     k_path_color<<<grid, kBlock, 0, st>>>(w, s->pb);
@@ -1836,7 +1919,7 @@ int do_adjoint_emission(luz_gpu_scene* s, const LuzRenderParams* p, const float*
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(w.pend_light, 0xff, sizeof(int32_t) * (std::size_t)w.n, st));
             k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, launches, T0, shade_kernel(3));
+            launch_bounces(s, w, st, launches, T0, shade_kernel(3), s->pb, s->ctrl);
             k_adjoint_emission_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
             launches += 2;
             waves++;
@@ -1918,7 +2001,7 @@ int do_adjoint_density(luz_gpu_scene* s, const LuzRenderParams* p, int32_t objec
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(w.dens_score, 0, sizeof(float2) * (std::size_t)w.n, st));
             k_raygen<<<grid, kBlock, 0, st>>>(w, s->pb, s->ctrl);
-            launch_bounces(s, w, st, launches, T0, shade_kernel(3));
+            launch_bounces(s, w, st, launches, T0, shade_kernel(3), s->pb, s->ctrl);
             k_adjoint_density_finish<<<grid, kBlock, 0, st>>>(s->ds, w, s->pb);
             launches += 2;
             waves++;
@@ -2676,7 +2759,7 @@ int luz_gpu_scene_set_path_budget(luz_gpu_scene* s, int64_t bytes)
 static void check_tune(const LuzTuneParams& t)
 {
     if (t.wave_paths < 0 || t.staged_top_nodes < 0 || t.staged_top_nodes > 1 || t.sort_rays < 0 || t.sort_rays > 1
-        || t.extend_blocks_per_sm < 0
+        || t.lanes < 0 || t.lanes > 1 || t.extend_blocks_per_sm < 0
         || t.shadow_blocks_per_sm < 0 || t.shade_blocks_per_sm < 0)
         throw Status(LUZ_E_INVALID, "Tuning parameters out of range.");
 }
@@ -2743,6 +2826,11 @@ int luz_gpu_autotune(luz_gpu_scene* s, const LuzRenderParams* p, LuzTuneParams* 
             {
                 LuzTuneParams t = best;
                 t.sort_rays = best.sort_rays ? 0 : 1;
+                consider(t);
+            }
+            {
+                LuzTuneParams t = best;
+                t.lanes = best.lanes ? 0 : 1;
                 consider(t);
             }
             for (int64_t wave : {int64_t(1) << 22, int64_t(1) << 24, int64_t(0)}) {
@@ -2972,7 +3060,7 @@ int luz_gpu_trace_paths(luz_gpu_scene* s, const LuzRenderParams* p, const int32_
                 CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
                 k_raygen<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(w, s->pb, s->ctrl);
                 StageTimer T;
-                launch_bounces(s, w, st, launches, T);
+                launch_bounces(s, w, st, launches, T, nullptr, s->pb, s->ctrl);
                 k_path_color<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(w, s->pb);
                 CK(cudaMemcpyAsync(host.data(), s->pb.color, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
                 finish_wave(s, st, nullptr, w.max_bounces);
@@ -3131,7 +3219,8 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     clear_error(s, st);
     const int64_t npix = (int64_t)p->width * p->height;
     // waves as the plain render makes them (samples inner), one cache update per wave
-    const int64_t n_cap = s->reserve_paths(std::min<int64_t>(kCacheWaveTarget, npix * (int64_t)p->spp));
+    const int64_t target = s->tune.wave_paths > 0 ? s->tune.wave_paths : kCacheWaveTarget;
+    const int64_t n_cap = s->reserve_paths(std::min<int64_t>(target, npix * (int64_t)p->spp));
     const int s_wave = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, n_cap / npix));
     const int64_t pix_wave = std::max<int64_t>(1, std::min<int64_t>(npix, n_cap / s_wave));
     const int64_t n_wave = pix_wave * s_wave;

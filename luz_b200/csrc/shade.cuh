@@ -14,6 +14,14 @@
 //                                   MeshInstance.cpp:393-547, DirectionalLight.cpp:68-91
 //   EnvironmentMap sample/pdf/lookup src/core/EnvironmentMap.cpp:457-623 (index math in FP64)
 #pragma once
+// Out of line by default (small code for the trace and adjoint kernels); the shade
+// kernels' translation unit defines these as __forceinline__.
+#ifndef LUZ_HIT_ATTR
+#define LUZ_HIT_ATTR __noinline__
+#endif
+#ifndef LUZ_LIGHT_ATTR
+#define LUZ_LIGHT_ATTR __noinline__
+#endif
 #include "trace.cuh"
 
 namespace luz {
@@ -116,7 +124,7 @@ __device__ __forceinline__ F3 transform_normal(const GObject& O, F3 n)
 // alone enlarges this out-of-line function's frame and slowed the shade stage
 // by 3.5% on scenes without such spheres).
 template <bool XUV>
-static __device__ __noinline__ Hit make_hit_t(const DScene& S, const TRay& r, const THit& th)
+static __device__ LUZ_HIT_ATTR Hit make_hit_t(const DScene& S, const TRay& r, const THit& th)
 {
     Hit h;
     const GObject O = S.objects[th.obj];
@@ -1007,7 +1015,7 @@ __device__ __forceinline__ void env_dir_to_uv(const GEnv& E, F3 dir, double& u, 
     u = wrap01d(0.5 + (phi / (2.0 * kPiD)) + (E.rotation / 360.0));
     v = clamp01d(0.5 + (asin(y) / kPiD));
 }
-static __device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, double v)
+static __device__ LUZ_LIGHT_ATTR F3 env_lookup_uv(const DScene& S, double u, double v)
 {
     const GEnv& E = S.k.env;
     u = wrap01d(u);
@@ -1034,7 +1042,7 @@ static __device__ __noinline__ F3 env_lookup_uv(const DScene& S, double u, doubl
     return F3{isfinite(c.x) ? fmaxf(0.f, c.x) : 0.f, isfinite(c.y) ? fmaxf(0.f, c.y) : 0.f,
               isfinite(c.z) ? fmaxf(0.f, c.z) : 0.f};
 }
-static __device__ __noinline__ F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
+static __device__ LUZ_LIGHT_ATTR F3 env_radiance(const DScene& S, F3 dir)   // sampleDirection
 {
     double u, v;
     env_dir_to_uv(S.k.env, dir, u, v);
@@ -1050,14 +1058,14 @@ __device__ __forceinline__ float env_pdf_uv(const DScene& S, double u, double v)
 }
 // EnvironmentMap::sampleDirection and ::pdf of one direction: both start from the same
 // directionToUV(direction), so it is evaluated once.
-static __device__ __noinline__ void env_query(const DScene& S, F3 dir, bool want_rad, bool want_pdf, F3& rad, float& pdf)
+static __device__ LUZ_LIGHT_ATTR void env_query(const DScene& S, F3 dir, bool want_rad, bool want_pdf, F3& rad, float& pdf)
 {
     double u, v;
     env_dir_to_uv(S.k.env, dir, u, v);
     if (want_rad) rad = env_lookup_uv(S, u, v);
     if (want_pdf) pdf = env_pdf_uv(S, u, v);
 }
-static __device__ __noinline__ float env_pdf(const DScene& S, F3 dir)
+static __device__ LUZ_LIGHT_ATTR float env_pdf(const DScene& S, F3 dir)
 {
     const GEnv& E = S.k.env;
     if (E.total_weight <= 0.0 || E.pdf_offset < 0) return 1.0f / (4.0f * kPiF);
@@ -1150,7 +1158,7 @@ __device__ __forceinline__ double clamp_sample(double v)
     return v;
 }
 // EnvironmentMap::sample (EnvironmentMap.cpp:468-513)
-static __device__ __noinline__ bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
+static __device__ LUZ_LIGHT_ATTR bool env_sample(const DScene& S, const Key& k, F3& dir, F3& radiance, float& pdf)
 {
     const GEnv& E = S.k.env;
     const double sel0 = sample1d(k, DIM_ENVIRONMENT_SELECTION);
@@ -1447,7 +1455,7 @@ __device__ __forceinline__ float light_select_prob(const DScene& S, int32_t i)
     return (float)(w / S.k.light_total_weight);
 }
 // lightPDFValue (ColorHelper.cpp:233-257)
-static __device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 dir)
+static __device__ LUZ_LIGHT_ATTR float lights_pdf(const DScene& S, F3 origin, F3 dir)
 {
     const int32_t n = S.k.light_count;
     if (n <= 0) return 0.0f;
@@ -1457,7 +1465,7 @@ static __device__ __noinline__ float lights_pdf(const DScene& S, F3 origin, F3 d
     return sum;
 }
 // selectLightIndex + sampleLight (ColorHelper.cpp:190-231, 925-971)
-static __device__ __noinline__ bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
+static __device__ LUZ_LIGHT_ATTR bool sample_light(const DScene& S, F3 origin, const Key& k, LightSample& ls)
 {
     ls.valid = false;
     const int32_t n = S.k.light_count;

@@ -9,100 +9,18 @@
 // lattice arithmetic (dmath.cuh) is written with explicit round-to-nearest
 // intrinsics, so it stays bit-exact with the reference in either unit.
 #define LUZ_NO_CACHE_KERNELS
-#include "wavefront.cuh"
+// Inlined here, out of line elsewhere: the sampler, the environment and light
+// sampling / pdf functions and the hit record. With the paths binned by material
+// class the shade kernel's instruction footprint no longer stalls it, and these
+// calls' argument traffic through local memory cost more (1080p glossy frame, 16
+// spp: shade stage 29.5 -> 25.8 ms). Inlining the BSDF functions as well made it
+// slower (37.7 ms: 128 registers could no longer hold the larger body).
+#define LUZ_SAMPLER_ATTR __forceinline__
+#define LUZ_LIGHT_ATTR __forceinline__
+#define LUZ_HIT_ATTR __forceinline__
+#include "shade_kernels.cuh"
 
 namespace luz {
-
-// Resident blocks per SM the register allocator is asked to allow: 4 measured
-// ahead of 3 and 5 on the 1080p glossy frame.
-#ifndef LUZ_SHADE_MIN_BLOCKS
-#define LUZ_SHADE_MIN_BLOCKS 4
-#endif
-
-// Path of shade slot i: slots run through the class segments in class order.
-__device__ __forceinline__ uint32_t binned_path(const PathBuf& P, const uint32_t* bin, uint32_t i)
-{
-    uint32_t k = 0, start = 0;
-    while (k < kShadeClasses - 1 && i >= start + bin[k]) {
-        start += bin[k];
-        k++;
-    }
-    return P.bins[k * P.bin_stride + (i - start)];
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade(const DScene* __restrict__ Sp, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
-{
-    const DScene& S = *Sp;
-    const uint32_t count = C->count[bounce];
-    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
-    uint32_t* nq = (bounce & 1) ? P.queue0 : P.queue1;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    for (uint32_t base = wid * 32u; base < count; base += warps * 32u) {
-        const uint32_t i = base + lane_id();
-        const bool valid = i < count;
-        ShadeOut o;
-        o.cont = false;
-        o.sh[0] = o.sh[1] = false;
-        uint32_t p = 0;
-        if (valid) {
-            p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
-            shade_path<MODE>(S, w, P, p, bounce, o);
-        }
-        __syncwarp();
-        const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
-        if (o.cont) nq[qi] = p;
-        for (int slot = 0; slot < 2; slot++) {
-            const uint32_t si = warp_append(&C->shadow[bounce], o.sh[slot]);
-            if (o.sh[slot]) {
-                P.sh_o[si] = make_float4(o.sh_o[slot].x, o.sh_o[slot].y, o.sh_o[slot].z, o.sh_t[slot]);
-                P.sh_d[si] = make_float4(o.sh_d[slot].x, o.sh_d[slot].y, o.sh_d[slot].z,
-                                         __uint_as_float(p | ((uint32_t)slot << 31)));
-                P.sh_x[si] = make_int2(o.xobj, o.xprim);
-            }
-        }
-    }
-}
-
-
-// k_shade over a multi-scene wave: the scene and wave arguments are the path's segment's.
-template <int MODE>
-__global__ void __launch_bounds__(kBlock, LUZ_SHADE_MIN_BLOCKS) k_shade_batch(const DScene* __restrict__ scenes,
-                                                                             const WaveArgs* __restrict__ segs,
-                                                                             PathBuf P, Ctrl* C, int bounce)
-{
-    const uint32_t count = C->count[bounce];
-    const uint32_t* q = (bounce & 1) ? P.queue1 : P.queue0;
-    uint32_t* nq = (bounce & 1) ? P.queue0 : P.queue1;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    for (uint32_t base = wid * 32u; base < count; base += warps * 32u) {
-        const uint32_t i = base + lane_id();
-        const bool valid = i < count;
-        ShadeOut o;
-        o.cont = false;
-        o.sh[0] = o.sh[1] = false;
-        uint32_t p = 0;
-        if (valid) {
-            p = P.bins ? binned_path(P, C->bin[bounce], i) : q[i];
-            const WaveArgs& w = segs[P.seg[p]];
-            shade_path<MODE>(scenes[w.batch_scene], w, P, p, bounce, o);
-        }
-        __syncwarp();
-        const uint32_t qi = warp_append(&C->count[bounce + 1], o.cont);
-        if (o.cont) nq[qi] = p;
-        for (int slot = 0; slot < 2; slot++) {
-            const uint32_t si = warp_append(&C->shadow[bounce], o.sh[slot]);
-            if (o.sh[slot]) {
-                P.sh_o[si] = make_float4(o.sh_o[slot].x, o.sh_o[slot].y, o.sh_o[slot].z, o.sh_t[slot]);
-                P.sh_d[si] = make_float4(o.sh_d[slot].x, o.sh_d[slot].y, o.sh_d[slot].z,
-                                         __uint_as_float(p | ((uint32_t)slot << 31)));
-                P.sh_x[si] = make_int2(o.xobj, o.xprim);
-            }
-        }
-    }
-}
 
 BatchShadeKernel batch_shade_kernel(int mode)
 {
@@ -113,7 +31,7 @@ ShadeKernel shade_kernel(int mode)
 {
     switch (mode) {
     case 1: return k_shade<1>;
-    case 2: return k_shade<2>;
+    case 2: return shade_kernel_cached();
     case 3: return k_shade<3>;
     default: return k_shade<0>;
     }

@@ -862,6 +862,7 @@ __device__ __forceinline__ F3 clean(F3 c)   // cleanColor (Threads.cpp:122-137)
 // caustic estimate, 2 radiance-cache render, 3 adjoint replay.
 using ShadeKernel = void (*)(const DScene*, WaveArgs, PathBuf, Ctrl*, int);
 ShadeKernel shade_kernel(int mode);
+ShadeKernel shade_kernel_cached();   // k_shade<2>, in its own translation unit
 
 // Multi-scene waves: every path finds its segment in P.seg, the segment's WaveArgs
 // in segs and its scene in scenes[segs[seg].batch_scene]. Modes 0 and 1 as above.

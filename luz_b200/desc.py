@@ -144,7 +144,7 @@ class TuneParams(C.Structure):
     """LuzTuneParams: launch tuning of a scene handle (zeros = defaults)."""
     _fields_ = [("wave_paths", C.c_int64), ("staged_top_nodes", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
                 ("shadow_blocks_per_sm", C.c_int32), ("shade_blocks_per_sm", C.c_int32), ("sort_rays", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("lanes", C.c_int32)]
 
 
 class TuneTrial(C.Structure):

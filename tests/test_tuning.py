@@ -1,7 +1,7 @@
 """Launch tuning and the autotuner (luz_gpu_scene_set_tuning, luz_gpu_autotune): no
 tuning choice changes a film. Staged top BVH nodes (shared memory), the coherence sort
-of the extension queue, wave sizes and persistent grid sizes give the same image bit
-for bit; the autotuner leaves its choice on the handle and reports its timed trials."""
+of the extension queue, wave sizes, one or two wave lanes and persistent grid sizes give
+the same image bit for bit; the autotuner leaves its choice on the handle and reports its timed trials."""
 import numpy as np
 import pytest
 
@@ -28,6 +28,31 @@ def test_tuning_choices_leave_the_film_unchanged(name):
         g.set_tuning()
         with pytest.raises(native.LuzError):
             g.set_tuning(staged_top_nodes=2)
+        with pytest.raises(native.LuzError):
+            g.set_tuning(lanes=2)
+    finally:
+        g.close()
+
+
+def test_two_wave_lanes_equal_one():
+    """A frame of several waves on two lanes (consecutive waves on two streams over the two
+    halves of the path state) gives the one-lane film and ray totals bit for bit; 8 Mi paths
+    of path state make two lanes of 4 Mi, four waves for this 16.8 M-path frame."""
+    from luz_b200 import scenes
+    w = scenes.mesh_glossy(256, 256, 256, 8, level=5)
+    g = native.GpuScene(w.scene.build())
+    try:
+        p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed)
+        g.set_tuning(wave_paths=1 << 23)
+        two, s2 = g.render(p)
+        g.set_tuning(wave_paths=1 << 23, lanes=1)
+        one, s1 = g.render(p)
+        g.set_tuning()
+        ref, s0 = g.render(p)
+        assert s2.waves == 4 and s1.waves == 2 and s0.waves == 1, (s2.waves, s1.waves, s0.waves)
+        assert np.array_equal(two, one) and np.array_equal(two, ref)
+        assert s2.extension_rays == s1.extension_rays == s0.extension_rays
+        assert s2.shadow_rays == s1.shadow_rays == s0.shadow_rays
     finally:
         g.close()
 
