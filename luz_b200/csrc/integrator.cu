@@ -68,6 +68,12 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 #ifndef LUZ_SHADOW_MIN_BLOCKS
 #define LUZ_SHADOW_MIN_BLOCKS 8
 #endif
+// The instantiations for scenes with instances (instance transform, two nested walks):
+// 4 blocks (128 registers, a few hundred bytes of spills instead of 1-2 KB at 96) took
+// the 1e5-instance frame's extend stage from 85.1 to 71.8 ms at 4 spp (6 blocks: 85.8).
+#ifndef LUZ_EXTEND_MIN_BLOCKS_INST
+#define LUZ_EXTEND_MIN_BLOCKS_INST 4
+#endif
 
 // Appends path p to the segment of its shade class; the lanes of vmask with the
 // same class share one atomic (match.any).
@@ -89,7 +95,8 @@ __device__ __forceinline__ void bin_append(uint32_t* bin_count, const PathBuf& P
 // COUNT instantiations add the record counts of LUZ_RENDER_COUNT; the others
 // carry no counting code (the shadow kernel counts under a runtime branch).
 template <uint32_t F, bool COUNT>
-__global__ void __launch_bounds__(kBlock, LUZ_EXTEND_MIN_BLOCKS) k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
+__global__ void __launch_bounds__(kBlock, (F & TF_INSTANCE) ? LUZ_EXTEND_MIN_BLOCKS_INST : LUZ_EXTEND_MIN_BLOCKS)
+    k_extend(DScene S, WaveArgs w, PathBuf P, Ctrl* C, int bounce)
 {
     if constexpr ((F & TF_STAGED) != 0) stage_top_nodes(S);
     LocalStack<true> st;

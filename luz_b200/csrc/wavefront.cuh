@@ -632,8 +632,16 @@ static __device__ void shade_path(const DScene& S, const WaveArgs& w, const Path
     {
         THit th{h4.x, obj, P.hit_prim[p], h4.y, h4.z};
         Hit h = make_hit(S, ray, th);
-        GMaterial m = S.materials[h.material];
-        resolve_material(S, m, h);
+        // The material is read where it lies (L1-cached global memory); only a Metal whose
+        // roughness comes from a texture gets a resolved copy.
+        const GMaterial* mp = S.materials + h.material;
+        GMaterial m_res;
+        if (mp->rtexture >= 0) {
+            m_res = *mp;
+            resolve_material(S, m_res, h);
+            mp = &m_res;
+        }
+        const GMaterial& m = *mp;
         if (bounce == 0 && w.nfor) store_hit_features(S, P, p, h, m);
         if (bounce == 0 && S.k.sky == 2) {   // compositePrimaryAtmosphereSegment (ColorHelper.cpp:645-659)
             double ao[3], ad[3];
