@@ -347,6 +347,7 @@ def run_ours(args):
                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
                "config": config_of(w, world),
+               "step_ms": [round(x, 2) for x in times],
                "e2e": {"value": samples_all / e2 / 1e3, "unit": UNIT, "h2d_bytes_per_step": 32,
                        "d2h_bytes_per_step": npix * 3 * 4, "ms_per_step": [round(x, 2) for x in e2e_ms],
                        "host_film": "pinned"},
