@@ -601,7 +601,7 @@ int luz_gpu_render_denoised(luz_gpu_scene* scene, const LuzRenderParams* params,
  * does not scatter specularly: the vertex's own emission and next-event
  * estimate stay explicit, and the cache's prediction times the path throughput
  * stands for the continuation (a biased estimate: the plain luz_gpu_render
- * stays the unbiased judge of it). One path in `train_every` instead continues
+ * stays the unbiased reference for it). One path in `train_every` instead continues
  * unbiased and supplies a training row: its inputs at that vertex and the
  * radiance its continuation gathered divided by its throughput there. Samples
  * run in waves as in luz_gpu_render; after each wave the cache takes one Adam

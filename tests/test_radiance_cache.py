@@ -151,7 +151,7 @@ def test_cached_render_against_plain():
     """Cornell 64 x 64, depth 8: after a training render, the cache's image at 32 spp is
     closer to the converged plain image (4096 spp) than the plain 32-spp image, it
     traces fewer rays, and its mean stays within 5% (the cache is biased; the plain
-    renderer is the judge)."""
+    renderer is the reference)."""
     from luz_b200 import scenes
     w = scenes.cornell(64, 64, 1, 8)
     g = native.GpuScene(w.scene.build())
