@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--cache-min-rough", type=float, default=None,
                     help="cache workloads: LuzCacheParams.min_roughness (default per workload)")
     ap.add_argument("--cache-batch", type=int, default=16384, help="cache workloads: training rows per step")
-    ap.add_argument("--cache-train-every", type=int, default=16, help="cache workloads: one training path in this many")
+    ap.add_argument("--cache-train-every", type=int, default=32, help="cache workloads: one training path in this many")
     ap.add_argument("--cache-wave", type=int, default=0,
                     help="cache workloads: paths per wave of the cached render (0: its default, 4 Mi)")
     return ap.parse_args()
@@ -624,7 +624,8 @@ def run_cache(args):
                       "error": "relative MSE mean((x - ref)^2 / (ref^2 + 0.01))"
                                + (", 1% largest pixels dropped" if sub is not None else ""), "reference": ref_kind,
                       "target": f"error of the plain {targets[-1]}-spp image",
-                      "cache": f"prefix 1, NEE explicit at the cache vertex, one training path in {args.cache_train_every}, "
+                      "cache": f"prefix 1, NEE explicit at the cache vertex, one training path in {args.cache_train_every} "
+                               "(self-training: it ends in the cache at its next eligible vertex), "
                                f"batch {args.cache_batch} (up to 16 steps per wave), lr 1e-2, first sample plain with 32 "
                                f"warm-up steps, min roughness {min_rough:g}, "
                                f"waves of {args.cache_wave or 4194304} paths"},

@@ -602,8 +602,11 @@ int luz_gpu_render_denoised(luz_gpu_scene* scene, const LuzRenderParams* params,
  * estimate stay explicit, and the cache's prediction times the path throughput
  * stands for the continuation (a biased estimate: the plain luz_gpu_render
  * stays the unbiased reference for it). One path in `train_every` instead continues
- * unbiased and supplies a training row: its inputs at that vertex and the
- * radiance its continuation gathered divided by its throughput there. Samples
+ * past that vertex and supplies a training row: its inputs at that vertex and the
+ * radiance its continuation gathered divided by its throughput there, where the
+ * continuation itself ends in the cache at its next such vertex (self-training:
+ * short training paths, low-variance targets; the first sample's training paths run
+ * to their end). Samples
  * run in waves as in luz_gpu_render; after each wave the cache takes one Adam
  * step per `batch` of that wave's rows (at most 16). Training rows are appended
  * in arrival order, so cached renders are not bit-reproducible. The cache
@@ -616,7 +619,7 @@ typedef struct LuzCacheParams {
     int32_t  batch;               /* training rows per step (16384); > 0                     */
     float    learning_rate;       /* Adam step size (1e-2); beta1 0.9, beta2 0.99, eps 1e-8 */
     int32_t  prefix;              /* first bounce whose vertex queries the cache (1); >= 0   */
-    int32_t  train_every;         /* one training path in this many (16); >= 1               */
+    int32_t  train_every;         /* one training path in this many (32); >= 1               */
     float    min_roughness;       /* in [0, 1]: a surface vertex whose roughness is below this
                                      continues the path and a later vertex queries the cache
                                      (0: the first vertex at or after `prefix` always does);

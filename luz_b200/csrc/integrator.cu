@@ -3279,6 +3279,8 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
             w.list_mode = 0;
             w.cache_wave = (uint32_t)waves;
             w.cache_train_every = warm ? 1u : (uint32_t)c->prm.train_every;
+            // after the warm-up wave, training paths end at their next eligible vertex in the cache
+            w.cache_self_train = warm ? 0u : 1u;
             CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), st));
             CK(cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), st));
             CK(cudaMemsetAsync(tflag, 0, (std::size_t)w.n, st));

@@ -103,6 +103,7 @@ struct WaveArgs {
     uint32_t* cache_count;        // [0] queries
     float cache_lo[3], cache_inv[3];   // position input = (p - lo) * inv
     float cache_min_rough;        // vertices rougher than this (cache_roughness) query the cache
+    uint32_t cache_self_train;    // 1: a training path queries the cache at its next eligible vertex
     const uint32_t* sorted_queue;   // extension queue in coherence order for bounces >= 1 (NULL: as shaded)
     // multi-scene waves (luz_gpu_batch_render): one WaveArgs per segment of a wave, the
     // segment's scene and the first wave slot it covers
@@ -693,10 +694,14 @@ static __device__ void shade_path(const DScene& S, const WaveArgs& w, const Path
         // Radiance cache: at the path's first surface vertex at or after the prefix
         // bounce, the vertex's own light (emission here, NEE below) stays explicit and
         // the cache answers for the continuation; one path in cache_train_every runs
-        // on and records what the continuation gathered.
+        // on and records what the continuation gathered, itself ended in the cache at
+        // the path's next eligible vertex (after the first wave).
         bool cache_query = false;
         if constexpr (MODE == 2) {
-            if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE) &&
+            if (bounce >= w.cache_prefix && !h.volume && (flags & PF_CACHE_DONE) && w.cache_self_train &&
+                w.cache_flag[p] == 1 && cache_roughness(m) >= w.cache_min_rough) {
+                cache_query = true;   // a training path's next eligible vertex: its target ends in the cache
+            } else if (bounce >= w.cache_prefix && !h.volume && !(flags & PF_CACHE_DONE) &&
                 cache_roughness(m) >= w.cache_min_rough) {
                 const uint64_t key = ((uint64_t)pix << 24) ^ (uint64_t)P.sample[p] ^ ((uint64_t)w.cache_wave << 48);
                 if (splitmix64(key) % w.cache_train_every == 0) {

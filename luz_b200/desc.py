@@ -192,7 +192,7 @@ class CacheParams(C.Structure):
                 ("train_every", C.c_int32), ("min_roughness", C.c_float)]
 
 
-def cache_params(seed=1, batch=16384, learning_rate=1e-2, prefix=1, train_every=16,
+def cache_params(seed=1, batch=16384, learning_rate=1e-2, prefix=1, train_every=32,
                  min_roughness=0.0) -> CacheParams:
     return CacheParams(seed, batch, learning_rate, prefix, train_every, min_roughness)
 

@@ -166,7 +166,7 @@ def test_cached_render_against_plain():
                  rmse=(rmse(cached, ref), rmse(plain, ref)))
     assert np.isfinite(cached).all()
     assert sc.samples == sp.samples
-    # one path in 4 trains and runs to full depth; the rest stop at their second surface vertex
+    # one path in 4 trains and runs on to its next surface vertex; the rest stop at their second
     assert sc.extension_rays < 0.8 * sp.extension_rays, facts
     assert abs(cached.mean() - ref.mean()) < 0.05 * ref.mean(), facts
     assert rmse(cached, ref) < rmse(plain, ref), facts
