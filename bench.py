@@ -243,6 +243,16 @@ def run_ours(args):
     p = native.params(w.width, w.height, w.spp, w.max_bounces, w.seed, 0, rank * w.spp)
     from luz_b200.shard import render_sharded
 
+    reduce_ev = []
+
+    def all_reduce(t):   # the film exchange, timed with events on the launching stream
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        dist.all_reduce(t)
+        a1.record(stream)
+        reduce_ev.append((a0, a1))
+
     def step():
         if dist is None:
             return g.render_device(p, film.data_ptr(), stream.cuda_stream)
@@ -252,20 +262,26 @@ def run_ours(args):
             pr = native.params(w.width, w.height, count, w.max_bounces, w.seed, 0, offset)
             out["st"] = g.render_device(pr, film.data_ptr(), stream.cuda_stream)
             return film
-        render_sharded(render_mean, w.spp * world, rank, world, lambda t: dist.all_reduce(t))
+        render_sharded(render_mean, w.spp * world, rank, world, all_reduce)
         return out["st"]
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
-    times, launches = [], 0
+    # A step's device time is the render's own CUDA events on the launching stream (recorded
+    # before its first and after its last GPU operation: LuzRenderStats.render_ms) plus the
+    # film all-reduce's events under torchrun (the two elementwise scalings of the 25 MB film
+    # around it are left out). The events around the whole call (outer) also
+    # hold the host's set-up before the first launch and its return after the last.
+    times, outer, launches = [], [], 0
     clocks.start()
     for _ in range(args.steps):
         flush.zero_()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+        reduce_ev.clear()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -273,7 +289,8 @@ def run_ours(args):
         e1.record(stream)
         torch.cuda.synchronize()
         launches += st.kernel_launches
-        times.append(e0.elapsed_time(e1))
+        outer.append(e0.elapsed_time(e1))
+        times.append(st.render_ms + sum(a0.elapsed_time(a1) for a0, a1 in reduce_ev))
     clk = clocks.stop()
     ms = float(np.mean(times))
     if dist is not None:
@@ -348,6 +365,7 @@ def run_ours(args):
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
                "config": config_of(w, world),
                "step_ms": [round(x, 2) for x in times],
+               "step_ms_outer": [round(x, 2) for x in outer],
                "e2e": {"value": samples_all / e2 / 1e3, "unit": UNIT, "h2d_bytes_per_step": 32,
                        "d2h_bytes_per_step": npix * 3 * 4, "ms_per_step": [round(x, 2) for x in e2e_ms],
                        "host_film": "pinned"},

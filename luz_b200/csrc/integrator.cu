@@ -1022,6 +1022,10 @@ struct luz_gpu_scene {
     int64_t reserve_paths(int64_t want, bool feat = false)
     {
         want = std::max<int64_t>(1, want);
+        // buffers already held serve without asking the driver for its free memory
+        // (cudaMemGetInfo costs host time on every render otherwise)
+        if (want <= cap && (!feat || pb.feat) && (path_budget < 0 || want * (kPathBytes + (feat ? kFeatBytes : 0)) <= path_budget))
+            return want;
         const int64_t per = kPathBytes + (feat ? kFeatBytes : 0);
         int64_t budget = path_budget;
         if (budget < 0) {
@@ -1417,13 +1421,13 @@ void render_enqueue(RenderJob& J)
     const cudaStream_t st = J.st;
     WaveArgs& w = J.w;
     CK(cudaSetDevice(s->device));
+    CK(cudaEventRecord(s->ev0, st));   // render_ms spans all of the render's work on the stream
     clear_error(s, st);
     if (J.counters) CK(cudaMemsetAsync(J.counters, 0, 8 * sizeof(unsigned long long), st));
     s->ds.counters = J.counters;
     CK(cudaMemcpyAsync(s->dds, &s->ds, sizeof(DScene), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(s->film, 0, sizeof(double) * 3 * J.npix, st));
     CK(cudaMemsetAsync(s->totals, 0, 2 * sizeof(unsigned long long), st));
-    CK(cudaEventRecord(s->ev0, st));
     const bool two = J.lanes == 2;
     const cudaStream_t lane_st[2] = {st, two ? s->stream2 : st};
     Ctrl* const lane_ctrl[2] = {s->ctrl, two ? s->ctrl2 : s->ctrl};
