@@ -14,6 +14,7 @@
 //   scene: Scene::updateAccelerationStructure (src/scene/Scene.cpp:655-688) and
 //          Scene::updateLights (src/scene/Scene.cpp:615-638).
 // The results are then rounded outward to FP32 (boxes) or to nearest (vertices).
+#include <thread>
 #include "pack.h"
 
 #include <algorithm>
@@ -310,7 +311,7 @@ struct Bin {
 struct MeshBuilder {
     const std::vector<Box64>& boxes;
     const std::vector<V3>& cent;
-    std::vector<std::size_t> idx;
+    std::vector<std::size_t>& idx;   // triangle order, partitioned in place (shared by sub-builders)
     std::vector<LuzMeshNode64>& out;
     int max_depth = 0;
 
@@ -426,6 +427,67 @@ struct MeshBuilder {
         out[node].right = (int64_t)r;
         return node;
     }
+
+    // The same build, with the two subtrees of the top `par` levels built on two
+    // threads: each subtree goes to a vector of its own (node numbers from 0) and is
+    // appended after its parent in build's order (the node, its left subtree, its right
+    // subtree), its child numbers shifted by where it lands. Subtrees own disjoint
+    // ranges of idx. The nodes, their numbers and the triangle order are build's.
+    std::size_t build_parallel(std::size_t s, std::size_t e, int depth, int par)
+    {
+        const std::size_t n = e - s;
+        if (par <= 0 || n < (std::size_t(1) << 15)) return build(s, e, depth);
+        max_depth = std::max(max_depth, depth);
+        const std::size_t node = out.size();
+        Box64 nb{};
+        bool has = false;
+        for (std::size_t i = s; i < e; i++) {
+            nb = has ? merge(nb, boxes[idx[i]]) : boxes[idx[i]];
+            has = true;
+        }
+        out.push_back(LuzMeshNode64{});
+        for (int a = 0; a < 3; a++) {
+            out[node].bmin[a] = nb.mn[a];
+            out[node].bmax[a] = nb.mx[a];
+        }
+        const Split sp = find_split(s, e);
+        std::size_t mid = s;
+        if (sp.found) {
+            auto it = std::partition(idx.begin() + s, idx.begin() + e, [&](std::size_t t) {
+                return bin_for(cent[t][sp.axis], sp.cmin, sp.scale) <= sp.split;
+            });
+            mid = static_cast<std::size_t>(it - idx.begin());
+        }
+        if (mid == s || mid == e) {
+            const int axis = largest_axis(nb);
+            mid = s + n / 2;
+            std::nth_element(idx.begin() + s, idx.begin() + mid, idx.begin() + e, [&](std::size_t a, std::size_t b) {
+                const double ca = cent[a][axis], cb = cent[b][axis];
+                if (ca == cb) return boxes[a].mn[axis] < boxes[b].mn[axis];
+                return ca < cb;
+            });
+        }
+        std::vector<LuzMeshNode64> lo, hi;
+        MeshBuilder L{boxes, cent, idx, lo, 0}, R{boxes, cent, idx, hi, 0};
+        std::thread t([&] { L.build_parallel(s, mid, depth + 1, par - 1); });
+        R.build_parallel(mid, e, depth + 1, par - 1);
+        t.join();
+        max_depth = std::max(max_depth, std::max(L.max_depth, R.max_depth));
+        auto append = [&](const std::vector<LuzMeshNode64>& sub) {
+            const int64_t base = (int64_t)out.size();
+            for (LuzMeshNode64 nd : sub) {
+                if (!nd.is_leaf) {
+                    nd.left += base;
+                    nd.right += base;
+                }
+                out.push_back(nd);
+            }
+            return base;
+        };
+        out[node].left = append(lo);
+        out[node].right = append(hi);
+        return node;
+    }
 };
 
 void build_mesh(const LuzMeshDesc& m, MeshBuild& mb)
@@ -488,13 +550,13 @@ void build_mesh(const LuzMeshDesc& m, MeshBuild& mb)
         cent[k] = (mn + mx) / 2.0;
         k++;
     }
-    MeshBuilder b{boxes, cent, {}, mb.nodes, 0};
-    b.idx.resize(n);
-    std::iota(b.idx.begin(), b.idx.end(), std::size_t(0));
+    std::vector<std::size_t> idx(n);
+    std::iota(idx.begin(), idx.end(), std::size_t(0));
+    MeshBuilder b{boxes, cent, idx, mb.nodes, 0};
     mb.nodes.reserve(2 * n);
-    b.build(0, n, 0);
+    b.build_parallel(0, n, 0, 3);   // up to 8 subtrees built at once
     mb.depth = b.max_depth;
-    mb.order.assign(b.idx.begin(), b.idx.end());
+    mb.order.assign(idx.begin(), idx.end());
     for (int a = 0; a < 3; a++) {
         mb.box.mn[a] = mb.nodes[0].bmin[a];
         mb.box.mx[a] = mb.nodes[0].bmax[a];
