@@ -322,63 +322,89 @@ struct MeshBuilder {
         double cmin = 0, scale = 0;
     };
 
-    Split find_split(std::size_t s, std::size_t e)
+    // The best split on one axis (cost, bin, range), as the reference's loop over that
+    // axis's bins finds it: strictly lower cost wins, so the first bin of equal cost stays.
+    Split axis_split(std::size_t s, std::size_t e, int axis, double& best_cost) const
     {
         const std::size_t n = e - s;
         const std::size_t min_side = std::max<std::size_t>(1, n / 16);
         Split best;
-        double best_cost = std::numeric_limits<double>::infinity();
-        for (int axis = 0; axis < 3; axis++) {
-            double cmin = std::numeric_limits<double>::infinity();
-            double cmax = -std::numeric_limits<double>::infinity();
-            for (std::size_t i = s; i < e; i++) {
-                const double c = cent[idx[i]][axis];
-                cmin = std::min(cmin, c);
-                cmax = std::max(cmax, c);
-            }
-            const double ext = cmax - cmin;
-            if (ext <= kCentroidEps) continue;
-            const double scale = static_cast<double>(kBins) / ext;
-            std::array<Bin, kBins> bins;
-            for (std::size_t i = s; i < e; i++) {
-                const std::size_t t = idx[i];
-                Bin& b = bins[bin_for(cent[t][axis], cmin, scale)];
-                b.box = b.has ? merge(b.box, boxes[t]) : boxes[t];
-                b.count++;
-                b.has = true;
-            }
-            std::array<Bin, kBins> left, right;
-            Bin rl, rr;
-            auto mergeBin = [](Bin& t, const Bin& src) {
-                if (!src.has) return;
-                t.box = t.has ? merge(t.box, src.box) : src.box;
-                t.count += src.count;
-                t.has = true;
-            };
-            for (std::size_t i = 0; i < kBins; i++) {
-                mergeBin(rl, bins[i]);
-                left[i] = rl;
-            }
-            for (std::size_t i = kBins; i > 0; i--) {
-                mergeBin(rr, bins[i - 1]);
-                right[i - 1] = rr;
-            }
-            for (std::size_t sb = 0; sb + 1 < kBins; sb++) {
-                const Bin& l = left[sb];
-                const Bin& r = right[sb + 1];
-                if (!l.has || !r.has || l.count < min_side || r.count < min_side) continue;
-                const double cost = (box_area(l.box) * static_cast<double>(l.count))
-                                    + (box_area(r.box) * static_cast<double>(r.count));
-                if (cost < best_cost) {
-                    best_cost = cost;
-                    best.found = true;
-                    best.axis = axis;
-                    best.split = sb;
-                    best.cmin = cmin;
-                    best.scale = scale;
-                }
+        best_cost = std::numeric_limits<double>::infinity();
+        double cmin = std::numeric_limits<double>::infinity();
+        double cmax = -std::numeric_limits<double>::infinity();
+        for (std::size_t i = s; i < e; i++) {
+            const double c = cent[idx[i]][axis];
+            cmin = std::min(cmin, c);
+            cmax = std::max(cmax, c);
+        }
+        const double ext = cmax - cmin;
+        if (ext <= kCentroidEps) return best;
+        const double scale = static_cast<double>(kBins) / ext;
+        std::array<Bin, kBins> bins;
+        for (std::size_t i = s; i < e; i++) {
+            const std::size_t t = idx[i];
+            Bin& b = bins[bin_for(cent[t][axis], cmin, scale)];
+            b.box = b.has ? merge(b.box, boxes[t]) : boxes[t];
+            b.count++;
+            b.has = true;
+        }
+        std::array<Bin, kBins> left, right;
+        Bin rl, rr;
+        auto mergeBin = [](Bin& t, const Bin& src) {
+            if (!src.has) return;
+            t.box = t.has ? merge(t.box, src.box) : src.box;
+            t.count += src.count;
+            t.has = true;
+        };
+        for (std::size_t i = 0; i < kBins; i++) {
+            mergeBin(rl, bins[i]);
+            left[i] = rl;
+        }
+        for (std::size_t i = kBins; i > 0; i--) {
+            mergeBin(rr, bins[i - 1]);
+            right[i - 1] = rr;
+        }
+        for (std::size_t sb = 0; sb + 1 < kBins; sb++) {
+            const Bin& l = left[sb];
+            const Bin& r = right[sb + 1];
+            if (!l.has || !r.has || l.count < min_side || r.count < min_side) continue;
+            const double cost = (box_area(l.box) * static_cast<double>(l.count))
+                                + (box_area(r.box) * static_cast<double>(r.count));
+            if (cost < best_cost) {
+                best_cost = cost;
+                best.found = true;
+                best.axis = axis;
+                best.split = sb;
+                best.cmin = cmin;
+                best.scale = scale;
             }
         }
+        return best;
+    }
+
+    // findBinnedSAHSplit: the axes in order, a strictly lower cost replacing the best so
+    // far. Large ranges evaluate the three axes on threads and then compare them in the
+    // same order, which picks the same split.
+    Split find_split(std::size_t s, std::size_t e) const
+    {
+        Split per[3];
+        double cost[3];
+        if (e - s >= (std::size_t(1) << 17)) {
+            std::thread t1([&] { per[1] = axis_split(s, e, 1, cost[1]); });
+            std::thread t2([&] { per[2] = axis_split(s, e, 2, cost[2]); });
+            per[0] = axis_split(s, e, 0, cost[0]);
+            t1.join();
+            t2.join();
+        } else {
+            for (int a = 0; a < 3; a++) per[a] = axis_split(s, e, a, cost[a]);
+        }
+        Split best;
+        double best_cost = std::numeric_limits<double>::infinity();
+        for (int a = 0; a < 3; a++)
+            if (per[a].found && cost[a] < best_cost) {
+                best_cost = cost[a];
+                best = per[a];
+            }
         return best;
     }
 
@@ -494,6 +520,18 @@ void build_mesh(const LuzMeshDesc& m, MeshBuild& mb)
 {
     if (m.triangle_count < 0 || (m.triangle_count > 0 && !m.positions)) invalid("Mesh positions are missing.");
     mb.material = m.material;
+    const std::size_t tc = (std::size_t)m.triangle_count;
+    mb.vtx.reserve(9 * tc);
+    mb.v0.reserve(3 * tc);
+    mb.e1.reserve(3 * tc);
+    mb.e2.reserve(3 * tc);
+    mb.fn.reserve(3 * tc);
+    mb.area.reserve(tc);
+    if (m.normals) {
+        mb.has_vn.reserve(tc);
+        mb.vn.reserve(9 * tc);
+    }
+    if (m.uvs) mb.uv.reserve(6 * tc);
     for (int64_t t = 0; t < m.triangle_count; t++) {
         const double* p = m.positions + 9 * t;
         const V3 a(p), b(p + 3), c(p + 6);
@@ -832,6 +870,13 @@ ScenePack* pack_scene(const LuzSceneDesc* d)
             for (std::size_t i = 0; i < mb.nodes.size(); i++)
                 if (!mb.nodes[i].is_leaf) gidx[i] = cnt++;
             const int32_t base = (int32_t)S.nodes.size();
+            S.nodes.reserve(S.nodes.size() + (std::size_t)cnt);
+            S.nodes4.reserve(S.nodes4.size() + (std::size_t)cnt);
+            S.tris.reserve(S.tris.size() + n);
+            S.tri_shade.reserve(S.tri_shade.size() + n);
+            S.cdf.reserve(S.cdf.size() + n);
+            if (!mb.vn.empty()) S.vnormals.reserve(S.vnormals.size() + 9 * n);
+            if (!mb.uv.empty()) S.vuvs.reserve(S.vuvs.size() + 6 * n);
             auto ref_of = [&](int64_t ni) -> uint32_t {
                 const LuzMeshNode64& nd = mb.nodes[(std::size_t)ni];
                 if (nd.is_leaf)
