@@ -10,10 +10,11 @@ namespace luz {
 namespace {
 
 
-// Resident blocks per SM the register allocator is asked to allow: 4 measured
-// ahead of 3 and 5 on the 1080p glossy frame.
+// Resident blocks per SM the register allocator is asked to allow, measured on the
+// 1080p glossy frame (16 spp, shade stage): 5 blocks (96 registers) 22.1 ms, 4 (128)
+// 22.6 ms, 3 (168) 25.2 ms.
 #ifndef LUZ_SHADE_MIN_BLOCKS
-#define LUZ_SHADE_MIN_BLOCKS 4
+#define LUZ_SHADE_MIN_BLOCKS 5
 #endif
 
 // Path of shade slot i: slots run through the class segments in class order.
