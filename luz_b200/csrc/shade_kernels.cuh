@@ -11,10 +11,11 @@ namespace {
 
 
 // Resident blocks per SM the register allocator is asked to allow, measured on the
-// 1080p glossy frame (16 spp, shade stage): 5 blocks (96 registers) 22.1 ms, 4 (128)
-// 22.6 ms, 3 (168) 25.2 ms.
+// 1080p glossy frame (16 spp, shade stage; the kernel is latency-bound, and more warps
+// hide more of it despite spills): 6 blocks (80 registers) 20.3 ms, 7 (72) 20.1 ms,
+// 8 (64) 20.7 ms, 5 (96) 22.1-22.4 ms, 4 (128) 22.6 ms, 3 (168) 25.2 ms.
 #ifndef LUZ_SHADE_MIN_BLOCKS
-#define LUZ_SHADE_MIN_BLOCKS 5
+#define LUZ_SHADE_MIN_BLOCKS 6
 #endif
 
 // Path of shade slot i: slots run through the class segments in class order.
