@@ -59,18 +59,18 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 // ---------------------------------------------------------------------------- extend (closest hit)
 
 // Resident blocks per SM the register allocator is asked to allow, measured on
-// B200 (1080p glossy frame at 16 spp, extend / shadow stage): extend 6 blocks (80
-// registers) 37.1 ms against 38.0 ms at 5 (96 registers, almost no spills; on an
-// earlier build with more local-memory traffic 5 blocks had led 6 and 7); shadow 8
-// blocks 16.0 ms, 10 16.7 ms, 12 18.4 ms (shade: shade_kernels.cu).
+// B200 (1080p glossy frame at 16 spp, extend / shadow stage): extend 7 blocks (72
+// registers) 35.8-35.9 ms, 8 (64) 36.8 ms, 6 (80) 37.1 ms, 5 (96, almost no spills)
+// 38.0 ms (on an earlier build with more local-memory traffic 5 blocks had led 6 and
+// 7); shadow 8 blocks 16.0 ms, 10 16.7 ms, 12 18.4 ms (shade: shade_kernels.cu).
 #ifndef LUZ_EXTEND_MIN_BLOCKS
-#define LUZ_EXTEND_MIN_BLOCKS 6
+#define LUZ_EXTEND_MIN_BLOCKS 7
 #endif
 #ifndef LUZ_SHADOW_MIN_BLOCKS
 #define LUZ_SHADOW_MIN_BLOCKS 8
 #endif
 // The instantiations for scenes with instances (instance transform, two nested walks),
-// measured at 4-6 blocks before the plain kernels moved to 6:
+// measured at 4-6 blocks (5 again on the final build: 85.5 against 72.0 ms):
 // 4 blocks (128 registers, a few hundred bytes of spills instead of 1-2 KB at 96) took
 // the 1e5-instance frame's extend stage from 85.1 to 71.8 ms at 4 spp (6 blocks: 85.8).
 #ifndef LUZ_EXTEND_MIN_BLOCKS_INST
