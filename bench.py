@@ -54,6 +54,8 @@ def parse():
                     help="cache workloads: LuzCacheParams.min_roughness (default per workload)")
     ap.add_argument("--cache-batch", type=int, default=16384, help="cache workloads: training rows per step")
     ap.add_argument("--cache-train-every", type=int, default=32, help="cache workloads: one training path in this many")
+    ap.add_argument("--cache-warm-steps", type=int, default=0,
+                    help="cache workloads: LuzCacheParams.warm_steps (0: the library's 64)")
     ap.add_argument("--cache-prefix", type=int, default=1,
                     help="cache workloads: first bounce whose vertex queries the cache")
     ap.add_argument("--cache-wave", type=int, default=0,
@@ -604,7 +606,7 @@ def run_cache(args):
 
     def new_cache():
         return native.RadianceCache(D.cache_params(seed=3, batch=args.cache_batch, train_every=args.cache_train_every,
-                                                   prefix=args.cache_prefix,
+                                                   prefix=args.cache_prefix, warm_steps=args.cache_warm_steps,
                                                    min_roughness=min_rough))
 
     for _ in range(max(1, args.warmup)):
@@ -647,8 +649,8 @@ def run_cache(args):
                       "target": f"error of the plain {targets[-1]}-spp image",
                       "cache": f"prefix {args.cache_prefix}, NEE explicit at the cache vertex, one training path in {args.cache_train_every} "
                                "(self-training: it ends in the cache at its next eligible vertex), "
-                               f"batch {args.cache_batch} (up to 16 steps per wave), lr 1e-2, first sample plain with 32 "
-                               f"warm-up steps, min roughness {min_rough:g}, "
+                               f"batch {args.cache_batch} (up to 16 steps per wave), lr 1e-2, first sample plain with "
+                               f"{args.cache_warm_steps or 64} warm-up steps, min roughness {min_rough:g}, "
                                f"waves of {args.cache_wave or 4194304} paths"},
            "speedup_at": at,
            "plain": {"curve": [{"spp": s, "ms": t, "relmse": e} for s, t, e in plain]},

@@ -77,6 +77,18 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WaveArgs w, PathBuf P, Ctrl* 
 #define LUZ_EXTEND_MIN_BLOCKS_INST 4
 #endif
 
+// Radiance-cache training steps: on the warm-up wave (the first sample of every pixel,
+// every path a training row) when LuzCacheParams.warm_steps is 0, and at most per later
+// wave. Cornell box 300x300, time to the plain 256-spp error: 16 warm-up steps 1.5-2.1x,
+// 32 2.81-2.88x, 48 2.91-3.09x, 64 3.06-3.17x; two warm-up samples per pixel with 64 or
+// 96 steps 2.86-3.01x. Four steps per later wave instead of 16: 2.81-2.83x (no change).
+#ifndef LUZ_CACHE_WARM_STEPS
+#define LUZ_CACHE_WARM_STEPS 64
+#endif
+#ifndef LUZ_CACHE_WAVE_STEPS
+#define LUZ_CACHE_WAVE_STEPS 16
+#endif
+
 // Appends path p to the segment of its shade class; the lanes of vmask with the
 // same class share one atomic (match.any).
 __device__ __forceinline__ void bin_append(uint32_t* bin_count, const PathBuf& P, unsigned vmask, uint32_t cls,
@@ -3270,8 +3282,10 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
     const int batch = c->prm.batch;
     int64_t launches = 0, waves = 0;
     // The first sample of every pixel is rendered plain, every path training the
-    // cache (kCacheWarmSteps steps over its rows); later waves use the cache.
-    constexpr int kCacheWarmSteps = 32;
+    // cache (warm_steps steps over its rows); later waves use the cache and
+    // train at most kCacheWaveSteps steps each.
+    const int warm_steps = c->prm.warm_steps > 0 ? c->prm.warm_steps : LUZ_CACHE_WARM_STEPS;
+    constexpr int64_t kCacheWaveSteps = LUZ_CACHE_WAVE_STEPS;
     for (int sb = 0; sb < p->spp;) {
         const bool warm = sb == 0;
         const int sc = warm ? 1 : std::min(s_wave, p->spp - sb);
@@ -3299,11 +3313,11 @@ int do_render_cached(luz_gpu_scene* s, luz_gpu_cache* c, const LuzRenderParams* 
             }
             k_cache_infer<<<(unsigned)(2 * s->sms), 128, kCacheInferSmem, st>>>(q, counts, 0, c->Wf, nullptr, s->pb.rad);
             k_cache_targets<<<(unsigned)((w.n + 255) / 256), 256, 0, st>>>(w, s->pb, rows, counts + 1);
-            // about n / train_every rows: one step per batch of them (at most 16 per wave);
-            // the warm-up wave cycles kCacheWarmSteps steps over its rows
+            // about n / train_every rows: one step per batch of them (at most kCacheWaveSteps);
+            // the warm-up wave cycles warm_steps steps over its rows
             const int64_t expect = (w.n + w.cache_train_every - 1) / w.cache_train_every;
             const int64_t chunks = std::max<int64_t>(1, (expect + batch - 1) / batch);
-            const int steps = warm ? kCacheWarmSteps : (int)std::min<int64_t>(16, chunks);
+            const int steps = warm ? warm_steps : (int)std::min<int64_t>(kCacheWaveSteps, chunks);
             for (int i = 0; i < steps; i++)
                 cache_step(c, rows, counts + 1, (int)((i % chunks) * batch), (int)std::min<int64_t>(batch, w.n), st);
             k_accumulate<<<(unsigned)((pc + 127) / 128), 128, 0, st>>>(w, s->pb, film);
@@ -3351,6 +3365,8 @@ int luz_gpu_cache_create(int32_t device, const LuzCacheParams* prm, luz_gpu_cach
         if (prm->train_every < 1) throw Status(LUZ_E_INVALID, "Cache training interval must be at least 1.");
         if (!(prm->min_roughness >= 0.0f && prm->min_roughness <= 1.0f))
             throw Status(LUZ_E_INVALID, "Cache minimum roughness must lie in [0, 1].");
+        if (prm->warm_steps < 0 || prm->warm_steps > 4096)
+            throw Status(LUZ_E_INVALID, "Cache warm-up steps must lie in [0, 4096].");
         CK(cudaSetDevice(device));
         std::unique_ptr<luz_gpu_cache> c(new luz_gpu_cache);
         c->device = device;

@@ -189,12 +189,12 @@ CACHE_PARAMS = 21504
 class CacheParams(C.Structure):
     """LuzCacheParams: learned radiance cache settings."""
     _fields_ = [("seed", C.c_uint32), ("batch", C.c_int32), ("learning_rate", C.c_float), ("prefix", C.c_int32),
-                ("train_every", C.c_int32), ("min_roughness", C.c_float)]
+                ("train_every", C.c_int32), ("min_roughness", C.c_float), ("warm_steps", C.c_int32)]
 
 
 def cache_params(seed=1, batch=16384, learning_rate=1e-2, prefix=1, train_every=32,
-                 min_roughness=0.0) -> CacheParams:
-    return CacheParams(seed, batch, learning_rate, prefix, train_every, min_roughness)
+                 min_roughness=0.0, warm_steps=0) -> CacheParams:
+    return CacheParams(seed, batch, learning_rate, prefix, train_every, min_roughness, warm_steps)
 
 
 class Hit(C.Structure):

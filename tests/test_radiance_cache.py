@@ -138,6 +138,9 @@ def test_invalid_arguments(cache):
     for bad in (-0.1, 1.5, float("nan")):
         with pytest.raises(native.LuzError):
             native.RadianceCache(D.cache_params(min_roughness=bad))
+    for bad in (-1, 4097):
+        with pytest.raises(native.LuzError):
+            native.RadianceCache(D.cache_params(warm_steps=bad))
     with pytest.raises(native.LuzError):
         cache.train(rows(5000), smooth_target(rows(5000)), steps=1)   # more rows than the batch
 
