@@ -407,8 +407,10 @@ int luz_gpu_trace_paths(luz_gpu_scene* scene, const LuzRenderParams* params,
  * LUZ_STATIC_MAX_PIXELS, otherwise LUZ_E_LIMIT; flags must be 0. The call
  * returns once the render has finished on the stream (it waits for the
  * stream to read the ray totals and the error word into the handle's pinned
- * buffer). The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * buffer), so the call itself cannot be captured into a CUDA graph. The first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress),
+ * which other threads' global-mode stream captures forbid: make that first
+ * call before such captures begin.
  * All calls share the array and it keeps the previous call's contents: calls
  * whose GPU work overlaps (other streams, other threads) race on it and must
  * be serialised by the caller.
