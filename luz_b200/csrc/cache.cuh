@@ -27,7 +27,8 @@ constexpr int kCacheEnc = 128;           // encoded width (120 + bias + padding)
 constexpr int kCacheHidden = 64;
 constexpr int kCacheOut = 16;            // padded output width (3 used)
 constexpr int kCacheLayers = 5;
-constexpr int kCacheRowsPerBlock = 64;   // training: 4 warps x 16 rows
+constexpr int kCacheRowsPerBlock = 128;  // training: 8 warps x 16 rows
+constexpr int kCacheGradThreads = 2 * kCacheRowsPerBlock;
 
 // Layer l: K inputs, N outputs, offsets of W (floats), of the forward FP16
 // copy [n][K + 8] and of the backward FP16 copy [k][N + 8] (halves).
@@ -252,13 +253,16 @@ __device__ __forceinline__ void cache_relu_mask(float (&c)[NT][4], const uint32_
     }
 }
 
-// Shared-memory layout of k_cache_grad (halves): forward and backward weight
-// copies, then per layer the block's 64 input rows X_l [64][K_l + 8] and output
-// gradients D_l [64][N_l + 8].
-constexpr int kGX0 = kCacheHalfF + kCacheHalfB;
-__host__ __device__ constexpr int cache_x_off(int l) { return kGX0 + (l == 0 ? 0 : 64 * 136 + (l - 1) * 64 * 72); }
-__host__ __device__ constexpr int cache_d_off(int l) { return cache_x_off(4) + 64 * 72 + l * 64 * 72; }
-constexpr int kCacheGradSmemHalves = cache_d_off(4) + 64 * 24;
+// Shared-memory layout of k_cache_grad (halves): first the forward and backward
+// weight copies; once every warp has finished its backward pass, the same memory
+// holds per layer the block's input rows X_l [R][K_l + 8] and output gradients
+// D_l [R][N_l + 8] (R = kCacheRowsPerBlock).
+constexpr int kGR = kCacheRowsPerBlock;
+__host__ __device__ constexpr int cache_x_off(int l) { return l == 0 ? 0 : kGR * 136 + (l - 1) * kGR * 72; }
+__host__ __device__ constexpr int cache_d_off(int l) { return cache_x_off(4) + kGR * 72 + l * kGR * 72; }
+constexpr int kCacheGradStageHalves = cache_d_off(4) + kGR * 24;
+constexpr int kCacheGradSmemHalves =
+    kCacheGradStageHalves > kCacheHalfF + kCacheHalfB ? kCacheGradStageHalves : kCacheHalfF + kCacheHalfB;
 
 // Rows of one training step: records [offset, offset + n) with n = min(*count -
 // offset, n_max), at least 0 (count NULL: n_max).
@@ -269,8 +273,8 @@ __device__ __forceinline__ int cache_step_rows(const uint32_t* count, int offset
 
 // Gradient of the summed loss over the step's rows (in: inputs, v: targets)
 // with respect to W, times the loss scale, added into G; the summed loss into
-// *loss. Launch with ceil(n_max / 64) blocks of 128.
-__global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, const uint32_t* count, int offset,
+// *loss. Launch with ceil(n_max / kCacheRowsPerBlock) blocks of kCacheGradThreads.
+__global__ void __launch_bounds__(kCacheGradThreads) k_cache_grad(const CacheRecord* rec, const uint32_t* count, int offset,
                                                     int n_max, const __half* Wf_g, const __half* Wb_g, float* G,
                                                     float* loss)
 {
@@ -343,7 +347,9 @@ __global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, cons
             cache_chain<8, false>(c, d[l - 1]);
         }
     }
-    // stage inputs and output gradients of every layer for the block's 64 rows
+    // stage inputs and output gradients of every layer for the block's rows, over
+    // the weight copies once every warp is done reading them
+    __syncthreads();
     cache_stage<8>(in, sm + cache_x_off(0), 136, row0);
 #pragma unroll
     for (int l = 1; l < 5; l++) cache_stage<4>(h[l - 1], sm + cache_x_off(l), 72, row0);
@@ -354,7 +360,7 @@ __global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, cons
         cache_stage<1>(dl, sm + cache_d_off(4), 24, row0);
     }
     __syncthreads();
-    // dW_l (K x N) = X_l^T D_l over the 64 rows: tiles of 16 k x 8 n, four 16-row steps
+    // dW_l (K x N) = X_l^T D_l over the block's rows: tiles of 16 k x 8 n, 16-row steps
     int tile = 0;
     for (int l = 0; l < kCacheLayers; l++) {
         const CacheLayer L = cache_layer(l);
@@ -363,10 +369,10 @@ __global__ void __launch_bounds__(128) k_cache_grad(const CacheRecord* rec, cons
         const int ldx = L.K + 8, ldd = L.N + 8;
         for (int mk = 0; mk < L.K / 16; mk++)
             for (int nj = 0; nj < L.N / 8; nj++, tile++) {
-                if ((tile & 3) != warp) continue;
+                if (tile % (kCacheGradThreads / 32) != warp) continue;
                 float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-                for (int kb = 0; kb < 4; kb++) {
+                for (int kb = 0; kb < kCacheRowsPerBlock / 16; kb++) {
                     const int b = 16 * kb + 2 * t, k = 16 * mk + g, j = 8 * nj + g;
                     auto hx = [&](int bb, int kk) { return X[bb * ldx + kk]; };
                     auto hd = [&](int bb, int jj) { return D[bb * ldd + jj]; };

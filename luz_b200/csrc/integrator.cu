@@ -3202,7 +3202,7 @@ void cache_set(luz_gpu_cache* c, const float* w)
 void cache_step(luz_gpu_cache* c, const CacheRecord* rows, const uint32_t* count, int offset, int n_max,
                 cudaStream_t st)
 {
-    k_cache_grad<<<(unsigned)((n_max + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem, st>>>(
+    k_cache_grad<<<(unsigned)((n_max + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), kCacheGradThreads, kCacheGradSmem, st>>>(
         rows, count, offset, n_max, c->Wf, c->Wb, c->G, c->loss);
     c->step++;
     const float b1 = 0.9f, b2 = 0.99f;
@@ -3446,7 +3446,7 @@ int luz_gpu_cache_gradient(luz_gpu_cache* c, const float* inputs, const float* t
         try {
             CK(cudaMemset(c->G, 0, sizeof(float) * kCacheParams));
             CK(cudaMemset(c->loss, 0, sizeof(float)));
-            k_cache_grad<<<(unsigned)((n + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), 128, kCacheGradSmem>>>(
+            k_cache_grad<<<(unsigned)((n + kCacheRowsPerBlock - 1) / kCacheRowsPerBlock), kCacheGradThreads, kCacheGradSmem>>>(
                 d, nullptr, 0, (int)n, c->Wf, c->Wb, c->G, c->loss);
             CK(cudaGetLastError());
             std::vector<float> g(kCacheParams);
