@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LUZ_GPU_ABI_VERSION 4
+#define LUZ_GPU_ABI_VERSION 5   /* 5: LuzCacheParams.warm_steps */
 
 /* status codes */
 #define LUZ_OK            0

@@ -15,7 +15,7 @@ from typing import List, Optional
 
 import numpy as np
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_EMISSIVE = 1, 2, 3, 4
 MAT_ISOTROPIC, MAT_HENYEY_GREENSTEIN, MAT_PRINCIPLED = 5, 6, 7
